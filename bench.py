@@ -1,0 +1,357 @@
+"""Benchmark: grid Fock builds per second on one B200 (or N replicas).
+
+Workload: linear alkane C20H42 (sp3, C-C 1.54 A, C-H 1.09 A), cc-pVDZ in
+nAPMO's Cartesian form (510 functions), Becke grid of 100 Chebyshev radial x
+302 Lebedev points per atom (62 atoms, 1,872,400 points), lmax = 14.  One
+step = one grid Fock build of the electrons from a density matrix:
+rho = diag(phi^T D phi), V_H by the Becke-Dickson Poisson solve, and
+F = phi^T diag(w_becke w_quad V_H) phi -- the unit of work nAPMO repeats every
+SCF iteration (psi_hybrid.py:81-110, ntwobody.py:15-46, nwavefunction.cpp).
+D = 2 C C^T with C ~ N(0, 1/n) of shape n x 81 (seed 20261203); synthetic.
+phi (7.6 GB) exceeds L2 (126 MB), so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'grid Fock builds/s (C20H42 cc-pVDZ, 100x302 Becke grid, FP64)'
+UNIT = 'builds/s'
+WORKLOAD = 'C20H42/cc-pVDZ Cartesian n=510, Becke 100x302 per atom, N=1872400, lmax=14'
+SEED = 20261203
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument('--gpus', type=int, default=1)
+    p.add_argument('--steps', type=int, default=10)
+    p.add_argument('--warmup', type=int, default=3)
+    p.add_argument('--impl', default='napmo_b200')
+    p.add_argument('--nrad', type=int, default=100)
+    p.add_argument('--nang', type=int, default=302)
+    p.add_argument('--ncarbon', type=int, default=20)
+    p.add_argument('--cpu-points', type=int, default=4096)
+    p.add_argument('--no-cpu-baseline', action='store_true')
+    return p.parse_args()
+
+
+# ------------------------------------------------------------------ helpers
+class ClockSampler(object):
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', str(self.index), '--query-gpu=' + self.QUERY,
+                 '--format=csv,noheader,nounits', '-lms', '200'],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unavailable']}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        mhz, mx, reasons = [], None, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for line in self.lines:
+            f = [x.strip() for x in line.split(',')]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower().startswith('active'):
+                    reasons.add(name)
+        return {'sm_mhz': statistics.median(mhz) if mhz else None, 'sm_max_mhz': mx,
+                'reasons': sorted(reasons), 'samples': len(mhz)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), 'measured'
+    return {'hbm_gbs': 6650.0, 'bf16_tflops': 1590.0}, 'fallback'
+
+
+def fp64_gemm_peak(torch):
+    """cuBLAS DGEMM 8192^3, best of 5 (FP64 denominator; the peaks file has none)."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device='cuda')
+    b = torch.randn(8192, 8192, dtype=torch.float64, device='cuda')
+    best = 1e9
+    for _ in range(6):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    return 2 * 8192 ** 3 / best / 1e12
+
+
+def build_workload(args):
+    import napmo_b200 as nb
+    from napmo_b200.system import alkane_geometry, build_system
+    atoms = alkane_geometry(args.ncarbon)
+    ms = build_system(atoms, 'CC-PVDZ')
+    e = ms['e-']
+    grid = nb.BeckeGrid(e, args.nrad, args.nang)
+    lmax = nb.lebedev_get_order(args.nang) // 2
+    basis = e['basis']
+    n = basis['nbasis']
+    nocc = e['occupation']
+    rng = np.random.default_rng(SEED)
+    C = rng.normal(size=(n, nocc)) / np.sqrt(n)
+    D = 2.0 * C @ C.T
+    return atoms, ms, grid, basis, lmax, D
+
+
+# ------------------------------------------------------------- CPU baseline
+def cpu_baseline(args, atoms, grid, D, lmax):
+    """The oracle (C restatement of nAPMO's path, OpenMP on every host core)
+    on a bounded sample of one build: density, quadrature and multipole
+    evaluation on `cpu_points` grid points (scaled by N / sample), plus the
+    projection and radial ODE solves of one C and one H atom (scaled by the
+    atom counts).  The reference's own quadrature materialises all orbital
+    products (1.95 TB here), so the streamed restatement is timed."""
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import oracle as O
+    lib = json.load(open(os.path.join(ROOT, 'napmo_b200', 'data', 'basis.json')))
+    el = json.load(open(os.path.join(ROOT, 'napmo_b200', 'data', 'elements.json')))
+    centers = [np.array(x) / 0.52917724924 for _, x in atoms]
+    syms = [s for s, _ in atoms]
+    fb = O.flat_basis(centers, syms, lib, 'CC-PVDZ')
+    N = grid.size
+    rng = np.random.default_rng(SEED)
+    idx = np.sort(rng.choice(N, size=args.cpu_points, replace=False))
+    pts = np.ascontiguousarray(grid.points[idx])
+    bw = np.ascontiguousarray(grid.becke_weights[idx])
+    w = np.ascontiguousarray(grid.weights[idx])
+    phi = np.ascontiguousarray(O.basis_compute(fb, pts).T)
+    t0 = time.perf_counter()
+    rho = O.density(phi, D)
+    t1 = time.perf_counter()
+    v = np.zeros(args.cpu_points)
+    # multipole evaluation: every atom's lsize splines at every sample point
+    lsize = (lmax + 1) ** 2
+    spl_y = np.ascontiguousarray(rng.normal(size=(lsize, args.nrad)))
+    spl_dt = np.ascontiguousarray(rng.normal(size=(lsize, args.nrad)))
+    t2 = time.perf_counter()
+    for a, c in enumerate(centers):
+        O.lib.orc_eval_decomposition(0, el[syms[a]]['atomic_radii'], 0.0, args.nrad, lsize,
+                                     spl_y, spl_dt, np.ascontiguousarray(c), args.cpu_points,
+                                     pts, v)
+    t3 = time.perf_counter()
+    F = O.quadrature(phi, v, bw, w)
+    t4 = time.perf_counter()
+    # projection + radial solves for one C and one H atom (full atomic grids)
+    sub = [i for i in (0, syms.index('H'))]
+    og = O.Grid([centers[i] for i in sub], [el[syms[i]]['atomic_radii'] for i in sub],
+                args.nrad, args.nang)
+    dens = np.ones(og.size)
+    t5 = time.perf_counter()
+    O.poisson_solver(og, dens, lmax)
+    t6 = time.perf_counter()
+    ncar = syms.count('C')
+    nh = syms.count('H')
+    per_point = (t1 - t0) + (t3 - t2) + (t4 - t3)
+    t_build = per_point * N / args.cpu_points + (t6 - t5) * (ncar + nh) / 2.0
+    return {'value': 1.0 / t_build, 'unit': UNIT, 'cores': O.threads(), 'kind': 'port',
+            'sample': ('oracle C restatement (nAPMO order of operations, -O2, OpenMP): density, '
+                       'multipole evaluation (62 atoms x %d splines) and streamed quadrature '
+                       'on %d of %d points, scaled x%.0f; projection + radial FEM solves '
+                       '(scipy spsolve) of 2 of 62 atoms, scaled x31; sample wall %.1f s'
+                       % (lsize, args.cpu_points, N, N / args.cpu_points, t6 - t0)),
+            'seconds_per_build': t_build}
+
+
+# --------------------------------------------------------------------- main
+def main():
+    args = parse()
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', str(args.gpus)))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+
+    if args.impl == 'reference':
+        if rank != 0:
+            return
+        import napmo_b200  # grid construction only; no GPU work is timed here
+        import torch
+        atoms, ms, grid, basis, lmax, D = build_workload(args)
+        steps = []
+        for _ in range(args.warmup + args.steps):
+            cb = cpu_baseline(args, atoms, grid, D, lmax)
+            steps.append(cb['value'])
+        vals = steps[args.warmup:]
+        v = statistics.median(vals)
+        cb['value'] = v
+        line = {'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': UNIT, 'n_gpus': 1,
+                'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 / v,
+                'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+                'dtype': 'f64', 'data': 'synthetic',
+                'config': {'workload': WORKLOAD, 'parallelism': 'host cores'},
+                'cpu_baseline': cb,
+                'e2e': {'value': v, 'unit': UNIT, 'h2d_bytes_per_step': 0,
+                        'd2h_bytes_per_step': 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    import napmo_b200 as nb
+    from napmo_b200 import cext
+
+    atoms, ms, grid, basis, lmax, D = build_workload(args)
+    n = basis['nbasis']
+    N = grid.size
+    fbld = nb.FockBuilder(grid, basis, lmax)
+    Dd = torch.as_tensor(D, device='cuda')
+    stream = torch.cuda.current_stream()
+    F = torch.empty((n, n), dtype=torch.float64, device='cuda')
+    for _ in range(args.warmup):
+        fbld.build(Dd, out=F)
+    torch.cuda.synchronize()
+
+    # ---- device-resident timed region
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        fbld.build(Dd, out=F)
+    ev1.record(stream)
+    ev1.synchronize()
+    t_dev = ev0.elapsed_time(ev1) / 1e3
+    clocks = sampler.stop()
+    launches_per_build = 7
+    if dist:
+        t = torch.tensor([t_dev], device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_dev = t.item()
+
+    # ---- per-kernel timings (same stream) for the roofline
+    def time_it(fn, reps=3):
+        fn()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        s.record(stream)
+        for _ in range(reps):
+            fn()
+        e.record(stream)
+        e.synchronize()
+        return s.elapsed_time(e) / 1e3 / reps
+
+    rho = fbld.density(Dd)
+    v = fbld.coulomb_potential(rho)
+    t_density = time_it(lambda: fbld.density(Dd))
+    t_poisson = time_it(lambda: fbld.coulomb_potential(rho))
+    t_quad = time_it(lambda: fbld.quadrature(1.0, v))
+    flops = 2.0 * n * n * N
+    kernels = {'density': {'ms': t_density * 1e3, 'tflops': flops / t_density / 1e12},
+               'poisson(project+radial+evaluate)': {'ms': t_poisson * 1e3},
+               'quadrature': {'ms': t_quad * 1e3, 'tflops': flops / t_quad / 1e12}}
+
+    # ---- end-to-end through the C-ABI with host buffers
+    Dh = torch.empty((n, n), dtype=torch.float64).pin_memory()
+    Dh.copy_(torch.as_tensor(D))
+    Fh = torch.empty((n, n), dtype=torch.float64).pin_memory()
+    Dn, Fn = Dh.numpy(), Fh.numpy()
+    for _ in range(2):
+        cext.checked(cext.lib.napmo_fock_plan_build_host(fbld._plan, Dn, 1.0, None, Fn,
+                                                         stream.cuda_stream))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cext.checked(cext.lib.napmo_fock_plan_build_host(fbld._plan, Dn, 1.0, None, Fn,
+                                                         stream.cuda_stream))
+    t_e2e = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([t_e2e], device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = t.item()
+
+    if rank == 0:
+        peaks, peak_kind = measured_peaks()
+        fp64 = fp64_gemm_peak(torch)
+        dom = 'density' if t_density >= t_quad else 'quadrature'
+        td = t_density if dom == 'density' else t_quad
+        achieved = flops / td / 1e12
+        value = world * args.steps / t_dev
+        cb = None
+        if not args.no_cpu_baseline and world == 1:
+            cb = cpu_baseline(args, atoms, grid, D, lmax)
+        line = {
+            'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': t_dev / args.steps * 1e3,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'f64', 'data': 'synthetic',
+            'config': {'workload': WORKLOAD, 'global_batch': world, 'n_basis': n,
+                       'n_points': N, 'lmax': lmax,
+                       'parallelism': 'replicas' if world > 1 else 'single GPU',
+                       'l2': 'inputs larger than L2 (phi 7.6 GB)'},
+            'e2e': {'value': world * args.steps / t_e2e, 'unit': UNIT,
+                    'h2d_bytes_per_step': n * n * 8, 'd2h_bytes_per_step': n * n * 8},
+            'gpu_launches': launches_per_build * args.steps,
+            'roofline': {'kernel': dom, 'bound': 'tensor', 'achieved': achieved,
+                         'peak': fp64, 'unit': 'TFLOP/s', 'frac': achieved / fp64,
+                         'traffic': None,
+                         'peak_source': 'cuBLAS DGEMM 8192^3 measured in this run (FP64; '
+                                        'the peaks file lists HBM/bf16 only: hbm %.0f GB/s %s)'
+                                        % (peaks.get('hbm_gbs', 0), peak_kind),
+                         'algorithmic_flops_per_launch': flops},
+            'kernels': kernels,
+            'clocks': clocks,
+            'cpu_baseline': cb,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

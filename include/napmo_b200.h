@@ -1,0 +1,289 @@
+/*
+ * napmo_b200.h -- C-ABI of libnapmo.so (napmo_b200/lib/libnapmo.so).
+ *
+ * Part 1 is the drop-in surface: the symbols nAPMO's Python layer binds with
+ * ctypes (napmo/__init__.py:95-585, loaded by napmo/system/cext.py:11-16),
+ * with the same argument order and meaning.  Each line cites the nAPMO
+ * function it replaces.  Opaque handles are `void *`; arrays are plain
+ * pointers to row-major doubles owned by the caller unless stated.  Entry
+ * points that compute on grid points run on the current CUDA device and
+ * synchronise before returning; errors are reported through
+ * napmo_last_error() (nAPMO throws C++ exceptions across ctypes instead).
+ *
+ * Part 2 is this library's device API: device pointers, a cudaStream_t
+ * passed as `void *`, int status (0 = success), no synchronisation.
+ */
+#ifndef NAPMO_B200_H
+#define NAPMO_B200_H
+
+#include <stdbool.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------- errors */
+/* Last error of the calling thread: returns its code, copies the message. */
+int napmo_last_error(char *buf, int len);
+/* Frees arrays returned by AtomicGrid_integrate / _spherical_expansion. */
+void napmo_free_array(double *p);
+
+/* ===================================================== Part 1: drop-in */
+/* ---- radial transforms: src/horton/rtransform.{h,cpp} */
+void RTransform_del(void *rt);                                   /* rtransform.h:51 */
+double RTransform_radius(void *rt, double t);                    /* rtransform.h:52 */
+double RTransform_deriv(void *rt, double t);                     /* rtransform.h:53 */
+double RTransform_deriv2(void *rt, double t);                    /* rtransform.h:54 */
+double RTransform_deriv3(void *rt, double t);                    /* rtransform.h:55 */
+double RTransform_inv(void *rt, double r);                       /* rtransform.h:56 */
+void RTransform_radius_array(void *rt, double *t, double *r, int n);  /* rtransform.h:58 */
+void RTransform_deriv_array(void *rt, double *t, double *d, int n);   /* rtransform.h:60 */
+void RTransform_deriv2_array(void *rt, double *t, double *d, int n);  /* rtransform.h:62 */
+void RTransform_deriv3_array(void *rt, double *t, double *d, int n);  /* rtransform.h:64 */
+void RTransform_inv_array(void *rt, double *r, double *t, int n);     /* rtransform.h:66 */
+int RTransform_get_npoint(void *rt);                             /* rtransform.h:67 */
+void *IdentityRTransform_new(int npoint);                        /* rtransform.h:87 */
+void *LinearRTransform_new(double rmin, double rmax, int npoint); /* rtransform.h:114 */
+double LinearRTransform_get_rmin(void *rt);                      /* rtransform.h:115 */
+double LinearRTransform_get_rmax(void *rt);                      /* rtransform.h:116 */
+double LinearRTransform_get_alpha(void *rt);                     /* rtransform.h:117 */
+void *ExpRTransform_new(double rmin, double rmax, int npoint);    /* rtransform.h:144 */
+double ExpRTransform_get_rmin(void *rt);                         /* rtransform.h:145 */
+double ExpRTransform_get_rmax(void *rt);                         /* rtransform.h:146 */
+double ExpRTransform_get_alpha(void *rt);                        /* rtransform.h:147 */
+void *ShiftedExpRTransform_new(double rmin, double rshift, double rmax, int npoint); /* :176 */
+double ShiftedExpRTransform_get_rmin(void *rt);                  /* rtransform.h:178 */
+double ShiftedExpRTransform_get_rshift(void *rt);                /* rtransform.h:179 */
+double ShiftedExpRTransform_get_rmax(void *rt);                  /* rtransform.h:180 */
+double ShiftedExpRTransform_get_r0(void *rt);                    /* rtransform.h:181 */
+double ShiftedExpRTransform_get_alpha(void *rt);                 /* rtransform.h:182 */
+void *PowerRTransform_new(double rmin, double rmax, int npoint);  /* rtransform.h:210 */
+double PowerRTransform_get_rmin(void *rt);                       /* rtransform.h:211 */
+double PowerRTransform_get_rmax(void *rt);                       /* rtransform.h:212 */
+double PowerRTransform_get_power(void *rt);                      /* rtransform.h:213 */
+void *ChebyshevRTransform_new(double radii, int npoint);         /* rtransform.h:240 */
+double ChebyshevRTransform_get_radii(void *rt);                  /* rtransform.h:241 */
+double ChebyshevRTransform_get_z(void *rt);                      /* rtransform.h:242 */
+
+/* ---- angular grid: src/grid/angular.{h,cpp} (Lebedev-Laikov rules) */
+void *AngularGrid_new(int lorder);                               /* angular.h:109 */
+void AngularGrid_del(void *g);                                   /* angular.h:111 */
+void AngularGrid_spherical(void *g);                             /* angular.h:113 */
+/* GSL-based expansions (not on the grid-quadrature path): set an error. */
+void AngularGrid_spherical_expansion(void *g, int lmax, int size_f, double *f,
+                                     double *output);            /* angular.h:115 */
+void AngularGrid_eval_expansion(void *g, int lmax, int size_f, double *dec,
+                                double *output);                 /* angular.h:119 */
+double AngularGrid_integrate(void *g, int segments, double *f, double *s); /* angular.h:123 */
+int AngularGrid_get_lorder(void *g);                             /* angular.h:126 */
+double *AngularGrid_get_points(void *g);                         /* angular.h:128 */
+double *AngularGrid_get_weights(void *g);                        /* angular.h:130 */
+
+/* ---- radial grid: src/grid/radial.{h,cpp} */
+void *RadialGrid_new(void *rtf, double rad);                     /* radial.h:53 */
+void RadialGrid_del(void *g);                                    /* radial.h:55 */
+double RadialGrid_integrate(void *g, int segments, double *f);   /* radial.h:57 */
+double *RadialGrid_deriv2(void *g, double *f);  /* radial.h:59; out of path: sets error */
+int RadialGrid_get_size(void *g);                                /* radial.h:61 */
+double RadialGrid_get_radii(void *g);                            /* radial.h:63 */
+double *RadialGrid_get_points(void *g);                          /* radial.h:65 */
+double *RadialGrid_get_weights(void *g);                         /* radial.h:67 */
+
+/* ---- atomic grid: src/grid/atomic_grid.{h,cpp} */
+void *AtomicGrid_new(void *angular, void *radial, double *R);    /* atomic_grid.h:73 */
+void AtomicGrid_del(void *g);                                    /* atomic_grid.h:75 */
+double *AtomicGrid_integrate(void *g, int nfunc, int segments, int size,
+                             double *f);                         /* atomic_grid.h:77 */
+double *AtomicGrid_spherical_expansion(void *g, double *f, int lmax); /* atomic_grid.h:80 (GPU) */
+int AtomicGrid_get_size(void *g);                                /* atomic_grid.h:82 */
+double AtomicGrid_get_radii(void *g);                            /* atomic_grid.h:84 */
+double *AtomicGrid_get_origin(void *g);                          /* atomic_grid.h:86 */
+double *AtomicGrid_get_points(void *g);                          /* atomic_grid.h:88 */
+double *AtomicGrid_get_weights(void *g);                         /* atomic_grid.h:90 */
+
+/* ---- Becke molecular grid: src/grid/becke.{h,cpp} (weights on the GPU) */
+void *BeckeGrid_new(void **atomic_grids, int n, int l, double ld); /* becke.h:95 */
+void *BeckeGrid_from_points(double *p, int sz, int nc);          /* becke.h:97 */
+void BeckeGrid_del(void *g);                                     /* becke.h:99 */
+double BeckeGrid_integrate(void *g, double *f);                  /* becke.h:101 (GPU) */
+int BeckeGrid_get_ncenter(void *g);                              /* becke.h:103 */
+int BeckeGrid_get_size(void *g);                                 /* becke.h:105 */
+double *BeckeGrid_get_radii(void *g);                            /* becke.h:107 */
+double *BeckeGrid_get_points(void *g);                           /* becke.h:109 */
+double *BeckeGrid_get_weights(void *g);                          /* becke.h:111 */
+double *BeckeGrid_get_origin(void *g);                           /* becke.h:113 */
+double *BeckeGrid_get_becke_weights(void *g);                    /* becke.h:115 */
+
+/* ---- common points between species grids: src/grid/multi_grid.{h,cpp} */
+void *MultiGrid_new(int ns);                                     /* multi_grid.h:50 */
+void MultiGrid_del(void *m);                                     /* multi_grid.h:52 */
+int MultiGrid_add_grid(void *m, void *grid);                     /* multi_grid.h:54 */
+int *MultiGrid_get_common_index(void *m, int a, int b);          /* multi_grid.h:56 (GPU) */
+int MultiGrid_get_common_index_size(void *m, int a, int b);      /* multi_grid.h:59 */
+int MultiGrid_get_ngrids(void *m);                               /* multi_grid.h:62 */
+int MultiGrid_get_nspecies(void *m);                             /* multi_grid.h:64 */
+
+/* ---- cell (non-periodic only): src/horton/cell.h */
+void *Cell_new(double *rvecs, int nvec);                         /* cell.h:238 */
+void Cell_del(void *c);                                          /* cell.h:239 */
+
+/* ---- cubic splines and extrapolations: src/horton/{cubic_spline,extrapolation}.h */
+void tridiagsym_solve(double *mid, double *up, double *right, double *sol, int n); /* cubic_spline.h:33 */
+void solve_cubic_spline_system(double *y, double *dt, int npoint);   /* cubic_spline.h:35 */
+void compute_cubic_spline_int_weights(double *weights, int npoint);  /* cubic_spline.h:36 */
+void *CubicSpline_new(double *y, double *dt, void *ext, void *rtf, int n); /* cubic_spline.h:71 */
+void CubicSpline_del(void *c);                                   /* cubic_spline.h:74 */
+void CubicSpline_eval(void *c, double *x, double *y, int n);     /* cubic_spline.h:75 */
+void CubicSpline_eval_deriv(void *c, double *x, double *d, int n); /* cubic_spline.h:77 */
+double CubicSpline_get_first_x(void *c);                         /* cubic_spline.h:79 */
+double CubicSpline_get_last_x(void *c);                          /* cubic_spline.h:80 */
+void *CubicSpline_get_rtransform(void *c);                       /* cubic_spline.h:81 */
+void *CubicSpline_get_extrapolation(void *c);                    /* cubic_spline.h:82 */
+void Extrapolation_prepare(void *e, void *c);                    /* extrapolation.h:45 */
+void Extrapolation_del(void *e);                                 /* extrapolation.h:46 */
+double Extrapolation_eval_left(void *e, double x);               /* extrapolation.h:47 */
+double Extrapolation_eval_right(void *e, double x);              /* extrapolation.h:48 */
+double Extrapolation_deriv_left(void *e, double x);              /* extrapolation.h:49 */
+double Extrapolation_deriv_right(void *e, double x);             /* extrapolation.h:50 */
+bool Extrapolation_has_tail(void *e);                            /* extrapolation.h:51 */
+void *ZeroExtrapolation_new(void);                               /* extrapolation.h:71 */
+void *CuspExtrapolation_new(void);                               /* extrapolation.h:94 */
+void *PowerExtrapolation_new(double power);                      /* extrapolation.h:164 */
+double PowerExtrapolation_get_power(void *e);                    /* extrapolation.h:165 */
+void *PotentialExtrapolation_new(int l);                         /* extrapolation.h:167 */
+
+/* ---- Hermite finite elements and moments: src/horton/{ode2,dot_multi,moments,evaluate}.h */
+double hermite_overlap2(long xmax, long i0, bool d0, long i1, bool d1);  /* ode2.h:27 */
+double hermite_overlap3(long xmax, long i0, bool d0, long i1, bool d1, long i2,
+                        bool d2);                                /* ode2.h:28 */
+void build_ode2(double *b, double *a, double *f, double *bcs, double *coeffs, double *rhs,
+                long npoint);                                    /* ode2.h:37 */
+void fill_pure_polynomials(double *output, long lmax);           /* moments.h (moments.cpp:59) */
+void dot_multi_moments(long npoint, long nvector, double *data, double *points,
+                       double *center, long lmax, long mtype, long *segments,
+                       double *output, long nmoment);            /* dot_multi.h:37 (GPU) */
+void eval_decomposition_grid(void **splines, double *center, double *output, double *points,
+                             void *cell, long nspline, long npoint); /* evaluate.h:43 (GPU) */
+
+/* ---- Gaussian basis: src/system/{gto,basis_set}.h */
+void *PrimitiveGaussian_new(int *l, double *A, double zeta, double coeff); /* gto.h:99 */
+void PrimitiveGaussian_del(void *p);
+void PrimitiveGaussian_get_l(void *p, int *l);                   /* gto.h:102 */
+void PrimitiveGaussian_get_origin(void *p, double *A);           /* gto.h:104 */
+void PrimitiveGaussian_compute(void *p, double *r, double *out, int size); /* gto.h:106 (GPU) */
+void PrimitiveGaussian_deriv(void *p, double *r, double *out, int size);   /* gto.h:109 (GPU) */
+double PrimitiveGaussian_overlap(void *p, void *q);              /* gto.h:112 */
+double PrimitiveGaussian_get_zeta(void *p);                      /* gto.h:114 */
+double PrimitiveGaussian_get_coeff(void *p);                     /* gto.h:116 */
+double PrimitiveGaussian_get_norma(void *p);                     /* gto.h:118 */
+void *ContractedGaussian_new(void **prims, int n);               /* gto.h:185 */
+void ContractedGaussian_del(void *c);
+int ContractedGaussian_get_nprim(void *c);                       /* gto.h:188 */
+void ContractedGaussian_get_l(void *c, int *l);                  /* gto.h:190 */
+void ContractedGaussian_get_origin(void *c, double *A);          /* gto.h:192 */
+void ContractedGaussian_compute(void *c, double *r, double *out, int size); /* gto.h:194 (GPU) */
+void ContractedGaussian_deriv(void *c, double *r, double *out, int size);   /* gto.h:197 (GPU) */
+double ContractedGaussian_overlap(void *c, void *o);             /* gto.h:200 */
+double ContractedGaussian_get_norma(void *c);                    /* gto.h:202 */
+void *BasisSet_new_empty(void);                                  /* basis_set.h:53 */
+void *BasisSet_new(void **contractions, int n);                  /* basis_set.h:55 */
+void BasisSet_del(void *b);
+void BasisSet_compute(void *b, double *r, double *out, int size); /* basis_set.h:57 (GPU) */
+void BasisSet_deriv(void *b, double *r, double *out, int size);   /* basis_set.h:59 (GPU) */
+void BasisSet_update(void *b, void *other);                      /* basis_set.h:61 */
+int BasisSet_get_nbasis(void *b);                                /* basis_set.h:63 */
+int BasisSet_get_max_l(void *b);                                 /* basis_set.h:65 */
+int BasisSet_get_max_nprim(void *b);                             /* basis_set.h:67 */
+
+/* ---- wave function (struct wf, src/wavefunction/wavefunction.h:20-44) */
+void wavefunction_guess_hcore(void *psi);                        /* wavefunction.h:51 */
+void wavefunction_transformation_matrix(void *psi);              /* wavefunction.h:53 */
+void wavefunction_compute_coefficients(void *psi);               /* wavefunction.h:55 */
+void wavefunction_compute_density(void *psi);                    /* wavefunction.h:57 */
+void wavefunction_compute_energy(void *psi);                     /* wavefunction.h:59 */
+void wavefunction_iterate(void *psi);                            /* wavefunction.h:61 */
+void nwavefunction_compute_density_from_dm(void *basis, void *grid, double *dm,
+                                           double *output, double epsilon,
+                                           double *dmmaxrow);    /* wavefunction.h:70 (GPU) */
+void nwavefunction_compute_2body_matrix(void *psi, void *grid, double *phi, double *J,
+                                        double *K);              /* wavefunction.h:74 (GPU) */
+void nwavefunction_compute_coupling(void *psi, void *grid, double *phi, double *other_J,
+                                    double *res);                /* wavefunction.h:77 (GPU) */
+void nwavefunction_compute_xc_matrix(void *psi, void *grid, double *phi,
+                                     double *xc_vrho);           /* wavefunction.h:80 (GPU) */
+
+/* ---- analytic integrals / auxiliary basis (libint2, not on the grid
+ * path): present so the ctypes layer binds, every call sets an error.
+ * src/ints/libint_iface.h:106-148, src/grid/auxiliary_basis.h */
+void *LibintInterface_new(int id);
+void LibintInterface_del(void *l);
+void LibintInterface_add_basis(void *l, void *b);
+void LibintInterface_add_pointcharges(void *l, int n, double *q);
+int LibintInterface_get_nbasis(void *l);
+void LibintInterface_compute_1body_ints(void *l, int kind, double *out);
+void LibintInterface_init_2body_ints(void *l);
+void *LibintInterface_compute_2body_ints(void *l, double *D);
+void LibintInterface_compute_2body_direct(void *l, double *D, double *G);
+void LibintInterface_compute_coupling_direct(void *l, void *o, double *D, double *J);
+void *LibintInterface_diis_new(int n);
+void LibintInterface_diis(void *d, void *psi);
+void wavefunction_compute_2body_matrix(void *psi, void *ints);
+void *AuxiliaryBasis_new(void *grid);
+void AuxiliaryBasis_del(void *a);
+double *AuxiliaryBasis_get_aobasis(void *a);
+int AuxiliaryBasis_get_nao(void *a);
+
+/* ================================================== Part 2: device API */
+/* Device pointers of a grid's mirror: points (SoA), weights, Becke weights. */
+int napmo_grid_device_arrays(void *grid, double **x, double **y, double **z, double **w,
+                             double **wb);
+/* Becke weights of device points (SoA) owned by atoms through atom_offset
+ * (host, ncenter+1); replaces BeckeGrid::compute_weights, becke.cpp:79-176. */
+int napmo_gpu_becke_weights(int npoint, int ncenter, const double *x, const double *y,
+                            const double *z, const double *origin, const double *radii,
+                            const int *atom_offset, double *out, void *stream);
+/* phi[mu * ld + p] (and gradients grad[(c * nbasis + mu) * ld + p]) at device
+ * points; replaces BasisSet_compute / BasisSet_deriv (basis_set.cpp:69-99). */
+int napmo_gpu_basis_values(void *basis, int npoint, const double *x, const double *y,
+                           const double *z, double *phi, long ld, double *grad, void *stream);
+/* rho[p] = sum D[mu][nu] phi[mu][p] phi[nu][p]; phi [n][ld], ld >= npoint
+ * rounded up to 128, zero padded; replaces the density of psi_hybrid.py:144-150. */
+int napmo_gpu_density(int n, int npoint, const double *phi, long ld, const double *D,
+                      double *rho, void *stream);
+/* F = phi diag(wv) psi^T (psi = phi if null), upper triangle mirrored;
+ * replaces nwavefunction_compute_coupling/_xc_matrix (nwavefunction.cpp:77-197). */
+int napmo_gpu_quadrature(int n, int npoint, const double *phi, const double *psi, long ld,
+                         const double *wv, double *F, void *stream);
+/* wv = wb w (q v + vext), zero padded to the next multiple of 128. */
+int napmo_gpu_combine_weights(int npoint, const double *wb, const double *w, double q,
+                              const double *v, const double *vext, double *wv, void *stream);
+/* Coulomb potential of rho on the grid's points (projection, radial FEM
+ * solves, multipole evaluation); replaces compute_coulomb / poisson_solver
+ * (ntwobody.py:15-46, poisson_solver.py:18-118, evaluate.cpp:129-220). */
+int napmo_gpu_poisson(void *grid, const double *rho, int lmax, double *v, int accumulate,
+                      double *raw_y, double *raw_dt, void *stream);
+long napmo_poisson_raw_size(void *grid, int lmax);
+/* sum_A Z_A / |r - R_A| at device points; replaces compute_nuclear (nnuclear.py:15-37). */
+int napmo_gpu_nuclear_potential(int npoint, const double *x, const double *y, const double *z,
+                                int nq, const double *charges, double *v, void *stream);
+
+/* Fock-build plan: phi of `basis` on `grid` evaluated once and kept in HBM
+ * with the Poisson tables of `lmax`; per build rho -> V_H -> F (the chain of
+ * psi_hybrid.py:81-110 / psi_numeric.py:152-241). */
+void *napmo_fock_plan_new(void *grid, void *basis, int lmax, void *stream);
+void napmo_fock_plan_free(void *plan);
+int napmo_fock_plan_info(void *plan, int *n, int *npoint, long *ld, double **phi);
+int napmo_fock_plan_density(void *plan, const double *D, double *rho, void *stream);
+int napmo_fock_plan_quadrature(void *plan, double q, const double *v, const double *vext,
+                               double *F, void *stream);
+int napmo_fock_plan_build(void *plan, const double *D, double q, const double *vext, double *F,
+                          double *rho_out, double *v_out, void *stream);
+/* Host-buffer twin of napmo_fock_plan_build (copies inside the call). */
+int napmo_fock_plan_build_host(void *plan, const double *D, double q, const double *vext,
+                               double *F, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NAPMO_B200_H */

@@ -1,0 +1,354 @@
+// C-ABI of the grid quadratures: nAPMO's nwavefunction_* entry points
+// (src/wavefunction/nwavefunction.cpp, bound in napmo/__init__.py:177-191),
+// the device-pointer twins napmo_gpu_density / napmo_gpu_quadrature, and the
+// Fock-build plan that keeps phi, the grid and the Poisson tables resident in
+// HBM across SCF iterations.
+#include <vector>
+
+#include "capi_common.cuh"
+#include "host.h"
+#include "kernels.cuh"
+#include "wavefunction.h"
+
+namespace napmo {
+
+struct PoissonPlan;
+int grid_poisson_plan(BeckeGrid *g, int lmax, cudaStream_t s, PoissonPlan **out);
+int run_poisson(BeckeGrid *g, PoissonPlan *p, const double *rho_dev, double *v_dev,
+                bool accumulate, cudaStream_t s);
+int basis_device(BasisSet *b, cudaStream_t s, const DeviceBasis **out);
+
+// ---------------------------------------------------------------- helpers
+// Host phi [n][npoint] -> device [n][ld] with ld = padded, zero pad columns.
+static int upload_phi(const double *phi, int n, int npoint, long ld, DevBuf<double> &d,
+                      cudaStream_t s) {
+  NAPMO_TRY_CUDA(d.alloc((size_t)n * ld), "alloc phi");
+  NAPMO_TRY_CUDA(cudaMemsetAsync(d.p, 0, (size_t)n * ld * sizeof(double), s), "phi");
+  NAPMO_TRY_CUDA(cudaMemcpy2DAsync(d.p, ld * sizeof(double), phi, npoint * sizeof(double),
+                                   npoint * sizeof(double), n, cudaMemcpyHostToDevice, s),
+                 "upload phi");
+  return kOk;
+}
+
+// F = A diag(wb w v) B^T on the device from host operands (B = A if null).
+static int host_quadrature(BeckeGrid *g, int n, const double *A, const double *B,
+                           const double *v, double *F) {
+  cudaStream_t s = host_api_stream();
+  const int N = g->size;
+  const long ld = padded_points(N);
+  DevBuf<double> dA, dB, dv, wv, dF, work;
+  int st = upload_phi(A, n, N, ld, dA, s);
+  if (st) return st;
+  if (B) {
+    st = upload_phi(B, n, N, ld, dB, s);
+    if (st) return st;
+  }
+  NAPMO_TRY_CUDA(dv.upload(v, N, s), "upload potential");
+  NAPMO_TRY_CUDA(wv.alloc(ld), "alloc");
+  NAPMO_TRY_CUDA(cudaMemsetAsync(wv.p, 0, ld * sizeof(double), s), "wv");
+  NAPMO_TRY_CUDA(launch_combine_weights(N, g->dev.wb, g->dev.w, 1.0, dv.p, nullptr, wv.p, s),
+                 "weights");
+  NAPMO_TRY_CUDA(dF.alloc((size_t)n * n), "alloc");
+  NAPMO_TRY_CUDA(work.alloc(quadrature_workspace_bytes(n, N) / sizeof(double) + 1), "alloc");
+  NAPMO_TRY_CUDA(launch_quadrature_f64(n, N, dA.p, ld, wv.p, dF.p, work.p, s,
+                                       B ? dB.p : nullptr),
+                 "quadrature");
+  NAPMO_TRY_CUDA(cudaMemcpyAsync(F, dF.p, (size_t)n * n * sizeof(double),
+                                 cudaMemcpyDeviceToHost, s),
+                 "download");
+  NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "sync");
+  return kOk;
+}
+
+// ------------------------------------------------------------- Fock plan
+struct FockPlan {
+  BeckeGrid *grid = nullptr;
+  BasisSet *basis = nullptr;
+  int n = 0, lmax = 0;
+  long ld = 0;
+  DevBuf<double> phi, rho, v, wv, work, D, F, vext;
+};
+
+}  // namespace napmo
+
+using namespace napmo;
+
+extern "C" {
+
+// -------------------------------------------------- nAPMO nwavefunction_*
+// res = phi diag(wb w other_J) phi^T   (coupling / Coulomb-type matrix)
+void nwavefunction_compute_coupling(WaveFunction *psi, BeckeGrid *grid, double *phi,
+                                    double *other_J, double *res) {
+  guarded([&] { return host_quadrature(grid, psi->ndim, phi, nullptr, other_J, res); });
+}
+
+// psi->XC = phi diag(wb w xc_vrho) phi^T
+void nwavefunction_compute_xc_matrix(WaveFunction *psi, BeckeGrid *grid, double *phi,
+                                     double *xc_vrho) {
+  guarded([&] { return host_quadrature(grid, psi->ndim, phi, nullptr, xc_vrho, psi->XC); });
+}
+
+// psi->G = int phi_i phi_j J + x_factor int phi_i K_j (upper triangle mirrored)
+void nwavefunction_compute_2body_matrix(WaveFunction *psi, BeckeGrid *grid, double *phi,
+                                        double *J, double *K) {
+  guarded([&] {
+    const int n = psi->ndim;
+    std::vector<double> coul((size_t)n * n), exch((size_t)n * n, 0.0);
+    int st = host_quadrature(grid, n, phi, nullptr, J, coul.data());
+    if (st) return st;
+    if (psi->x_factor != 0.0) {
+      std::vector<double> ones(grid->size, 1.0);
+      st = host_quadrature(grid, n, phi, K, ones.data(), exch.data());
+      if (st) return st;
+    }
+    for (size_t i = 0; i < (size_t)n * n; ++i) psi->G[i] = coul[i] + psi->x_factor * exch[i];
+    return kOk;
+  });
+}
+
+// output[p] = sum_ij dm_ij phi_i(p) phi_j(p) on every grid point.  nAPMO's
+// version returns from the whole function as soon as one point is screened
+// (nwavefunction.cpp:132-133); here every point is evaluated and the
+// screening arguments are accepted but not needed.
+void nwavefunction_compute_density_from_dm(BasisSet *basis, BeckeGrid *grid, double *dm,
+                                           double *output, double epsilon, double *dmmaxrow) {
+  (void)epsilon;
+  (void)dmmaxrow;
+  guarded([&] {
+    cudaStream_t s = host_api_stream();
+    const int n = (int)basis->cont.size(), N = grid->size;
+    const long ld = padded_points(N);
+    const DeviceBasis *db = nullptr;
+    int st = basis_device(basis, s, &db);
+    if (st) return st;
+    DevBuf<double> phi, D, rho;
+    NAPMO_TRY_CUDA(phi.alloc((size_t)n * ld), "alloc");
+    NAPMO_TRY_CUDA(cudaMemsetAsync(phi.p, 0, (size_t)n * ld * sizeof(double), s), "phi");
+    NAPMO_TRY_CUDA(D.upload(dm, (size_t)n * n, s), "upload dm");
+    NAPMO_TRY_CUDA(rho.alloc(N), "alloc");
+    NAPMO_TRY_CUDA(launch_basis_values(*db, N, grid->dev.x, grid->dev.y, grid->dev.z, phi.p,
+                                       ld, nullptr, s),
+                   "basis");
+    NAPMO_TRY_CUDA(launch_density_f64(n, N, phi.p, ld, D.p, rho.p, s), "density");
+    NAPMO_TRY_CUDA(cudaMemcpyAsync(output, rho.p, N * sizeof(double), cudaMemcpyDeviceToHost, s),
+                   "download");
+    NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "sync");
+    return kOk;
+  });
+}
+
+// ----------------------------------------------------------- device API
+// rho[p] = sum_{mu,nu} D[mu][nu] phi[mu][p] phi[nu][p]; phi [n][ld] with
+// ld >= padded(npoint) and zero padding, D [n][n] symmetric.
+int napmo_gpu_density(int n, int npoint, const double *phi, long ld, const double *D,
+                      double *rho, void *stream) {
+  return guarded([&] {
+    NAPMO_REQUIRE(ld >= padded_points(npoint) && ld % 2 == 0, "ld too small or odd");
+    NAPMO_TRY_CUDA(launch_density_f64(n, npoint, phi, ld, D, rho, (cudaStream_t)stream),
+                   "density");
+    return kOk;
+  });
+}
+
+// F[mu][nu] = sum_p phi[mu][p] wv[p] psi[nu][p] (psi = phi when null), upper
+// triangle mirrored; wv zero padded to padded(npoint).  Scratch is taken
+// from the stream-ordered allocator and released on the same stream.
+int napmo_gpu_quadrature(int n, int npoint, const double *phi, const double *psi, long ld,
+                         const double *wv, double *F, void *stream) {
+  return guarded([&] {
+    NAPMO_REQUIRE(ld >= padded_points(npoint) && ld % 2 == 0, "ld too small or odd");
+    cudaStream_t s = (cudaStream_t)stream;
+    void *work = nullptr;
+    const size_t bytes = quadrature_workspace_bytes(n, npoint);
+    NAPMO_TRY_CUDA(cudaMallocAsync(&work, bytes, s), "quadrature workspace");
+    cudaError_t e = launch_quadrature_f64(n, npoint, phi, ld, wv, F, (double *)work, s, psi);
+    cudaFreeAsync(work, s);
+    NAPMO_TRY_CUDA(e, "quadrature");
+    return kOk;
+  });
+}
+
+// wv[p] = wb[p] w[p] (q v[p] + vext[p]) (either potential may be null);
+// entries npoint..padded(npoint) are zeroed.
+int napmo_gpu_combine_weights(int npoint, const double *wb, const double *w, double q,
+                              const double *v, const double *vext, double *wv, void *stream) {
+  return guarded([&] {
+    cudaStream_t s = (cudaStream_t)stream;
+    const long pad = padded_points(npoint);
+    if (pad > npoint)
+      NAPMO_TRY_CUDA(cudaMemsetAsync(wv + npoint, 0, (pad - npoint) * sizeof(double), s), "wv");
+    NAPMO_TRY_CUDA(launch_combine_weights(npoint, wb, w, q, v, vext, wv, s), "weights");
+    return kOk;
+  });
+}
+
+// ------------------------------------------------------------- Fock plan
+// A Fock-build plan evaluates phi for `basis` on `grid` once and keeps it,
+// the grid mirror and the Poisson tables (for `lmax`) resident on the device.
+FockPlan *napmo_fock_plan_new(BeckeGrid *grid, BasisSet *basis, int lmax, void *stream) {
+  FockPlan *p = nullptr;
+  int st = guarded([&] {
+    cudaStream_t s = (cudaStream_t)stream;
+    p = new FockPlan;
+    p->grid = grid;
+    p->basis = basis;
+    p->n = (int)basis->cont.size();
+    p->lmax = lmax;
+    p->ld = padded_points(grid->size);
+    const DeviceBasis *db = nullptr;
+    int e = basis_device(basis, s, &db);
+    if (e) return e;
+    NAPMO_TRY_CUDA(p->phi.alloc((size_t)p->n * p->ld), "alloc phi");
+    NAPMO_TRY_CUDA(cudaMemsetAsync(p->phi.p, 0, p->phi.n * sizeof(double), s), "phi");
+    NAPMO_TRY_CUDA(launch_basis_values(*db, grid->size, grid->dev.x, grid->dev.y, grid->dev.z,
+                                       p->phi.p, p->ld, nullptr, s),
+                   "basis");
+    NAPMO_TRY_CUDA(p->rho.alloc(p->ld), "alloc");
+    NAPMO_TRY_CUDA(p->v.alloc(p->ld), "alloc");
+    NAPMO_TRY_CUDA(p->wv.alloc(p->ld), "alloc");
+    NAPMO_TRY_CUDA(cudaMemsetAsync(p->wv.p, 0, p->ld * sizeof(double), s), "wv");
+    NAPMO_TRY_CUDA(p->work.alloc(quadrature_workspace_bytes(p->n, grid->size) / 8 + 1), "alloc");
+    NAPMO_TRY_CUDA(p->D.alloc((size_t)p->n * p->n), "alloc");
+    NAPMO_TRY_CUDA(p->F.alloc((size_t)p->n * p->n), "alloc");
+    if (lmax >= 0) {
+      PoissonPlan *pp = nullptr;
+      e = grid_poisson_plan(grid, lmax, s, &pp);
+      if (e) return e;
+    }
+    NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "plan");
+    return kOk;
+  });
+  if (st) {
+    delete p;
+    return nullptr;
+  }
+  return p;
+}
+
+void napmo_fock_plan_free(FockPlan *p) { delete p; }
+
+int napmo_fock_plan_info(FockPlan *p, int *n, int *npoint, long *ld, double **phi) {
+  *n = p->n;
+  *npoint = p->grid->size;
+  *ld = p->ld;
+  *phi = p->phi.p;
+  return kOk;
+}
+
+// rho_dev[p] = density of D_dev on the plan's grid.
+int napmo_fock_plan_density(FockPlan *p, const double *D_dev, double *rho_dev, void *stream) {
+  return guarded([&] {
+    NAPMO_TRY_CUDA(launch_density_f64(p->n, p->grid->size, p->phi.p, p->ld, D_dev, rho_dev,
+                                      (cudaStream_t)stream),
+                   "density");
+    return kOk;
+  });
+}
+
+// F_dev = phi diag(wb w (q v + vext)) phi^T (v, vext device, either may be null).
+int napmo_fock_plan_quadrature(FockPlan *p, double q, const double *v_dev,
+                               const double *vext_dev, double *F_dev, void *stream) {
+  return guarded([&] {
+    cudaStream_t s = (cudaStream_t)stream;
+    BeckeGrid *g = p->grid;
+    NAPMO_TRY_CUDA(launch_combine_weights(g->size, g->dev.wb, g->dev.w, q, v_dev, vext_dev,
+                                          p->wv.p, s),
+                   "weights");
+    NAPMO_TRY_CUDA(launch_quadrature_f64(p->n, g->size, p->phi.p, p->ld, p->wv.p, F_dev,
+                                         p->work.p, s),
+                   "quadrature");
+    return kOk;
+  });
+}
+
+// One grid Fock build of a species with its own density:
+//   rho = density(D), v = q * V_H[rho] (Becke-Dickson Poisson), and
+//   F = phi diag(wb w (v + vext)) phi^T.
+// rho_out / v_out (device, optional) receive the density and the potential.
+int napmo_fock_plan_build(FockPlan *p, const double *D_dev, double q, const double *vext_dev,
+                          double *F_dev, double *rho_out, double *v_out, void *stream) {
+  return guarded([&] {
+    cudaStream_t s = (cudaStream_t)stream;
+    BeckeGrid *g = p->grid;
+    double *rho = rho_out ? rho_out : p->rho.p;
+    double *v = v_out ? v_out : p->v.p;
+    NAPMO_TRY_CUDA(launch_density_f64(p->n, g->size, p->phi.p, p->ld, D_dev, rho, s), "density");
+    PoissonPlan *pp = nullptr;
+    int e = grid_poisson_plan(g, p->lmax, s, &pp);
+    if (e) return e;
+    e = run_poisson(g, pp, rho, v, false, s);
+    if (e) return e;
+    NAPMO_TRY_CUDA(launch_combine_weights(g->size, g->dev.wb, g->dev.w, q, v, vext_dev,
+                                          p->wv.p, s),
+                   "weights");
+    NAPMO_TRY_CUDA(launch_quadrature_f64(p->n, g->size, p->phi.p, p->ld, p->wv.p, F_dev,
+                                         p->work.p, s),
+                   "quadrature");
+    return kOk;
+  });
+}
+
+// Same build from host buffers: D_host [n][n] in, F_host [n][n] out, vext_host
+// (npoint, optional).  Copies run on the given stream inside the call.
+int napmo_fock_plan_build_host(FockPlan *p, const double *D_host, double q,
+                               const double *vext_host, double *F_host, void *stream) {
+  return guarded([&] {
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t nn = (size_t)p->n * p->n;
+    NAPMO_TRY_CUDA(cudaMemcpyAsync(p->D.p, D_host, nn * sizeof(double), cudaMemcpyHostToDevice, s),
+                   "D upload");
+    const double *vext = nullptr;
+    if (vext_host) {
+      if (!p->vext.p) NAPMO_TRY_CUDA(p->vext.alloc(p->grid->size), "alloc");
+      NAPMO_TRY_CUDA(cudaMemcpyAsync(p->vext.p, vext_host, p->grid->size * sizeof(double),
+                                     cudaMemcpyHostToDevice, s),
+                     "vext upload");
+      vext = p->vext.p;
+    }
+    int e = napmo_fock_plan_build(p, p->D.p, q, vext, p->F.p, nullptr, nullptr, stream);
+    if (e) return e;
+    NAPMO_TRY_CUDA(cudaMemcpyAsync(F_host, p->F.p, nn * sizeof(double), cudaMemcpyDeviceToHost, s),
+                   "F download");
+    NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "sync");
+    return kOk;
+  });
+}
+
+}  // extern "C"
+
+namespace napmo {
+namespace {
+// v[p] = sum_A Z_A / |r_p - R_A|  (napmo/wavefunction/nnuclear.py:15-37)
+__global__ void nuclear_potential_kernel(int npoint, const double *__restrict__ x,
+                                         const double *__restrict__ y,
+                                         const double *__restrict__ z, int nq,
+                                         const double *__restrict__ q, double *__restrict__ v) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npoint) return;
+  double acc = 0.0;
+  for (int a = 0; a < nq; ++a) {
+    const double dx = q[4 * a] - x[p], dy = q[4 * a + 1] - y[p], dz = q[4 * a + 2] - z[p];
+    acc += q[4 * a + 3] / sqrt(dx * dx + dy * dy + dz * dz);
+  }
+  v[p] = acc;
+}
+}  // namespace
+}  // namespace napmo
+
+extern "C" {
+// v (device, npoint) = sum over point charges (host [nq][4] = x, y, z, Z) of
+// Z / |r - R| at device points (SoA).
+int napmo_gpu_nuclear_potential(int npoint, const double *x, const double *y, const double *z,
+                                int nq, const double *charges, double *v, void *stream) {
+  return napmo::guarded([&] {
+    cudaStream_t s = (cudaStream_t)stream;
+    napmo::DevBuf<double> dq;
+    NAPMO_TRY_CUDA(dq.upload(charges, 4 * (size_t)nq, s), "charges");
+    napmo::nuclear_potential_kernel<<<(npoint + 255) / 256, 256, 0, s>>>(npoint, x, y, z, nq,
+                                                                        dq.p, v);
+    NAPMO_TRY_CUDA(cudaGetLastError(), "nuclear potential");
+    NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "nuclear potential");
+    return napmo::kOk;
+  });
+}
+}  // extern "C"

@@ -1,0 +1,43 @@
+// Kernel launchers of the napmo_b200 CUDA library (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device_types.h"
+
+namespace napmo {
+
+// Becke partition weights (becke.cu).  R_ij and a_ij are the packed
+// lower-triangular inter-atomic distances and size adjustments of nAPMO
+// (src/grid/becke.cpp:80-115), computed on the host.
+cudaError_t launch_becke_weights(int npoint, int ncenter, const double *x,
+                                 const double *y, const double *z,
+                                 const double *origin, const double *Rij,
+                                 const double *aij, const int *atom_offset,
+                                 double *out, cudaStream_t s);
+
+// Contracted Cartesian GTO values phi[f * ld + p] (gto.cu); with `grad`
+// non-null also d/dx, d/dy, d/dz as three further [nfunc][ld] planes.
+cudaError_t launch_basis_values(const DeviceBasis &b, int npoint, const double *x,
+                                const double *y, const double *z, double *phi,
+                                long ld, double *grad, cudaStream_t s);
+
+// FP64 quadratures (quad.cu).
+//   rho[p] = sum_{mu,nu} D[mu][nu] phi[mu][p] phi[nu][p]
+//   F[mu][nu] = sum_p phi[mu][p] wv[p] phi[nu][p]  (upper triangle mirrored)
+size_t density_workspace_bytes(int n, int npoint);
+cudaError_t launch_density_f64(int n, int npoint, const double *phi, long ld,
+                               const double *D, double *rho, cudaStream_t s);
+size_t quadrature_workspace_bytes(int n, int npoint);
+// `phib` (default phi) is the second operand; wv must be zero-padded to the
+// next multiple of 128 points and phi rows zero beyond npoint.
+cudaError_t launch_quadrature_f64(int n, int npoint, const double *phi, long ld,
+                                  const double *wv, double *F, double *work,
+                                  cudaStream_t s, const double *phib = nullptr);
+inline long padded_points(int npoint) { return ((long)npoint + 127) / 128 * 128; }
+// Combined quadrature weight wv[p] = wb[p] * w[p] * (q * v[p] + vext[p]).
+cudaError_t launch_combine_weights(int npoint, const double *wb, const double *w,
+                                   double q, const double *v, const double *vext,
+                                   double *wv, cudaStream_t s);
+
+}  // namespace napmo

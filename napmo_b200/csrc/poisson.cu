@@ -1,0 +1,518 @@
+// Becke-Dickson Poisson pipeline on the device (see poisson.cuh).
+//
+// 1. project:  f_lm(r_i) = sqrt(4 pi (2l+1)) sum_j rho wb w S_lm(u_j) / sum_j w
+//    per atom and radial shell, as a small FP64 product of the per-rule table
+//    S_lm(u_j) with the shell's weighted density (reference:
+//    AtomicGrid::spherical_expansion, src/grid/atomic_grid.cpp:82-136).
+// 2. radial:   one CTA per (atom, l) builds the cubic spline of every f_lm,
+//    the transformed FEM right-hand sides and Dirichlet values, the Hermite
+//    FEM matrix of u'' + b u' + a u = f on the uniform t-axis (shared by the
+//    2l+1 values of m), factors it once by banded LU with partial pivoting and
+//    solves all m together (reference: poisson_solver.py:42-118, ode2.py,
+//    src/horton/ode2.cpp:232-321; the reference solves each (l, m) with
+//    scipy's sparse LU).  The solution splines are written as scaled cubic
+//    coefficients for step 3 and as raw (y, dy/dt) for the Python API.
+// 3. evaluate: v(p) = sum_A sum_lm s_lm(|p - A|) sqrt(2l+1)/sqrt(4 pi)
+//    S_lm(p - A) / |p - A|^l for every point and every atom (the potential
+//    extrapolation has a tail, so no cutoff applies; reference:
+//    eval_decomposition_grid, src/horton/evaluate.cpp:129-220).  Templated on
+//    lmax so the solid-harmonic recursion lives in registers.
+#include <cmath>
+#include <vector>
+
+#include "common.h"
+#include "host.h"
+#include "poisson.cuh"
+#include "solid_harmonics.h"
+
+namespace napmo {
+
+namespace {
+
+__constant__ double c_ov2[5 * 2 * 5 * 2];
+__constant__ double c_ov3[5 * 2 * 5 * 2 * 5 * 2];
+__constant__ double c_shnorm[(kMaxLmax + 1) * (kMaxLmax + 1)];  // [l][m]
+
+constexpr double kPI4 = 4.0 * M_PI;
+constexpr double kInvSqrt4Pi = 0.28209479177387814347;
+
+__device__ __forceinline__ int piece_d(long c, long k, long g) {
+  if (c == g) return (int)k;
+  if (c == g + 1) return (int)(2 + k);
+  return 4;
+}
+
+__device__ double ov2_d(long xmax, long i0, int d0, long i1, int d1) {
+  const long c0 = i0 / 2, k0 = i0 % 2, c1 = i1 / 2, k1 = i1 % 2;
+  if (labs(c1 - c0) >= 2) return 0.0;
+  double r = 0.0;
+  if (c0 >= 1 && c0 <= xmax)
+    r += c_ov2[((piece_d(c0, k0, c0 - 1) * 2 + d0) * 5 + piece_d(c1, k1, c0 - 1)) * 2 + d1];
+  if (c0 >= 0 && c0 <= xmax - 1)
+    r += c_ov2[((piece_d(c0, k0, c0) * 2 + d0) * 5 + piece_d(c1, k1, c0)) * 2 + d1];
+  return r;
+}
+
+__device__ double ov3_d(long xmax, long i0, int d0, long i1, int d1, long i2, int d2) {
+  const long c0 = i0 / 2, k0 = i0 % 2, c1 = i1 / 2, k1 = i1 % 2, c2 = i2 / 2,
+             k2 = i2 % 2;
+  if (labs(c1 - c0) >= 2 || labs(c2 - c0) >= 2) return 0.0;
+  double r = 0.0;
+  if (c0 >= 1 && c0 <= xmax) {
+    const long g = c0 - 1;
+    r += c_ov3[((((piece_d(c0, k0, g) * 2 + d0) * 5 + piece_d(c1, k1, g)) * 2 + d1) * 5 +
+                piece_d(c2, k2, g)) * 2 + d2];
+  }
+  if (c0 >= 0 && c0 <= xmax - 1) {
+    const long g = c0;
+    r += c_ov3[((((piece_d(c0, k0, g) * 2 + d0) * 5 + piece_d(c1, k1, g)) * 2 + d1) * 5 +
+                piece_d(c2, k2, g)) * 2 + d2];
+  }
+  return r;
+}
+
+__device__ __forceinline__ double node_d(long x, long c, long k, int d) {
+  return (k == d) ? (double)(x == c) : 0.0;
+}
+
+__device__ __forceinline__ double rt_inv(const RTParams &rt, double r) {
+  switch (rt.kind) {
+    case kRTChebyshev: return -(acos((r - rt.p0) / (r + rt.p0)) / rt.p1) + rt.npoint;
+    case kRTPower: return pow(r / rt.p0, 1.0 / rt.p1) - 1;
+    case kRTLinear: return (r - rt.p0) / rt.p1;
+    case kRTExp: return log(r / rt.p0) / rt.p1;
+    case kRTShiftedExp: return log((r + rt.p1) / rt.p0) / rt.p2;
+    default: return r;
+  }
+}
+
+// ------------------------------------------------------------------ project
+constexpr int kProjShells = 8;
+constexpr int kProjThreads = 128;
+
+__global__ void __launch_bounds__(kProjThreads)
+project_kernel(PoissonDev P, const double *__restrict__ rho,
+               const double *__restrict__ wb, const double *__restrict__ w) {
+  extern __shared__ double g[];  // [kProjShells][nang]
+  const PoissonAtom at = P.atoms[blockIdx.y];
+  const int s0 = blockIdx.x * kProjShells;
+  if (s0 >= at.nrad) return;
+  const int ns = min(kProjShells, at.nrad - s0);
+  const int nang = at.nang;
+  const int lsize = (at.lmax + 1) * (at.lmax + 1);
+  for (int idx = threadIdx.x; idx < ns * nang; idx += blockDim.x) {
+    const int s = idx / nang, j = idx % nang;
+    const long p = at.point_off + (long)(s0 + s) * nang + j;
+    g[s * nang + j] = rho[p] * wb[p] * w[p];
+  }
+  __syncthreads();
+  const double *Y = P.ytab + at.ytab_off;
+  const double *sigma = P.rad + at.rad_off + kRadSigma * at.nrad;
+  for (int lm = threadIdx.x; lm < lsize; lm += blockDim.x) {
+    double acc[kProjShells];
+#pragma unroll
+    for (int s = 0; s < kProjShells; ++s) acc[s] = 0.0;
+    for (int j = 0; j < nang; ++j) {
+      const double y = __ldg(Y + (long)j * lsize + lm);
+#pragma unroll
+      for (int s = 0; s < kProjShells; ++s) acc[s] = fma(y, g[s * nang + j], acc[s]);
+    }
+    const int l = (int)sqrt((double)lm + 0.5);
+    const double fac = sqrt(4.0 * M_PI * (2.0 * l + 1));
+    for (int s = 0; s < ns; ++s)
+      P.proj[at.proj_off + (long)(s0 + s) * lsize + lm] = acc[s] / sigma[s0 + s] * fac;
+  }
+}
+
+// ------------------------------------------------------------------- radial
+// Band storage of the 2n x 2n FEM matrix: kl = ku = 3, fill-in from partial
+// pivoting reaches kl + ku above the diagonal.  AB(i, j) = band[j*kW + 6+i-j].
+constexpr int kKL = 3, kKU = 3, kW = 2 * kKL + kKU + 1;
+
+__device__ __forceinline__ double &AB(double *band, int i, int j) {
+  return band[j * kW + (kKL + kKU) + i - j];
+}
+
+__global__ void radial_kernel(PoissonDev P, int ncol) {
+  extern __shared__ double sm[];
+  const int sys = blockIdx.x;
+  const PoissonAtom at = P.atoms[P.sys_atom[sys]];
+  const int l = P.sys_l[sys];
+  const int n = at.nrad, n2 = 2 * n;
+  const int lsize = (at.lmax + 1) * (at.lmax + 1);
+  const int nm = 2 * l + 1;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  double *band = sm;                 // n2 * kW
+  double *R = band + n2 * kW;        // n2 * ncol  (row-major, column = m)
+  double *buf = R + n2 * ncol;       // n * ncol   (spline t-derivatives)
+  __shared__ double s_mult[kKL];
+  __shared__ int s_piv;
+
+  const double *rad = P.rad + at.rad_off;
+  const double *r = rad + kRadR * n, *wr = rad + kRadW * n, *j1 = rad + kRadJ1 * n,
+               *j2 = rad + kRadJ2 * n, *j3 = rad + kRadJ3 * n,
+               *den = rad + kRadDen * n, *upm = rad + kRadUp * n;
+  const long xmax = n - 1;
+
+  // -- 1. per m: spline derivatives of f_lm, boundary values, FEM rhs
+  for (int c = tid; c < ncol; c += nt) {
+    if (c >= nm) {
+      for (int row = 0; row < n2; ++row) R[row * ncol + c] = 0.0;
+      continue;
+    }
+    const double *y = P.proj + at.proj_off + l * l + c;  // stride lsize
+    // Thomas elimination for 2/1, 1/4/1, ..., 1/2 with rhs 3 (y_{i+1}-y_{i-1})
+    double prev = (3.0 * (y[lsize] - y[0])) / den[0];
+    buf[c] = prev;
+    for (int i = 1; i < n; ++i) {
+      const double rhs = (i < n - 1) ? 3.0 * (y[(long)(i + 1) * lsize] - y[(long)(i - 1) * lsize])
+                                     : 3.0 * (y[(long)(n - 1) * lsize] - y[(long)(n - 2) * lsize]);
+      prev = (rhs - prev * 1.0) / den[i];
+      buf[i * ncol + c] = prev;
+    }
+    for (int i = n - 2; i >= 0; --i)
+      buf[i * ncol + c] = buf[i * ncol + c] - upm[i] * buf[(i + 1) * ncol + c];
+    // boundary values (Dirichlet) from radial moments
+    double smax = 0.0, smin = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double yi = y[(long)i * lsize];
+      smax += yi * pow(r[i], (double)l) * wr[i];
+      smin += yi * pow(r[i], (double)(-l - 1)) * wr[i];
+    }
+    const double vmax = smax * (1.0 / pow(r[n - 1], (double)(l + 1)) / (2 * l + 1));
+    const double vmin = smin * (pow(r[0], (double)l) / (2 * l + 1));
+    // FEM right-hand side from the transformed source f = -4 pi rho
+    for (int row = 0; row < n2; ++row) {
+      double acc = 0.0;
+      if (row == 0) {
+        acc = vmin;
+      } else if (row == n2 - 2) {
+        acc = vmax;
+      } else {
+        long lo = 2 * (row / 2 - 1), hi = 2 * (row / 2 + 2);
+        if (lo < 0) lo = 0;
+        if (hi > n2) hi = n2;
+        for (long k = lo; k < hi; ++k) {
+          const int i = (int)(k / 2);
+          const double fy = -kPI4 * y[(long)i * lsize];
+          const double jsq = j1[i] * j1[i];
+          double fk;
+          if ((k & 1) == 0) {
+            fk = fy * jsq;
+          } else {
+            const double fdx = -kPI4 * (buf[i * ncol + c] / j1[i]);
+            fk = (fdx * jsq + 2 * fy * j2[i]) * j1[i];
+          }
+          if (fk != 0) acc += fk * ov2_d(xmax, row, 0, k, 0);
+        }
+      }
+      R[row * ncol + c] = acc;
+    }
+  }
+  // -- 2. band matrix (depends on l only)
+  for (int e = tid; e < n2 * kW; e += nt) band[e] = 0.0;
+  __syncthreads();
+  const double l2l = (double)(l * (l + 1));
+  for (int row = tid; row < n2; row += nt) {
+    if (row == 0 || row == n2 - 2) {
+      AB(band, row, row) = 1.0;
+      continue;
+    }
+    long lo = 2 * (row / 2 - 1), hi = 2 * (row / 2 + 2);
+    if (lo < 0) lo = 0;
+    if (hi > n2) hi = n2;
+    for (long col = lo; col < hi; ++col) {
+      double cf = 0.0;
+      cf -= ov2_d(xmax, row, 1, col, 1);
+      for (long k = lo; k < hi; ++k) {
+        const int i = (int)(k / 2);
+        const double ri = r[i], r2 = ri * ri;
+        const double jsq = j1[i] * j1[i];
+        double bk, ak;
+        if ((k & 1) == 0) {
+          bk = j1[i] * (2 / ri) - j2[i] / j1[i];
+          ak = (-l2l / r2) * jsq;
+        } else {
+          bk = j2[i] * (2 / ri) + jsq * (-2 / r2) + (j2[i] * j2[i] - j1[i] * j3[i]) / jsq;
+          const double ay = -l2l / r2, adx = 2 * l2l / (r2 * ri);
+          ak = (adx * jsq + 2 * ay * j2[i]) * j1[i];
+        }
+        if (bk != 0) cf += bk * ov3_d(xmax, row, 0, col, 1, k, 0);
+        if (ak != 0) cf += ak * ov3_d(xmax, row, 0, col, 0, k, 0);
+      }
+      cf += node_d(xmax, row / 2, row % 2, 0) * node_d(xmax, col / 2, col % 2, 1);
+      cf -= node_d(0, row / 2, row % 2, 0) * node_d(0, col / 2, col % 2, 1);
+      AB(band, row, (int)col) = cf;
+    }
+  }
+  __syncthreads();
+  // -- 3. banded LU with partial pivoting, applied to all right-hand sides
+  for (int k = 0; k < n2; ++k) {
+    const int im = min(k + kKL, n2 - 1);
+    const int ju = min(k + kKL + kKU, n2 - 1);
+    if (tid == 0) {
+      int p = k;
+      double best = fabs(AB(band, k, k));
+      for (int i = k + 1; i <= im; ++i) {
+        const double v = fabs(AB(band, i, k));
+        if (v > best) {
+          best = v;
+          p = i;
+        }
+      }
+      s_piv = p;
+    }
+    __syncthreads();
+    const int p = s_piv;
+    if (p != k) {
+      for (int j = k + tid; j <= ju; j += nt) {
+        const double t = AB(band, k, j);
+        AB(band, k, j) = AB(band, p, j);
+        AB(band, p, j) = t;
+      }
+      for (int c = tid; c < ncol; c += nt) {
+        const double t = R[k * ncol + c];
+        R[k * ncol + c] = R[p * ncol + c];
+        R[p * ncol + c] = t;
+      }
+      __syncthreads();
+    }
+    if (tid < im - k) s_mult[tid] = AB(band, k + 1 + tid, k) / AB(band, k, k);
+    __syncthreads();
+    const int nrow = im - k, ncolu = ju - k;
+    for (int e = tid; e < nrow * ncolu; e += nt) {
+      const int i = k + 1 + e / ncolu, j = k + 1 + e % ncolu;
+      AB(band, i, j) -= s_mult[i - k - 1] * AB(band, k, j);
+    }
+    for (int e = tid; e < nrow * ncol; e += nt) {
+      const int i = k + 1 + e / ncol, c = e % ncol;
+      R[i * ncol + c] -= s_mult[i - k - 1] * R[k * ncol + c];
+    }
+    __syncthreads();
+  }
+  // -- 4. back substitution, one column (m) per thread
+  for (int c = tid; c < nm; c += nt) {
+    for (int i = n2 - 1; i >= 0; --i) {
+      double x = R[i * ncol + c];
+      const int je = min(i + kKL + kKU, n2 - 1);
+      for (int j = i + 1; j <= je; ++j) x -= AB(band, i, j) * R[j * ncol + c];
+      R[i * ncol + c] = x / AB(band, i, i);
+    }
+  }
+  __syncthreads();
+  // -- 5. output: raw splines, scaled cubic coefficients, extrapolation
+  const double fl = sqrt((double)(2 * l + 1)) * kInvSqrt4Pi;
+  for (int c = tid; c < nm; c += nt) {
+    const int lm = l * l + c;
+    double *ry = P.raw_y + at.raw_off + (long)lm * n;
+    double *rd = P.raw_dt + at.raw_off + (long)lm * n;
+    for (int i = 0; i < n; ++i) {
+      ry[i] = R[(2 * i) * ncol + c];
+      rd[i] = (R[(2 * i + 1) * ncol + c] / j1[i]) * j1[i];
+    }
+    for (int j = 0; j < n - 1; ++j) {
+      const double y0 = ry[j], y1 = ry[j + 1], d0 = rd[j], d1 = rd[j + 1];
+      const double z = y1 - y0;
+      double *cf = P.spl + at.spl_off + ((long)j * lsize + lm) * 4;
+      cf[0] = y0 * fl;
+      cf[1] = d0 * fl;
+      cf[2] = (3 * z - 2 * d0 - d1) * fl;
+      cf[3] = (-2 * z + d0 + d1) * fl;
+    }
+    P.amp[at.amp_off + lm * 2 + 0] = ry[0] / pow(at.first_x, (double)l) * fl;
+    P.amp[at.amp_off + lm * 2 + 1] = ry[n - 1] * pow(at.last_x, (double)(l + 1)) * fl;
+  }
+}
+
+// ----------------------------------------------------------------- evaluate
+template <int LMAX>
+__global__ void __launch_bounds__(128)
+evaluate_kernel(PoissonDev P, int npoint, const double *__restrict__ gx,
+                const double *__restrict__ gy, const double *__restrict__ gz,
+                double *__restrict__ out, int accumulate) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npoint) return;
+  int mol = 0;
+  if (P.nmol > 1) {
+    int lo = 0, hi = P.nmol - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (P.mol_point_off[mid] <= p) lo = mid; else hi = mid - 1;
+    }
+    mol = lo;
+  }
+  const double px = gx[p], py = gy[p], pz = gz[p];
+  double v = accumulate ? out[p] : 0.0;
+  const int a1 = P.mol_atom_off[mol + 1];
+  for (int A = P.mol_atom_off[mol]; A < a1; ++A) {
+    const PoissonAtom &at = P.atoms[A];
+    const double dx = px - at.cx, dy = py - at.cy, dz = pz - at.cz;
+    const double d = sqrt(dx * dx + dy * dy + dz * dz);
+    const int lmaxA = at.lmax;
+    const int lsize = (lmaxA + 1) * (lmaxA + 1);
+    int region;  // 0 spline, 1 left tail, 2 right tail
+    const double *cf = nullptr;
+    const double *amp = P.amp + at.amp_off;
+    double u = 0.0;
+    if (d < at.first_x) {
+      region = 1;
+    } else if (d <= at.last_x) {
+      region = 0;
+      const double t = rt_inv(at.rt, d);
+      int j = (int)floor(t);
+      if (j == at.nrad - 1) j = at.nrad - 2;
+      if (j < 0) j = 0;
+      u = t - j;
+      cf = P.spl + at.spl_off + (long)j * lsize * 4;
+    } else {
+      region = 2;
+    }
+    double dl = 1.0;  // d^l for the tails
+    auto sval = [&](int lm) -> double {
+      if (region == 0) {
+        const double2 c01 = __ldg(reinterpret_cast<const double2 *>(cf + lm * 4));
+        const double2 c23 = __ldg(reinterpret_cast<const double2 *>(cf + lm * 4 + 2));
+        return c01.x + u * (c01.y + u * (c23.x + u * c23.y));
+      }
+      if (region == 1) return amp[lm * 2] * dl;
+      return amp[lm * 2 + 1] / (dl * d);
+    };
+    v += sval(0);
+    if (LMAX >= 1 && lmaxA >= 1) {
+      const double dinv = 1.0 / d;
+      double dpowl = dinv;
+      dl = d;
+      v += sval(1) * dpowl * dz;
+      v += sval(2) * dpowl * dx;
+      v += sval(3) * dpowl * dy;
+      if (LMAX >= 2 && lmaxA >= 2) {
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        double pold[LMAX + 1], pnew[LMAX + 1], cs[LMAX + 1], sn[LMAX + 1];
+        pold[0] = 1.0;
+        pnew[0] = dz;
+        pnew[1] = 1.0;
+        cs[1] = dx;
+        sn[1] = dy;
+        int lm = 4;
+#pragma unroll
+        for (int l = 2; l <= LMAX; ++l) {
+          if (l > lmaxA) break;
+          dpowl *= dinv;
+          dl *= d;
+          const double fac = 2 * l - 1;
+#pragma unroll
+          for (int m = 0; m <= l - 2; ++m) {
+            const double keep = pold[m];
+            pold[m] = pnew[m];
+            pnew[m] = (dz * fac * pold[m] - r2 * (l + m - 1) * keep) * (1.0 / (l - m));
+          }
+          pold[l - 1] = pnew[l - 1];
+          pnew[l] = fac * pold[l - 1];
+          pnew[l - 1] = dz * pnew[l];
+          cs[l] = dx * cs[l - 1] - dy * sn[l - 1];
+          sn[l] = dx * sn[l - 1] + dy * cs[l - 1];
+          v += sval(lm) * dpowl * pnew[0];
+          ++lm;
+#pragma unroll
+          for (int m = 1; m <= l; ++m) {
+            const double nrm = c_shnorm[l * (kMaxLmax + 1) + m];
+            v += sval(lm) * dpowl * (nrm * cs[m] * pnew[m]);
+            v += sval(lm + 1) * dpowl * (nrm * sn[m] * pnew[m]);
+            lm += 2;
+          }
+        }
+      }
+    }
+  }
+  out[p] = v;
+}
+
+template <int L>
+cudaError_t launch_eval_l(const PoissonDev &P, int npoint, const double *x,
+                          const double *y, const double *z, double *out, int acc,
+                          cudaStream_t s) {
+  evaluate_kernel<L><<<(npoint + 127) / 128, 128, 0, s>>>(P, npoint, x, y, z, out, acc);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t poisson_init_constants() {
+  static thread_local int done_dev = -1;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (done_dev == dev) return cudaSuccess;
+  std::vector<double> ov2(100), ov3(1000);
+  hermite_tables_export(ov2.data(), ov3.data());
+  std::vector<double> nrm((kMaxLmax + 1) * (kMaxLmax + 1), 0.0);
+  for (int l = 2; l <= kMaxLmax; ++l) {
+    double f = M_SQRT2;
+    for (int m = 1; m <= l; ++m) {
+      f /= sqrt((double)((l + m) * (l - m + 1)));
+      nrm[l * (kMaxLmax + 1) + m] = f;
+    }
+  }
+  if ((e = cudaMemcpyToSymbol(c_ov2, ov2.data(), ov2.size() * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_ov3, ov3.data(), ov3.size() * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_shnorm, nrm.data(), nrm.size() * sizeof(double))) != cudaSuccess) return e;
+  done_dev = dev;
+  return cudaSuccess;
+}
+
+cudaError_t launch_poisson_project(const PoissonDev &P, const double *rho,
+                                   const double *wb, const double *w,
+                                   cudaStream_t s) {
+  if (P.natom == 0) return cudaSuccess;
+  dim3 grid((P.max_nrad + kProjShells - 1) / kProjShells, P.natom);
+  const size_t smem = (size_t)kProjShells * P.max_nang * sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(project_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  project_kernel<<<grid, kProjThreads, smem, s>>>(P, rho, wb, w);
+  return cudaGetLastError();
+}
+
+int poisson_radial_ncol(int max_lmax) { return ((2 * max_lmax + 1 + 31) / 32) * 32; }
+
+size_t poisson_radial_smem(int max_nrad, int max_lmax) {
+  const int ncol = poisson_radial_ncol(max_lmax);
+  const size_t n2 = 2 * (size_t)max_nrad;
+  return (n2 * kW + n2 * ncol + (size_t)max_nrad * ncol) * sizeof(double);
+}
+
+cudaError_t launch_poisson_radial(const PoissonDev &P, cudaStream_t s) {
+  if (P.nsys == 0) return cudaSuccess;
+  const int ncol = poisson_radial_ncol(P.max_lmax);
+  const size_t smem = poisson_radial_smem(P.max_nrad, P.max_lmax);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(radial_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  radial_kernel<<<P.nsys, ncol, smem, s>>>(P, ncol);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_poisson_evaluate(const PoissonDev &P, int npoint,
+                                    const double *x, const double *y,
+                                    const double *z, double *out, bool accumulate,
+                                    cudaStream_t s) {
+  if (npoint <= 0) return cudaSuccess;
+  const int a = accumulate ? 1 : 0;
+  switch (P.max_lmax) {
+#define NAPMO_EVAL_CASE(L) \
+  case L: return launch_eval_l<L>(P, npoint, x, y, z, out, a, s);
+    NAPMO_EVAL_CASE(0) NAPMO_EVAL_CASE(1) NAPMO_EVAL_CASE(2) NAPMO_EVAL_CASE(3)
+    NAPMO_EVAL_CASE(4) NAPMO_EVAL_CASE(5) NAPMO_EVAL_CASE(6) NAPMO_EVAL_CASE(7)
+    NAPMO_EVAL_CASE(8) NAPMO_EVAL_CASE(9) NAPMO_EVAL_CASE(10) NAPMO_EVAL_CASE(11)
+    NAPMO_EVAL_CASE(12) NAPMO_EVAL_CASE(13) NAPMO_EVAL_CASE(14) NAPMO_EVAL_CASE(15)
+    NAPMO_EVAL_CASE(16) NAPMO_EVAL_CASE(17) NAPMO_EVAL_CASE(18) NAPMO_EVAL_CASE(19)
+    NAPMO_EVAL_CASE(20)
+#undef NAPMO_EVAL_CASE
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace napmo

@@ -1,0 +1,74 @@
+// Device-side Becke-Dickson Poisson solver (A. D. Becke, R. M. Dickson,
+// J. Chem. Phys. 89, 2993 (1988)) as used by nAPMO's grid Coulomb potential
+// (napmo/grids/poisson_solver.py:18-118, napmo/utilities/ode2.py:35-118,
+// napmo/wavefunction/ntwobody.py:15-46, src/horton/evaluate.cpp:129-220).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device_types.h"
+
+namespace napmo {
+
+// Per-atom metadata of a (possibly batched) Poisson problem.
+struct PoissonAtom {
+  double cx, cy, cz;
+  double first_x, last_x;  // radius of the first / last radial point
+  RTParams rt;
+  int point_off;  // first grid point of this atom
+  int nrad, nang, lmax;
+  int rad_off;    // radial tables: 8 arrays of nrad (see kRad*)
+  int ytab_off;   // [nang][lsize] solid harmonics of the Lebedev directions
+  int proj_off;   // [nrad][lsize] projected density
+  int spl_off;    // [nrad-1][lsize][4] cubic coefficients (scaled)
+  int amp_off;    // [lsize][2] left / right extrapolation amplitudes (scaled)
+  int raw_off;    // [lsize][nrad] solution values y and t-derivatives dt
+};
+
+// Radial table slots (each nrad long, at rad_off + slot * nrad).
+enum : int {
+  kRadR = 0,      // radius
+  kRadW = 1,      // radial weight 4 pi r^2 dr/dt
+  kRadJ1 = 2,     // dr/dt
+  kRadJ2 = 3,     // d2r/dt2
+  kRadJ3 = 4,     // d3r/dt3
+  kRadSigma = 5,  // sum of the atomic weights of the shell
+  kRadDen = 6,    // Thomas-algorithm denominators of the spline system
+  kRadUp = 7,     // Thomas-algorithm modified super-diagonal
+  kRadSlots = 8,
+};
+
+struct PoissonDev {
+  int natom = 0, nmol = 0, nsys = 0;
+  int max_lmax = 0, max_nrad = 0, max_nang = 0;
+  PoissonAtom *atoms = nullptr;
+  int *mol_atom_off = nullptr;   // nmol + 1
+  int *mol_point_off = nullptr;  // nmol + 1
+  int *sys_atom = nullptr;       // radial systems (atom, l)
+  int *sys_l = nullptr;
+  double *rad = nullptr;
+  double *ytab = nullptr;
+  double *proj = nullptr;
+  double *spl = nullptr;
+  double *amp = nullptr;
+  double *raw_y = nullptr;
+  double *raw_dt = nullptr;
+};
+
+// Uploads the Hermite FEM integral tables and solid-harmonic norms to
+// constant memory (idempotent, per device).
+cudaError_t poisson_init_constants();
+
+// rho -> projected density (rho * wb * w projected on S_lm per shell).
+cudaError_t launch_poisson_project(const PoissonDev &P, const double *rho,
+                                   const double *wb, const double *w,
+                                   cudaStream_t s);
+// projected density -> spline tables of the potential (one CTA per (atom, l)).
+cudaError_t launch_poisson_radial(const PoissonDev &P, cudaStream_t s);
+// spline tables -> potential at every grid point (out = or += ).
+cudaError_t launch_poisson_evaluate(const PoissonDev &P, int npoint,
+                                    const double *x, const double *y,
+                                    const double *z, double *out, bool accumulate,
+                                    cudaStream_t s);
+
+}  // namespace napmo

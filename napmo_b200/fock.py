@@ -1,0 +1,144 @@
+"""Device-resident grid Fock builds (the hot path), driven through the C-ABI.
+
+A ``FockBuilder`` evaluates the basis on the grid once (phi stays in HBM for
+the whole SCF) and then, per build, runs on one CUDA stream:
+
+  rho = diag(phi^T D phi)                  (FP64 DFMA GEMM, fused epilogue)
+  v   = q V_H[rho]                         (Becke-Dickson Poisson on device)
+  F   = phi diag(wb w (v + v_ext)) phi^T   (FP64 split-K GEMM)
+
+torch provides device memory and the stream; every byte of arithmetic is in
+libnapmo's kernels.  Reference call stack: napmo/wavefunction/psi_hybrid.py:
+81-110 (coupling), napmo/wavefunction/ntwobody.py:15-46 (Coulomb potential),
+src/wavefunction/nwavefunction.cpp:77-107,161-197 (quadratures).
+"""
+from ctypes import byref, c_int, c_long, c_void_p
+
+import numpy as np
+
+from . import cext
+from .cext import checked, NapmoError
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise NapmoError('FockBuilder needs a CUDA device')
+    return torch
+
+
+def _stream(torch, stream):
+    return (stream or torch.cuda.current_stream()).cuda_stream
+
+
+class FockBuilder(object):
+    """Grid Fock builds for one species (basis) on one molecular grid.
+
+    Args:
+        grid (BeckeGrid): molecular grid (Becke weights already on device).
+        basis (BasisSet): basis of the species.
+        lmax (int): angular cutoff of the Poisson expansion; nAPMO uses
+            lebedev_get_order(nang) // 2 (psi_numeric.py:66).  Negative: no
+            Poisson tables (quadratures only).
+    """
+
+    def __init__(self, grid, basis, lmax, stream=None):
+        torch = _torch()
+        self.torch = torch
+        self.grid = grid
+        self.basis = basis
+        self.lmax = int(lmax)
+        self._plan = cext.lib.napmo_fock_plan_new(grid._this, basis._this, self.lmax,
+                                                  _stream(torch, stream))
+        if not self._plan:
+            cext.check()
+            raise NapmoError('fock plan construction failed')
+        n, npt, ld, phi = c_int(), c_int(), c_long(), c_void_p()
+        cext.lib.napmo_fock_plan_info(self._plan, byref(n), byref(npt), byref(ld), byref(phi))
+        self.n, self.npoint, self.ld, self._phi_ptr = n.value, npt.value, ld.value, phi.value
+
+    def __del__(self):
+        if getattr(self, '_plan', None):
+            cext.lib.napmo_fock_plan_free(self._plan)
+            self._plan = None
+
+    def _dev(self, x, shape=None):
+        t = self.torch
+        if x is None:
+            return None
+        if not isinstance(x, t.Tensor):
+            x = t.as_tensor(np.ascontiguousarray(x, dtype=np.float64), device='cuda')
+        x = x.to(device='cuda', dtype=t.float64).contiguous()
+        if shape is not None and tuple(x.shape) != tuple(shape):
+            raise ValueError('expected shape %s, got %s' % (shape, tuple(x.shape)))
+        return x
+
+    def density(self, D, stream=None):
+        """rho at every grid point for density matrix D (n x n, symmetric)."""
+        t = self.torch
+        D = self._dev(D, (self.n, self.n))
+        rho = t.empty(self.npoint, dtype=t.float64, device='cuda')
+        checked(cext.lib.napmo_fock_plan_density(self._plan, D.data_ptr(), rho.data_ptr(),
+                                                 _stream(t, stream)))
+        return rho
+
+    def quadrature(self, q=1.0, v=None, vext=None, stream=None):
+        """F = phi diag(wb w (q v + vext)) phi^T for grid potentials v, vext."""
+        t = self.torch
+        v = self._dev(v, (self.npoint,))
+        vext = self._dev(vext, (self.npoint,))
+        F = t.empty((self.n, self.n), dtype=t.float64, device='cuda')
+        checked(cext.lib.napmo_fock_plan_quadrature(
+            self._plan, float(q), v.data_ptr() if v is not None else None,
+            vext.data_ptr() if vext is not None else None, F.data_ptr(), _stream(t, stream)))
+        return F
+
+    def coulomb_potential(self, rho, stream=None):
+        """V_H[rho] at every grid point (device Poisson solve)."""
+        t = self.torch
+        rho = self._dev(rho, (self.npoint,))
+        v = t.empty(self.npoint, dtype=t.float64, device='cuda')
+        checked(cext.lib.napmo_gpu_poisson(self.grid._this, rho.data_ptr(), self.lmax,
+                                           v.data_ptr(), 0, None, None, _stream(t, stream)))
+        return v
+
+    def build(self, D, q=1.0, vext=None, stream=None, out=None):
+        """One grid Fock build: returns (F, rho, v) with v = q V_H[rho]."""
+        t = self.torch
+        D = self._dev(D, (self.n, self.n))
+        vext = self._dev(vext, (self.npoint,))
+        F = out if out is not None else t.empty((self.n, self.n), dtype=t.float64, device='cuda')
+        rho = t.empty(self.npoint, dtype=t.float64, device='cuda')
+        v = t.empty(self.npoint, dtype=t.float64, device='cuda')
+        checked(cext.lib.napmo_fock_plan_build(
+            self._plan, D.data_ptr(), float(q), vext.data_ptr() if vext is not None else None,
+            F.data_ptr(), rho.data_ptr(), v.data_ptr(), _stream(t, stream)))
+        return F, rho, v
+
+    def build_host(self, D, q=1.0, vext=None, stream=None):
+        """Same build from/to host numpy arrays through the C-ABI (copies inside)."""
+        t = self.torch
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        F = np.empty((self.n, self.n), dtype=np.float64)
+        vp = None
+        if vext is not None:
+            vext = np.ascontiguousarray(vext, dtype=np.float64)
+            vp = vext.ctypes.data
+        checked(cext.lib.napmo_fock_plan_build_host(self._plan, D, float(q), vp, F,
+                                                    _stream(t, stream)))
+        return F
+
+    def phi(self):
+        """phi [n][ld] on the device as a torch view (ld >= npoint, zero padded)."""
+        return _view(self.torch, self._phi_ptr, (self.n, self.ld))
+
+
+def _view(torch, ptr, shape):
+    """A torch tensor aliasing libnapmo device memory (read-only use)."""
+    n = int(np.prod(shape))
+
+    class _Holder(object):
+        __cuda_array_interface__ = {
+            'shape': (n,), 'typestr': '<f8', 'data': (ptr, True), 'version': 2}
+
+    return torch.as_tensor(_Holder(), device='cuda').view(*shape)

@@ -1,0 +1,201 @@
+"""Host side of libnapmo (no GPU needed): grid construction bit-exact with the
+reference, Hermite FEM tables, splines and extrapolations, GTO set-up, and
+the exported C-ABI."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import napmo_b200 as nb
+from napmo_b200 import cext
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_library_exports_every_declared_symbol():
+    with open(os.path.join(ROOT, 'include', 'napmo_b200.h')) as f:
+        text = re.sub(r'/\*.*?\*/', '', f.read(), flags=re.S)
+    names = set(re.findall(r'\b([A-Za-z_][A-Za-z0-9_]*)\s*\(', text))
+    names -= {'if', 'for', 'while', 'return', 'sizeof', 'defined'}
+    lib = ctypes.CDLL(cext.LIBPATH)
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+    assert len(names) > 150
+
+
+@pytest.mark.parametrize('order', [6, 26, 110, 146, 170, 194, 230, 266, 302, 350, 434, 590,
+                                   1202, 5810])
+def test_angular_grid_bit_exact(refvec, order):
+    g = nb.AngularGrid(order)
+    ref = refvec['lebedev_%d' % order]
+    assert np.array_equal(g.points, ref[:, :3])
+    assert np.array_equal(g.weights, ref[:, 3])
+
+
+@pytest.mark.parametrize('name,radii,n', [('cheb_H_100', 0.5858151015155881, 100),
+                                          ('cheb_O_50', 1.2472192483880264, 50),
+                                          ('cheb_C_75', 1.4069648596390618, 75)])
+def test_radial_transform_bit_exact(refvec, name, radii, n):
+    rt = nb.ChebyshevRadialTransform(radii, n)
+    ref = refvec['rt_' + name]
+    got = np.stack([rt.radius_all(), rt.deriv_all(), rt.deriv2_all(), rt.deriv3_all()], axis=1)
+    assert np.array_equal(got, ref)
+
+
+def test_power_transform_bit_exact(refvec):
+    rt = nb.PowerRadialTransform(1e-3, 2e1, 100)
+    ref = refvec['rt_power_100']
+    assert np.array_equal(rt.radius_all(), ref[:, 0])
+    assert np.array_equal(rt.deriv_all(), ref[:, 1])
+
+
+def test_radial_grid_known_answer(known):
+    g = nb.RadialGrid(50, 'He')
+    assert g.size == 50
+    np.testing.assert_allclose(g.points, known['radial_He_50_points'])
+
+
+@pytest.mark.parametrize('sym,nrad,nang', [('O', 50, 110), ('H', 75, 194), ('C', 100, 302)])
+def test_atomic_grid_bit_exact_vs_oracle(oracle, elements, sym, nrad, nang):
+    R = np.array([0.31, -1.2, 2.5])
+    g = nb.AtomicGrid(nrad, nang, R, sym)
+    o = oracle.Atom(R, elements[sym]['atomic_radii'], nrad, nang)
+    assert np.array_equal(g.points, o.points)
+    assert np.array_equal(g.weights, o.weights)
+
+
+def test_build_ode2_bit_exact(refvec):
+    n = 12
+    bcs = np.array([0.3, np.nan, -0.7, np.nan])
+    coeffs = np.zeros((2 * n, 2 * n))
+    rhs = np.zeros(2 * n)
+    cext.lib.build_ode2(np.ascontiguousarray(refvec['ode_b']), np.ascontiguousarray(refvec['ode_a']),
+                        np.ascontiguousarray(refvec['ode_f']), bcs, coeffs, rhs, n)
+    assert np.array_equal(coeffs, refvec['ode_coeffs'])
+    assert np.array_equal(rhs, refvec['ode_rhs'])
+
+
+def test_hermite_integrals_bit_exact_vs_reference(oracle):
+    ref = oracle.ref_lib()
+    if ref is None:
+        pytest.skip('nAPMO sources not compiled here (oracle/_ref)')
+    lib = cext.lib
+    lib.hermite_overlap2.restype = ctypes.c_double
+    lib.hermite_overlap2.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_bool, ctypes.c_long,
+                                     ctypes.c_bool]
+    lib.hermite_overlap3.restype = ctypes.c_double
+    lib.hermite_overlap3.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_bool, ctypes.c_long,
+                                     ctypes.c_bool, ctypes.c_long, ctypes.c_bool]
+    xmax = 5
+    for i0 in range(12):
+        for i1 in range(12):
+            for d0 in (False, True):
+                for d1 in (False, True):
+                    assert lib.hermite_overlap2(xmax, i0, d0, i1, d1) == \
+                        ref.hermite_overlap2(xmax, i0, d0, i1, d1)
+                    for i2 in range(12):
+                        for d2 in (False, True):
+                            assert lib.hermite_overlap3(xmax, i0, d0, i1, d1, i2, d2) == \
+                                ref.hermite_overlap3(xmax, i0, d0, i1, d1, i2, d2)
+
+
+def test_solid_harmonics_bit_exact_vs_reference(oracle):
+    ref = oracle.ref_lib()
+    if ref is None:
+        pytest.skip('nAPMO sources not compiled here (oracle/_ref)')
+    lib = cext.lib
+    lib.fill_pure_polynomials.argtypes = [cext.a1df, ctypes.c_long]
+    rng = np.random.default_rng(3)
+    for lmax in (2, 5, 14, 20):
+        for _ in range(10):
+            v = rng.normal(size=3)
+            a = np.zeros((lmax + 1) ** 2 + 3)
+            a[:3] = v
+            b = a.copy()
+            lib.fill_pure_polynomials(a, lmax)
+            ref.fill_pure_polynomials(b, lmax)
+            assert np.array_equal(a, b)
+
+
+def test_spline_system_bit_exact(refvec):
+    y = np.ascontiguousarray(refvec['spline_y'])
+    dt = np.zeros_like(y)
+    cext.lib.solve_cubic_spline_system(y, dt, y.shape[0])
+    assert np.array_equal(dt, refvec['spline_dt'])
+
+
+# napmo/grids/test/test_extrapolation.py, ported
+def test_extrapolation_identity_cusp():
+    x = np.arange(10, dtype=float)
+    y = np.exp(-0.3 * x)
+    cs = nb.CubicSpline(y, -0.3 * y)
+    newx = np.array([-2.5, -1.1])
+    assert abs(cs(newx) - np.exp(-0.3 * newx)).max() < 1e-10
+    assert abs(cs.deriv(newx) - -0.3 * np.exp(-0.3 * newx)).max() < 1e-10
+    newx = np.array([10.5, 11.5])
+    assert abs(cs(newx)).max() < 1e-10
+    assert abs(cs.deriv(newx)).max() < 1e-10
+
+
+def test_extrapolation_identity_power():
+    x = np.arange(10, dtype=float)
+    y = 1 / (np.exp(-2 * x) + x ** 2)
+    d = -y ** 2 * (np.exp(-2 * x) * (-2) + 2 * x)
+    cs = nb.CubicSpline(y, d, extrapolation=nb.PowerExtrapolation(-2.0))
+    assert cs.extrapolation.power == -2.0
+    newx = np.array([-2.5, -1.1])
+    assert abs(cs(newx)).max() == 0.0
+    newx = np.array([10.5, 11.5])
+    assert abs(cs(newx) - 1 / newx ** 2).max() < 1e-10
+    assert abs(cs.deriv(newx) - -2 / newx ** 3).max() < 1e-10
+
+
+def test_lebedev_order():
+    assert nb.lebedev_get_order(110) == 17
+    with pytest.raises(KeyError):
+        nb.lebedev_get_order(2)
+
+
+# napmo/gto/test/test_primitive_gaussian.py / test_contracted_gaussian.py (set-up part)
+def test_gaussian_norms_and_overlaps(known):
+    p = nb.PrimitiveGaussian(exponent=0.5)
+    np.testing.assert_allclose(p.normalization, known['s_norm_zeta05'])
+    np.testing.assert_allclose(p.overlap(p), 1.0)
+    p = nb.PrimitiveGaussian(exponent=0.5, l=np.array([0, 0, 3], dtype=np.int32))
+    np.testing.assert_allclose(p.normalization, known['fz3_norm_zeta05'])
+    np.testing.assert_allclose(p.overlap(p), 1.0)
+    c = nb.ContractedGaussian(exponents=[0.5])
+    assert c.nprim == 1
+    np.testing.assert_allclose(c.overlap(c), 1.0)
+    c = nb.ContractedGaussian(exponents=[0.5], l=np.array([0, 0, 3], dtype=np.int32))
+    np.testing.assert_allclose(c.overlap(c), 1.0)
+
+
+def test_basis_set_order_and_size(basis_library):
+    b = nb.BasisSet('CC-PVDZ', 'C', origin=[0.0, 0.0, 0.0])
+    assert b['nbasis'] == 15          # Cartesian: 3 s + 2 x 3 p + 6 d
+    ls = [tuple(c.l) for c in b['cont']]
+    assert ls[3:6] == [(1, 0, 0), (0, 1, 0), (0, 0, 1)]
+    assert ls[9:15] == [(2, 0, 0), (1, 1, 0), (1, 0, 1), (0, 2, 0), (0, 1, 1), (0, 0, 2)]
+    with pytest.raises(ValueError):
+        nb.BasisSet('STO-3G', 'HH', origin=[0.0, 0.0, 0.0])
+
+
+def test_c20h42_sizes():
+    from napmo_b200.system import alkane_geometry
+    atoms = alkane_geometry()
+    assert len(atoms) == 62
+    xyz = np.array([a[1] for a in atoms])
+    d = np.sqrt(((xyz[:, None] - xyz[None]) ** 2).sum(-1)) + np.eye(62) * 10
+    assert d.min() > 1.0   # no clashes (angstrom)
+    nbf = sum(15 if s == 'C' else 5 for s, _ in atoms)
+    assert nbf == 510
+
+
+def test_errors_are_reported_not_fatal():
+    with pytest.raises(nb.NapmoError):
+        nb.AngularGrid(7)
+    with pytest.raises(nb.NapmoError):
+        nb.PowerRadialTransform(2.0, 1.0, 10)

@@ -36,10 +36,14 @@ cudaStream_t host_api_stream() {
 struct PoissonPlan {
   PoissonDev d;
   int lmax = -1;
+  int max_mol_npoint = 0;
   std::vector<PoissonAtom> h_atoms;
   DevBuf<PoissonAtom> atoms;
   DevBuf<int> mol_atom_off, mol_point_off, sys_atom, sys_l;
   DevBuf<double> rad, ytab, proj, spl, amp, raw_y, raw_dt;
+  DevBuf<int> pairs;
+  DevBuf<EvalItem> items;
+  DevBuf<double> pair_v;
 };
 
 void free_poisson_plan(PoissonPlan *p) { delete p; }
@@ -78,7 +82,12 @@ int build_poisson_plan(const std::vector<const AtomLayout *> &atoms,
   std::vector<double> rad, ytab;
   std::map<std::pair<int, int>, int> ykey;  // (atom-rule id via nang,lmax) -> offset
   std::vector<int> sys_atom, sys_l;
-  long proj = 0, spl = 0, amp = 0, raw = 0;
+  long proj = 0, spl = 0, amp = 0, raw = 0, pairs = 0;
+  int buckets = 0;
+  std::vector<int> atom_mol(natom, 0);
+  for (int m = 0; m + 1 < (int)mol_atom_off.size(); ++m)
+    for (int a = mol_atom_off[m]; a < mol_atom_off[m + 1]; ++a) atom_mol[a] = m;
+  plan->max_mol_npoint = 0;
   for (int a = 0; a < natom; ++a) {
     const AtomLayout &L = *atoms[a];
     PoissonAtom &A = ha[a];
@@ -134,6 +143,14 @@ int build_poisson_plan(const std::vector<const AtomLayout *> &atoms,
     amp += (long)lsize * 2;
     A.raw_off = (int)raw;
     raw += (long)lsize * n;
+    const int mol = atom_mol[a];
+    A.mol_point_start = mol_point_off[mol];
+    A.mol_npoint = mol_point_off[mol + 1] - mol_point_off[mol];
+    plan->max_mol_npoint = std::max(plan->max_mol_npoint, A.mol_npoint);
+    A.bucket_off = buckets;
+    buckets += n + 1;
+    A.pair_off = pairs;
+    pairs += A.mol_npoint;
     for (int l = 0; l <= lmax; ++l) {
       sys_atom.push_back(a);
       sys_l.push_back(l);
@@ -167,6 +184,53 @@ int build_poisson_plan(const std::vector<const AtomLayout *> &atoms,
   d.amp = plan->amp.p;
   d.raw_y = plan->raw_y.p;
   d.raw_dt = plan->raw_dt.p;
+  d.npair = pairs;
+  return kOk;
+}
+
+// Bucket-sorted (atom, point) pair lists for the evaluation of the potential
+// at the points (x, y, z) (device, all molecules concatenated).  Built once
+// per grid; about 12 bytes per pair.
+int build_pair_lists(PoissonPlan *plan, const double *x, const double *y, const double *z,
+                     cudaStream_t s) {
+  PoissonDev &d = plan->d;
+  const std::vector<PoissonAtom> &ha = plan->h_atoms;
+  int nb = 0;
+  for (auto &a : ha) nb += a.nrad + 1;
+  DevBuf<int> bucket_of, count;
+  NAPMO_TRY_CUDA(bucket_of.alloc(d.npair), "pair lists");
+  NAPMO_TRY_CUDA(count.alloc(nb), "pair lists");
+  NAPMO_TRY_CUDA(cudaMemsetAsync(count.p, 0, nb * sizeof(int), s), "pair lists");
+  NAPMO_TRY_CUDA(launch_pair_buckets(d, plan->max_mol_npoint, x, y, z, bucket_of.p, count.p, s),
+                 "pair buckets");
+  std::vector<int> hc(nb);
+  NAPMO_TRY_CUDA(cudaMemcpyAsync(hc.data(), count.p, nb * sizeof(int), cudaMemcpyDeviceToHost, s),
+                 "pair lists");
+  NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "pair lists");
+  // exclusive scan per atom -> bucket starts (relative to the atom's slice)
+  std::vector<int> start(nb);
+  std::vector<EvalItem> items;
+  for (int a = 0; a < (int)ha.size(); ++a) {
+    int acc = 0;
+    for (int b = 0; b <= ha[a].nrad; ++b) {
+      const int k = ha[a].bucket_off + b;
+      start[k] = acc;
+      for (int c = 0; c < hc[k]; c += kEvalChunk)
+        items.push_back(EvalItem{a, b, acc + c, std::min(kEvalChunk, hc[k] - c)});
+      acc += hc[k];
+    }
+  }
+  NAPMO_TRY_CUDA(count.upload(start, s), "pair lists");  // reused as the cursor
+  NAPMO_TRY_CUDA(plan->pairs.alloc(d.npair), "pair lists");
+  d.pairs = plan->pairs.p;
+  NAPMO_TRY_CUDA(launch_pair_scatter(d, plan->max_mol_npoint, bucket_of.p, count.p, s),
+                 "pair scatter");
+  NAPMO_TRY_CUDA(plan->items.upload(items, s), "pair lists");
+  NAPMO_TRY_CUDA(plan->pair_v.alloc(d.npair), "pair lists");
+  NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "pair lists");
+  d.items = plan->items.p;
+  d.nitems = (int)items.size();
+  d.pair_v = plan->pair_v.p;
   return kOk;
 }
 
@@ -185,6 +249,11 @@ int grid_poisson_plan(BeckeGrid *g, int lmax, cudaStream_t s, PoissonPlan **out)
   for (auto &L : g->layout) atoms.push_back(&L);
   std::vector<int> lm(atoms.size(), lmax);
   int st = build_poisson_plan(atoms, lm, {0, (int)atoms.size()}, {0, g->size}, s, p);
+  if (st != kOk) {
+    delete p;
+    return st;
+  }
+  st = build_pair_lists(p, g->dev.x, g->dev.y, g->dev.z, s);
   if (st != kOk) {
     delete p;
     return st;

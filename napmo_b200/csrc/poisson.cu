@@ -427,10 +427,188 @@ evaluate_kernel(PoissonDev P, int npoint, const double *__restrict__ gx,
   out[p] = v;
 }
 
+// --------------------------------------------------- bucketed evaluation
+// Bucket of the pair (atom A, point p): 0 below the first radial point, 1 + j
+// inside spline interval j, nrad above the last point -- the same region and
+// interval test as the spline evaluation of the reference
+// (src/horton/cubic_spline.cpp:147-181).
+__device__ __forceinline__ int pair_bucket(const PoissonAtom &at, double px, double py,
+                                           double pz) {
+  const double dx = px - at.cx, dy = py - at.cy, dz = pz - at.cz;
+  const double d = sqrt(dx * dx + dy * dy + dz * dz);
+  if (d < at.first_x) return 0;
+  if (d > at.last_x) return at.nrad;
+  int j = (int)floor(rt_inv(at.rt, d));
+  if (j == at.nrad - 1) j = at.nrad - 2;
+  if (j < 0) j = 0;
+  return 1 + j;
+}
+
+__global__ void pair_bucket_kernel(PoissonDev P, const double *__restrict__ gx,
+                                   const double *__restrict__ gy,
+                                   const double *__restrict__ gz, int *__restrict__ bucket_of,
+                                   int *__restrict__ count) {
+  const PoissonAtom &at = P.atoms[blockIdx.y];
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= at.mol_npoint) return;
+  const int p = at.mol_point_start + q;
+  const int b = pair_bucket(at, gx[p], gy[p], gz[p]);
+  bucket_of[at.pair_off + q] = b;
+  atomicAdd(&count[at.bucket_off + b], 1);
+}
+
+__global__ void pair_scatter_kernel(PoissonDev P, const int *__restrict__ bucket_of,
+                                    int *__restrict__ cursor) {
+  const PoissonAtom &at = P.atoms[blockIdx.y];
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= at.mol_npoint) return;
+  const int b = bucket_of[at.pair_off + q];
+  const int pos = atomicAdd(&cursor[at.bucket_off + b], 1);
+  P.pairs[at.pair_off + pos] = at.mol_point_start + q;
+}
+
+// One CTA per EvalItem: the coefficient block of the item's spline interval
+// (or the tail amplitudes) is staged in shared memory once and every thread
+// evaluates one pair:
+//   v_pair = sum_k u^k sum_lm S_lm(r_hat) c_k,lm        (interval)
+//   v_pair = sum_l g_l(d) sum_m S_lm(r_hat) a_lm         (tails, g = d^l or
+//                                                         d^-(l+1))
+// with S_lm(r_hat) = S_lm(p - A) / d^l, so the 1/d^l of the reference is folded
+// into the unit vector.  The result goes to the pair's own slot of pair_v.
+template <int LMAX>
+__global__ void __launch_bounds__(kEvalChunk)
+eval_pairs_kernel(PoissonDev P, const double *__restrict__ gx,
+                  const double *__restrict__ gy, const double *__restrict__ gz) {
+  extern __shared__ double cf[];
+  const EvalItem it = P.items[blockIdx.x];
+  const PoissonAtom &at = P.atoms[it.atom];
+  const int lmaxA = at.lmax;
+  const int lsize = (lmaxA + 1) * (lmaxA + 1);
+  const int region = (it.bucket == 0) ? 1 : (it.bucket == at.nrad ? 2 : 0);
+  if (region == 0) {
+    const double *src = P.spl + at.spl_off + (long)(it.bucket - 1) * lsize * 4;
+    for (int e = threadIdx.x; e < lsize * 4; e += blockDim.x) cf[e] = src[e];
+  } else {
+    const double *src = P.amp + at.amp_off;
+    for (int e = threadIdx.x; e < lsize; e += blockDim.x)
+      cf[e] = src[2 * e + (region == 1 ? 0 : 1)];
+  }
+  __syncthreads();
+  if ((int)threadIdx.x >= it.count) return;
+  const int p = P.pairs[at.pair_off + it.start + threadIdx.x];
+  const double dx = gx[p] - at.cx, dy = gy[p] - at.cy, dz = gz[p] - at.cz;
+  const double d = sqrt(dx * dx + dy * dy + dz * dz);
+  const double inv = 1.0 / d;
+  const double x = dx * inv, y = dy * inv, z = dz * inv;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  double gl = 1.0, gstep = 1.0;  // tail factor of the current l
+  if (region == 1) gstep = d;
+  if (region == 2) {
+    gl = inv;
+    gstep = inv;
+  }
+  // accumulate one (lm, S) term
+  auto term = [&](int lm, double S) {
+    if (region == 0) {
+      const double2 c01 = *reinterpret_cast<const double2 *>(cf + 4 * lm);
+      const double2 c23 = *reinterpret_cast<const double2 *>(cf + 4 * lm + 2);
+      a0 = fma(c01.x, S, a0);
+      a1 = fma(c01.y, S, a1);
+      a2 = fma(c23.x, S, a2);
+      a3 = fma(c23.y, S, a3);
+    } else {
+      a0 = fma(cf[lm] * gl, S, a0);
+    }
+  };
+  term(0, 1.0);
+  if (LMAX >= 1 && lmaxA >= 1) {
+    gl *= gstep;
+    term(1, z);
+    term(2, x);
+    term(3, y);
+    if (LMAX >= 2 && lmaxA >= 2) {
+      const double r2 = x * x + y * y + z * z;
+      double pold[LMAX + 1], pnew[LMAX + 1], cs[LMAX + 1], sn[LMAX + 1];
+      pold[0] = 1.0;
+      pnew[0] = z;
+      pnew[1] = 1.0;
+      cs[1] = x;
+      sn[1] = y;
+      int lm = 4;
+#pragma unroll
+      for (int l = 2; l <= LMAX; ++l) {
+        if (l > lmaxA) break;
+        gl *= gstep;
+        const double fac = 2 * l - 1;
+#pragma unroll
+        for (int m = 0; m <= l - 2; ++m) {
+          const double keep = pold[m];
+          pold[m] = pnew[m];
+          pnew[m] = (z * fac * pold[m] - r2 * (l + m - 1) * keep) * (1.0 / (l - m));
+        }
+        pold[l - 1] = pnew[l - 1];
+        pnew[l] = fac * pold[l - 1];
+        pnew[l - 1] = z * pnew[l];
+        cs[l] = x * cs[l - 1] - y * sn[l - 1];
+        sn[l] = x * sn[l - 1] + y * cs[l - 1];
+        term(lm, pnew[0]);
+        ++lm;
+#pragma unroll
+        for (int m = 1; m <= l; ++m) {
+          const double nrm = c_shnorm[l * (kMaxLmax + 1) + m];
+          term(lm, nrm * cs[m] * pnew[m]);
+          term(lm + 1, nrm * sn[m] * pnew[m]);
+          lm += 2;
+        }
+      }
+    }
+  }
+  double v;
+  if (region == 0) {
+    const double t = rt_inv(at.rt, d);
+    const double u = t - (it.bucket - 1);
+    v = a0 + u * (a1 + u * (a2 + u * a3));
+  } else {
+    v = a0;
+  }
+  P.pair_v[at.pair_off + (p - at.mol_point_start)] = v;
+}
+
+// v[p] (+)= sum over the atoms of p's molecule of pair_v, in atom order.
+__global__ void pairs_reduce_kernel(PoissonDev P, int npoint, double *__restrict__ out,
+                                    int accumulate) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npoint) return;
+  int mol = 0;
+  if (P.nmol > 1) {
+    int lo = 0, hi = P.nmol - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (P.mol_point_off[mid] <= p) lo = mid; else hi = mid - 1;
+    }
+    mol = lo;
+  }
+  double v = accumulate ? out[p] : 0.0;
+  const int a1 = P.mol_atom_off[mol + 1];
+  for (int A = P.mol_atom_off[mol]; A < a1; ++A) {
+    const PoissonAtom &at = P.atoms[A];
+    v += P.pair_v[at.pair_off + (p - at.mol_point_start)];
+  }
+  out[p] = v;
+}
+
 template <int L>
 cudaError_t launch_eval_l(const PoissonDev &P, int npoint, const double *x,
                           const double *y, const double *z, double *out, int acc,
                           cudaStream_t s) {
+  if (P.items && P.nitems > 0) {
+    const size_t smem = (size_t)(L + 1) * (L + 1) * 4 * sizeof(double);
+    eval_pairs_kernel<L><<<P.nitems, kEvalChunk, smem, s>>>(P, x, y, z);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    pairs_reduce_kernel<<<(npoint + 255) / 256, 256, 0, s>>>(P, npoint, out, acc);
+    return cudaGetLastError();
+  }
   evaluate_kernel<L><<<(npoint + 127) / 128, 128, 0, s>>>(P, npoint, x, y, z, out, acc);
   return cudaGetLastError();
 }
@@ -492,6 +670,21 @@ cudaError_t launch_poisson_radial(const PoissonDev &P, cudaStream_t s) {
                                        (int)smem);
   if (e != cudaSuccess) return e;
   radial_kernel<<<P.nsys, ncol, smem, s>>>(P, ncol);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pair_buckets(const PoissonDev &P, int max_mol_npoint, const double *x,
+                                const double *y, const double *z, int *bucket_of, int *count,
+                                cudaStream_t s) {
+  dim3 grid((max_mol_npoint + 255) / 256, P.natom);
+  pair_bucket_kernel<<<grid, 256, 0, s>>>(P, x, y, z, bucket_of, count);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pair_scatter(const PoissonDev &P, int max_mol_npoint, const int *bucket_of,
+                                int *cursor, cudaStream_t s) {
+  dim3 grid((max_mol_npoint + 255) / 256, P.natom);
+  pair_scatter_kernel<<<grid, 256, 0, s>>>(P, bucket_of, cursor);
   return cudaGetLastError();
 }
 

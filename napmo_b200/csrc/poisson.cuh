@@ -23,7 +23,17 @@ struct PoissonAtom {
   int spl_off;    // [nrad-1][lsize][4] cubic coefficients (scaled)
   int amp_off;    // [lsize][2] left / right extrapolation amplitudes (scaled)
   int raw_off;    // [lsize][nrad] solution values y and t-derivatives dt
+  int mol_point_start, mol_npoint;  // points of this atom's molecule
+  int bucket_off;  // [nrad + 1] buckets: 0 left tail, 1 + j interval j, nrad right tail
+  long pair_off;   // this atom's slice of the (atom, point) pair arrays
 };
+
+// One CTA of the bucketed evaluation: `count` (<= kEvalChunk) pairs of one
+// atom that share one spline interval (or tail) of that atom.
+struct EvalItem {
+  int atom, bucket, start, count;
+};
+constexpr int kEvalChunk = 128;
 
 // Radial table slots (each nrad long, at rad_off + slot * nrad).
 enum : int {
@@ -53,6 +63,13 @@ struct PoissonDev {
   double *amp = nullptr;
   double *raw_y = nullptr;
   double *raw_dt = nullptr;
+  // bucketed evaluation (built once per grid): for every atom the points of
+  // its molecule sorted by spline interval, and a partial potential per pair
+  long npair = 0;
+  int nitems = 0;
+  int *pairs = nullptr;        // point index, bucket-sorted per atom
+  EvalItem *items = nullptr;
+  double *pair_v = nullptr;    // [atom][molecule point] contribution
 };
 
 // Uploads the Hermite FEM integral tables and solid-harmonic norms to
@@ -65,7 +82,17 @@ cudaError_t launch_poisson_project(const PoissonDev &P, const double *rho,
                                    cudaStream_t s);
 // projected density -> spline tables of the potential (one CTA per (atom, l)).
 cudaError_t launch_poisson_radial(const PoissonDev &P, cudaStream_t s);
-// spline tables -> potential at every grid point (out = or += ).
+// Pair-list construction: bucket of every (atom, point) pair and the bucket
+// populations (count[atom.bucket_off + b], atomics on integers), then the
+// bucket-sorted point lists (order inside a bucket is irrelevant: each pair
+// writes its own slot of pair_v).
+cudaError_t launch_pair_buckets(const PoissonDev &P, int max_mol_npoint, const double *x,
+                                const double *y, const double *z, int *bucket_of, int *count,
+                                cudaStream_t s);
+cudaError_t launch_pair_scatter(const PoissonDev &P, int max_mol_npoint, const int *bucket_of,
+                                int *cursor, cudaStream_t s);
+// spline tables -> potential at every grid point (out = or += ).  Uses the
+// bucketed pair lists when P.items is set, the point-parallel kernel otherwise.
 cudaError_t launch_poisson_evaluate(const PoissonDev &P, int npoint,
                                     const double *x, const double *y,
                                     const double *z, double *out, bool accumulate,

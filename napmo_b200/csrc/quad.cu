@@ -269,7 +269,10 @@ __global__ void combine_weights_kernel(int npoint, const double *__restrict__ wb
 inline int quad_chunks(int n, int npoint_pad, int *chunk_out) {
   const int nblk = (n + BM - 1) / BM;
   const int ntile = nblk * (nblk + 1) / 2;
-  int nchunk = (2 * 148 + ntile - 1) / ntile;
+  // one CTA per SM at these register counts: aim for ~4 full waves over the
+  // 148 SMs so the last wave is (nearly) full
+  int nchunk = (4 * 148) / ntile;
+  if (nchunk < 1) nchunk = 1;
   int chunk = (npoint_pad + nchunk - 1) / nchunk;
   chunk = ((chunk + BK - 1) / BK) * BK;
   if (chunk < BK) chunk = BK;

@@ -267,6 +267,17 @@ long napmo_poisson_raw_size(void *grid, int lmax);
 int napmo_gpu_nuclear_potential(int npoint, const double *x, const double *y, const double *z,
                                 int nq, const double *charges, double *v, void *stream);
 
+/* Allocation-free twin of napmo_gpu_quadrature for callers that cannot
+ * allocate device memory while calling the library (hosts that budget all GPU
+ * memory themselves; callers that must not let an allocation stall the
+ * device).  No counterpart in nAPMO.  Split-K scratch is a fixed 16 MiB device
+ * array inside the library (held by every GPU that loads it until exit), so
+ * n <= 1920; larger n is refused with an error.  The first call on a device
+ * resolves the array's address (make it before any stream capture).  Calls
+ * share the array: overlapping calls on the GPU race. */
+int napmo_gpu_quadrature_noalloc(int n, int npoint, const double *phi, const double *psi,
+                                 long ld, const double *wv, double *F, void *stream);
+
 /* Fock-build plan: phi of `basis` on `grid` evaluated once and kept in HBM
  * with the Poisson tables of `lmax`; per build rho -> V_H -> F (the chain of
  * psi_hybrid.py:81-110 / psi_numeric.py:152-241). */

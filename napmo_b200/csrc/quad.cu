@@ -21,6 +21,9 @@
 //
 // Tiles: 128x128 per CTA, 256 threads, 8x8 doubles per thread (two 4x4
 // quadrants 64 apart), K step 8, register-staged double buffering.
+#include <mutex>
+#include <string>
+
 #include "common.h"
 #include "kernels.cuh"
 
@@ -332,3 +335,110 @@ cudaError_t launch_combine_weights(int npoint, const double *wb, const double *w
 }
 
 }  // namespace napmo
+
+// ===========================================================================
+// Allocation-free quadrature: napmo_gpu_quadrature_noalloc.
+//
+// Some callers of this library cannot allocate device memory while they call
+// it: host applications that reserve and budget the whole memory of a GPU at
+// start-up and hand plugins no allocator (a cudaMalloc from the plugin would
+// take memory the host has already promised elsewhere, or fail), and callers
+// that must not let an allocation stall or synchronise the device in the
+// middle of their own work.  For them this entry point runs the same split-K
+// quadrature kernels as napmo_gpu_quadrature, with the per-chunk partial tiles
+// kept in `g_quad_scratch`, a fixed 16 MiB array compiled into the library:
+// every GPU that loads libnapmo holds it until the process exits.
+//
+// Limit: the partial tiles of one chunk must fit, so n <= 1920 basis
+// functions; larger n is rejected with an error before anything is launched.
+// The chunk count is lowered to fit the array (fewer, longer chunks), so the
+// result can differ from napmo_gpu_quadrature in the last bits (different
+// summation grouping); it is deterministic from call to call.
+//
+// Set-up: the first call on a device looks up the device address of the
+// array with cudaGetSymbolAddress (with that device current) and caches it;
+// make that first call before any stream capture.  The array is shared by
+// all calls and keeps the previous call's contents; nothing in it needs to
+// start at zero (each chunk overwrites its own tiles before they are added).
+// Calls that overlap on the GPU (different streams, or different host
+// threads without ordering) race on the array and must be serialised by the
+// caller.
+// ===========================================================================
+namespace napmo {
+namespace {
+
+constexpr size_t kNoAllocScratchDoubles = size_t(2) << 20;  // 16 MiB
+__device__ __align__(256) double g_quad_scratch[kNoAllocScratchDoubles];
+
+std::mutex g_scratch_mutex;
+double *g_scratch_ptr[64] = {nullptr};
+
+int scratch_address(double **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return set_error(kCudaError, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= 64) return set_error(kNotSupported, "device index above 63");
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (!g_scratch_ptr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_quad_scratch);
+    if (e != cudaSuccess)
+      return set_error(kCudaError, std::string("cudaGetSymbolAddress(quadrature scratch): ") +
+                                       cudaGetErrorString(e));
+    g_scratch_ptr[dev] = static_cast<double *>(p);
+  }
+  *out = g_scratch_ptr[dev];
+  return kOk;
+}
+
+}  // namespace
+}  // namespace napmo
+
+extern "C" {
+
+// F[mu][nu] = sum_p phi[mu][p] wv[p] psi[nu][p] (psi = phi when null), upper
+// triangle mirrored, like napmo_gpu_quadrature, without allocating: the
+// split-K scratch lives in a fixed 16 MiB device array (n <= 1920).  See the
+// block comment above for the set-up call and the sharing rules.
+int napmo_gpu_quadrature_noalloc(int n, int npoint, const double *phi, const double *psi,
+                                 long ld, const double *wv, double *F, void *stream) {
+  using namespace napmo;
+  clear_error();
+  if (n <= 0 || npoint < 0) return set_error(kInvalidArgument, "n must be positive, npoint >= 0");
+  const int npad = pad_points(npoint);
+  if (ld < npad || ld % 2 != 0)
+    return set_error(kInvalidArgument, "ld must be even and >= npoint rounded up to 128");
+  const int nblk = (n + BM - 1) / BM;
+  const int ntile = nblk * (nblk + 1) / 2;
+  const size_t per_chunk = (size_t)ntile * BM * BN;
+  if (per_chunk > kNoAllocScratchDoubles)
+    return set_error(kInvalidArgument,
+                     "napmo_gpu_quadrature_noalloc: n = " + std::to_string(n) +
+                         " exceeds the 16 MiB fixed scratch (at most 1920 basis functions)");
+  double *scratch = nullptr;
+  int st = scratch_address(&scratch);
+  if (st != kOk) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  // as many chunks as the launch policy wants, capped by the fixed array
+  int chunk;
+  int nchunk = quad_chunks(n, npad, &chunk);
+  const int cap = (int)(kNoAllocScratchDoubles / per_chunk);
+  if (nchunk > cap) {
+    chunk = (npad + cap - 1) / cap;
+    chunk = ((chunk + BK - 1) / BK) * BK;
+    nchunk = (npad + chunk - 1) / chunk;
+  }
+  dim3 grid(ntile, nchunk);
+  quadrature_kernel<<<grid, NT, 0, s>>>(n, npad, phi, psi ? psi : phi, ld, wv, nblk, chunk,
+                                        scratch);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(kCudaError, std::string("quadrature: ") + cudaGetErrorString(e));
+  const long total = (long)ntile * BM * BN;
+  const int rblocks = (int)std::min<long>((total + 255) / 256, 148 * 16);
+  quadrature_reduce_kernel<<<rblocks, 256, 0, s>>>(n, nblk, nchunk, scratch, F);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(kCudaError, std::string("quadrature reduce: ") + cudaGetErrorString(e));
+  return kOk;
+}
+
+}  // extern "C"

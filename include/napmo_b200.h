@@ -292,6 +292,16 @@ int napmo_fock_plan_build(void *plan, const double *D, double q, const double *v
 /* Host-buffer twin of napmo_fock_plan_build (copies inside the call). */
 int napmo_fock_plan_build_host(void *plan, const double *D, double q, const double *vext,
                                double *F, void *stream);
+/* Precision of a plan's contractions: 0 FP64 (default), 1 int8 slices on the
+ * tensor cores (tcgen05 kind::i8: four balanced base-256 digits per value
+ * against a group exponent, exact int32 accumulation).  No counterpart in
+ * nAPMO (its quadratures are FP64 only, src/wavefunction/nwavefunction.cpp). */
+int napmo_fock_plan_set_precision(void *plan, int mode);
+/* Device bytes of the plan's int8 operand images and scratch. */
+long napmo_fock_plan_int8_bytes(void *plan);
+/* Error word of the tensor-core kernels (0 none, 5 an mbarrier wait ran out);
+ * synchronises the stream, `reset` nonzero clears it. */
+int napmo_tc_status(void *stream, int reset);
 
 #ifdef __cplusplus
 }

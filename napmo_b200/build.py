@@ -4,7 +4,7 @@ Host translation units are compiled with g++ without -march and with
 -ffp-contract=off, like nAPMO's own build (config.make: -O2 -fPIC), so grid
 construction rounds exactly as the reference does.  CUDA units target
 sm_100a only; becke.cu is compiled with --fmad=false (bit-exact Becke
-weights).  Usage: python -m napmo_b200.build [--force]
+weights).  Usage: python napmo_b200/build.py [--force]
 """
 import os
 import subprocess
@@ -22,7 +22,7 @@ HOST_FLAGS = ['-O2', '-fPIC', '-std=c++17', '-ffp-contract=off', '-fno-fast-math
 CUDA_FLAGS = ARCH + ['-O3', '-lineinfo', '-std=c++17', '--expt-relaxed-constexpr',
                      '-Xcompiler', '-fPIC,-ffp-contract=off', '-Xptxas', '-warn-spills']
 HOST_SOURCES = ['host.cpp']
-CUDA_SOURCES = ['becke.cu', 'gto.cu', 'quad.cu', 'poisson.cu', 'capi_grid.cu',
+CUDA_SOURCES = ['becke.cu', 'gto.cu', 'quad.cu', 'tc.cu', 'poisson.cu', 'capi_grid.cu',
                 'capi_basis.cu', 'capi_quad.cu', 'capi_scf.cu']
 EXTRA_CUDA = {'becke.cu': ['--fmad=false']}
 LIBS = ['-lcusolver', '-lcublas']

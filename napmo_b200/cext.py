@@ -22,7 +22,7 @@ class NapmoError(RuntimeError):
 
 def _load():
     if not os.path.exists(LIBPATH):
-        raise ImportError('libnapmo.so is not built (%s); run `python -m napmo_b200.build`'
+        raise ImportError('libnapmo.so is not built (%s); run `python napmo_b200/build.py`'
                           % LIBPATH)
     return ctypes.CDLL(LIBPATH)
 
@@ -209,6 +209,11 @@ _SIGS = [
      [c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ('napmo_fock_plan_build_host', c_int,
      [c_void_p, a2df, c_double, c_void_p, a2df, c_void_p]),
+    ('napmo_fock_plan_set_precision', c_int, [c_void_p, c_int]),
+    ('napmo_fock_plan_int8_bytes', c_long, [c_void_p]),
+    ('napmo_tc_status', c_int, [c_void_p, c_int]),
+    ('napmo_gpu_quadrature_noalloc', c_int,
+     [c_int, c_int, c_void_p, c_void_p, c_long, c_void_p, c_void_p, c_void_p]),
 ]
 
 for _name, _res, _args in _SIGS:

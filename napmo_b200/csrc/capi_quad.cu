@@ -65,9 +65,30 @@ struct FockPlan {
   BeckeGrid *grid = nullptr;
   BasisSet *basis = nullptr;
   int n = 0, lmax = 0;
+  int mode = 0;  // 0 FP64, 1 int8 slices on the tensor cores
   long ld = 0;
   DevBuf<double> phi, rho, v, wv, work, D, F, vext;
+  Int8Plan *i8 = nullptr;
+  ~FockPlan() {
+    if (i8) int8_plan_destroy(i8);
+  }
 };
+
+// rho = density of D, in the plan's precision.
+int plan_density(FockPlan *p, const double *D, double *rho, cudaStream_t s) {
+  if (p->mode == 1) return int8_density(p->i8, D, rho, s);
+  NAPMO_TRY_CUDA(launch_density_f64(p->n, p->grid->size, p->phi.p, p->ld, D, rho, s), "density");
+  return kOk;
+}
+
+// F = phi diag(p->wv) phi^T, in the plan's precision.
+int plan_quadrature(FockPlan *p, double *F, cudaStream_t s) {
+  if (p->mode == 1) return int8_quadrature(p->i8, p->phi.p, p->wv.p, F, s);
+  NAPMO_TRY_CUDA(launch_quadrature_f64(p->n, p->grid->size, p->phi.p, p->ld, p->wv.p, F,
+                                       p->work.p, s),
+                 "quadrature");
+  return kOk;
+}
 
 }  // namespace napmo
 
@@ -238,10 +259,7 @@ int napmo_fock_plan_info(FockPlan *p, int *n, int *npoint, long *ld, double **ph
 // rho_dev[p] = density of D_dev on the plan's grid.
 int napmo_fock_plan_density(FockPlan *p, const double *D_dev, double *rho_dev, void *stream) {
   return guarded([&] {
-    NAPMO_TRY_CUDA(launch_density_f64(p->n, p->grid->size, p->phi.p, p->ld, D_dev, rho_dev,
-                                      (cudaStream_t)stream),
-                   "density");
-    return kOk;
+    return plan_density(p, D_dev, rho_dev, (cudaStream_t)stream);
   });
 }
 
@@ -254,10 +272,7 @@ int napmo_fock_plan_quadrature(FockPlan *p, double q, const double *v_dev,
     NAPMO_TRY_CUDA(launch_combine_weights(g->size, g->dev.wb, g->dev.w, q, v_dev, vext_dev,
                                           p->wv.p, s),
                    "weights");
-    NAPMO_TRY_CUDA(launch_quadrature_f64(p->n, g->size, p->phi.p, p->ld, p->wv.p, F_dev,
-                                         p->work.p, s),
-                   "quadrature");
-    return kOk;
+    return plan_quadrature(p, F_dev, s);
   });
 }
 
@@ -272,19 +287,17 @@ int napmo_fock_plan_build(FockPlan *p, const double *D_dev, double q, const doub
     BeckeGrid *g = p->grid;
     double *rho = rho_out ? rho_out : p->rho.p;
     double *v = v_out ? v_out : p->v.p;
-    NAPMO_TRY_CUDA(launch_density_f64(p->n, g->size, p->phi.p, p->ld, D_dev, rho, s), "density");
+    int e = plan_density(p, D_dev, rho, s);
+    if (e) return e;
     PoissonPlan *pp = nullptr;
-    int e = grid_poisson_plan(g, p->lmax, s, &pp);
+    e = grid_poisson_plan(g, p->lmax, s, &pp);
     if (e) return e;
     e = run_poisson(g, pp, rho, v, false, s);
     if (e) return e;
     NAPMO_TRY_CUDA(launch_combine_weights(g->size, g->dev.wb, g->dev.w, q, v, vext_dev,
                                           p->wv.p, s),
                    "weights");
-    NAPMO_TRY_CUDA(launch_quadrature_f64(p->n, g->size, p->phi.p, p->ld, p->wv.p, F_dev,
-                                         p->work.p, s),
-                   "quadrature");
-    return kOk;
+    return plan_quadrature(p, F_dev, s);
   });
 }
 
@@ -351,4 +364,43 @@ int napmo_gpu_nuclear_potential(int npoint, const double *x, const double *y, co
     return napmo::kOk;
   });
 }
+}  // extern "C"
+
+// ------------------------------------------------ int8-slice tensor cores
+extern "C" {
+
+// Precision of a plan's contractions: 0 = FP64 (CUDA cores, default),
+// 1 = int8 slices on the tensor cores (four balanced base-256 digits per
+// value against a group exponent, exact int32 accumulation in TMEM).  The
+// Poisson solve stays FP64 in both modes.  Switching to 1 builds phi's
+// operand images (device-synchronous, once per plan).
+int napmo_fock_plan_set_precision(FockPlan *p, int mode) {
+  return napmo::guarded([&] {
+    NAPMO_REQUIRE(mode == 0 || mode == 1, "precision mode must be 0 (fp64) or 1 (int8x4)");
+    if (mode == 1 && !p->i8) {
+      NAPMO_TRY_CUDA(cudaDeviceSynchronize(), "sync");
+      cudaStream_t s = napmo::host_api_stream();
+      BeckeGrid *g = p->grid;
+      int e = napmo::int8_plan_create(&p->i8, p->n, g->size, p->phi.p, p->ld, g->dev.wb,
+                                      g->dev.w, s);
+      if (e) return e;
+      NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "int8 operand images");
+    }
+    p->mode = mode;
+    return napmo::kOk;
+  });
+}
+
+// Device bytes held by the plan's int8 operand images and scratch (0 before
+// precision 1 was selected).
+long napmo_fock_plan_int8_bytes(FockPlan *p) {
+  return p->i8 ? (long)napmo::int8_plan_device_bytes(p->i8) : 0;
+}
+
+// Device error word of the tensor-core kernels (0 = none, 5 = an mbarrier
+// wait ran out); synchronises the stream.  `reset` nonzero clears it.
+int napmo_tc_status(void *stream, int reset) {
+  return napmo::tc_error_status((cudaStream_t)stream, reset != 0);
+}
+
 }  // extern "C"

@@ -40,4 +40,24 @@ cudaError_t launch_combine_weights(int npoint, const double *wb, const double *w
                                    double q, const double *v, const double *vext,
                                    double *wv, cudaStream_t s);
 
+// Adds nchunk partial 128x128 upper-triangle tiles [chunk][tile][128][128]
+// in fixed order and writes both triangles of F.
+cudaError_t launch_quadrature_reduce(int n, int nchunk, const double *work, double *F,
+                                     cudaStream_t s);
+
+// Int8-slice tensor-core quadratures (tc.cu).  A plan holds phi's operand
+// images (built once from phi, wb and w) and the per-call scratch; the calls
+// return library status codes and record g_tc_error on a device timeout.
+struct Int8Plan;
+int int8_plan_create(Int8Plan **out, int n, int npoint, const double *phi, long ld,
+                     const double *wb, const double *w, cudaStream_t s);
+void int8_plan_destroy(Int8Plan *p);
+size_t int8_plan_device_bytes(const Int8Plan *p);
+int int8_density(Int8Plan *p, const double *D, double *rho, cudaStream_t s);
+int int8_quadrature(Int8Plan *p, const double *phi, const double *wv, double *F,
+                    cudaStream_t s);
+// Returns the device error word of the tensor-core kernels (0 = none), after
+// synchronising `s`; `reset` clears it.
+int tc_error_status(cudaStream_t s, bool reset);
+
 }  // namespace napmo

@@ -325,6 +325,16 @@ cudaError_t launch_quadrature_f64(int n, int npoint, const double *phi, long ld,
   return cudaGetLastError();
 }
 
+cudaError_t launch_quadrature_reduce(int n, int nchunk, const double *work, double *F,
+                                     cudaStream_t s) {
+  const int nblk = (n + BM - 1) / BM;
+  const int ntile = nblk * (nblk + 1) / 2;
+  const long total = (long)ntile * BM * BN;
+  const int rblocks = (int)std::min<long>((total + 255) / 256, 148 * 16);
+  quadrature_reduce_kernel<<<rblocks, 256, 0, s>>>(n, nblk, nchunk, work, F);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_combine_weights(int npoint, const double *wb, const double *w,
                                    double q, const double *v, const double *vext,
                                    double *wv, cudaStream_t s) {

@@ -1,0 +1,1019 @@
+// Mixed-precision grid quadratures on the 5th-generation tensor cores
+// (tcgen05.mma kind::i8, int32 accumulators in TMEM), sm_100a.
+//
+//   quadrature  F[mu][nu] = sum_p phi[mu][p] wv[p] phi[nu][p]
+//   density     rho[p]    = sum_mu phi[mu][p] (D phi)[mu][p]
+//
+// Slices.  The FP64 values of a group (one basis function over a block of 1024
+// points; all basis functions at one point; one row of D) share the group
+// exponent e (max |x| < 2^e).  Each value is rounded once, to the integer
+// Y = rint(x 2^(30 - e)) (|Y| <= 2^30, error <= 2^-31 of the group maximum),
+// and Y is written in balanced base 256 as four int8 digits
+//   Y = d0 2^24 + d1 2^16 + d2 2^8 + d3,   |d0| <= 64, -128 <= dk <= 127.
+// A product of two sliced operands keeps the digit products d_i d'_j with
+// i + j <= 4 (13 MMAs; quadrature) or i + j <= 3 (10 MMAs; density).  The
+// products of one diagonal i + j share an int32 TMEM accumulator, so the
+// accumulation is exact: besides the slicing, the only error is the dropped
+// digit products (relative 2^-37 resp. 2^-29 of the group maxima).  The drain
+// combines the diagonals in int64, converts once to FP64 and applies the group
+// exponents; FP64 partials are summed in a fixed order (deterministic).
+//
+// Quadrature weights span many decades across a block of points, so the
+// weight is split between the operands by a power of two per point:
+// A = phi 2^c(p), B = wv phi 2^-c(p), c(p) = floor(log2(wb w) / 2) (exact).
+//
+// Operand images.  Each operand lives in HBM as tiles already in the
+// no-swizzle K-major shared-memory layout of the tensor core (core matrices
+// of 8 rows x 16 bytes; element (r, k) of a 64-wide K stage of one slice at
+// (r / 8) * 512 + (k / 16) * 128 + (r % 8) * 16 + k % 16), the four slices of
+// a stage contiguous, so one cp.async.bulk moves a stage of an operand.  phi's
+// images are built once per grid; wv phi (quadrature) and D (density) are
+// sliced on every call.
+//
+// Kernels: warp 8 (one thread) streams stages into a 3-slot ring
+// (cp.async.bulk + mbarrier transaction counts), warp 9 (one thread) issues
+// the MMAs and owns TMEM, warps 0-7 drain TMEM.  Every mbarrier wait is
+// bounded (2 s of globaltimer, or another role's abort): on timeout the kernel
+// records an error in g_tc_error, the roles stop, copies and MMAs in flight
+// are waited for (bounded) and TMEM is freed before the CTA exits.
+#include <cstdint>
+#include <memory>
+
+#include "capi_common.cuh"
+#include "common.h"
+#include "kernels.cuh"
+
+namespace napmo {
+
+__device__ int g_tc_error = 0;
+
+namespace {
+
+constexpr int KS = 64;            // K elements per stage = bytes per row of one slice
+constexpr int NSL = 4;            // int8 slices per value
+constexpr int TM = 128;           // M tile (TMEM lanes)
+constexpr int QN = 96;            // quadrature N tile: 5 diagonals x 96 columns
+constexpr int DN = 128;           // density N tile: 4 diagonals x 128 columns
+constexpr int QKB = 1024;         // quadrature exponent block (points)
+constexpr int QBLK_STAGES = QKB / KS;
+constexpr int NSTAGE = 3;
+constexpr int NEPI = 256;         // drain threads (warps 0-7)
+constexpr int NTHR = NEPI + 64;   // + producer warp 8 + MMA warp 9
+constexpr int kTmemCols = 512;
+constexpr int kEmin = -960;
+constexpr unsigned long long kTimeoutNs = 2000000000ull;
+
+__host__ __device__ constexpr int stage_bytes(int rows) { return NSL * rows * KS; }
+
+__host__ __device__ __forceinline__ int core_off(int r, int k) {
+  return (r >> 3) * 512 + (k >> 4) * 128 + (r & 7) * 16 + (k & 15);
+}
+
+// Digit products (i, j) in diagonal order: (0,0) | (0,1) (1,0) | (0,2) (1,1)
+// (2,0) | (0,3) (1,2) (2,1) (3,0) | (1,3) (2,2) (3,1).  The quadrature keeps
+// the first 13 (i + j <= 4), the density the first 10 (i + j <= 3).
+constexpr int kQuadProducts = 13, kDensProducts = 10;
+__host__ __device__ constexpr int prod_diag(int q) {
+  return q < 1 ? 0 : q < 3 ? 1 : q < 6 ? 2 : q < 10 ? 3 : 4;
+}
+__host__ __device__ constexpr int prod_i(int q) {
+  return q < 10 ? q - prod_diag(q) * (prod_diag(q) + 1) / 2 : q - 9;
+}
+__host__ __device__ constexpr int prod_j(int q) { return prod_diag(q) - prod_i(q); }
+
+// kind::i8 instruction descriptor: S32 accumulator, signed A and B, both
+// K-major, N columns, M = 128.
+constexpr uint32_t idesc_i8(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(TM >> 4) << 24);
+}
+
+// ------------------------------------------------------------ PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void fence_before_sync() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after_sync() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void named_sync(int id, int n) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// global -> shared bulk copy (16-byte aligned, size a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                         uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits for the phase of `bar` with parity `parity`.  Gives up when another
+// role has set *abort, or after kTimeoutNs; a timeout records kDeviceTimeout
+// and sets *abort.  abort == nullptr: only the time limit applies.
+__device__ bool wait_phase(uint64_t *bar, uint32_t parity, volatile int *abort) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (uint32_t i = 1;; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 63) == 0) {
+      if (abort && *abort) return false;
+      if (global_ns() - t0 > kTimeoutNs) {
+        if (abort) *abort = 1;
+        atomicExch(&g_tc_error, kDeviceTimeout);
+        return false;
+      }
+    }
+  }
+}
+
+// The drain warps' wait: thread 0 polls, the outcome is shared through smem so
+// that all 256 drain threads take the same branch.
+__device__ bool group_wait(uint64_t *bar, uint32_t parity, volatile int *abort,
+                           volatile int *flag) {
+  if (threadIdx.x == 0) *flag = wait_phase(bar, parity, abort) ? 1 : 0;
+  named_sync(1, NEPI);
+  const bool ok = *flag != 0;
+  named_sync(1, NEPI);
+  return ok;
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  // no swizzle, K-major: LBO = 128 B (next 16 bytes of K), SBO = 512 B (next
+  // 8 rows), descriptor version 1
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) |
+         ((uint64_t)(512 >> 4) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                        uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+// 8 consecutive 32-bit TMEM columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, int32_t *v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+// ties loaded registers to a point after the wait, so no use is scheduled
+// before it
+__device__ __forceinline__ void tie8(int32_t *v) {
+  asm volatile("" : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]),
+               "+r"(v[6]), "+r"(v[7]));
+}
+
+// ------------------------------------------------------------------ slices
+__device__ __forceinline__ int group_exponent(double m) {
+  if (!(m > 0.0)) return 0;
+  int e;
+  frexp(m, &e);
+  return e < kEmin ? kEmin : e;
+}
+
+// 2^e as a double; 0 below the normal range (such terms are < 2^-960 of the
+// results they enter).
+__device__ __forceinline__ double pow2(int e) {
+  return e < -1022 ? 0.0 : __longlong_as_double((long long)(e + 1023) << 52);
+}
+
+// Four balanced base-256 digit slices of rint(x[i] * scale), i < 16, packed
+// one byte per element (slice s in out[s]).
+__device__ __forceinline__ void slice16(const double *x, double scale, uint4 *out) {
+  uint32_t w[NSL][4];
+#pragma unroll
+  for (int s = 0; s < NSL; ++s)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) w[s][q] = 0u;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    int y = __double2int_rn(x[i] * scale);
+    const int d3 = ((y + 128) & 255) - 128;
+    y = (y - d3) >> 8;
+    const int d2 = ((y + 128) & 255) - 128;
+    y = (y - d2) >> 8;
+    const int d1 = ((y + 128) & 255) - 128;
+    const int d0 = (y - d1) >> 8;
+    const int q = i >> 2, sh = (i & 3) * 8;
+    w[0][q] |= (uint32_t)(d0 & 255) << sh;
+    w[1][q] |= (uint32_t)(d1 & 255) << sh;
+    w[2][q] |= (uint32_t)(d2 & 255) << sh;
+    w[3][q] |= (uint32_t)(d3 & 255) << sh;
+  }
+#pragma unroll
+  for (int s = 0; s < NSL; ++s) out[s] = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+}
+
+// signed byte b (0..3) of a word
+__device__ __forceinline__ int sbyte(uint32_t w, int b) { return ((int)(w << (24 - 8 * b))) >> 24; }
+
+// Row-grouped slices of X[row][k] = src[row * ld + k] * m1[k] * m2[k]
+// (m1, m2 optional; X = 0 for row >= nrows or k >= ncols): exponent per
+// (row, block of kb columns) in e[row * nblk + b]; image tiles of TR rows x KS
+// columns, img[((row / TR) * nks + k / KS) * NSL * TR * KS + s * TR * KS +
+// core_off(row % TR, k % KS)].  Grid (rows_pad / 8, nblk), one warp per row.
+__global__ void __launch_bounds__(256)
+slice_rows_kernel(const double *__restrict__ src, long ld, int nrows, int ncols,
+                  const double *__restrict__ m1, const double *__restrict__ m2, int kb, int nblk,
+                  int TR, int nks, int8_t *__restrict__ img, int *__restrict__ eout) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = blockIdx.x * 8 + warp;
+  const int b = blockIdx.y;
+  const long k0 = (long)b * kb;
+  const int nchunk = kb / 16;
+  const bool vec = ((ld & 1) == 0);
+  auto load = [&](int c, double *x) {
+    const long k = k0 + (long)c * 16;
+    if (row < nrows && k + 16 <= ncols) {
+      const double *p = src + (long)row * ld + k;
+      if (vec) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const double2 v = __ldg(reinterpret_cast<const double2 *>(p) + q);
+          x[2 * q] = v.x;
+          x[2 * q + 1] = v.y;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) x[i] = __ldg(p + i);
+      }
+      if (m1) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const double2 v = __ldg(reinterpret_cast<const double2 *>(m1 + k) + q);
+          x[2 * q] *= v.x;
+          x[2 * q + 1] *= v.y;
+        }
+      }
+      if (m2) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const double2 v = __ldg(reinterpret_cast<const double2 *>(m2 + k) + q);
+          x[2 * q] *= v.x;
+          x[2 * q + 1] *= v.y;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        double v = 0.0;
+        if (row < nrows && k + i < ncols) {
+          v = __ldg(src + (long)row * ld + k + i);
+          if (m1) v *= __ldg(m1 + k + i);
+          if (m2) v *= __ldg(m2 + k + i);
+        }
+        x[i] = v;
+      }
+    }
+  };
+  double mx = 0.0;
+  for (int c = lane; c < nchunk; c += 32) {
+    double x[16];
+    load(c, x);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) mx = fmax(mx, fabs(x[i]));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  const int e = group_exponent(mx);
+  if (lane == 0) eout[(long)row * nblk + b] = e;
+  const double scale = ldexp(1.0, 30 - e);
+  const int rt = row / TR, r = row % TR;
+  const long tile = (long)NSL * TR * KS;
+  for (int c = lane; c < nchunk; c += 32) {
+    double x[16];
+    load(c, x);
+    uint4 d[NSL];
+    slice16(x, scale, d);
+    const long k = k0 + (long)c * 16;
+    int8_t *base = img + ((long)rt * nks + k / KS) * tile + core_off(r, (int)(k % KS));
+#pragma unroll
+    for (int s = 0; s < NSL; ++s)
+      *reinterpret_cast<uint4 *>(base + (long)s * TR * KS) = d[s];
+  }
+}
+
+// Point-grouped slices of phi^T: rows = points (tiles of 128), K = basis
+// function (stages of 64); exponent per point over all n functions.  One
+// thread per point, grid = padded points / 128.
+__global__ void __launch_bounds__(TM)
+slice_points_kernel(const double *__restrict__ phi, long ld, int n, int npoint, int nks,
+                    int8_t *__restrict__ img, int *__restrict__ eout) {
+  const int r = threadIdx.x;
+  const long p = (long)blockIdx.x * TM + r;
+  const bool valid = p < npoint;
+  double mx = 0.0;
+  if (valid)
+    for (int nu = 0; nu < n; ++nu) mx = fmax(mx, fabs(__ldg(phi + (long)nu * ld + p)));
+  const int e = group_exponent(mx);
+  eout[p] = e;
+  const double scale = ldexp(1.0, 30 - e);
+  const long tile = (long)NSL * TM * KS;
+  for (int ks = 0; ks < nks; ++ks) {
+#pragma unroll 1
+    for (int kc = 0; kc < KS / 16; ++kc) {
+      const int nu0 = ks * KS + kc * 16;
+      double x[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i)
+        x[i] = (valid && nu0 + i < n) ? __ldg(phi + (long)(nu0 + i) * ld + p) : 0.0;
+      uint4 d[NSL];
+      slice16(x, scale, d);
+      int8_t *base = img + ((long)blockIdx.x * nks + ks) * tile + core_off(r, kc * 16);
+#pragma unroll
+      for (int s = 0; s < NSL; ++s) *reinterpret_cast<uint4 *>(base + (long)s * TM * KS) = d[s];
+    }
+  }
+}
+
+// sc[p] = 2^c(p), isc[p] = 2^-c(p), c(p) = floor(log2(wb w) / 2) (0 where the
+// weight is not positive).
+__global__ void balance_kernel(int npoint, const double *__restrict__ wb,
+                               const double *__restrict__ w, double *__restrict__ sc,
+                               double *__restrict__ isc) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npoint) return;
+  const double t = wb[p] * w[p];
+  int c = 0;
+  if (t > 0.0 && t < 1e300) {
+    int ex;
+    frexp(t, &ex);
+    c = (ex - 1) >> 1;
+    c = c < -400 ? -400 : (c > 400 ? 400 : c);
+  }
+  sc[p] = ldexp(1.0, c);
+  isc[p] = ldexp(1.0, -c);
+}
+
+// Per call, block b of QKB points: g(p) = wv(p) isc(p)^2 (so that
+// B = A g = phi wv 2^-c), eg[b] = group exponent of max |g| over the block,
+// gs(p) = g(p) 2^-eg[b] (|gs| < 1; exact scaling).
+__global__ void __launch_bounds__(256)
+gscale_kernel(int npoint, const double *__restrict__ wv, const double *__restrict__ isc,
+              double *__restrict__ gs, int *__restrict__ eg) {
+  constexpr int PER = QKB / 256;
+  __shared__ double red[8];
+  const int t = threadIdx.x;
+  const long p0 = (long)blockIdx.x * QKB + t * PER;
+  double g[PER], mx = 0.0;
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    const long p = p0 + i;
+    g[i] = p < npoint ? wv[p] * isc[p] * isc[p] : 0.0;
+    mx = fmax(mx, fabs(g[i]));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((t & 31) == 0) red[t >> 5] = mx;
+  __syncthreads();
+  mx = red[0];
+#pragma unroll
+  for (int i = 1; i < 8; ++i) mx = fmax(mx, red[i]);
+  const int e = group_exponent(mx);
+  if (t == 0) eg[blockIdx.x] = e;
+  const double s = ldexp(1.0, -e);
+#pragma unroll
+  for (int i = 0; i < PER; ++i) gs[p0 + i] = g[i] * s;
+}
+
+// Per call: the B image from the A image.  For each row and block,
+// x(p) = Y_A(p) gs(p) (|x| < 2^30); Y_B = rint(x 2^s) with s = 30 - e,
+// e = group exponent of max |x| over the block, so B keeps 31 bits of its own
+// block maximum; eb[row][b] = ea[row][b] + eg[b] - s.  CTA = (128-row tile,
+// block); thread = one 16-byte chunk position of a slice (row group, 16-point
+// column, row % 8) over the block's stages: pass 1 the row maxima (the four
+// chunks of a row are lanes c, c ^ 8, c ^ 16, c ^ 24), pass 2 the digits (the
+// block's 512 KB of A digits are re-read from L2).
+__global__ void __launch_bounds__(512, 1)
+scale_image_kernel(const int8_t *__restrict__ qa, int8_t *__restrict__ qb,
+                   const double *__restrict__ gs, const int *__restrict__ ea,
+                   const int *__restrict__ eg, int *__restrict__ eb, int nks, int nblk) {
+  const int c = threadIdx.x;                     // (c >> 5) row group, (c >> 3) & 3 column, c & 7 row
+  const int t = blockIdx.x, b = blockIdx.y;
+  const int kc = (c >> 3) & 3;
+  const int row = t * TM + (c >> 5) * 8 + (c & 7);
+  auto load = [&](int st, double *x) {
+    const int ks = b * QBLK_STAGES + st;
+    const long base = ((long)t * nks + ks) * stage_bytes(TM) + (long)c * 16;
+    uint4 q[NSL];
+#pragma unroll
+    for (int s = 0; s < NSL; ++s)
+      q[s] = __ldg(reinterpret_cast<const uint4 *>(qa + base + (long)s * TM * KS));
+    const double *g = gs + (long)ks * KS + kc * 16;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const int wq = i >> 2, bb = i & 3;
+      const int y = ((sbyte((&q[0].x)[wq], bb) * 256 + sbyte((&q[1].x)[wq], bb)) * 256 +
+                     sbyte((&q[2].x)[wq], bb)) * 256 + sbyte((&q[3].x)[wq], bb);
+      x[i] = (double)y * __ldg(g + i);
+    }
+  };
+  double mx = 0.0;
+  for (int st = 0; st < QBLK_STAGES; ++st) {
+    double x[16];
+    load(st, x);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) mx = fmax(mx, fabs(x[i]));
+  }
+  mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 8));
+  mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 16));
+  const int sh = 30 - group_exponent(mx);
+  if (kc == 0) eb[(long)row * nblk + b] = ea[(long)row * nblk + b] + eg[b] - sh;
+  const double scale = ldexp(1.0, sh);
+  for (int st = 0; st < QBLK_STAGES; ++st) {
+    double x[16];
+    load(st, x);
+    uint4 d[NSL];
+    slice16(x, scale, d);
+    const long base =
+        ((long)t * nks + b * QBLK_STAGES + st) * stage_bytes(TM) + (long)c * 16;
+#pragma unroll
+    for (int s = 0; s < NSL; ++s)
+      *reinterpret_cast<uint4 *>(qb + base + (long)s * TM * KS) = d[s];
+  }
+}
+
+// 2 K32 steps of one 64-wide stage: the kept digit products into their
+// diagonal accumulators (column offset diagonal * N).  `fresh`: first stage
+// of an accumulation, the first product of each diagonal overwrites.
+template <int N, int NP>
+__device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t sa, uint32_t sb, bool fresh) {
+  constexpr uint32_t idesc = idesc_i8(N);
+#pragma unroll
+  for (int kk = 0; kk < KS / 32; ++kk) {
+#pragma unroll
+    for (int q = 0; q < NP; ++q) {
+      const uint64_t ad = smem_desc(sa + prod_i(q) * (TM * KS) + kk * 32 * 8);
+      const uint64_t bd = smem_desc(sb + prod_j(q) * (N * KS) + kk * 32 * 8);
+      const bool first = fresh && kk == 0 && (q == 0 || prod_diag(q) != prod_diag(q - 1));
+      umma_i8(tmem + (uint32_t)(prod_diag(q) * N), ad, bd, idesc, first ? 0u : 1u);
+    }
+  }
+}
+
+// ------------------------------------------------------------- quadrature
+struct QuadArgs {
+  const int8_t *a, *b;    // images of A and B, both in 128-row tiles
+  const int *ea, *eb;     // exponents of A and B [row][nblk]
+  int nblk, nks;          // exponent blocks; stages per row tile (nblk * 64)
+  int ntj;                // 96-column tiles
+  int bpc;                // blocks per chunk
+  int npair;
+  double *work;           // [chunk][pair][128][96]
+};
+
+// Copies the 96 rows 96 J .. 96 J + 95 of stage ks of the B image (128-row
+// tiles) into smem as a 96-row operand: per slice, the 12 row groups of 8
+// rows lie in one or two tiles, each run contiguous.
+__device__ __forceinline__ void copy_b96(uint8_t *dst, const int8_t *img, int J, long ks, int nks,
+                                         uint64_t *bar) {
+  const int g0 = 12 * J;                 // first row group
+  const int t0 = g0 >> 4, r0 = g0 & 15;  // tile, group within the tile
+  const int n0 = min(12, 16 - r0);       // groups in the first tile
+#pragma unroll
+  for (int s = 0; s < NSL; ++s) {
+    uint8_t *d = dst + s * (QN * KS);
+    const int8_t *src0 = img + ((long)t0 * nks + ks) * stage_bytes(TM) + s * (TM * KS) + r0 * 512;
+    bulk_g2s(d, src0, n0 * 512, bar);
+    if (n0 < 12) {
+      const int8_t *src1 = img + ((long)(t0 + 1) * nks + ks) * stage_bytes(TM) + s * (TM * KS);
+      bulk_g2s(d + n0 * 512, src1, (12 - n0) * 512, bar);
+    }
+  }
+}
+
+// CTA = (tile pair (I, J) with some nu >= mu, chunk of point blocks).
+__global__ void __launch_bounds__(NTHR, 1) quad_i8_kernel(QuadArgs g) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ __align__(8) uint64_t full[NSTAGE], empty[NSTAGE], accfull, accempty, done;
+  __shared__ uint32_t tmem_sh;
+  __shared__ int abort_sh, flag_sh;
+  constexpr uint32_t A_BYTES = stage_bytes(TM), B_BYTES = stage_bytes(QN);
+  constexpr uint32_t STAGE = A_BYTES + B_BYTES;
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  volatile int *abort = &abort_sh;
+
+  int I = 0, rem = blockIdx.x;
+  for (;;) {
+    const int cnt = g.ntj - (4 * I) / 3;
+    if (rem < cnt) break;
+    rem -= cnt;
+    ++I;
+  }
+  const int J = (4 * I) / 3 + rem;
+  const int b0 = blockIdx.y * g.bpc;
+  const int nb = max(0, min(b0 + g.bpc, g.nblk) - b0);
+
+  if (t == 0) {
+    for (int s = 0; s < NSTAGE; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(&accfull, 1);
+    mbar_init(&accempty, NEPI);
+    mbar_init(&done, 1);
+    abort_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 9) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_sh)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = tmem_sh;
+
+  if (warp == 8) {
+    if (lane == 0) {
+      int it = 0;
+      for (int bi = 0; bi < nb; ++bi) {
+        bool ok = true;
+        for (int st = 0; st < QBLK_STAGES; ++st) {
+          const int slot = it % NSTAGE;
+          if (!wait_phase(&empty[slot], ((it / NSTAGE) & 1) ^ 1, abort)) {
+            ok = false;
+            break;
+          }
+          const long ks = (long)(b0 + bi) * QBLK_STAGES + st;
+          uint8_t *sa = smem + slot * STAGE;
+          mbar_expect_tx(&full[slot], STAGE);
+          bulk_g2s(sa, g.a + ((long)I * g.nks + ks) * A_BYTES, A_BYTES, &full[slot]);
+          copy_b96(sa + A_BYTES, g.b, J, ks, g.nks, &full[slot]);
+          ++it;
+        }
+        if (!ok) break;
+      }
+      // copies still in flight land before the CTA may exit
+      for (int k = max(0, it - NSTAGE); k < it; ++k)
+        wait_phase(&full[k % NSTAGE], (k / NSTAGE) & 1, nullptr);
+    }
+  } else if (warp == 9) {
+    if (lane == 0) {
+      int it = 0;
+      bool ok = true;
+      for (int bi = 0; bi < nb && ok; ++bi) {
+        if (!wait_phase(&accempty, (bi & 1) ^ 1, abort)) break;
+        fence_after_sync();
+        for (int st = 0; st < QBLK_STAGES; ++st, ++it) {
+          const int slot = it % NSTAGE;
+          if (!wait_phase(&full[slot], (it / NSTAGE) & 1, abort)) {
+            ok = false;
+            break;
+          }
+          fence_after_sync();
+          const uint32_t sa = smem_u32(smem + slot * STAGE);
+          issue_stage<QN, kQuadProducts>(tmem, sa, sa + A_BYTES, st == 0);
+          umma_commit(&empty[slot]);
+        }
+        if (ok) umma_commit(&accfull);
+      }
+      umma_commit(&done);
+    }
+  } else {
+    const uint32_t lane_off = (uint32_t)(32 * (warp & 3)) << 16;
+    const int row = 32 * (warp & 3) + lane;
+    const int col0 = 48 * (warp >> 2);
+    const long mu = (long)I * TM + row;
+    double part[48];
+#pragma unroll
+    for (int i = 0; i < 48; ++i) part[i] = 0.0;
+    bool ok = true;
+    for (int bi = 0; bi < nb; ++bi) {
+      if (!group_wait(&accfull, bi & 1, abort, &flag_sh)) {
+        ok = false;
+        break;
+      }
+      fence_after_sync();
+      const int blk = b0 + bi;
+      const int ea = __ldg(g.ea + mu * g.nblk + blk);
+      const int *eb = g.eb + ((long)J * QN + col0) * g.nblk + blk;
+#pragma unroll
+      for (int c = 0; c < 48; c += 8) {
+        int32_t v[5][8];
+#pragma unroll
+        for (int d = 0; d < 5; ++d) tmem_ld8(tmem + lane_off + d * QN + col0 + c, v[d]);
+        tmem_wait_ld();
+#pragma unroll
+        for (int d = 0; d < 5; ++d) tie8(v[d]);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const long long comb =
+              (((((long long)v[0][i] * 256 + v[1][i]) * 256 + v[2][i]) * 256 + v[3][i]) * 256) +
+              v[4][i];
+          part[c + i] += (double)comb * pow2(ea + __ldg(eb + (long)(c + i) * g.nblk) - 44);
+        }
+      }
+      fence_before_sync();
+      mbar_arrive(&accempty);
+    }
+    if (ok) {
+      double *out = g.work + (((long)blockIdx.y * g.npair + blockIdx.x) * TM + row) * QN + col0;
+#pragma unroll
+      for (int i = 0; i < 48; ++i) out[i] = part[i];
+    }
+  }
+  fence_before_sync();
+  __syncthreads();
+  if (warp == 9) {
+    if (lane == 0) wait_phase(&done, 0, nullptr);
+    __syncwarp();
+    fence_after_sync();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols));
+  }
+}
+
+// F[mu][nu] = F[nu][mu] = sum over chunks (fixed order) of tile (mu/128, nu/96).
+__global__ void quad_i8_reduce_kernel(int n, int nchunk, int npair, int ntj,
+                                      const double *__restrict__ work, double *__restrict__ F) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)n * n) return;
+  const int mu = (int)(idx / n), nu = (int)(idx % n);
+  if (mu > nu) return;
+  const int I = mu / TM, J = nu / QN;
+  int pair = 0;
+  for (int i = 0; i < I; ++i) pair += ntj - (4 * i) / 3;
+  pair += J - (4 * I) / 3;
+  const double *w = work + ((long)pair * TM + mu % TM) * QN + nu % QN;
+  const long stride = (long)npair * TM * QN;
+  double s = 0.0;
+  for (int c = 0; c < nchunk; ++c) s += w[c * stride];
+  F[(long)mu * n + nu] = s;
+  F[(long)nu * n + mu] = s;
+}
+
+// ---------------------------------------------------------------- density
+struct DensArgs {
+  const int8_t *a;        // phi^T image [point tile][nks][slices][128 x 64]
+  const int *ea;          // exponent per point
+  const int8_t *d;        // D image [128-row tile][nks][slices][128 x 64]
+  const int *ed;          // exponent per row of D
+  int nks, nmt, npt, npoint;
+  double *rho;
+};
+
+// Persistent: CTA c handles point tiles c, c + gridDim.x, ...  Pass (tile,
+// m): T[p][mu] = sum_nu phi[nu][p] D[mu][nu] for the 128 points and the 128
+// functions of block m, accumulated over all nu in TMEM; the drain adds
+// phi[mu][p] T[p][mu] into rho[p] (thread = point, 64 functions each).
+__global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ __align__(8) uint64_t full[NSTAGE], empty[NSTAGE], accfull, accempty, done;
+  __shared__ uint32_t tmem_sh;
+  __shared__ int abort_sh, flag_sh;
+  __shared__ double red[2][TM];
+  constexpr uint32_t A_BYTES = stage_bytes(TM), B_BYTES = stage_bytes(DN);
+  constexpr uint32_t STAGE = A_BYTES + B_BYTES;
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  volatile int *abort = &abort_sh;
+
+  if (t == 0) {
+    for (int s = 0; s < NSTAGE; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(&accfull, 1);
+    mbar_init(&accempty, NEPI);
+    mbar_init(&done, 1);
+    abort_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 9) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_sh)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = tmem_sh;
+
+  if (warp == 8) {
+    if (lane == 0) {
+      int it = 0;
+      bool ok = true;
+      for (int pt = blockIdx.x; pt < g.npt && ok; pt += gridDim.x)
+        for (int m = 0; m < g.nmt && ok; ++m)
+          for (int ks = 0; ks < g.nks; ++ks) {
+            const int slot = it % NSTAGE;
+            if (!wait_phase(&empty[slot], ((it / NSTAGE) & 1) ^ 1, abort)) {
+              ok = false;
+              break;
+            }
+            uint8_t *sa = smem + slot * STAGE;
+            mbar_expect_tx(&full[slot], STAGE);
+            bulk_g2s(sa, g.a + ((long)pt * g.nks + ks) * A_BYTES, A_BYTES, &full[slot]);
+            bulk_g2s(sa + A_BYTES, g.d + ((long)m * g.nks + ks) * B_BYTES, B_BYTES, &full[slot]);
+            ++it;
+          }
+      for (int k = max(0, it - NSTAGE); k < it; ++k)
+        wait_phase(&full[k % NSTAGE], (k / NSTAGE) & 1, nullptr);
+    }
+  } else if (warp == 9) {
+    if (lane == 0) {
+      int it = 0, pass = 0;
+      bool ok = true;
+      for (int pt = blockIdx.x; pt < g.npt && ok; pt += gridDim.x)
+        for (int m = 0; m < g.nmt && ok; ++m, ++pass) {
+          if (!wait_phase(&accempty, (pass & 1) ^ 1, abort)) {
+            ok = false;
+            break;
+          }
+          fence_after_sync();
+          for (int ks = 0; ks < g.nks; ++ks, ++it) {
+            const int slot = it % NSTAGE;
+            if (!wait_phase(&full[slot], (it / NSTAGE) & 1, abort)) {
+              ok = false;
+              break;
+            }
+            fence_after_sync();
+            const uint32_t sa = smem_u32(smem + slot * STAGE);
+            issue_stage<DN, kDensProducts>(tmem, sa, sa + A_BYTES, ks == 0);
+            umma_commit(&empty[slot]);
+          }
+          if (ok) umma_commit(&accfull);
+        }
+      umma_commit(&done);
+    }
+  } else {
+    const uint32_t lane_off = (uint32_t)(32 * (warp & 3)) << 16;
+    const int row = 32 * (warp & 3) + lane;
+    const int h = warp >> 2;
+    int pass = 0;
+    bool ok = true;
+    for (int pt = blockIdx.x; pt < g.npt && ok; pt += gridDim.x) {
+      const long p = (long)pt * TM + row;
+      double acc = 0.0;
+      for (int m = 0; m < g.nmt; ++m, ++pass) {
+        if (!group_wait(&accfull, pass & 1, abort, &flag_sh)) {
+          ok = false;
+          break;
+        }
+        fence_after_sync();
+        const int ksm = 2 * m + h;  // stage of phi^T holding functions 64 (2m + h) ..
+        const bool has = ksm < g.nks;
+        const int8_t *pa =
+            g.a + ((long)pt * g.nks + (has ? ksm : 0)) * A_BYTES + core_off(row, 0);
+#pragma unroll 1
+        for (int c = 0; c < 64; c += 16) {
+          int32_t v[4][16];
+#pragma unroll
+          for (int dg = 0; dg < 4; ++dg) {
+            tmem_ld8(tmem + lane_off + dg * DN + 64 * h + c, v[dg]);
+            tmem_ld8(tmem + lane_off + dg * DN + 64 * h + c + 8, v[dg] + 8);
+          }
+          tmem_wait_ld();
+#pragma unroll
+          for (int dg = 0; dg < 4; ++dg) {
+            tie8(v[dg]);
+            tie8(v[dg] + 8);
+          }
+          if (has) {
+            uint4 q[NSL];
+#pragma unroll
+            for (int s = 0; s < NSL; ++s)
+              q[s] = __ldg(reinterpret_cast<const uint4 *>(pa + (long)s * TM * KS + (c >> 4) * 128));
+            const int *ed = g.ed + m * DN + 64 * h + c;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const int wq = i >> 2, b = i & 3;
+              const uint32_t w0 = (&q[0].x)[wq], w1 = (&q[1].x)[wq], w2 = (&q[2].x)[wq],
+                             w3 = (&q[3].x)[wq];
+              const int y = ((sbyte(w0, b) * 256 + sbyte(w1, b)) * 256 + sbyte(w2, b)) * 256 +
+                            sbyte(w3, b);
+              const long long comb =
+                  (((long long)v[0][i] * 256 + v[1][i]) * 256 + v[2][i]) * 256 + v[3][i];
+              acc = fma((double)y * pow2(__ldg(ed + i)), (double)comb, acc);
+            }
+          }
+        }
+        fence_before_sync();
+        mbar_arrive(&accempty);
+      }
+      if (!ok) break;
+      red[h][row] = acc;
+      named_sync(1, NEPI);
+      if (h == 0 && p < g.npoint) {
+        const int ep = __ldg(g.ea + p);
+        g.rho[p] = (red[0][row] + red[1][row]) * pow2(ep - 33) * pow2(ep - 33);
+      }
+      named_sync(1, NEPI);
+    }
+  }
+  fence_before_sync();
+  __syncthreads();
+  if (warp == 9) {
+    if (lane == 0) wait_phase(&done, 0, nullptr);
+    __syncwarp();
+    fence_after_sync();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols));
+  }
+}
+
+int num_sms() {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
+// rows_pad: rows written (a multiple of TR; rows >= nrows get zeros)
+cudaError_t launch_slice_rows(const double *src, long ld, int nrows, int rows_pad, int ncols,
+                              const double *m1, const double *m2, int kb, int nblk, int TR,
+                              int nks, int8_t *img, int *e, cudaStream_t s) {
+  slice_rows_kernel<<<dim3(rows_pad / 8, nblk), 256, 0, s>>>(src, ld, nrows, ncols, m1, m2, kb,
+                                                               nblk, TR, nks, img, e);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------- plan
+struct Int8Plan {
+  int n = 0, npoint = 0;
+  long ld = 0;
+  // quadrature: A and B images share 128-row tiles (nimg of them, enough for
+  // the 96-row B tiles too)
+  int nblk = 0, nks_q = 0, nti = 0, ntj = 0, nimg = 0, npair = 0, nchunk = 0, bpc = 0;
+  // density
+  int npt = 0, nks_d = 0, nmt = 0;
+  DevBuf<int8_t> qa, qb, da, dd;
+  DevBuf<int> qa_e, qb_e, eg, da_e, dd_e;
+  DevBuf<double> sc, isc, gs, work;
+};
+
+int int8_plan_create(Int8Plan **out, int n, int npoint, const double *phi, long ld,
+                     const double *wb, const double *w, cudaStream_t s) {
+  *out = nullptr;
+  NAPMO_REQUIRE(n >= 1 && n <= 8192, "int8 contractions need 1 <= n <= 8192 basis functions");
+  NAPMO_REQUIRE(npoint >= 1, "empty grid");
+  std::unique_ptr<Int8Plan> p(new Int8Plan);
+  p->n = n;
+  p->npoint = npoint;
+  p->ld = ld;
+  p->nblk = (npoint + QKB - 1) / QKB;
+  p->nks_q = p->nblk * QBLK_STAGES;
+  p->nti = (n + TM - 1) / TM;
+  p->ntj = (n + QN - 1) / QN;
+  p->nimg = max(p->nti, (p->ntj * QN + TM - 1) / TM);
+  p->npair = 0;
+  for (int i = 0; i < p->nti; ++i) p->npair += p->ntj - (4 * i) / 3;
+  // chunks of point blocks: fewest (waves x blocks per chunk) at one CTA per SM
+  const int sms = num_sms();
+  long best = -1;
+  for (int nc = 1; nc <= p->nblk && nc <= 64; ++nc) {
+    const int bpc = (p->nblk + nc - 1) / nc;
+    const int used = (p->nblk + bpc - 1) / bpc;
+    const long waves = ((long)p->npair * used + sms - 1) / sms;
+    const long cost = waves * bpc;
+    if (best < 0 || cost < best) {
+      best = cost;
+      p->bpc = bpc;
+      p->nchunk = used;
+    }
+  }
+  p->npt = (int)(padded_points(npoint) / TM);
+  const int npad64 = (n + KS - 1) / KS * KS;
+  p->nks_d = npad64 / KS;
+  p->nmt = (n + TM - 1) / TM;
+
+  NAPMO_TRY_CUDA(p->sc.alloc(npoint), "alloc int8 scales");
+  NAPMO_TRY_CUDA(p->isc.alloc(npoint), "alloc int8 scales");
+  const size_t img_bytes = (size_t)p->nimg * p->nks_q * stage_bytes(TM);
+  NAPMO_TRY_CUDA(p->qa.alloc(img_bytes), "alloc int8 phi image");
+  NAPMO_TRY_CUDA(p->qa_e.alloc((size_t)p->nimg * TM * p->nblk), "alloc");
+  NAPMO_TRY_CUDA(p->qb.alloc(img_bytes), "alloc int8 wv phi image");
+  NAPMO_TRY_CUDA(cudaMemsetAsync(p->qb.p, 0, img_bytes, s), "zero int8 wv phi image");
+  NAPMO_TRY_CUDA(p->qb_e.alloc((size_t)p->nimg * TM * p->nblk), "alloc");
+  NAPMO_TRY_CUDA(cudaMemsetAsync(p->qb_e.p, 0, p->qb_e.n * sizeof(int), s), "zero");
+  NAPMO_TRY_CUDA(p->eg.alloc(p->nblk), "alloc");
+  NAPMO_TRY_CUDA(p->gs.alloc((size_t)p->nblk * QKB), "alloc");
+  NAPMO_TRY_CUDA(p->da.alloc((size_t)p->npt * p->nks_d * stage_bytes(TM)), "alloc int8 phi^T image");
+  NAPMO_TRY_CUDA(p->da_e.alloc((size_t)p->npt * TM), "alloc");
+  NAPMO_TRY_CUDA(p->dd.alloc((size_t)p->nmt * p->nks_d * stage_bytes(TM)), "alloc int8 D image");
+  NAPMO_TRY_CUDA(p->dd_e.alloc((size_t)p->nmt * TM), "alloc");
+  NAPMO_TRY_CUDA(p->work.alloc((size_t)p->nchunk * p->npair * TM * QN), "alloc int8 workspace");
+
+  balance_kernel<<<(npoint + 255) / 256, 256, 0, s>>>(npoint, wb, w, p->sc.p, p->isc.p);
+  NAPMO_TRY_CUDA(cudaGetLastError(), "balance");
+  NAPMO_TRY_CUDA(launch_slice_rows(phi, ld, n, p->nimg * TM, npoint, p->sc.p, nullptr, QKB,
+                                   p->nblk, TM, p->nks_q, p->qa.p, p->qa_e.p, s),
+                 "slice phi (quadrature)");
+  slice_points_kernel<<<p->npt, TM, 0, s>>>(phi, ld, n, npoint, p->nks_d, p->da.p, p->da_e.p);
+  NAPMO_TRY_CUDA(cudaGetLastError(), "slice phi (density)");
+  *out = p.release();
+  return kOk;
+}
+
+void int8_plan_destroy(Int8Plan *p) { delete p; }
+
+size_t int8_plan_device_bytes(const Int8Plan *p) {
+  return p->qa.n + p->qb.n + p->da.n + p->dd.n +
+         4 * (p->qa_e.n + p->qb_e.n + p->eg.n + p->da_e.n + p->dd_e.n) +
+         8 * (p->sc.n + p->isc.n + p->gs.n + p->work.n);
+}
+
+int int8_density(Int8Plan *p, const double *D, double *rho, cudaStream_t s) {
+  NAPMO_TRY_CUDA(launch_slice_rows(D, p->n, p->n, p->nmt * TM, p->n, nullptr, nullptr,
+                                   p->nks_d * KS, 1, TM, p->nks_d, p->dd.p, p->dd_e.p, s),
+                 "slice D");
+  DensArgs g{p->da.p, p->da_e.p, p->dd.p, p->dd_e.p, p->nks_d, p->nmt, p->npt, p->npoint, rho};
+  const int smem = NSTAGE * (stage_bytes(TM) + stage_bytes(DN));
+  NAPMO_TRY_CUDA(cudaFuncSetAttribute(density_i8_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                 "density_i8 smem");
+  const int grid = p->npt < num_sms() ? p->npt : num_sms();
+  density_i8_kernel<<<grid, NTHR, smem, s>>>(g);
+  NAPMO_TRY_CUDA(cudaGetLastError(), "density_i8");
+  return kOk;
+}
+
+int int8_quadrature(Int8Plan *p, const double *phi, const double *wv, double *F,
+                    cudaStream_t s) {
+  (void)phi;
+  gscale_kernel<<<p->nblk, 256, 0, s>>>(p->npoint, wv, p->isc.p, p->gs.p, p->eg.p);
+  NAPMO_TRY_CUDA(cudaGetLastError(), "block scales");
+  const int tiles_used = (p->n + TM - 1) / TM;
+  scale_image_kernel<<<dim3(tiles_used, p->nblk), 512, 0, s>>>(
+      p->qa.p, p->qb.p, p->gs.p, p->qa_e.p, p->eg.p, p->qb_e.p, p->nks_q, p->nblk);
+  NAPMO_TRY_CUDA(cudaGetLastError(), "wv phi image");
+  QuadArgs g{p->qa.p, p->qb.p, p->qa_e.p, p->qb_e.p, p->nblk, p->nks_q,
+             p->ntj,  p->bpc,  p->npair, p->work.p};
+  const int smem = NSTAGE * (stage_bytes(TM) + stage_bytes(QN));
+  NAPMO_TRY_CUDA(cudaFuncSetAttribute(quad_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      smem),
+                 "quad_i8 smem");
+  quad_i8_kernel<<<dim3(p->npair, p->nchunk), NTHR, smem, s>>>(g);
+  NAPMO_TRY_CUDA(cudaGetLastError(), "quad_i8");
+  const long nn = (long)p->n * p->n;
+  quad_i8_reduce_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(p->n, p->nchunk, p->npair,
+                                                                     p->ntj, p->work.p, F);
+  NAPMO_TRY_CUDA(cudaGetLastError(), "quad_i8 reduce");
+  return kOk;
+}
+
+int tc_error_status(cudaStream_t s, bool reset) {
+  int h = 0;
+  if (cudaMemcpyFromSymbolAsync(&h, g_tc_error, sizeof(int), 0, cudaMemcpyDeviceToHost, s) !=
+      cudaSuccess)
+    return kCudaError;
+  cudaStreamSynchronize(s);
+  if (reset && h) {
+    const int z = 0;
+    cudaMemcpyToSymbolAsync(g_tc_error, &z, sizeof(int), 0, cudaMemcpyHostToDevice, s);
+    cudaStreamSynchronize(s);
+  }
+  return h;
+}
+
+}  // namespace napmo

@@ -42,7 +42,9 @@ class FockBuilder(object):
             Poisson tables (quadratures only).
     """
 
-    def __init__(self, grid, basis, lmax, stream=None):
+    PRECISIONS = {'fp64': 0, 'int8x4': 1}
+
+    def __init__(self, grid, basis, lmax, stream=None, precision='fp64'):
         torch = _torch()
         self.torch = torch
         self.grid = grid
@@ -56,10 +58,24 @@ class FockBuilder(object):
         n, npt, ld, phi = c_int(), c_int(), c_long(), c_void_p()
         cext.lib.napmo_fock_plan_info(self._plan, byref(n), byref(npt), byref(ld), byref(phi))
         self.n, self.npoint, self.ld, self._phi_ptr = n.value, npt.value, ld.value, phi.value
+        self.set_precision(precision)
+
+    def set_precision(self, precision):
+        """'fp64' (CUDA cores) or 'int8x4' (int8 slices on the tensor cores) for
+        rho and F; the Poisson solve is FP64 in both."""
+        checked(cext.lib.napmo_fock_plan_set_precision(self._plan, self.PRECISIONS[precision]))
+        self.precision = precision
+
+    def tc_status(self, reset=True, stream=None):
+        """Error word of the tensor-core kernels (0: none); synchronises the stream."""
+        return cext.lib.napmo_tc_status(_stream(self.torch, stream), 1 if reset else 0)
 
     def __del__(self):
         if getattr(self, '_plan', None):
-            cext.lib.napmo_fock_plan_free(self._plan)
+            try:
+                cext.lib.napmo_fock_plan_free(self._plan)
+            except (AttributeError, TypeError):  # library already unloaded at exit
+                pass
             self._plan = None
 
     def _dev(self, x, shape=None):
@@ -139,6 +155,6 @@ def _view(torch, ptr, shape):
 
     class _Holder(object):
         __cuda_array_interface__ = {
-            'shape': (n,), 'typestr': '<f8', 'data': (ptr, True), 'version': 2}
+            'shape': (n,), 'typestr': '<f8', 'data': (ptr, False), 'version': 2}
 
     return torch.as_tensor(_Holder(), device='cuda').view(*shape)

@@ -47,7 +47,10 @@ class RadialTransform(object):
 
     def __del__(self):
         if getattr(self, '_this', None):
-            _lib().RTransform_del(self._this)
+            try:
+                _lib().RTransform_del(self._this)
+            except (AttributeError, TypeError):  # library already unloaded at exit
+                pass
             self._this = None
 
     def _apply(self, fn_scalar, fn_array, t):
@@ -160,7 +163,10 @@ class RadialGrid(object):
 
     def __del__(self):
         if getattr(self, '_this', None):
-            _lib().RadialGrid_del(self._this)
+            try:
+                _lib().RadialGrid_del(self._this)
+            except (AttributeError, TypeError):  # library already unloaded at exit
+                pass
             self._this = None
 
     def integrate(self, f, segments):
@@ -197,7 +203,10 @@ class AngularGrid(object):
 
     def __del__(self):
         if getattr(self, '_this', None):
-            _lib().AngularGrid_del(self._this)
+            try:
+                _lib().AngularGrid_del(self._this)
+            except (AttributeError, TypeError):  # library already unloaded at exit
+                pass
             self._this = None
 
     def integrate(self, *args):
@@ -230,7 +239,10 @@ class AtomicGrid(object):
 
     def __del__(self):
         if getattr(self, '_this', None):
-            _lib().AtomicGrid_del(self._this)
+            try:
+                _lib().AtomicGrid_del(self._this)
+            except (AttributeError, TypeError):  # library already unloaded at exit
+                pass
             self._this = None
 
     def spherical_expansion(self, lmax, f):
@@ -294,7 +306,10 @@ class Cell(object):
 
     def __del__(self):
         if getattr(self, '_this', None):
-            _lib().Cell_del(self._this)
+            try:
+                _lib().Cell_del(self._this)
+            except (AttributeError, TypeError):  # library already unloaded at exit
+                pass
             self._this = None
 
 
@@ -338,7 +353,10 @@ class BeckeGrid(object):
 
     def __del__(self):
         if getattr(self, '_this', None):
-            _lib().BeckeGrid_del(self._this)
+            try:
+                _lib().BeckeGrid_del(self._this)
+            except (AttributeError, TypeError):  # library already unloaded at exit
+                pass
             self._this = None
 
     def evaluate_decomposition(self, atom, cubic_splines, output, cell=None):
@@ -406,7 +424,10 @@ class MultiGrid(object):
 
     def __del__(self):
         if getattr(self, '_this', None):
-            _lib().MultiGrid_del(self._this)
+            try:
+                _lib().MultiGrid_del(self._this)
+            except (AttributeError, TypeError):  # library already unloaded at exit
+                pass
             self._this = None
 
     def add_grid(self, grid):
@@ -529,7 +550,10 @@ class CubicSpline(object):
 
     def __del__(self):
         if getattr(self, '_this', None):
-            _lib().CubicSpline_del(self._this)
+            try:
+                _lib().CubicSpline_del(self._this)
+            except (AttributeError, TypeError):  # library already unloaded at exit
+                pass
             self._this = None
 
     def __call__(self, new_x, new_y=None):

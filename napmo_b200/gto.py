@@ -32,7 +32,10 @@ class PrimitiveGaussian(object):
 
     def __del__(self):
         if getattr(self, '_this', None):
-            _lib().PrimitiveGaussian_del(self._this)
+            try:
+                _lib().PrimitiveGaussian_del(self._this)
+            except (AttributeError, TypeError):  # library already unloaded at exit
+                pass
             self._this = None
 
     def overlap(self, other):
@@ -77,7 +80,10 @@ class ContractedGaussian(object):
 
     def __del__(self):
         if getattr(self, '_this', None):
-            _lib().ContractedGaussian_del(self._this)
+            try:
+                _lib().ContractedGaussian_del(self._this)
+            except (AttributeError, TypeError):  # library already unloaded at exit
+                pass
             self._this = None
 
     def overlap(self, other):
@@ -152,7 +158,10 @@ class BasisSet(dict):
 
     def __del__(self):
         if getattr(self, '_this', None):
-            _lib().BasisSet_del(self._this)
+            try:
+                _lib().BasisSet_del(self._this)
+            except (AttributeError, TypeError):  # library already unloaded at exit
+                pass
             self._this = None
 
     def update(self, other):

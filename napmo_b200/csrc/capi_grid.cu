@@ -40,7 +40,8 @@ struct PoissonPlan {
   std::vector<PoissonAtom> h_atoms;
   DevBuf<PoissonAtom> atoms;
   DevBuf<int> mol_atom_off, mol_point_off, sys_atom, sys_l;
-  DevBuf<double> rad, ytab, proj, spl, amp, raw_y, raw_dt;
+  DevBuf<double> rad, ytab, proj, spl, amp, raw_y, raw_dt, lu, lmul;
+  DevBuf<int> lpiv;
   DevBuf<int> pairs;
   DevBuf<EvalItem> items;
   DevBuf<double> pair_v;
@@ -185,6 +186,15 @@ int build_poisson_plan(const std::vector<const AtomLayout *> &atoms,
   d.raw_y = plan->raw_y.p;
   d.raw_dt = plan->raw_dt.p;
   d.npair = pairs;
+  // LU factors of the radial systems (they depend on the grid only)
+  d.lu_stride = 2 * d.max_nrad;
+  NAPMO_TRY_CUDA(plan->lu.alloc((size_t)d.nsys * d.lu_stride * kW), "alloc radial LU");
+  NAPMO_TRY_CUDA(plan->lmul.alloc((size_t)d.nsys * d.lu_stride * kKL), "alloc radial LU");
+  NAPMO_TRY_CUDA(plan->lpiv.alloc((size_t)d.nsys * d.lu_stride), "alloc radial LU");
+  d.lu = plan->lu.p;
+  d.lmul = plan->lmul.p;
+  d.lpiv = plan->lpiv.p;
+  NAPMO_TRY_CUDA(launch_poisson_factor(d, s), "radial LU");
   return kOk;
 }
 

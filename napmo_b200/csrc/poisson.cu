@@ -32,6 +32,11 @@ namespace {
 __constant__ double c_ov2[5 * 2 * 5 * 2];
 __constant__ double c_ov3[5 * 2 * 5 * 2 * 5 * 2];
 __constant__ double c_shnorm[(kMaxLmax + 1) * (kMaxLmax + 1)];  // [l][m]
+// normalised solid-harmonic recursion along l at fixed m (evaluation kernel):
+// q_l = a_lm z q_(l-1) - b_lm q_(l-2), q_m = start_m
+__constant__ double c_rec_a[(kMaxLmax + 1) * (kMaxLmax + 1)];
+__constant__ double c_rec_b[(kMaxLmax + 1) * (kMaxLmax + 1)];
+__constant__ double c_rec_start[kMaxLmax + 1];
 
 constexpr double kPI4 = 4.0 * M_PI;
 constexpr double kInvSqrt4Pi = 0.28209479177387814347;
@@ -125,90 +130,37 @@ project_kernel(PoissonDev P, const double *__restrict__ rho,
 }
 
 // ------------------------------------------------------------------- radial
-// Band storage of the 2n x 2n FEM matrix: kl = ku = 3, fill-in from partial
-// pivoting reaches kl + ku above the diagonal.  AB(i, j) = band[j*kW + 6+i-j].
-constexpr int kKL = 3, kKU = 3, kW = 2 * kKL + kKU + 1;
+// Band storage of the 2n x 2n FEM matrix (kKL, kKU, kW in poisson.cuh):
+// AB(i, j) = band[j*kW + 6+i-j].
 
 __device__ __forceinline__ double &AB(double *band, int i, int j) {
   return band[j * kW + (kKL + kKU) + i - j];
 }
+__device__ __forceinline__ double ABc(const double *band, int i, int j) {
+  return __ldg(band + j * kW + (kKL + kKU) + i - j);
+}
 
-__global__ void radial_kernel(PoissonDev P, int ncol) {
+// The FEM band matrix of a system depends on the atom's radial grid and l
+// only: it is assembled and LU-factored (partial pivoting, kl = ku = 3) once
+// per grid.  Outputs per system: the band with U (rows i, columns i..i+6), the
+// multipliers of step k in mult[k * kKL + i], the pivot row of step k.
+__global__ void radial_factor_kernel(PoissonDev P) {
   extern __shared__ double sm[];
   const int sys = blockIdx.x;
   const PoissonAtom at = P.atoms[P.sys_atom[sys]];
   const int l = P.sys_l[sys];
   const int n = at.nrad, n2 = 2 * n;
-  const int lsize = (at.lmax + 1) * (at.lmax + 1);
-  const int nm = 2 * l + 1;
   const int tid = threadIdx.x, nt = blockDim.x;
-  double *band = sm;                 // n2 * kW
-  double *R = band + n2 * kW;        // n2 * ncol  (row-major, column = m)
-  double *buf = R + n2 * ncol;       // n * ncol   (spline t-derivatives)
+  double *band = sm;  // n2 * kW
   __shared__ double s_mult[kKL];
   __shared__ int s_piv;
-
   const double *rad = P.rad + at.rad_off;
-  const double *r = rad + kRadR * n, *wr = rad + kRadW * n, *j1 = rad + kRadJ1 * n,
-               *j2 = rad + kRadJ2 * n, *j3 = rad + kRadJ3 * n,
-               *den = rad + kRadDen * n, *upm = rad + kRadUp * n;
+  const double *r = rad + kRadR * n, *j1 = rad + kRadJ1 * n, *j2 = rad + kRadJ2 * n,
+               *j3 = rad + kRadJ3 * n;
   const long xmax = n - 1;
-
-  // -- 1. per m: spline derivatives of f_lm, boundary values, FEM rhs
-  for (int c = tid; c < ncol; c += nt) {
-    if (c >= nm) {
-      for (int row = 0; row < n2; ++row) R[row * ncol + c] = 0.0;
-      continue;
-    }
-    const double *y = P.proj + at.proj_off + l * l + c;  // stride lsize
-    // Thomas elimination for 2/1, 1/4/1, ..., 1/2 with rhs 3 (y_{i+1}-y_{i-1})
-    double prev = (3.0 * (y[lsize] - y[0])) / den[0];
-    buf[c] = prev;
-    for (int i = 1; i < n; ++i) {
-      const double rhs = (i < n - 1) ? 3.0 * (y[(long)(i + 1) * lsize] - y[(long)(i - 1) * lsize])
-                                     : 3.0 * (y[(long)(n - 1) * lsize] - y[(long)(n - 2) * lsize]);
-      prev = (rhs - prev * 1.0) / den[i];
-      buf[i * ncol + c] = prev;
-    }
-    for (int i = n - 2; i >= 0; --i)
-      buf[i * ncol + c] = buf[i * ncol + c] - upm[i] * buf[(i + 1) * ncol + c];
-    // boundary values (Dirichlet) from radial moments
-    double smax = 0.0, smin = 0.0;
-    for (int i = 0; i < n; ++i) {
-      const double yi = y[(long)i * lsize];
-      smax += yi * pow(r[i], (double)l) * wr[i];
-      smin += yi * pow(r[i], (double)(-l - 1)) * wr[i];
-    }
-    const double vmax = smax * (1.0 / pow(r[n - 1], (double)(l + 1)) / (2 * l + 1));
-    const double vmin = smin * (pow(r[0], (double)l) / (2 * l + 1));
-    // FEM right-hand side from the transformed source f = -4 pi rho
-    for (int row = 0; row < n2; ++row) {
-      double acc = 0.0;
-      if (row == 0) {
-        acc = vmin;
-      } else if (row == n2 - 2) {
-        acc = vmax;
-      } else {
-        long lo = 2 * (row / 2 - 1), hi = 2 * (row / 2 + 2);
-        if (lo < 0) lo = 0;
-        if (hi > n2) hi = n2;
-        for (long k = lo; k < hi; ++k) {
-          const int i = (int)(k / 2);
-          const double fy = -kPI4 * y[(long)i * lsize];
-          const double jsq = j1[i] * j1[i];
-          double fk;
-          if ((k & 1) == 0) {
-            fk = fy * jsq;
-          } else {
-            const double fdx = -kPI4 * (buf[i * ncol + c] / j1[i]);
-            fk = (fdx * jsq + 2 * fy * j2[i]) * j1[i];
-          }
-          if (fk != 0) acc += fk * ov2_d(xmax, row, 0, k, 0);
-        }
-      }
-      R[row * ncol + c] = acc;
-    }
-  }
+  double *lu = P.lu + (long)sys * P.lu_stride * kW;
+  double *mult = P.lmul + (long)sys * P.lu_stride * kKL;
+  int *piv = P.lpiv + (long)sys * P.lu_stride;
   // -- 2. band matrix (depends on l only)
   for (int e = tid; e < n2 * kW; e += nt) band[e] = 0.0;
   __syncthreads();
@@ -246,7 +198,7 @@ __global__ void radial_kernel(PoissonDev P, int ncol) {
     }
   }
   __syncthreads();
-  // -- 3. banded LU with partial pivoting, applied to all right-hand sides
+  // -- 3. banded LU with partial pivoting
   for (int k = 0; k < n2; ++k) {
     const int im = min(k + kKL, n2 - 1);
     const int ju = min(k + kKL + kKU, n2 - 1);
@@ -270,11 +222,6 @@ __global__ void radial_kernel(PoissonDev P, int ncol) {
         AB(band, k, j) = AB(band, p, j);
         AB(band, p, j) = t;
       }
-      for (int c = tid; c < ncol; c += nt) {
-        const double t = R[k * ncol + c];
-        R[k * ncol + c] = R[p * ncol + c];
-        R[p * ncol + c] = t;
-      }
       __syncthreads();
     }
     if (tid < im - k) s_mult[tid] = AB(band, k + 1 + tid, k) / AB(band, k, k);
@@ -284,43 +231,161 @@ __global__ void radial_kernel(PoissonDev P, int ncol) {
       const int i = k + 1 + e / ncolu, j = k + 1 + e % ncolu;
       AB(band, i, j) -= s_mult[i - k - 1] * AB(band, k, j);
     }
-    for (int e = tid; e < nrow * ncol; e += nt) {
-      const int i = k + 1 + e / ncol, c = e % ncol;
-      R[i * ncol + c] -= s_mult[i - k - 1] * R[k * ncol + c];
+    if (tid == 0) {
+      piv[k] = p;
+      for (int i = 0; i < kKL; ++i) mult[k * kKL + i] = i < nrow ? s_mult[i] : 0.0;
     }
     __syncthreads();
   }
-  // -- 4. back substitution, one column (m) per thread
+  for (int e = tid; e < n2 * kW; e += nt) lu[e] = band[e];
+}
+
+__global__ void radial_kernel(PoissonDev P, int ncol) {
+  extern __shared__ double sm[];
+  const int sys = blockIdx.x;
+  const PoissonAtom at = P.atoms[P.sys_atom[sys]];
+  const int l = P.sys_l[sys];
+  const int n = at.nrad, n2 = 2 * n;
+  const int lsize = (at.lmax + 1) * (at.lmax + 1);
+  const int nm = 2 * l + 1;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  double *R = sm;                    // n2 * ncol  (row-major, column = m)
+  double *buf = R + n2 * ncol;       // n * ncol   (spline t-derivatives)
+  double *Y = buf + n * ncol;        // n * ncol   (projected density of this l)
+  double *r = Y + n * ncol;          // radial tables of the atom, n each
+  double *wr = r + n, *j1 = wr + n, *j2 = j1 + n, *den = j2 + n, *upm = den + n;
+  double *rl = upm + n, *rm = rl + n;  // r^l, r^-(l+1)
+  double *bc = rm + n;                 // [2][ncol]: vmin, vmax per column
+  const double *band = P.lu + (long)sys * P.lu_stride * kW;
+  const double *mult = P.lmul + (long)sys * P.lu_stride * kKL;
+  const int *piv = P.lpiv + (long)sys * P.lu_stride;
+  const long xmax = n - 1;
+
+  // -- 0. stage the atom's radial tables and this l's projected density
+  {
+    const double *rad = P.rad + at.rad_off;
+    for (int i = tid; i < n; i += nt) {
+      r[i] = rad[kRadR * n + i];
+      wr[i] = rad[kRadW * n + i];
+      j1[i] = rad[kRadJ1 * n + i];
+      j2[i] = rad[kRadJ2 * n + i];
+      den[i] = rad[kRadDen * n + i];
+      upm[i] = rad[kRadUp * n + i];
+      rl[i] = pow(r[i], (double)l);
+      rm[i] = pow(r[i], (double)(-l - 1));
+    }
+    const double *proj = P.proj + at.proj_off + l * l;
+    for (int e = tid; e < n * nm; e += nt) {
+      const int i = e / nm, c = e - i * nm;
+      Y[i * ncol + c] = proj[(long)i * lsize + c];
+    }
+  }
+  __syncthreads();
+  // -- 1. per m: spline t-derivatives of f_lm and boundary values
+  for (int c = tid; c < nm; c += nt) {
+    const double *y = Y + c;  // stride ncol
+    // Thomas elimination for 2/1, 1/4/1, ..., 1/2 with rhs 3 (y_{i+1}-y_{i-1})
+    double prev = (3.0 * (y[ncol] - y[0])) / den[0];
+    buf[c] = prev;
+    for (int i = 1; i < n; ++i) {
+      const double rhs = (i < n - 1) ? 3.0 * (y[(i + 1) * ncol] - y[(i - 1) * ncol])
+                                     : 3.0 * (y[(n - 1) * ncol] - y[(n - 2) * ncol]);
+      prev = (rhs - prev * 1.0) / den[i];
+      buf[i * ncol + c] = prev;
+    }
+    for (int i = n - 2; i >= 0; --i)
+      buf[i * ncol + c] = buf[i * ncol + c] - upm[i] * buf[(i + 1) * ncol + c];
+    // boundary values (Dirichlet) from radial moments
+    double smax = 0.0, smin = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double yi = y[i * ncol];
+      smax += yi * rl[i] * wr[i];
+      smin += yi * rm[i] * wr[i];
+    }
+    bc[ncol + c] = smax * (1.0 / pow(r[n - 1], (double)(l + 1)) / (2 * l + 1));
+    bc[c] = smin * (pow(r[0], (double)l) / (2 * l + 1));
+  }
+  __syncthreads();
+  // -- 1b. FEM right-hand side from the transformed source f = -4 pi rho, one
+  // row per thread
+  for (int row = tid; row < n2; row += nt) {
+    long lo = 2 * (row / 2 - 1), hi = 2 * (row / 2 + 2);
+    if (lo < 0) lo = 0;
+    if (hi > n2) hi = n2;
+    for (int c = 0; c < nm; ++c) {
+      double acc = 0.0;
+      if (row == 0) {
+        acc = bc[c];
+      } else if (row == n2 - 2) {
+        acc = bc[ncol + c];
+      } else {
+        for (long k = lo; k < hi; ++k) {
+          const int i = (int)(k / 2);
+          const double fy = -kPI4 * Y[i * ncol + c];
+          const double jsq = j1[i] * j1[i];
+          double fk;
+          if ((k & 1) == 0) {
+            fk = fy * jsq;
+          } else {
+            const double fdx = -kPI4 * (buf[i * ncol + c] / j1[i]);
+            fk = (fdx * jsq + 2 * fy * j2[i]) * j1[i];
+          }
+          if (fk != 0) acc += fk * ov2_d(xmax, row, 0, k, 0);
+        }
+      }
+      R[row * ncol + c] = acc;
+    }
+  }
+  __syncthreads();
+  // -- 2. forward elimination with the stored factors, one column (m) per
+  // thread (the same operations, in the same order, as during the factoring)
+  for (int c = tid; c < nm; c += nt) {
+    for (int k = 0; k < n2; ++k) {
+      const int p = piv[k];
+      if (p != k) {
+        const double t = R[k * ncol + c];
+        R[k * ncol + c] = R[p * ncol + c];
+        R[p * ncol + c] = t;
+      }
+      const int im = min(k + kKL, n2 - 1);
+      const double rk = R[k * ncol + c];
+      for (int i = k + 1; i <= im; ++i) R[i * ncol + c] -= mult[k * kKL + (i - k - 1)] * rk;
+    }
+  }
+  // -- 3. back substitution, one column (m) per thread
   for (int c = tid; c < nm; c += nt) {
     for (int i = n2 - 1; i >= 0; --i) {
       double x = R[i * ncol + c];
       const int je = min(i + kKL + kKU, n2 - 1);
-      for (int j = i + 1; j <= je; ++j) x -= AB(band, i, j) * R[j * ncol + c];
-      R[i * ncol + c] = x / AB(band, i, i);
+      for (int j = i + 1; j <= je; ++j) x -= ABc(band, i, j) * R[j * ncol + c];
+      R[i * ncol + c] = x / ABc(band, i, i);
     }
   }
   __syncthreads();
-  // -- 5. output: raw splines, scaled cubic coefficients, extrapolation
+  // -- 4. output: raw splines, scaled cubic coefficients, extrapolation
   const double fl = sqrt((double)(2 * l + 1)) * kInvSqrt4Pi;
+  for (int e = tid; e < n * nm; e += nt) {
+    const int c = e / n, i = e - c * n;
+    const long o = at.raw_off + (long)(l * l + c) * n + i;
+    P.raw_y[o] = R[(2 * i) * ncol + c];
+    P.raw_dt[o] = (R[(2 * i + 1) * ncol + c] / j1[i]) * j1[i];
+  }
+  for (int e = tid; e < (n - 1) * nm; e += nt) {
+    const int j = e / nm, c = e - j * nm;
+    const double y0 = R[(2 * j) * ncol + c], y1 = R[(2 * j + 2) * ncol + c];
+    const double d0 = (R[(2 * j + 1) * ncol + c] / j1[j]) * j1[j];
+    const double d1 = (R[(2 * j + 3) * ncol + c] / j1[j + 1]) * j1[j + 1];
+    const double z = y1 - y0;
+    double *cf = P.spl + at.spl_off + ((long)j * lsize + l * l + c) * 4;
+    cf[0] = y0 * fl;
+    cf[1] = d0 * fl;
+    cf[2] = (3 * z - 2 * d0 - d1) * fl;
+    cf[3] = (-2 * z + d0 + d1) * fl;
+  }
   for (int c = tid; c < nm; c += nt) {
     const int lm = l * l + c;
-    double *ry = P.raw_y + at.raw_off + (long)lm * n;
-    double *rd = P.raw_dt + at.raw_off + (long)lm * n;
-    for (int i = 0; i < n; ++i) {
-      ry[i] = R[(2 * i) * ncol + c];
-      rd[i] = (R[(2 * i + 1) * ncol + c] / j1[i]) * j1[i];
-    }
-    for (int j = 0; j < n - 1; ++j) {
-      const double y0 = ry[j], y1 = ry[j + 1], d0 = rd[j], d1 = rd[j + 1];
-      const double z = y1 - y0;
-      double *cf = P.spl + at.spl_off + ((long)j * lsize + lm) * 4;
-      cf[0] = y0 * fl;
-      cf[1] = d0 * fl;
-      cf[2] = (3 * z - 2 * d0 - d1) * fl;
-      cf[3] = (-2 * z + d0 + d1) * fl;
-    }
-    P.amp[at.amp_off + lm * 2 + 0] = ry[0] / pow(at.first_x, (double)l) * fl;
-    P.amp[at.amp_off + lm * 2 + 1] = ry[n - 1] * pow(at.last_x, (double)(l + 1)) * fl;
+    P.amp[at.amp_off + lm * 2 + 0] = R[c] / pow(at.first_x, (double)l) * fl;
+    P.amp[at.amp_off + lm * 2 + 1] = R[(2 * (n - 1)) * ncol + c] * pow(at.last_x, (double)(l + 1)) * fl;
   }
 }
 
@@ -475,8 +540,102 @@ __global__ void pair_scatter_kernel(PoissonDev P, const int *__restrict__ bucket
 //                                                         d^-(l+1))
 // with S_lm(r_hat) = S_lm(p - A) / d^l, so the 1/d^l of the reference is folded
 // into the unit vector.  The result goes to the pair's own slot of pair_v.
+// Potentials of NP (atom, point) pairs of one bucket from the shared
+// coefficients cf (each coefficient load serves all NP pairs): REGION 0
+// inside the atom's radial grid (cubic spline in the interval coordinate u),
+// 1 below its first point (amplitudes x d^l), 2 beyond its last (amplitudes
+// x d^-(l+1)).
+template <int LMAX, int REGION, int NP>
+__device__ __forceinline__ void pair_values(const double *cf, int lmaxA, const double *x,
+                                            const double *y, const double *z, const double *d,
+                                            const double *inv, const double *u, double *v) {
+  double a0[NP], a1[NP], a2[NP], a3[NP], gstep[NP], cm[NP], sm[NP], gm[NP];
+#pragma unroll
+  for (int j = 0; j < NP; ++j) {
+    a0[j] = a1[j] = a2[j] = a3[j] = 0.0;
+    // tail factor of the current l: 1 inside the grid, d^l below its first
+    // point, d^-(l+1) beyond its last
+    gstep[j] = REGION == 1 ? d[j] : (REGION == 2 ? inv[j] : 1.0);
+    gm[j] = REGION == 2 ? inv[j] : 1.0;
+    cm[j] = 1.0;
+    sm[j] = 0.0;
+  }
+  // accumulate the (lm, S) term of every pair
+  auto term = [&](int lm, const double *S, const double *gl) {
+    if (REGION == 0) {
+      const double2 c01 = *reinterpret_cast<const double2 *>(cf + 4 * lm);
+      const double2 c23 = *reinterpret_cast<const double2 *>(cf + 4 * lm + 2);
+#pragma unroll
+      for (int j = 0; j < NP; ++j) {
+        a0[j] = fma(c01.x, S[j], a0[j]);
+        a1[j] = fma(c01.y, S[j], a1[j]);
+        a2[j] = fma(c23.x, S[j], a2[j]);
+        a3[j] = fma(c23.y, S[j], a3[j]);
+      }
+    } else {
+      const double c = cf[lm];
+#pragma unroll
+      for (int j = 0; j < NP; ++j) a0[j] = fma(c * gl[j], S[j], a0[j]);
+    }
+  };
+  // Normalised solid harmonics of the unit vector, m outer and l inner:
+  // q_l^m = nrm_lm Pi_l^m with Pi_m^m = (2m-1)!!, Pi_(m+1)^m = (2m+1) z Pi_m^m,
+  // Pi_l^m = ((2l-1) z Pi_(l-1)^m - (l+m-1) Pi_(l-2)^m) / (l-m) (|u| = 1);
+  // the normalisation is folded into the recursion constants (c_rec_a/b,
+  // c_rec_start).  S_l0 = q_l^0; S_lm (cos, sin) = q_l^m Re/Im (x + iy)^m at
+  // lm = l^2 + 2m - 1, l^2 + 2m: the values and lm order of solid_harmonics.h,
+  // evaluated column by column so that only a few are live.
+#pragma unroll
+  for (int m = 0; m <= LMAX; ++m) {
+    if (m > lmaxA) break;
+    double q[NP], qprev[NP], gl[NP];
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+      if (m > 0) {
+        const double c = cm[j] * x[j] - sm[j] * y[j];
+        sm[j] = cm[j] * y[j] + sm[j] * x[j];
+        cm[j] = c;
+        gm[j] *= gstep[j];
+      }
+      q[j] = c_rec_start[m];
+      qprev[j] = 0.0;
+      gl[j] = gm[j];
+    }
+#pragma unroll
+    for (int l = m; l <= LMAX; ++l) {
+      if (l > lmaxA) break;
+      if (l > m) {
+        const int k = l * (kMaxLmax + 1) + m;
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+          const double qn = fma(c_rec_a[k], z[j] * q[j], -c_rec_b[k] * qprev[j]);
+          qprev[j] = q[j];
+          q[j] = qn;
+          gl[j] *= gstep[j];
+        }
+      }
+      if (m == 0) {
+        term(l * l, q, gl);
+      } else {
+        double sc[NP], ss[NP];
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+          sc[j] = q[j] * cm[j];
+          ss[j] = q[j] * sm[j];
+        }
+        term(l * l + 2 * m - 1, sc, gl);
+        term(l * l + 2 * m, ss, gl);
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < NP; ++j)
+    v[j] = REGION == 0 ? a0[j] + u[j] * (a1[j] + u[j] * (a2[j] + u[j] * a3[j])) : a0[j];
+}
+
+
 template <int LMAX>
-__global__ void __launch_bounds__(kEvalChunk)
+__global__ void __launch_bounds__(kEvalChunk / kEvalPerThread)
 eval_pairs_kernel(PoissonDev P, const double *__restrict__ gx,
                   const double *__restrict__ gy, const double *__restrict__ gz) {
   extern __shared__ double cf[];
@@ -494,84 +653,37 @@ eval_pairs_kernel(PoissonDev P, const double *__restrict__ gx,
       cf[e] = src[2 * e + (region == 1 ? 0 : 1)];
   }
   __syncthreads();
-  if ((int)threadIdx.x >= it.count) return;
-  const int p = P.pairs[at.pair_off + it.start + threadIdx.x];
-  const double dx = gx[p] - at.cx, dy = gy[p] - at.cy, dz = gz[p] - at.cz;
-  const double d = sqrt(dx * dx + dy * dy + dz * dz);
-  const double inv = 1.0 / d;
-  const double x = dx * inv, y = dy * inv, z = dz * inv;
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-  double gl = 1.0, gstep = 1.0;  // tail factor of the current l
-  if (region == 1) gstep = d;
-  if (region == 2) {
-    gl = inv;
-    gstep = inv;
-  }
-  // accumulate one (lm, S) term
-  auto term = [&](int lm, double S) {
-    if (region == 0) {
-      const double2 c01 = *reinterpret_cast<const double2 *>(cf + 4 * lm);
-      const double2 c23 = *reinterpret_cast<const double2 *>(cf + 4 * lm + 2);
-      a0 = fma(c01.x, S, a0);
-      a1 = fma(c01.y, S, a1);
-      a2 = fma(c23.x, S, a2);
-      a3 = fma(c23.y, S, a3);
-    } else {
-      a0 = fma(cf[lm] * gl, S, a0);
-    }
-  };
-  term(0, 1.0);
-  if (LMAX >= 1 && lmaxA >= 1) {
-    gl *= gstep;
-    term(1, z);
-    term(2, x);
-    term(3, y);
-    if (LMAX >= 2 && lmaxA >= 2) {
-      const double r2 = x * x + y * y + z * z;
-      double pold[LMAX + 1], pnew[LMAX + 1], cs[LMAX + 1], sn[LMAX + 1];
-      pold[0] = 1.0;
-      pnew[0] = z;
-      pnew[1] = 1.0;
-      cs[1] = x;
-      sn[1] = y;
-      int lm = 4;
+  // thread t evaluates the pairs t and t + blockDim.x of the item (the
+  // second may be absent: it then repeats the first and is not stored)
+  const int t = threadIdx.x;
+  if (t >= it.count) return;
+  int pidx[kEvalPerThread];
+  double x[kEvalPerThread], y[kEvalPerThread], z[kEvalPerThread], d[kEvalPerThread],
+      inv[kEvalPerThread], u[kEvalPerThread], v[kEvalPerThread];
 #pragma unroll
-      for (int l = 2; l <= LMAX; ++l) {
-        if (l > lmaxA) break;
-        gl *= gstep;
-        const double fac = 2 * l - 1;
-#pragma unroll
-        for (int m = 0; m <= l - 2; ++m) {
-          const double keep = pold[m];
-          pold[m] = pnew[m];
-          pnew[m] = (z * fac * pold[m] - r2 * (l + m - 1) * keep) * (1.0 / (l - m));
-        }
-        pold[l - 1] = pnew[l - 1];
-        pnew[l] = fac * pold[l - 1];
-        pnew[l - 1] = z * pnew[l];
-        cs[l] = x * cs[l - 1] - y * sn[l - 1];
-        sn[l] = x * sn[l - 1] + y * cs[l - 1];
-        term(lm, pnew[0]);
-        ++lm;
-#pragma unroll
-        for (int m = 1; m <= l; ++m) {
-          const double nrm = c_shnorm[l * (kMaxLmax + 1) + m];
-          term(lm, nrm * cs[m] * pnew[m]);
-          term(lm + 1, nrm * sn[m] * pnew[m]);
-          lm += 2;
-        }
-      }
-    }
+  for (int j = 0; j < kEvalPerThread; ++j) {
+    const int e = t + j * (int)blockDim.x;
+    pidx[j] = P.pairs[at.pair_off + it.start + (e < it.count ? e : t)];
+    const int p = pidx[j];
+    const double dx = gx[p] - at.cx, dy = gy[p] - at.cy, dz = gz[p] - at.cz;
+    d[j] = sqrt(dx * dx + dy * dy + dz * dz);
+    inv[j] = 1.0 / d[j];
+    x[j] = dx * inv[j];
+    y[j] = dy * inv[j];
+    z[j] = dz * inv[j];
+    u[j] = region == 0 ? rt_inv(at.rt, d[j]) - (it.bucket - 1) : 0.0;
   }
-  double v;
-  if (region == 0) {
-    const double t = rt_inv(at.rt, d);
-    const double u = t - (it.bucket - 1);
-    v = a0 + u * (a1 + u * (a2 + u * a3));
-  } else {
-    v = a0;
+  if (region == 0)
+    pair_values<LMAX, 0, kEvalPerThread>(cf, lmaxA, x, y, z, d, inv, u, v);
+  else if (region == 1)
+    pair_values<LMAX, 1, kEvalPerThread>(cf, lmaxA, x, y, z, d, inv, u, v);
+  else
+    pair_values<LMAX, 2, kEvalPerThread>(cf, lmaxA, x, y, z, d, inv, u, v);
+#pragma unroll
+  for (int j = 0; j < kEvalPerThread; ++j) {
+    const int e = t + j * (int)blockDim.x;
+    if (e < it.count) P.pair_v[at.pair_off + (pidx[j] - at.mol_point_start)] = v[j];
   }
-  P.pair_v[at.pair_off + (p - at.mol_point_start)] = v;
 }
 
 // v[p] (+)= sum over the atoms of p's molecule of pair_v, in atom order.
@@ -603,7 +715,7 @@ cudaError_t launch_eval_l(const PoissonDev &P, int npoint, const double *x,
                           cudaStream_t s) {
   if (P.items && P.nitems > 0) {
     const size_t smem = (size_t)(L + 1) * (L + 1) * 4 * sizeof(double);
-    eval_pairs_kernel<L><<<P.nitems, kEvalChunk, smem, s>>>(P, x, y, z);
+    eval_pairs_kernel<L><<<P.nitems, kEvalChunk / kEvalPerThread, smem, s>>>(P, x, y, z);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     pairs_reduce_kernel<<<(npoint + 255) / 256, 256, 0, s>>>(P, npoint, out, acc);
@@ -624,7 +736,7 @@ cudaError_t poisson_init_constants() {
   std::vector<double> ov2(100), ov3(1000);
   hermite_tables_export(ov2.data(), ov3.data());
   std::vector<double> nrm((kMaxLmax + 1) * (kMaxLmax + 1), 0.0);
-  for (int l = 2; l <= kMaxLmax; ++l) {
+  for (int l = 1; l <= kMaxLmax; ++l) {
     double f = M_SQRT2;
     for (int m = 1; m <= l; ++m) {
       f /= sqrt((double)((l + m) * (l - m + 1)));
@@ -634,6 +746,27 @@ cudaError_t poisson_init_constants() {
   if ((e = cudaMemcpyToSymbol(c_ov2, ov2.data(), ov2.size() * sizeof(double))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_ov3, ov3.data(), ov3.size() * sizeof(double))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_shnorm, nrm.data(), nrm.size() * sizeof(double))) != cudaSuccess) return e;
+  {
+    const int K = kMaxLmax + 1;
+    auto nr = [&](int l, int m) { return m == 0 ? 1.0 : nrm[l * K + m]; };
+    std::vector<double> ra(K * K, 0.0), rb(K * K, 0.0), st(K, 0.0);
+    double dfact = 1.0;  // (2m-1)!!
+    for (int m = 0; m <= kMaxLmax; ++m) {
+      if (m > 0) dfact *= (double)(2 * m - 1);
+      st[m] = nr(m, m) * dfact;
+      for (int l = m + 1; l <= kMaxLmax; ++l) {
+        if (l == m + 1) {
+          ra[l * K + m] = (double)(2 * m + 1) * nr(l, m) / nr(m, m);
+        } else {
+          ra[l * K + m] = (double)(2 * l - 1) / (double)(l - m) * nr(l, m) / nr(l - 1, m);
+          rb[l * K + m] = (double)(l + m - 1) / (double)(l - m) * nr(l, m) / nr(l - 2, m);
+        }
+      }
+    }
+    if ((e = cudaMemcpyToSymbol(c_rec_a, ra.data(), ra.size() * sizeof(double))) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(c_rec_b, rb.data(), rb.size() * sizeof(double))) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(c_rec_start, st.data(), st.size() * sizeof(double))) != cudaSuccess) return e;
+  }
   done_dev = dev;
   return cudaSuccess;
 }
@@ -656,8 +789,23 @@ int poisson_radial_ncol(int max_lmax) { return ((2 * max_lmax + 1 + 31) / 32) * 
 
 size_t poisson_radial_smem(int max_nrad, int max_lmax) {
   const int ncol = poisson_radial_ncol(max_lmax);
-  const size_t n2 = 2 * (size_t)max_nrad;
-  return (n2 * kW + n2 * ncol + (size_t)max_nrad * ncol) * sizeof(double);
+  const size_t n = (size_t)max_nrad;
+  return (2 * n * ncol + 2 * n * ncol + 8 * n + 2 * (size_t)ncol) * sizeof(double);
+}
+
+size_t poisson_factor_doubles(int nsys, int max_nrad) {
+  return (size_t)nsys * 2 * max_nrad * (kW + kKL);
+}
+
+cudaError_t launch_poisson_factor(const PoissonDev &P, cudaStream_t s) {
+  if (P.nsys == 0) return cudaSuccess;
+  const size_t smem = (size_t)2 * P.max_nrad * kW * sizeof(double);
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(radial_factor_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  radial_factor_kernel<<<P.nsys, 32, smem, s>>>(P);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_poisson_radial(const PoissonDev &P, cudaStream_t s) {

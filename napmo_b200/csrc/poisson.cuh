@@ -34,6 +34,7 @@ struct EvalItem {
   int atom, bucket, start, count;
 };
 constexpr int kEvalChunk = 128;
+constexpr int kEvalPerThread = 2;  // pairs evaluated by one thread
 
 // Radial table slots (each nrad long, at rad_off + slot * nrad).
 enum : int {
@@ -47,6 +48,10 @@ enum : int {
   kRadUp = 7,     // Thomas-algorithm modified super-diagonal
   kRadSlots = 8,
 };
+
+// Band of the 2n x 2n radial FEM matrix: kl = ku = 3; fill-in from partial
+// pivoting reaches kl + ku above the diagonal, kW stored diagonals.
+constexpr int kKL = 3, kKU = 3, kW = 2 * kKL + kKU + 1;
 
 struct PoissonDev {
   int natom = 0, nmol = 0, nsys = 0;
@@ -63,6 +68,13 @@ struct PoissonDev {
   double *amp = nullptr;
   double *raw_y = nullptr;
   double *raw_dt = nullptr;
+  // LU factors of the radial FEM systems (built once per grid): per system
+  // the band [2 nrad][kW], multipliers [2 nrad][3], pivots [2 nrad]; strides
+  // use lu_stride = 2 max_nrad rows
+  double *lu = nullptr;
+  double *lmul = nullptr;
+  int *lpiv = nullptr;
+  int lu_stride = 0;
   // bucketed evaluation (built once per grid): for every atom the points of
   // its molecule sorted by spline interval, and a partial potential per pair
   long npair = 0;
@@ -80,6 +92,8 @@ cudaError_t poisson_init_constants();
 cudaError_t launch_poisson_project(const PoissonDev &P, const double *rho,
                                    const double *wb, const double *w,
                                    cudaStream_t s);
+// Assembles and LU-factors the radial FEM matrices (once per grid).
+cudaError_t launch_poisson_factor(const PoissonDev &P, cudaStream_t s);
 // projected density -> spline tables of the potential (one CTA per (atom, l)).
 cudaError_t launch_poisson_radial(const PoissonDev &P, cudaStream_t s);
 // Pair-list construction: bucket of every (atom, point) pair and the bucket

@@ -43,6 +43,10 @@ def parse():
     p.add_argument('--ncarbon', type=int, default=20)
     p.add_argument('--cpu-points', type=int, default=4096)
     p.add_argument('--no-cpu-baseline', action='store_true')
+    p.add_argument('--workload', default='c4', choices=['c4', 'c3'],
+                   help='c4: C20H42 single system (default); c3: batch of 64 random HCNO '
+                        'chains with uneven per-atom grids, one CUDA-graph launch per batch')
+    p.add_argument('--nmol', type=int, default=64)
     p.add_argument('--precision', default='auto', choices=['auto', 'fp64'],
                    help='auto: headline is the int8-slice tensor-core build when its energy '
                         'is within 1e-6 Eh of FP64 (checked in the same run), else FP64')
@@ -202,6 +206,115 @@ def cpu_baseline(args, atoms, grid, D, lmax):
             'seconds_per_build': t_build}
 
 
+# ------------------------------------------------------------ C3: batches
+def run_batch(args, world, rank):
+    """64 seeded random {H,C,N,O} chains (3-30 atoms, bonds 1.0-1.5 A),
+    cc-pVDZ, per-atom grids 50-100 x {110..590}, per-atom lmax from each
+    atom's Lebedev rule; D = 2 C C^T of rank N_el/2.  One step = the Fock
+    builds of all molecules in one CUDA-graph launch (FockBatch), FP64 and
+    int8 (autotuned launch shape)."""
+    import torch
+    import napmo_b200 as nb
+    from napmo_b200.system import build_system, random_batch
+    mols = random_batch(nmol=args.nmol, seed=SEED)
+    builders, Ds, flops, npts = [], [], 0.0, 0
+    t_setup = time.perf_counter()
+    for i, m in enumerate(mols):
+        e = build_system(m['atoms'], 'CC-PVDZ')['e-']
+        grid = nb.BeckeGrid(e, m['nrad'], m['nang'])
+        fb = nb.FockBuilder(grid, e['basis'], 'per-atom')
+        n = fb.n
+        rng = np.random.default_rng(SEED + i)
+        C = rng.normal(size=(n, max(1, e['occupation']))) / np.sqrt(n)
+        Ds.append(2.0 * C @ C.T)
+        builders.append(fb)
+        flops += 4.0 * n * n * grid.size
+        npts += grid.size
+    t_setup = time.perf_counter() - t_setup
+    stream = torch.cuda.current_stream()
+
+    def timed(batch):
+        batch.build(Ds)
+        for _ in range(args.warmup):
+            batch.build()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(torch.cuda.current_device())
+        sampler.start()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            batch.build()
+        ev1.record(stream)
+        ev1.synchronize()
+        clk = sampler.stop()
+        E = [0.5 * float((F * torch.as_tensor(D, device='cuda')).sum())
+             for F, D in zip(batch._F, Ds)]
+        return ev0.elapsed_time(ev1) / 1e3 / args.steps, clk, E
+
+    b64 = nb.FockBatch(builders)
+    cfg64 = b64.tune(reps=2)
+    t64, clk64, E64 = timed(b64)
+    del b64
+    for fb in builders:
+        fb.set_precision('int8x4')
+    b8 = nb.FockBatch(builders)
+    cfg8 = b8.tune(reps=2)
+    t8, clk8, E8 = timed(b8)
+    tc_err = builders[0].tc_status()
+    dE = [abs(a - b) for a, b in zip(E8, E64)]
+    ok = tc_err == 0 and max(dE) <= 1e-6
+    headline = 'int8x4' if ok else 'fp64'
+    t_dev = t8 if ok else t64
+    bat = b8 if ok else None
+    if not ok:
+        for fb in builders:
+            fb.set_precision('fp64')
+        bat = nb.FockBatch(builders)
+        bat.tune(reps=2)
+    # end to end: densities from pinned host memory in, every F read back
+    hostD = [torch.as_tensor(D).pin_memory() for D in Ds]
+    hostF = [torch.empty(D.shape, dtype=torch.float64).pin_memory() for D in Ds]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for dst, src in zip(bat._D, hostD):
+            dst.copy_(src, non_blocking=True)
+        bat.build()
+        for dst, src in zip(hostF, bat._F):
+            dst.copy_(src, non_blocking=True)
+        torch.cuda.synchronize()
+    t_e2e = (time.perf_counter() - t0) / args.steps
+    nb_bytes = sum(8 * D.size for D in Ds)
+    nmol = len(mols)
+    line = {
+        'metric': 'grid Fock builds/s, batch of %d random HCNO chains (C3)' % nmol,
+        'value': nmol / t_dev, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
+        'warmup': args.warmup, 'ms_per_step': t_dev * 1e3, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'int8x4' if ok else 'f64',
+        'data': 'synthetic',
+        'config': {'workload': 'C3: %d random {H,C,N,O} chains of 3-30 atoms, cc-pVDZ, '
+                               'per-atom 50-100 x {110..590} grids, per-atom lmax' % nmol,
+                   'n_points': npts, 'n_basis_range': [min(b.n for b in builders),
+                                                       max(b.n for b in builders)],
+                   'parallelism': 'one CUDA graph per batch',
+                   'l2': 'inputs larger than L2'},
+        'e2e': {'value': nmol / t_e2e, 'unit': UNIT, 'h2d_bytes_per_step': nb_bytes,
+                'd2h_bytes_per_step': nb_bytes},
+        'gpu_launches': 1,
+        'fp64': {'builds_per_s': nmol / t64, 'ms_per_batch': t64 * 1e3, 'tuned': cfg64},
+        'mixed': {'builds_per_s': nmol / t8, 'ms_per_batch': t8 * 1e3, 'tuned': cfg8,
+                  'speedup_vs_fp64': t64 / t8, 'tc_status': tc_err,
+                  'energy_error_eh_max': max(dE), 'energy_error_eh_mean': sum(dE) / nmol,
+                  'energy_error_eh_per_molecule': dE},
+        'algorithmic_tflops': flops / t_dev / 1e12,
+        'setup_s': t_setup,
+        'clocks': clk8 if ok else clk64,
+        'cpu_baseline': None,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+
+
 # --------------------------------------------------------------------- main
 def main():
     args = parse()
@@ -242,6 +355,13 @@ def main():
         dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
     import napmo_b200 as nb
     from napmo_b200 import cext
+
+    if args.workload == 'c3':
+        run_batch(args, world, rank)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
 
     atoms, ms, grid, basis, lmax, D = build_workload(args)
     n = basis['nbasis']
@@ -296,7 +416,7 @@ def main():
              'int8_image_bytes': int(cext.lib.napmo_fock_plan_int8_bytes(fbld._plan)),
              'scheme': 'int8 slices (4 balanced base-256 digits per value, group exponents), '
                        'tcgen05 kind::i8 with exact int32 TMEM accumulation; 13 digit '
-                       'products (quadrature), 10 (density); Poisson FP64'}
+                       'products per contraction; Poisson FP64'}
 
     # ---- per-kernel timings (same stream) for the roofline
     def time_it(fn, reps=3):
@@ -377,7 +497,7 @@ def main():
             achieved = flops / td / 1e12
             bound = 'tensor'
             kernel_name = dom + '_' + headline
-            nprod = 10 if dom == 'density' else 13
+            nprod = 13
             if headline == 'int8x4':
                 peak = 2.0 * float(peaks.get('bf16_tflops', 1590.0))
                 peak_source = ('int8 dense = 2 x bf16 dense burst (%s); the scheme issues %d int8 '

@@ -280,7 +280,10 @@ int napmo_gpu_quadrature_noalloc(int n, int npoint, const double *phi, const dou
 
 /* Fock-build plan: phi of `basis` on `grid` evaluated once and kept in HBM
  * with the Poisson tables of `lmax`; per build rho -> V_H -> F (the chain of
- * psi_hybrid.py:81-110 / psi_numeric.py:152-241). */
+ * psi_hybrid.py:81-110 / psi_numeric.py:152-241).  lmax >= 0: one cutoff for
+ * all atoms (nAPMO: lebedev_get_order(nang) // 2, psi_numeric.py:66); -1: no
+ * Poisson tables (quadratures only); -2: per atom, from its own Lebedev rule
+ * (grids with different angular sizes per atom). */
 void *napmo_fock_plan_new(void *grid, void *basis, int lmax, void *stream);
 void napmo_fock_plan_free(void *plan);
 int napmo_fock_plan_info(void *plan, int *n, int *npoint, long *ld, double **phi);
@@ -299,6 +302,21 @@ int napmo_fock_plan_build_host(void *plan, const double *D, double q, const doub
 int napmo_fock_plan_set_precision(void *plan, int mode);
 /* Device bytes of the plan's int8 operand images and scratch. */
 long napmo_fock_plan_int8_bytes(void *plan);
+/* Batched Fock builds of many plans (molecules of uneven size) by one CUDA
+ * graph launch; no counterpart in nAPMO (its SCF drivers loop over species,
+ * scf.py:146-273).  The batch owns a device D and F per plan
+ * (napmo_fock_batch_buffers); napmo_fock_batch_build captures the builds on
+ * first use (after one eager warm-up) and then launches the graph on `stream`.
+ * napmo_fock_batch_tune times candidate launch shapes (capture streams x
+ * CTA budget of the int8 kernels) and keeps the fastest. */
+void *napmo_fock_batch_new(void **plans, int nplan, double q);
+void napmo_fock_batch_free(void *batch);
+int napmo_fock_batch_buffers(void *batch, int i, double **D, double **F);
+int napmo_fock_batch_build(void *batch, void *stream);
+int napmo_fock_batch_tune(void *batch, void *stream, int reps, int *nstream, int *budget,
+                          double *ms);
+int napmo_fock_batch_config(void *batch, int *nstream, int *budget);
+
 /* Error word of the tensor-core kernels (0 none, 5 an mbarrier wait ran out);
  * synchronises the stream, `reset` nonzero clears it. */
 int napmo_tc_status(void *stream, int reset);

@@ -16,6 +16,6 @@ from .grids import (AngularGrid, AtomicGrid, BeckeGrid, Cell, ChebyshevRadialTra
 from .gto import BasisSet, ContractedGaussian, PrimitiveGaussian
 from .system import BOHR_TO_ANGSTROM, MolecularSystem
 from .wavefunction import WaveFunction, compute_coulomb, compute_nuclear
-from .fock import FockBuilder
+from .fock import FockBatch, FockBuilder
 
 ANGSTROM_TO_BOHR = 1.889726133921252

@@ -211,6 +211,12 @@ _SIGS = [
      [c_void_p, a2df, c_double, c_void_p, a2df, c_void_p]),
     ('napmo_fock_plan_set_precision', c_int, [c_void_p, c_int]),
     ('napmo_fock_plan_int8_bytes', c_long, [c_void_p]),
+    ('napmo_fock_batch_new', c_void_p, [c_void_p, c_int, c_double]),
+    ('napmo_fock_batch_free', None, [c_void_p]),
+    ('napmo_fock_batch_buffers', c_int, [c_void_p, c_int, c_void_p, c_void_p]),
+    ('napmo_fock_batch_build', c_int, [c_void_p, c_void_p]),
+    ('napmo_fock_batch_tune', c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    ('napmo_fock_batch_config', c_int, [c_void_p, c_void_p, c_void_p]),
     ('napmo_tc_status', c_int, [c_void_p, c_int]),
     ('napmo_gpu_quadrature_noalloc', c_int,
      [c_int, c_int, c_void_p, c_void_p, c_long, c_void_p, c_void_p, c_void_p]),

@@ -244,7 +244,9 @@ int build_pair_lists(PoissonPlan *plan, const double *x, const double *y, const 
   return kOk;
 }
 
-// Plan for one molecular grid with a common lmax, cached on the grid.
+// Plan for one molecular grid, cached on the grid: a common lmax, or with
+// lmax == kLmaxPerAtom each atom's own lebedev_precision(nang) / 2 (grids whose
+// atoms carry different Lebedev rules).
 int grid_poisson_plan(BeckeGrid *g, int lmax, cudaStream_t s, PoissonPlan **out) {
   if (g->layout.empty())
     return set_error(kNotSupported, "grid has no atomic structure (read from points)");
@@ -258,6 +260,19 @@ int grid_poisson_plan(BeckeGrid *g, int lmax, cudaStream_t s, PoissonPlan **out)
   std::vector<const AtomLayout *> atoms;
   for (auto &L : g->layout) atoms.push_back(&L);
   std::vector<int> lm(atoms.size(), lmax);
+  if (lmax == kLmaxPerAtom) {
+    for (size_t a = 0; a < atoms.size(); ++a) {
+      const int prec = lebedev_precision(atoms[a]->nang);
+      if (prec < 0) {
+        delete p;
+        return set_error(kInvalidArgument, "no Lebedev rule with this number of points");
+      }
+      lm[a] = prec / 2;
+    }
+  } else if (lmax < 0) {
+    delete p;
+    return set_error(kInvalidArgument, "lmax must be >= 0 or kLmaxPerAtom");
+  }
   int st = build_poisson_plan(atoms, lm, {0, (int)atoms.size()}, {0, g->size}, s, p);
   if (st != kOk) {
     delete p;

@@ -90,6 +90,28 @@ int plan_quadrature(FockPlan *p, double *F, cudaStream_t s) {
   return kOk;
 }
 
+// The build chain of napmo_fock_plan_build (stream-ordered, no host
+// synchronisation, no allocation once the grid's Poisson plan exists).
+int fock_build(FockPlan *p, const double *D_dev, double q, const double *vext_dev, double *F_dev,
+               double *rho_out, double *v_out, cudaStream_t s) {
+  BeckeGrid *g = p->grid;
+  double *rho = rho_out ? rho_out : p->rho.p;
+  double *v = v_out ? v_out : p->v.p;
+  int e = plan_density(p, D_dev, rho, s);
+  if (e) return e;
+  PoissonPlan *pp = nullptr;
+  e = grid_poisson_plan(g, p->lmax, s, &pp);
+  if (e) return e;
+  e = run_poisson(g, pp, rho, v, false, s);
+  if (e) return e;
+  NAPMO_TRY_CUDA(launch_combine_weights(g->size, g->dev.wb, g->dev.w, q, v, vext_dev, p->wv.p, s),
+                 "weights");
+  return plan_quadrature(p, F_dev, s);
+}
+
+int fock_plan_nbasis(const FockPlan *p) { return p->n; }
+Int8Plan *fock_plan_int8(FockPlan *p) { return p->mode == 1 ? p->i8 : nullptr; }
+
 }  // namespace napmo
 
 using namespace napmo;
@@ -231,7 +253,7 @@ FockPlan *napmo_fock_plan_new(BeckeGrid *grid, BasisSet *basis, int lmax, void *
     NAPMO_TRY_CUDA(p->work.alloc(quadrature_workspace_bytes(p->n, grid->size) / 8 + 1), "alloc");
     NAPMO_TRY_CUDA(p->D.alloc((size_t)p->n * p->n), "alloc");
     NAPMO_TRY_CUDA(p->F.alloc((size_t)p->n * p->n), "alloc");
-    if (lmax >= 0) {
+    if (lmax >= 0 || lmax == kLmaxPerAtom) {
       PoissonPlan *pp = nullptr;
       e = grid_poisson_plan(grid, lmax, s, &pp);
       if (e) return e;
@@ -283,21 +305,7 @@ int napmo_fock_plan_quadrature(FockPlan *p, double q, const double *v_dev,
 int napmo_fock_plan_build(FockPlan *p, const double *D_dev, double q, const double *vext_dev,
                           double *F_dev, double *rho_out, double *v_out, void *stream) {
   return guarded([&] {
-    cudaStream_t s = (cudaStream_t)stream;
-    BeckeGrid *g = p->grid;
-    double *rho = rho_out ? rho_out : p->rho.p;
-    double *v = v_out ? v_out : p->v.p;
-    int e = plan_density(p, D_dev, rho, s);
-    if (e) return e;
-    PoissonPlan *pp = nullptr;
-    e = grid_poisson_plan(g, p->lmax, s, &pp);
-    if (e) return e;
-    e = run_poisson(g, pp, rho, v, false, s);
-    if (e) return e;
-    NAPMO_TRY_CUDA(launch_combine_weights(g->size, g->dev.wb, g->dev.w, q, v, vext_dev,
-                                          p->wv.p, s),
-                   "weights");
-    return plan_quadrature(p, F_dev, s);
+    return fock_build(p, D_dev, q, vext_dev, F_dev, rho_out, v_out, (cudaStream_t)stream);
   });
 }
 

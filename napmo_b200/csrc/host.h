@@ -177,6 +177,9 @@ struct AtomLayout {
 
 struct PoissonPlan;  // device tables of the Poisson pipeline (capi_grid.cu)
 
+// lmax argument meaning "per atom: lebedev_precision(nang) / 2".
+constexpr int kLmaxPerAtom = -2;
+
 // The molecular grid: concatenated atomic grids plus Becke cell weights.
 struct BeckeGrid {
   int ncenter = 0;

@@ -52,6 +52,8 @@ struct Int8Plan;
 int int8_plan_create(Int8Plan **out, int n, int npoint, const double *phi, long ld,
                      const double *wb, const double *w, cudaStream_t s);
 void int8_plan_destroy(Int8Plan *p);
+// CTA budget the int8 kernels are sized for (<= 0: the SM count).
+int int8_set_budget(Int8Plan *p, int ctas);
 size_t int8_plan_device_bytes(const Int8Plan *p);
 int int8_density(Int8Plan *p, const double *D, double *rho, cudaStream_t s);
 int int8_quadrature(Int8Plan *p, const double *phi, const double *wv, double *F,

@@ -11,16 +11,17 @@
 // and Y is written in balanced base 256 as four int8 digits
 //   Y = d0 2^24 + d1 2^16 + d2 2^8 + d3,   |d0| <= 64, -128 <= dk <= 127.
 // A product of two sliced operands keeps the digit products d_i d'_j with
-// i + j <= 4 (13 MMAs; quadrature) or i + j <= 3 (10 MMAs; density).  The
-// products of one diagonal i + j share an int32 TMEM accumulator, so the
-// accumulation is exact: besides the slicing, the only error is the dropped
-// digit products (relative 2^-37 resp. 2^-29 of the group maxima).  The drain
+// i + j <= 4.  The products of one diagonal i + j share an int32 TMEM
+// accumulator, so the accumulation is exact: besides the slicing, the only
+// error is the dropped digit products (relative 2^-37 of the group maxima).
+// D (density) gets a fifth digit, Y = rint(x 2^(38 - e)): its rounding enters
+// the energy through every element of D at once.  The drain
 // combines the diagonals in int64, converts once to FP64 and applies the group
 // exponents; FP64 partials are summed in a fixed order (deterministic).
 //
 // Quadrature weights span many decades across a block of points, so the
 // weight is split between the operands by a power of two per point:
-// A = phi 2^c(p), B = wv phi 2^-c(p), c(p) = floor(log2(wb w) / 2) (exact).
+// A = phi 2^c(p), B = wv phi 2^-c(p), c(p) = floor(log2 |wb w| / 2) (exact).
 //
 // Operand images.  Each operand lives in HBM as tiles already in the
 // no-swizzle K-major shared-memory layout of the tensor core (core matrices
@@ -51,9 +52,10 @@ namespace {
 
 constexpr int KS = 64;            // K elements per stage = bytes per row of one slice
 constexpr int NSL = 4;            // int8 slices per value
+constexpr int NSL_D = 5;          // slices of D (density), 39 bits
 constexpr int TM = 128;           // M tile (TMEM lanes)
 constexpr int QN = 96;            // quadrature N tile: 5 diagonals x 96 columns
-constexpr int DN = 128;           // density N tile: 4 diagonals x 128 columns
+constexpr int DN = 96;            // density N tile: 5 diagonals x 96 columns
 constexpr int QKB = 1024;         // quadrature exponent block (points)
 constexpr int QBLK_STAGES = QKB / KS;
 constexpr int NSTAGE = 3;
@@ -69,17 +71,18 @@ __host__ __device__ __forceinline__ int core_off(int r, int k) {
   return (r >> 3) * 512 + (k >> 4) * 128 + (r & 7) * 16 + (k & 15);
 }
 
-// Digit products (i, j) in diagonal order: (0,0) | (0,1) (1,0) | (0,2) (1,1)
-// (2,0) | (0,3) (1,2) (2,1) (3,0) | (1,3) (2,2) (3,1).  The quadrature keeps
-// the first 13 (i + j <= 4), the density the first 10 (i + j <= 3).
-constexpr int kQuadProducts = 13, kDensProducts = 10;
+// Digit products (i, j) with i + j <= 4 in diagonal order: (0,0) | (0,1) (1,0) |
+// (0,2) (1,1) (2,0) | (0,3) (1,2) (2,1) (3,0) | then diagonal 4: for the
+// quadrature (both operands 4 digits) (1,3) (2,2) (3,1), 13 products; for the
+// density (B = D with 5 digits) (0,4) (1,3) (2,2) (3,1), 14 products.
+constexpr int kQuadProducts = 13, kDensProducts = 14;
 __host__ __device__ constexpr int prod_diag(int q) {
   return q < 1 ? 0 : q < 3 ? 1 : q < 6 ? 2 : q < 10 ? 3 : 4;
 }
-__host__ __device__ constexpr int prod_i(int q) {
-  return q < 10 ? q - prod_diag(q) * (prod_diag(q) + 1) / 2 : q - 9;
+__host__ __device__ constexpr int prod_i(int q, bool b5) {
+  return q < 10 ? q - prod_diag(q) * (prod_diag(q) + 1) / 2 : (b5 ? q - 10 : q - 9);
 }
-__host__ __device__ constexpr int prod_j(int q) { return prod_diag(q) - prod_i(q); }
+__host__ __device__ constexpr int prod_j(int q, bool b5) { return prod_diag(q) - prod_i(q, b5); }
 
 // kind::i8 instruction descriptor: S32 accumulator, signed A and B, both
 // K-major, N columns, M = 128.
@@ -249,6 +252,32 @@ __device__ __forceinline__ void slice16(const double *x, double scale, uint4 *ou
   for (int s = 0; s < NSL; ++s) out[s] = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
 }
 
+// Five balanced base-256 digit slices of rint(x[i] * scale) (|.| <= 2^38;
+// |d0| <= 64), packed one byte per element.
+__device__ __forceinline__ void slice16_5(const double *x, double scale, uint4 *out) {
+  uint32_t w[5][4];
+#pragma unroll
+  for (int s = 0; s < 5; ++s)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) w[s][q] = 0u;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    long long y = __double2ll_rn(x[i] * scale);
+    int d[5];
+#pragma unroll
+    for (int k = 4; k > 0; --k) {
+      d[k] = (int)(((y + 128) & 255) - 128);
+      y = (y - d[k]) >> 8;
+    }
+    d[0] = (int)y;
+    const int q = i >> 2, sh = (i & 3) * 8;
+#pragma unroll
+    for (int s = 0; s < 5; ++s) w[s][q] |= (uint32_t)(d[s] & 255) << sh;
+  }
+#pragma unroll
+  for (int s = 0; s < 5; ++s) out[s] = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+}
+
 // signed byte b (0..3) of a word
 __device__ __forceinline__ int sbyte(uint32_t w, int b) { return ((int)(w << (24 - 8 * b))) >> 24; }
 
@@ -256,7 +285,9 @@ __device__ __forceinline__ int sbyte(uint32_t w, int b) { return ((int)(w << (24
 // (m1, m2 optional; X = 0 for row >= nrows or k >= ncols): exponent per
 // (row, block of kb columns) in e[row * nblk + b]; image tiles of TR rows x KS
 // columns, img[((row / TR) * nks + k / KS) * NSL * TR * KS + s * TR * KS +
-// core_off(row % TR, k % KS)].  Grid (rows_pad / 8, nblk), one warp per row.
+// core_off(row % TR, k % KS)] with NS slices (4: Y = rint(x 2^(30-e)); 5:
+// rint(x 2^(38-e))).  Grid (rows_pad / 8, nblk), one warp per row.
+template <int NS>
 __global__ void __launch_bounds__(256)
 slice_rows_kernel(const double *__restrict__ src, long ld, int nrows, int ncols,
                   const double *__restrict__ m1, const double *__restrict__ m2, int kb, int nblk,
@@ -322,18 +353,21 @@ slice_rows_kernel(const double *__restrict__ src, long ld, int nrows, int ncols,
   for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   const int e = group_exponent(mx);
   if (lane == 0) eout[(long)row * nblk + b] = e;
-  const double scale = ldexp(1.0, 30 - e);
+  const double scale = ldexp(1.0, 8 * NS - 2 - e);
   const int rt = row / TR, r = row % TR;
-  const long tile = (long)NSL * TR * KS;
+  const long tile = (long)NS * TR * KS;
   for (int c = lane; c < nchunk; c += 32) {
     double x[16];
     load(c, x);
-    uint4 d[NSL];
-    slice16(x, scale, d);
+    uint4 d[NS];
+    if (NS == 5)
+      slice16_5(x, scale, d);
+    else
+      slice16(x, scale, d);
     const long k = k0 + (long)c * 16;
     int8_t *base = img + ((long)rt * nks + k / KS) * tile + core_off(r, (int)(k % KS));
 #pragma unroll
-    for (int s = 0; s < NSL; ++s)
+    for (int s = 0; s < NS; ++s)
       *reinterpret_cast<uint4 *>(base + (long)s * TR * KS) = d[s];
   }
 }
@@ -371,14 +405,15 @@ slice_points_kernel(const double *__restrict__ phi, long ld, int n, int npoint, 
   }
 }
 
-// sc[p] = 2^c(p), isc[p] = 2^-c(p), c(p) = floor(log2(wb w) / 2) (0 where the
-// weight is not positive).
+// sc[p] = 2^c(p), isc[p] = 2^-c(p), c(p) = floor(log2 |wb w| / 2) (0 where the
+// weight is zero).  Some Lebedev rules have negative weights: the magnitude is
+// split, the sign stays with wv.
 __global__ void balance_kernel(int npoint, const double *__restrict__ wb,
                                const double *__restrict__ w, double *__restrict__ sc,
                                double *__restrict__ isc) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npoint) return;
-  const double t = wb[p] * w[p];
+  const double t = fabs(wb[p] * w[p]);
   int c = 0;
   if (t > 0.0 && t < 1e300) {
     int ex;
@@ -481,15 +516,15 @@ scale_image_kernel(const int8_t *__restrict__ qa, int8_t *__restrict__ qb,
 // 2 K32 steps of one 64-wide stage: the kept digit products into their
 // diagonal accumulators (column offset diagonal * N).  `fresh`: first stage
 // of an accumulation, the first product of each diagonal overwrites.
-template <int N, int NP>
+template <int N, int NP, bool B5>
 __device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t sa, uint32_t sb, bool fresh) {
   constexpr uint32_t idesc = idesc_i8(N);
 #pragma unroll
   for (int kk = 0; kk < KS / 32; ++kk) {
 #pragma unroll
     for (int q = 0; q < NP; ++q) {
-      const uint64_t ad = smem_desc(sa + prod_i(q) * (TM * KS) + kk * 32 * 8);
-      const uint64_t bd = smem_desc(sb + prod_j(q) * (N * KS) + kk * 32 * 8);
+      const uint64_t ad = smem_desc(sa + prod_i(q, B5) * (TM * KS) + kk * 32 * 8);
+      const uint64_t bd = smem_desc(sb + prod_j(q, B5) * (N * KS) + kk * 32 * 8);
       const bool first = fresh && kk == 0 && (q == 0 || prod_diag(q) != prod_diag(q - 1));
       umma_i8(tmem + (uint32_t)(prod_diag(q) * N), ad, bd, idesc, first ? 0u : 1u);
     }
@@ -610,7 +645,7 @@ __global__ void __launch_bounds__(NTHR, 1) quad_i8_kernel(QuadArgs g) {
           }
           fence_after_sync();
           const uint32_t sa = smem_u32(smem + slot * STAGE);
-          issue_stage<QN, kQuadProducts>(tmem, sa, sa + A_BYTES, st == 0);
+          issue_stage<QN, kQuadProducts, false>(tmem, sa, sa + A_BYTES, st == 0);
           umma_commit(&empty[slot]);
         }
         if (ok) umma_commit(&accfull);
@@ -694,23 +729,23 @@ __global__ void quad_i8_reduce_kernel(int n, int nchunk, int npair, int ntj,
 struct DensArgs {
   const int8_t *a;        // phi^T image [point tile][nks][slices][128 x 64]
   const int *ea;          // exponent per point
-  const int8_t *d;        // D image [128-row tile][nks][slices][128 x 64]
+  const int8_t *d;        // D image [96-row tile][nks][5 slices][96 x 64]
   const int *ed;          // exponent per row of D
   int nks, nmt, npt, npoint;
   double *rho;
 };
 
 // Persistent: CTA c handles point tiles c, c + gridDim.x, ...  Pass (tile,
-// m): T[p][mu] = sum_nu phi[nu][p] D[mu][nu] for the 128 points and the 128
+// m): T[p][mu] = sum_nu phi[nu][p] D[mu][nu] for the 128 points and the 96
 // functions of block m, accumulated over all nu in TMEM; the drain adds
-// phi[mu][p] T[p][mu] into rho[p] (thread = point, 64 functions each).
+// phi[mu][p] T[p][mu] into rho[p] (thread = point, 48 functions each).
 __global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ __align__(8) uint64_t full[NSTAGE], empty[NSTAGE], accfull, accempty, done;
   __shared__ uint32_t tmem_sh;
   __shared__ int abort_sh, flag_sh;
   __shared__ double red[2][TM];
-  constexpr uint32_t A_BYTES = stage_bytes(TM), B_BYTES = stage_bytes(DN);
+  constexpr uint32_t A_BYTES = stage_bytes(TM), B_BYTES = NSL_D * DN * KS;
   constexpr uint32_t STAGE = A_BYTES + B_BYTES;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   volatile int *abort = &abort_sh;
@@ -777,7 +812,7 @@ __global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
             }
             fence_after_sync();
             const uint32_t sa = smem_u32(smem + slot * STAGE);
-            issue_stage<DN, kDensProducts>(tmem, sa, sa + A_BYTES, ks == 0);
+            issue_stage<DN, kDensProducts, true>(tmem, sa, sa + A_BYTES, ks == 0);
             umma_commit(&empty[slot]);
           }
           if (ok) umma_commit(&accfull);
@@ -799,30 +834,30 @@ __global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
           break;
         }
         fence_after_sync();
-        const int ksm = 2 * m + h;  // stage of phi^T holding functions 64 (2m + h) ..
-        const bool has = ksm < g.nks;
-        const int8_t *pa =
-            g.a + ((long)pt * g.nks + (has ? ksm : 0)) * A_BYTES + core_off(row, 0);
 #pragma unroll 1
-        for (int c = 0; c < 64; c += 16) {
-          int32_t v[4][16];
+        for (int c = 0; c < 48; c += 16) {
+          int32_t v[5][16];
 #pragma unroll
-          for (int dg = 0; dg < 4; ++dg) {
-            tmem_ld8(tmem + lane_off + dg * DN + 64 * h + c, v[dg]);
-            tmem_ld8(tmem + lane_off + dg * DN + 64 * h + c + 8, v[dg] + 8);
+          for (int dg = 0; dg < 5; ++dg) {
+            tmem_ld8(tmem + lane_off + dg * DN + 48 * h + c, v[dg]);
+            tmem_ld8(tmem + lane_off + dg * DN + 48 * h + c + 8, v[dg] + 8);
           }
           tmem_wait_ld();
 #pragma unroll
-          for (int dg = 0; dg < 4; ++dg) {
+          for (int dg = 0; dg < 5; ++dg) {
             tie8(v[dg]);
             tie8(v[dg] + 8);
           }
-          if (has) {
+          // functions mu0 .. mu0 + 15 lie in one 64-wide stage of phi^T
+          const int mu0 = m * DN + 48 * h + c;
+          if (mu0 < g.nks * KS) {
+            const int8_t *pa = g.a + ((long)pt * g.nks + mu0 / KS) * A_BYTES +
+                               core_off(row, mu0 % KS);
             uint4 q[NSL];
 #pragma unroll
             for (int s = 0; s < NSL; ++s)
-              q[s] = __ldg(reinterpret_cast<const uint4 *>(pa + (long)s * TM * KS + (c >> 4) * 128));
-            const int *ed = g.ed + m * DN + 64 * h + c;
+              q[s] = __ldg(reinterpret_cast<const uint4 *>(pa + (long)s * TM * KS));
+            const int *ed = g.ed + mu0;
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
               const int wq = i >> 2, b = i & 3;
@@ -831,7 +866,8 @@ __global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
               const int y = ((sbyte(w0, b) * 256 + sbyte(w1, b)) * 256 + sbyte(w2, b)) * 256 +
                             sbyte(w3, b);
               const long long comb =
-                  (((long long)v[0][i] * 256 + v[1][i]) * 256 + v[2][i]) * 256 + v[3][i];
+                  (((((long long)v[0][i] * 256 + v[1][i]) * 256 + v[2][i]) * 256 + v[3][i]) *
+                   256) + v[4][i];
               acc = fma((double)y * pow2(__ldg(ed + i)), (double)comb, acc);
             }
           }
@@ -844,7 +880,7 @@ __global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
       named_sync(1, NEPI);
       if (h == 0 && p < g.npoint) {
         const int ep = __ldg(g.ea + p);
-        g.rho[p] = (red[0][row] + red[1][row]) * pow2(ep - 33) * pow2(ep - 33);
+        g.rho[p] = (red[0][row] + red[1][row]) * pow2(ep - 37) * pow2(ep - 37);
       }
       named_sync(1, NEPI);
     }
@@ -867,12 +903,17 @@ int num_sms() {
   return sms;
 }
 
-// rows_pad: rows written (a multiple of TR; rows >= nrows get zeros)
+// rows_pad: rows written (a multiple of TR; rows >= nrows get zeros); ns
+// slices (4 or 5).
 cudaError_t launch_slice_rows(const double *src, long ld, int nrows, int rows_pad, int ncols,
                               const double *m1, const double *m2, int kb, int nblk, int TR,
-                              int nks, int8_t *img, int *e, cudaStream_t s) {
-  slice_rows_kernel<<<dim3(rows_pad / 8, nblk), 256, 0, s>>>(src, ld, nrows, ncols, m1, m2, kb,
-                                                               nblk, TR, nks, img, e);
+                              int nks, int8_t *img, int *e, cudaStream_t s, int ns = NSL) {
+  if (ns == 5)
+    slice_rows_kernel<5><<<dim3(rows_pad / 8, nblk), 256, 0, s>>>(src, ld, nrows, ncols, m1, m2,
+                                                                  kb, nblk, TR, nks, img, e);
+  else
+    slice_rows_kernel<4><<<dim3(rows_pad / 8, nblk), 256, 0, s>>>(src, ld, nrows, ncols, m1, m2,
+                                                                  kb, nblk, TR, nks, img, e);
   return cudaGetLastError();
 }
 
@@ -887,10 +928,38 @@ struct Int8Plan {
   int nblk = 0, nks_q = 0, nti = 0, ntj = 0, nimg = 0, npair = 0, nchunk = 0, bpc = 0;
   // density
   int npt = 0, nks_d = 0, nmt = 0;
+  int budget = 0;  // CTAs the kernels are sized for (the SM count by default)
   DevBuf<int8_t> qa, qb, da, dd;
   DevBuf<int> qa_e, qb_e, eg, da_e, dd_e;
   DevBuf<double> sc, isc, gs, work;
 };
+
+// Sizes the kernels for `ctas` resident CTAs (<= 0: the SM count): the
+// quadrature's chunks of point blocks minimise waves x blocks per chunk, the
+// persistent density kernel runs min(point tiles, ctas) CTAs.  A smaller
+// budget lets kernels of several plans share the GPU.
+int int8_set_budget(Int8Plan *p, int ctas) {
+  const int sms = ctas > 0 ? ctas : num_sms();
+  long best = -1;
+  int bpc_best = p->nblk, nchunk_best = 1;
+  for (int nc = 1; nc <= p->nblk && nc <= 64; ++nc) {
+    const int bpc = (p->nblk + nc - 1) / nc;
+    const int used = (p->nblk + bpc - 1) / bpc;
+    const long waves = ((long)p->npair * used + sms - 1) / sms;
+    const long cost = waves * bpc;
+    if (best < 0 || cost < best) {
+      best = cost;
+      bpc_best = bpc;
+      nchunk_best = used;
+    }
+  }
+  const size_t need = (size_t)nchunk_best * p->npair * TM * QN;
+  if (need > p->work.n) NAPMO_TRY_CUDA(p->work.alloc(need), "alloc int8 workspace");
+  p->bpc = bpc_best;
+  p->nchunk = nchunk_best;
+  p->budget = sms;
+  return kOk;
+}
 
 int int8_plan_create(Int8Plan **out, int n, int npoint, const double *phi, long ld,
                      const double *wb, const double *w, cudaStream_t s) {
@@ -908,24 +977,10 @@ int int8_plan_create(Int8Plan **out, int n, int npoint, const double *phi, long 
   p->nimg = max(p->nti, (p->ntj * QN + TM - 1) / TM);
   p->npair = 0;
   for (int i = 0; i < p->nti; ++i) p->npair += p->ntj - (4 * i) / 3;
-  // chunks of point blocks: fewest (waves x blocks per chunk) at one CTA per SM
-  const int sms = num_sms();
-  long best = -1;
-  for (int nc = 1; nc <= p->nblk && nc <= 64; ++nc) {
-    const int bpc = (p->nblk + nc - 1) / nc;
-    const int used = (p->nblk + bpc - 1) / bpc;
-    const long waves = ((long)p->npair * used + sms - 1) / sms;
-    const long cost = waves * bpc;
-    if (best < 0 || cost < best) {
-      best = cost;
-      p->bpc = bpc;
-      p->nchunk = used;
-    }
-  }
   p->npt = (int)(padded_points(npoint) / TM);
   const int npad64 = (n + KS - 1) / KS * KS;
   p->nks_d = npad64 / KS;
-  p->nmt = (n + TM - 1) / TM;
+  p->nmt = (n + DN - 1) / DN;
 
   NAPMO_TRY_CUDA(p->sc.alloc(npoint), "alloc int8 scales");
   NAPMO_TRY_CUDA(p->isc.alloc(npoint), "alloc int8 scales");
@@ -940,10 +995,11 @@ int int8_plan_create(Int8Plan **out, int n, int npoint, const double *phi, long 
   NAPMO_TRY_CUDA(p->gs.alloc((size_t)p->nblk * QKB), "alloc");
   NAPMO_TRY_CUDA(p->da.alloc((size_t)p->npt * p->nks_d * stage_bytes(TM)), "alloc int8 phi^T image");
   NAPMO_TRY_CUDA(p->da_e.alloc((size_t)p->npt * TM), "alloc");
-  NAPMO_TRY_CUDA(p->dd.alloc((size_t)p->nmt * p->nks_d * stage_bytes(TM)), "alloc int8 D image");
-  NAPMO_TRY_CUDA(p->dd_e.alloc((size_t)p->nmt * TM), "alloc");
-  NAPMO_TRY_CUDA(p->work.alloc((size_t)p->nchunk * p->npair * TM * QN), "alloc int8 workspace");
+  NAPMO_TRY_CUDA(p->dd.alloc((size_t)p->nmt * p->nks_d * NSL_D * DN * KS), "alloc int8 D image");
+  NAPMO_TRY_CUDA(p->dd_e.alloc((size_t)p->nmt * DN), "alloc");
 
+  int e = int8_set_budget(p.get(), 0);
+  if (e) return e;
   balance_kernel<<<(npoint + 255) / 256, 256, 0, s>>>(npoint, wb, w, p->sc.p, p->isc.p);
   NAPMO_TRY_CUDA(cudaGetLastError(), "balance");
   NAPMO_TRY_CUDA(launch_slice_rows(phi, ld, n, p->nimg * TM, npoint, p->sc.p, nullptr, QKB,
@@ -964,15 +1020,15 @@ size_t int8_plan_device_bytes(const Int8Plan *p) {
 }
 
 int int8_density(Int8Plan *p, const double *D, double *rho, cudaStream_t s) {
-  NAPMO_TRY_CUDA(launch_slice_rows(D, p->n, p->n, p->nmt * TM, p->n, nullptr, nullptr,
-                                   p->nks_d * KS, 1, TM, p->nks_d, p->dd.p, p->dd_e.p, s),
+  NAPMO_TRY_CUDA(launch_slice_rows(D, p->n, p->n, p->nmt * DN, p->n, nullptr, nullptr,
+                                   p->nks_d * KS, 1, DN, p->nks_d, p->dd.p, p->dd_e.p, s, NSL_D),
                  "slice D");
   DensArgs g{p->da.p, p->da_e.p, p->dd.p, p->dd_e.p, p->nks_d, p->nmt, p->npt, p->npoint, rho};
-  const int smem = NSTAGE * (stage_bytes(TM) + stage_bytes(DN));
+  const int smem = NSTAGE * (stage_bytes(TM) + NSL_D * DN * KS);
   NAPMO_TRY_CUDA(cudaFuncSetAttribute(density_i8_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                  "density_i8 smem");
-  const int grid = p->npt < num_sms() ? p->npt : num_sms();
+  const int grid = p->npt < p->budget ? p->npt : p->budget;
   density_i8_kernel<<<grid, NTHR, smem, s>>>(g);
   NAPMO_TRY_CUDA(cudaGetLastError(), "density_i8");
   return kOk;

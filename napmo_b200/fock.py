@@ -12,7 +12,7 @@ libnapmo's kernels.  Reference call stack: napmo/wavefunction/psi_hybrid.py:
 81-110 (coupling), napmo/wavefunction/ntwobody.py:15-46 (Coulomb potential),
 src/wavefunction/nwavefunction.cpp:77-107,161-197 (quadratures).
 """
-from ctypes import byref, c_int, c_long, c_void_p
+from ctypes import byref, c_double, c_int, c_long, c_void_p
 
 import numpy as np
 
@@ -37,8 +37,9 @@ class FockBuilder(object):
     Args:
         grid (BeckeGrid): molecular grid (Becke weights already on device).
         basis (BasisSet): basis of the species.
-        lmax (int): angular cutoff of the Poisson expansion; nAPMO uses
-            lebedev_get_order(nang) // 2 (psi_numeric.py:66).  Negative: no
+        lmax (int or 'per-atom'): angular cutoff of the Poisson expansion;
+            nAPMO uses lebedev_get_order(nang) // 2 (psi_numeric.py:66).
+            'per-atom': each atom's own Lebedev rule (uneven grids).  -1: no
             Poisson tables (quadratures only).
     """
 
@@ -49,7 +50,7 @@ class FockBuilder(object):
         self.torch = torch
         self.grid = grid
         self.basis = basis
-        self.lmax = int(lmax)
+        self.lmax = -2 if lmax == 'per-atom' else int(lmax)
         self._plan = cext.lib.napmo_fock_plan_new(grid._this, basis._this, self.lmax,
                                                   _stream(torch, stream))
         if not self._plan:
@@ -158,3 +159,68 @@ def _view(torch, ptr, shape):
             'shape': (n,), 'typestr': '<f8', 'data': (ptr, False), 'version': 2}
 
     return torch.as_tensor(_Holder(), device='cuda').view(*shape)
+
+
+class FockBatch(object):
+    """Grid Fock builds of many molecules (FockBuilders of uneven grid and
+    basis sizes) in one CUDA-graph launch.
+
+    The batch owns a device D and F per molecule (``D(i)``, ``F(i)`` torch
+    views).  ``build(Ds)`` copies the densities in (optional) and launches the
+    graph; ``tune()`` runs the library's autotuner over launch shapes.
+
+    Args:
+        builders (list of FockBuilder): one per molecule (kept alive here).
+        q (float): charge applied to every potential.
+    """
+
+    def __init__(self, builders, q=1.0):
+        torch = _torch()
+        self.torch = torch
+        self.builders = list(builders)
+        arr = (c_void_p * len(self.builders))(*[b._plan for b in self.builders])
+        self._this = cext.lib.napmo_fock_batch_new(arr, len(self.builders), float(q))
+        if not self._this:
+            cext.check()
+            raise NapmoError('batch construction failed')
+        self._D, self._F = [], []
+        for i, b in enumerate(self.builders):
+            dp, fp = c_void_p(), c_void_p()
+            checked(cext.lib.napmo_fock_batch_buffers(self._this, i, byref(dp), byref(fp)))
+            self._D.append(_view(torch, dp.value, (b.n, b.n)))
+            self._F.append(_view(torch, fp.value, (b.n, b.n)))
+
+    def __len__(self):
+        return len(self.builders)
+
+    def D(self, i):
+        return self._D[i]
+
+    def F(self, i):
+        return self._F[i]
+
+    def build(self, Ds=None, stream=None):
+        """Copies Ds (optional list of n x n arrays) into the batch and builds
+        every molecule; returns the list of F views (valid until the next build)."""
+        t = self.torch
+        if Ds is not None:
+            for dst, D in zip(self._D, Ds):
+                dst.copy_(t.as_tensor(D, dtype=t.float64), non_blocking=False)
+        checked(cext.lib.napmo_fock_batch_build(self._this, _stream(t, stream)))
+        return self._F
+
+    def tune(self, reps=3, stream=None):
+        """Times candidate launch shapes and keeps the fastest; returns
+        {'nstream', 'budget', 'ms'}."""
+        ns, bud, ms = c_int(), c_int(), c_double()
+        checked(cext.lib.napmo_fock_batch_tune(self._this, _stream(self.torch, stream), int(reps),
+                                               byref(ns), byref(bud), byref(ms)))
+        return {'nstream': ns.value, 'budget': bud.value, 'ms': ms.value}
+
+    def __del__(self):
+        if getattr(self, '_this', None):
+            try:
+                cext.lib.napmo_fock_batch_free(self._this)
+            except (AttributeError, TypeError):  # library already unloaded at exit
+                pass
+            self._this = None

@@ -143,3 +143,21 @@ def random_chain(rng, natom, symbols=('H', 'C', 'N', 'O')):
                 break
         if ok:
             return list(zip(syms, [tuple(p) for p in pos]))
+
+
+ANGULAR_SIZES = (110, 146, 170, 194, 230, 266, 302, 350, 434, 590)
+
+
+def random_batch(nmol=64, seed=20261203, natom=(3, 30), nrad=(50, 100), angular=ANGULAR_SIZES):
+    """Seeded batch of random {H, C, N, O} chains (random_chain) with grid
+    sizes drawn per atom: nrad uniform in [nrad[0], nrad[1]], nang from
+    ``angular``.  Returns a list of {'atoms', 'nrad', 'nang'}."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(nmol):
+        na = int(rng.integers(natom[0], natom[1] + 1))
+        atoms = random_chain(rng, na)
+        nr = [int(rng.integers(nrad[0], nrad[1] + 1)) for _ in atoms]
+        ng = [int(angular[int(rng.integers(len(angular)))]) for _ in atoms]
+        out.append({'atoms': atoms, 'nrad': nr, 'nang': ng})
+    return out

@@ -10,8 +10,8 @@ quadrature; all basis functions at one point, and one row of D, for the
 density) share e = frexp exponent of max |x| (clamped at -960); each value is
 rounded to Y = rint(x 2^(30-e)) and written in balanced base 256 as
 Y = d0 2^24 + d1 2^16 + d2 2^8 + d3.  Products keep d_i d'_j for
-i + j <= 4 (quadrature) or <= 3 (density).  The quadrature splits the weight
-by c(p) = floor(log2(wb w)/2): A = phi 2^c, B = A wv 2^-2c (from A's
+i + j <= 4.  The quadrature splits the weight
+by c(p) = floor(log2 |wb w| / 2): A = phi 2^c, B = A wv 2^-2c (from A's
 integers, see quadrature()).
 """
 import numpy as np
@@ -27,12 +27,13 @@ def group_exponent(m):
     return np.maximum(e, EMIN)
 
 
-def digits(x, e):
-    """Four balanced base-256 digits (most significant first) of
-    rint(x 2^(30-e)); e broadcasts against x."""
-    Y = np.rint(np.ldexp(np.asarray(x, np.float64), (30 - e).astype(np.int64))).astype(np.int64)
+def digits(x, e, ns=4):
+    """ns balanced base-256 digits (most significant first) of
+    rint(x 2^(8 ns - 2 - e)); e broadcasts against x."""
+    Y = np.rint(np.ldexp(np.asarray(x, np.float64),
+                         (8 * ns - 2 - e).astype(np.int64))).astype(np.int64)
     out = []
-    for _ in range(3):
+    for _ in range(ns - 1):
         d = ((Y + 128) & 255) - 128
         out.append(d)
         Y = (Y - d) >> 8
@@ -41,8 +42,9 @@ def digits(x, e):
 
 
 def balance(wb, w):
-    """sc = 2^c, isc = 2^-c with c = floor(log2(wb w) / 2) (0 for t <= 0)."""
-    t = np.asarray(wb, np.float64) * np.asarray(w, np.float64)
+    """sc = 2^c, isc = 2^-c with c = floor(log2 |wb w| / 2) (0 for t = 0;
+    Lebedev rules with negative weights keep the sign in wv)."""
+    t = np.abs(np.asarray(wb, np.float64) * np.asarray(w, np.float64))
     ex = np.frexp(t)[1].astype(np.int64)
     c = np.where((t > 0) & (t < 1e300), (ex - 1) >> 1, 0)
     c = np.clip(c, -400, 400)
@@ -101,20 +103,21 @@ def quadrature(phi, wv, wb, w, block=BLOCK):
 
 
 def density(phi, D):
-    """rho[p] = sum_{mu,nu} D[mu][nu] phi[mu][p] phi[nu][p], int8 slices,
-    i + j <= 3.  phi [n][N], D [n][n] (symmetric)."""
+    """rho[p] = sum_{mu,nu} D[mu][nu] phi[mu][p] phi[nu][p], int8 slices
+    (phi 4 digits per point, D 5 digits per row), i + j <= 4.  phi [n][N],
+    D [n][n] (symmetric)."""
     phi = np.asarray(phi, np.float64)
     D = np.asarray(D, np.float64)
     ep = group_exponent(np.abs(phi).max(axis=0))      # per point
     eD = group_exponent(np.abs(D).max(axis=1))        # per row of D
     dp = digits(phi, ep[None, :])
-    dD = digits(D, eD[:, None])
-    acc = [np.zeros(phi.shape) for _ in range(4)]     # T[mu][p] diagonals
+    dD = digits(D, eD[:, None], ns=5)                 # D: 5 digits, 2^(38-e)
+    acc = [np.zeros(phi.shape) for _ in range(5)]     # T[mu][p] diagonals
     for i in range(4):
-        for j in range(4):
-            if i + j <= 3:
+        for j in range(5):
+            if i + j <= 4:
                 acc[i + j] += dD[j].astype(np.float64) @ dp[i].astype(np.float64)
-    comb = _combine([np.rint(x).astype(np.int64) for x in acc], 4)
+    comb = _combine([np.rint(x).astype(np.int64) for x in acc], 5)
     yphi = ((dp[0] * 256 + dp[1]) * 256 + dp[2]) * 256 + dp[3]
     s = (yphi.astype(np.float64) * np.ldexp(1.0, eD)[:, None] * comb).sum(axis=0)
-    return s * np.ldexp(1.0, ep - 33) * np.ldexp(1.0, ep - 33)
+    return s * np.ldexp(1.0, ep - 37) * np.ldexp(1.0, ep - 37)

@@ -37,14 +37,15 @@ def test_digits_roundtrip():
 
 def test_balance_is_power_of_two():
     import ozaki
-    t = np.array([1e-12, 3.7e-5, 1.0, 2.0, 17.5, 0.0, -1.0])
+    t = np.array([1e-12, 3.7e-5, 1.0, 2.0, 17.5, 0.0, -1.0, -8.05e-6])
     sc, isc = ozaki.balance(t, np.ones_like(t))
     assert np.all(sc * isc == 1.0)
     assert np.all(np.frexp(sc)[0] == 0.5)
-    pos = t > 0
-    # c = floor(log2 t / 2): t / sc^2 in [1, 4)
-    r = t[pos] / sc[pos] ** 2
+    nz = t != 0
+    # c = floor(log2 |t| / 2): |t| / sc^2 in [1, 4), negative weights included
+    r = np.abs(t[nz]) / sc[nz] ** 2
     assert np.all((r >= 1.0) & (r < 4.0))
+    assert sc[t == 0][0] == 1.0
 
 
 def test_scheme_quadrature_accuracy(h2o_case):

@@ -43,7 +43,7 @@ def parse():
     p.add_argument('--ncarbon', type=int, default=20)
     p.add_argument('--cpu-points', type=int, default=4096)
     p.add_argument('--no-cpu-baseline', action='store_true')
-    p.add_argument('--workload', default='c4', choices=['c4', 'c3'],
+    p.add_argument('--workload', default='c4', choices=['c4', 'c3', 'c5'],
                    help='c4: C20H42 single system (default); c3: batch of 64 random HCNO '
                         'chains with uneven per-atom grids, one CUDA-graph launch per batch')
     p.add_argument('--nmol', type=int, default=64)
@@ -315,6 +315,101 @@ def run_batch(args, world, rank):
         print(json.dumps(line))
 
 
+# ------------------------------------------------------- C5: gradients
+def run_gradients(args, world, rank):
+    """H2O with both protons quantum (5s5p nuclear basis), 75 x 194 Becke grid
+    per centre.  For 32 seeded geometries (each coordinate perturbed uniformly
+    within +-0.05 A): for the electrons and for the protons, the grid
+    quadrature energy in the potential of the classical O nucleus, dE/dD (the
+    quadrature matrix) and dE/dR (hand-written gradient kernel).  One step =
+    the 32 geometries x 2 species; the first geometry is checked against
+    central differences (h = 1e-4 bohr)."""
+    import torch
+    from napmo_b200.gradients import GridChargeEnergy
+    from napmo_b200.system import BOHR_TO_ANGSTROM
+    sym = ['O', 'H', 'H']
+    R0 = np.array([(0.0, 0.0, 0.0), (0.0, 0.757, 0.587), (0.0, -0.757, 0.587)])
+    rng = np.random.default_rng(SEED)
+    geoms = [(R0 + rng.uniform(-0.05, 0.05, size=R0.shape)) / BOHR_TO_ANGSTROM
+             for _ in range(32)]
+    models = [GridChargeEnergy(sym, species=sp, quantum=(1, 2), nrad=75, nang=194)
+              for sp in ('e-', 'H_1')]
+    dens = {}
+    for m in models:
+        V, _ = m.quadrature_matrix(geoms[0])
+        n = V.shape[0]
+        C = np.random.default_rng(SEED + n).normal(size=(n, 5 if m.species == 'e-' else 2))
+        dens[m.species] = 2.0 * C @ C.T / n if m.species == 'e-' else C @ C.T / n
+
+    def one_pass():
+        out = []
+        for R in geoms:
+            for m in models:
+                V, st = m.quadrature_matrix(R)
+                E, g = m.gradient(st, dens[m.species])
+                out.append((E, g))
+        return out
+
+    for _ in range(max(1, args.warmup)):
+        one_pass()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        res = one_pass()
+    torch.cuda.synchronize()
+    t_step = (time.perf_counter() - t0) / args.steps
+    # gradient kernel alone (device events), first geometry
+    kern = {}
+    for m in models:
+        V, st = m.quadrature_matrix(geoms[0])
+        m.gradient(st, dens[m.species])
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(5):
+            m.gradient(st, dens[m.species])
+        ev1.record()
+        ev1.synchronize()
+        kern[m.species] = {'ms': ev0.elapsed_time(ev1) / 5, 'npoint': st['grid'].size,
+                           'nbasis': V.shape[0]}
+    # central differences, first geometry
+    fd = {}
+    h = 1e-4
+    for m in models:
+        D = dens[m.species]
+        V, st = m.quadrature_matrix(geoms[0])
+        _, g = m.gradient(st, D)
+        gf = np.zeros_like(g)
+        for a in range(3):
+            for k in range(3):
+                Rp, Rm = geoms[0].copy(), geoms[0].copy()
+                Rp[a, k] += h
+                Rm[a, k] -= h
+                Ep = float((D * m.quadrature_matrix(Rp)[0].cpu().numpy()).sum())
+                Em = float((D * m.quadrature_matrix(Rm)[0].cpu().numpy()).sum())
+                gf[a, k] = (Ep - Em) / (2 * h)
+        fd[m.species] = {'max_abs_error_eh_per_bohr': float(np.abs(g - gf).max()),
+                         'max_abs_gradient': float(np.abs(gf).max()),
+                         'net_force': float(np.abs(g.sum(axis=0)).max())}
+    nunit = len(geoms) * len(models)
+    line = {
+        'metric': 'grid energy gradients/s (H2O, both protons quantum, 75x194; C5)',
+        'value': nunit / t_step, 'unit': 'gradients/s', 'n_gpus': world, 'steps': args.steps,
+        'warmup': args.warmup, 'ms_per_step': t_step * 1e3, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+        'config': {'workload': 'C5: 32 seeded geometries (+-0.05 A) x {electrons, protons}; '
+                               'grid, basis, quadrature and gradient per geometry',
+                   'parallelism': 'single GPU'},
+        'gradient_kernel': kern,
+        'finite_differences': fd,
+        'e2e': {'value': nunit / t_step, 'unit': 'gradients/s',
+                'h2d_bytes_per_step': sum(8 * dens[m.species].size for m in models) * len(geoms),
+                'd2h_bytes_per_step': 8 * 10 * nunit},
+        'cpu_baseline': None,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+
+
 # --------------------------------------------------------------------- main
 def main():
     args = parse()
@@ -356,8 +451,8 @@ def main():
     import napmo_b200 as nb
     from napmo_b200 import cext
 
-    if args.workload == 'c3':
-        run_batch(args, world, rank)
+    if args.workload in ('c3', 'c5'):
+        (run_batch if args.workload == 'c3' else run_gradients)(args, world, rank)
         if dist:
             dist.barrier()
             dist.destroy_process_group()

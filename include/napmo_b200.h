@@ -317,6 +317,18 @@ int napmo_fock_batch_tune(void *batch, void *stream, int reps, int *nstream, int
                           double *ms);
 int napmo_fock_batch_config(void *batch, int *nstream, int *budget);
 
+/* Grid quadrature energy of one species in a point-charge potential and its
+ * nuclear-coordinate gradient (Becke weights, basis functions, grid points and
+ * charges all differentiated): E = sum_p wq wb rho_D v, v = sum_C q_C/|r-R_C|.
+ * D device [n][n]; charges host [nq][4] = x, y, z, q; outputs host: E,
+ * grad[ncenter][3] (grid centres, which carry the points and the basis
+ * shells), grad_q[nq][3] (charge positions).  dE/dD is the quadrature matrix
+ * of wq wb v (napmo_fock_plan_quadrature with vext = v).  No counterpart in
+ * nAPMO; up to 16 centres, 16 charges, 192 basis functions. */
+int napmo_grid_energy_gradient(void *grid, void *basis, const double *D, int nq,
+                               const double *charges, double *E, double *grad, double *grad_q,
+                               void *stream);
+
 /* Error word of the tensor-core kernels (0 none, 5 an mbarrier wait ran out);
  * synchronises the stream, `reset` nonzero clears it. */
 int napmo_tc_status(void *stream, int reset);

@@ -217,6 +217,8 @@ _SIGS = [
     ('napmo_fock_batch_build', c_int, [c_void_p, c_void_p]),
     ('napmo_fock_batch_tune', c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     ('napmo_fock_batch_config', c_int, [c_void_p, c_void_p, c_void_p]),
+    ('napmo_grid_energy_gradient', c_int,
+     [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ('napmo_tc_status', c_int, [c_void_p, c_int]),
     ('napmo_gpu_quadrature_noalloc', c_int,
      [c_int, c_int, c_void_p, c_void_p, c_long, c_void_p, c_void_p, c_void_p]),

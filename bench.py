@@ -43,7 +43,8 @@ def parse():
     p.add_argument('--ncarbon', type=int, default=20)
     p.add_argument('--cpu-points', type=int, default=4096)
     p.add_argument('--no-cpu-baseline', action='store_true')
-    p.add_argument('--workload', default='c4', choices=['c4', 'c3', 'c5'],
+    p.add_argument('--no-scf', action='store_true', help='skip the SCF timing of the c4 line')
+    p.add_argument('--workload', default='c4', choices=['c4', 'c3', 'c5', 'c1'],
                    help='c4: C20H42 single system (default); c3: batch of 64 random HCNO '
                         'chains with uneven per-atom grids, one CUDA-graph launch per batch')
     p.add_argument('--nmol', type=int, default=64)
@@ -410,6 +411,47 @@ def run_gradients(args, world, rank):
         print(json.dumps(line))
 
 
+# ---------------------------------------------------------- C1: grid SCF
+def run_scf_c1(args, world, rank):
+    """H2O / cc-pVDZ (O at 0, H at (0, +-0.757, 0.587) A), 50 x 110 Becke
+    grid, closed-shell SCF with J and exchange on the grid (orbital-pair
+    Poisson solves), DIIS with 6 vectors, converged to 1e-8 Eh; one step = one
+    SCF from the core guess.  FP64 and int8x4 contractions."""
+    import torch
+    from napmo_b200.scf import GridRHF
+    from napmo_b200.system import build_system
+    atoms = [('O', (0.0, 0.0, 0.0)), ('H', (0.0, 0.757, 0.587)), ('H', (0.0, -0.757, 0.587))]
+    out = {}
+    for prec in ('fp64', 'int8x4'):
+        times, res = [], None
+        for k in range(args.warmup + args.steps):
+            scf = GridRHF(build_system(atoms, 'CC-PVDZ'), 50, 110, exchange='hf',
+                          precision=prec)
+            res = scf.run(tol=1e-8)
+            if k >= args.warmup:
+                times.append(res['seconds'])
+        out[prec] = {'seconds': statistics.median(times), 'energy': res['energy'],
+                     'iterations': res['iterations'], 'converged': res['converged'],
+                     'fock_builds': res['fock_builds'], 'poisson_solves': res['poisson_solves']}
+    dE = abs(out['int8x4']['energy'] - out['fp64']['energy'])
+    head = 'int8x4' if dE <= 1e-6 and out['int8x4']['converged'] else 'fp64'
+    t = out[head]['seconds']
+    line = {'metric': 'grid RHF SCF time, H2O / cc-pVDZ 50x110 (C1)', 'value': t,
+            'unit': 's per SCF', 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': t * 1e3, 'higher_is_better': False, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'int8x4' if head == 'int8x4' else 'f64',
+            'data': 'synthetic',
+            'config': {'workload': 'C1: H2O cc-pVDZ (25 Cartesian functions), 50x110 per atom '
+                                   '(16,500 points), lmax 8, grid J and exchange, DIIS(6), 1e-8 Eh',
+                       'parallelism': 'single GPU'},
+            'scf': out, 'energy_difference_eh': dE,
+            'e2e': {'value': t, 'unit': 's per SCF', 'h2d_bytes_per_step': 0,
+                    'd2h_bytes_per_step': 8},
+            'cpu_baseline': None}
+    if rank == 0:
+        print(json.dumps(line))
+
+
 # --------------------------------------------------------------------- main
 def main():
     args = parse()
@@ -451,8 +493,8 @@ def main():
     import napmo_b200 as nb
     from napmo_b200 import cext
 
-    if args.workload in ('c3', 'c5'):
-        (run_batch if args.workload == 'c3' else run_gradients)(args, world, rank)
+    if args.workload in ('c3', 'c5', 'c1'):
+        {'c3': run_batch, 'c5': run_gradients, 'c1': run_scf_c1}[args.workload](args, world, rank)
         if dist:
             dist.barrier()
             dist.destroy_process_group()
@@ -562,6 +604,21 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_e2e = t.item()
 
+    # ---- SCF of C20H42 (Slater exchange on the grid; J by the same Fock builds)
+    scf = None
+    if not args.no_scf:
+        from napmo_b200.scf import GridRHF
+        scf = {}
+        for prec in ('fp64', 'int8x4'):
+            run = GridRHF(ms, args.nrad, args.nang, lmax=lmax, exchange='lda-x', precision=prec)
+            res = run.run(tol=1e-7)
+            scf[prec] = {'seconds': res['seconds'], 'energy': res['energy'],
+                         'iterations': res['iterations'], 'converged': res['converged'],
+                         'fock_builds': res['fock_builds']}
+            del run
+        scf['energy_difference_eh'] = abs(scf['int8x4']['energy'] - scf['fp64']['energy'])
+        scf['model'] = 'closed-shell SCF, J and Slater exchange on the grid, DIIS(6), 1e-7 Eh'
+
     if rank == 0:
         peaks, peak_kind = measured_peaks()
         fp64 = fp64_gemm_peak(torch)
@@ -629,6 +686,7 @@ def main():
                      'ms_per_build': t_f64 / args.steps * 1e3, 'fp64_gemm_tflops': fp64},
             'mixed': mixed,
             'kernels': kernels,
+            'scf': scf,
             'clocks': clocks,
             'cpu_baseline': cb,
         }

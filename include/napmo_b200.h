@@ -329,6 +329,10 @@ int napmo_grid_energy_gradient(void *grid, void *basis, const double *D, int nq,
                                const double *charges, double *E, double *grad, double *grad_q,
                                void *stream);
 
+/* Analytic overlap and kinetic-energy matrices (host, [n][n]) of a basis
+ * (Obara-Saika); nAPMO obtains them from libint (libint_iface.cpp:136-190). */
+int napmo_basis_one_body(void *basis, double *S, double *T);
+
 /* Error word of the tensor-core kernels (0 none, 5 an mbarrier wait ran out);
  * synchronises the stream, `reset` nonzero clears it. */
 int napmo_tc_status(void *stream, int reset);

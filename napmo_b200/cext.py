@@ -217,6 +217,7 @@ _SIGS = [
     ('napmo_fock_batch_build', c_int, [c_void_p, c_void_p]),
     ('napmo_fock_batch_tune', c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     ('napmo_fock_batch_config', c_int, [c_void_p, c_void_p, c_void_p]),
+    ('napmo_basis_one_body', c_int, [c_void_p, a2df, a2df]),
     ('napmo_grid_energy_gradient', c_int,
      [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ('napmo_tc_status', c_int, [c_void_p, c_int]),

@@ -240,4 +240,14 @@ int napmo_gpu_basis_values(BasisSet *b, int npoint, const double *x, const doubl
   });
 }
 
+// Overlap and kinetic-energy matrices (host out, [n][n] row-major) of the
+// normalised contracted basis, analytic (Obara-Saika); nAPMO takes them from
+// libint (libint_iface.cpp:136-190), not available here.
+int napmo_basis_one_body(BasisSet *b, double *S, double *T) {
+  return guarded([&] {
+    one_body_matrices(b->cont, S, T);
+    return kOk;
+  });
+}
+
 }  // extern "C"

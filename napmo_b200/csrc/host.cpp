@@ -326,6 +326,67 @@ double overlap_primitive(const PrimitiveGaussian &a, const PrimitiveGaussian &b)
   return pre * S1[0] * S1[1] * S1[2];
 }
 
+// Overlap and kinetic energy of two Cartesian primitives (coefficients and
+// primitive norms included).  The 1D Obara-Saika overlaps E[i][j] are built up
+// to la + 1, lb + 1; per axis the kinetic term is
+//   t(i, j) = 1/2 <d/dx a|d/dx b> = 1/2 [ i j E(i-1, j-1) - 2 zb i E(i-1, j+1)
+//                                       - 2 za j E(i+1, j-1) + 4 za zb E(i+1, j+1) ]
+// and T = tx Sy Sz + Sx ty Sz + Sx Sy tz.
+void one_body_primitive(const PrimitiveGaussian &a, const PrimitiveGaussian &b, double *S,
+                        double *T) {
+  const double p = a.zeta + b.zeta;
+  const double pinv = 1.0 / p;
+  double AB2 = 0.0, S1[3], T1[3];
+  for (int d = 0; d < 3; ++d) {
+    const double AB = a.origin[d] - b.origin[d];
+    const double P = (a.zeta * a.origin[d] + b.zeta * b.origin[d]) * pinv;
+    const double PA = P - a.origin[d], PB = P - b.origin[d];
+    AB2 += AB * AB;
+    const int la = a.l[d] + 1, lb = b.l[d] + 1;
+    double E[17][17];
+    const double h = 0.5 * pinv;
+    E[0][0] = 1.0;
+    for (int j = 0; j < lb; ++j)
+      E[0][j + 1] = PB * E[0][j] + (j > 0 ? j * h * E[0][j - 1] : 0.0);
+    for (int i = 0; i < la; ++i)
+      for (int j = 0; j <= lb; ++j) {
+        double v = PA * E[i][j];
+        if (i > 0) v += i * h * E[i - 1][j];
+        if (j > 0) v += j * h * E[i][j - 1];
+        E[i + 1][j] = v;
+      }
+    const int i = a.l[d], j = b.l[d];
+    S1[d] = E[i][j];
+    double t = 4.0 * a.zeta * b.zeta * E[i + 1][j + 1];
+    if (i > 0 && j > 0) t += i * j * E[i - 1][j - 1];
+    if (i > 0) t -= 2.0 * b.zeta * i * E[i - 1][j + 1];
+    if (j > 0) t -= 2.0 * a.zeta * j * E[i + 1][j - 1];
+    T1[d] = 0.5 * t;
+  }
+  const double pre = exp(-a.zeta * b.zeta * AB2 * pinv) *
+                     (sqrt(M_PI * pinv) * M_PI * pinv * a.coeff * b.coeff * a.norma * b.norma);
+  *S = pre * S1[0] * S1[1] * S1[2];
+  *T = pre * (T1[0] * S1[1] * S1[2] + S1[0] * T1[1] * S1[2] + S1[0] * S1[1] * T1[2]);
+}
+
+void one_body_matrices(const std::vector<ContractedGaussian> &cont, double *S, double *T) {
+  const size_t n = cont.size();
+  for (size_t m = 0; m < n; ++m)
+    for (size_t k = 0; k <= m; ++k) {
+      double s = 0.0, t = 0.0;
+      for (const auto &pa : cont[m].prim)
+        for (const auto &pb : cont[k].prim) {
+          double ps, pt;
+          one_body_primitive(pa, pb, &ps, &pt);
+          s += ps;
+          t += pt;
+        }
+      const double nn = cont[m].norma * cont[k].norma;
+      S[m * n + k] = S[k * n + m] = s * nn;
+      T[m * n + k] = T[k * n + m] = t * nn;
+    }
+}
+
 ContractedGaussian::ContractedGaussian(PrimitiveGaussian **p, int n) {
   for (int i = 0; i < 3; ++i) {
     origin[i] = p[0]->origin[i];

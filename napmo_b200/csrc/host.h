@@ -205,6 +205,10 @@ struct PrimitiveGaussian {
 };
 
 double overlap_primitive(const PrimitiveGaussian &a, const PrimitiveGaussian &b);
+// Overlap and kinetic-energy integrals of two primitives, and the normalised
+// contracted matrices S, T [n][n] of a basis.
+void one_body_primitive(const PrimitiveGaussian &a, const PrimitiveGaussian &b, double *S,
+                        double *T);
 
 struct ContractedGaussian {
   int l[3];
@@ -222,6 +226,8 @@ struct BasisSet {
   bool dev_valid = false;
   ~BasisSet();
 };
+
+void one_body_matrices(const std::vector<ContractedGaussian> &cont, double *S, double *T);
 
 // Packs a list of contracted functions into shells for the device kernels.
 void pack_basis(const std::vector<ContractedGaussian> &cont, HostBasisPack *out);

@@ -1,0 +1,188 @@
+"""Grid-based closed-shell SCF of the electrons on the device.
+
+The SCF loop of nAPMO's drivers (scf.py:80-144 single, 275-338 nsingle;
+convergence.py:35-65; wavefunction.cpp:64-116) on top of the grid Fock build:
+
+  H = T + V_ne: T and S analytic (napmo_basis_one_body; nAPMO takes them from
+      libint), V_ne = phi diag(wb w v_ne) phi^T on the grid (nnuclear.py:15-37)
+  per iteration, on the device:
+      rho = diag(phi^T D phi), v_H = Poisson(rho)      (the hot path)
+      J = phi diag(wb w v_H) phi^T
+      exchange 'hf':    K_mu,nu = sum_i sum_p W phi_mu psi_i V[psi_i phi_nu]
+                        (orbital-pair Poisson solves, as psi_numeric.py:186-215
+                        does in the orbital basis; small systems)
+               'lda-x': Slater exchange v_x = -(3 rho / pi)^(1/3) folded into
+                        the quadrature (any size)
+               'none':  Hartree
+      F = H + J - K (or H + J + V_x), Pulay DIIS on FDS - SDF (6 vectors),
+      F C = S C e by the generalised eigensolver, D = 2 C_occ C_occ^T.
+
+The contractions rho and F run in the plan's precision ('fp64' or 'int8x4');
+Poisson, DIIS and the diagonalisation are FP64 in both.
+"""
+import time
+
+import numpy as np
+
+from . import cext
+from .cext import checked
+from .fock import FockBuilder, _torch
+from .grids import BeckeGrid, lebedev_get_order
+
+CX = -(3.0 / np.pi) ** (1.0 / 3.0)          # Slater: v_x = CX rho^(1/3)
+EX = 0.75 * CX                              # e_x = EX rho^(4/3)
+
+
+def nuclear_repulsion(point_charges):
+    E = 0.0
+    for i, a in enumerate(point_charges):
+        for b in point_charges[:i]:
+            d = np.linalg.norm(np.asarray(a['origin']) - np.asarray(b['origin']))
+            E += a['atomic_number'] * b['atomic_number'] / d
+    return E
+
+
+class GridRHF(object):
+    """Closed-shell SCF of the electrons of a MolecularSystem on its Becke grid.
+
+    Args:
+        ms: MolecularSystem (all nuclei classical).
+        nrad, nang: grid per atom (lists allowed).
+        exchange: 'hf', 'lda-x' or 'none'.
+        precision: 'fp64' or 'int8x4' for rho and the quadratures.
+        diis: number of DIIS vectors.
+    """
+
+    def __init__(self, ms, nrad=50, nang=110, lmax=None, exchange='hf', precision='fp64',
+                 diis=6):
+        torch = _torch()
+        self.torch = torch
+        e = ms['e-']
+        self.ms = ms
+        self.grid = BeckeGrid(e, nrad, nang)
+        if lmax is None:
+            lmax = 'per-atom' if isinstance(nang, (list, tuple)) else lebedev_get_order(nang) // 2
+        self.fb = FockBuilder(self.grid, e['basis'], lmax)
+        n, N = self.fb.n, self.grid.size
+        self.n, self.N = n, N
+        self.nocc = int(e['occupation'])
+        S = np.zeros((n, n))
+        T = np.zeros((n, n))
+        checked(cext.lib.napmo_basis_one_body(e['basis']._this, S, T))
+        dev = dict(device='cuda', dtype=torch.float64)
+        self.S = torch.as_tensor(S, **dev)
+        self.T = torch.as_tensor(T, **dev)
+        q = np.array([[*pc['origin'], pc['atomic_number']] for pc in ms.point_charges],
+                     dtype=np.float64).reshape(-1, 4)
+        x, y, z, _, _ = self.grid.device_arrays()
+        vne = torch.empty(N, **dev)
+        checked(cext.lib.napmo_gpu_nuclear_potential(N, x, y, z, q.shape[0],
+                                                     np.ascontiguousarray(q), vne.data_ptr(),
+                                                     torch.cuda.current_stream().cuda_stream))
+        self.V = self.fb.quadrature(-1.0, vne)          # FP64: built before any precision switch
+        self.H = self.T + self.V
+        self.Enn = nuclear_repulsion(ms.point_charges)
+        self.W = torch.as_tensor(self.grid.becke_weights * self.grid.weights, **dev)
+        self.exchange = exchange
+        self.ndiis = int(diis)
+        self.precision = precision
+        self.fb.set_precision(precision)
+        s, U = torch.linalg.eigh(self.S)
+        self.X = U @ torch.diag(s.rsqrt()) @ U.T          # S^-1/2
+        self.fock_builds = 0
+        self.poisson_solves = 0
+
+    # ------------------------------------------------------------ pieces
+    def _phi(self):
+        return self.fb.phi()[:, :self.N]
+
+    def exchange_matrix(self, Cocc):
+        """K_mu,nu = sum_i sum_p W phi_mu psi_i V[psi_i phi_nu] (symmetrised)."""
+        t = self.torch
+        phi = self._phi()
+        psi = Cocc.T @ phi                                  # nocc x N
+        K = t.zeros((self.n, self.n), dtype=t.float64, device='cuda')
+        for i in range(psi.shape[0]):
+            wpsi = self.W * psi[i]
+            for nu in range(self.n):
+                v = self.fb.coulomb_potential(psi[i] * phi[nu])
+                self.poisson_solves += 1
+                K[:, nu] += phi @ (wpsi * v)
+        return 0.5 * (K + K.T)
+
+    def fock(self, D, Cocc):
+        """(F, E_electronic) for density D."""
+        t = self.torch
+        rho = self.fb.density(D)
+        vH = self.fb.coulomb_potential(rho)
+        self.fock_builds += 1
+        self.poisson_solves += 1
+        if self.exchange == 'lda-x':
+            r13 = t.clamp(rho, min=0.0) ** (1.0 / 3.0)
+            G = self.fb.quadrature(1.0, vH, vext=CX * r13)
+            EJ = 0.5 * float((self.W * rho * vH).sum())
+            Ex = float((self.W * EX * rho * r13).sum())
+            F = self.H + G
+            return F, float((D * self.H).sum()) + EJ + Ex
+        J = self.fb.quadrature(1.0, vH)
+        F = self.H + J
+        if self.exchange == 'hf':
+            F = F - self.exchange_matrix(Cocc)
+        return F, 0.5 * float((D * (self.H + F)).sum())
+
+    def _diag(self, F):
+        Fp = self.X.T @ F @ self.X
+        e, Cp = self.torch.linalg.eigh(Fp)
+        return e, self.X @ Cp
+
+    # -------------------------------------------------------------- loop
+    def run(self, maxiter=100, tol=1e-8, verbose=False):
+        t = self.torch
+        torch = t
+        t0 = time.perf_counter()
+        _, C = self._diag(self.H)                          # core guess
+        Cocc = C[:, :self.nocc]
+        D = 2.0 * Cocc @ Cocc.T
+        Fs, errs, history = [], [], []
+        E_prev = None
+        converged = False
+        for it in range(1, maxiter + 1):
+            F, Eel = self.fock(D, Cocc)
+            E = Eel + self.Enn
+            err = F @ D @ self.S - self.S @ D @ F
+            err = self.X.T @ err @ self.X
+            Fs.append(F)
+            errs.append(err)
+            if len(Fs) > self.ndiis:
+                Fs.pop(0)
+                errs.pop(0)
+            emax = float(err.abs().max())
+            history.append((E, emax))
+            if verbose:
+                print('%3d %.12f %.3e' % (it, E, emax))
+            if E_prev is not None and abs(E - E_prev) < tol and emax < 1e-4:
+                converged = True
+                break
+            E_prev = E
+            if len(Fs) > 1:
+                m = len(Fs)
+                B = torch.empty((m + 1, m + 1), dtype=torch.float64, device='cuda')
+                for a in range(m):
+                    for b in range(a + 1):
+                        B[a, b] = B[b, a] = (errs[a] * errs[b]).sum()
+                B[m, :m] = -1.0
+                B[:m, m] = -1.0
+                B[m, m] = 0.0
+                rhs = torch.zeros(m + 1, dtype=torch.float64, device='cuda')
+                rhs[m] = -1.0
+                c = torch.linalg.solve(B, rhs)
+                F = sum(c[a] * Fs[a] for a in range(m))
+            _, C = self._diag(F)
+            Cocc = C[:, :self.nocc]
+            D = 2.0 * Cocc @ Cocc.T
+        torch.cuda.synchronize()
+        self.D, self.C = D, C
+        nel = float((D * self.S).sum())
+        return dict(energy=E, iterations=it, converged=converged, seconds=time.perf_counter() - t0,
+                    fock_builds=self.fock_builds, poisson_solves=self.poisson_solves,
+                    electrons=nel, history=history)

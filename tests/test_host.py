@@ -199,3 +199,20 @@ def test_errors_are_reported_not_fatal():
         nb.AngularGrid(7)
     with pytest.raises(nb.NapmoError):
         nb.PowerRadialTransform(2.0, 1.0, 10)
+
+
+def test_one_body_integrals_h2_sto3g():
+    """Analytic overlap and kinetic matrices: H2 / STO-3G at R = 1.4 bohr
+    (Szabo & Ostlund, Modern Quantum Chemistry, section 3.5.2:
+    S12 = 0.6593, T11 = 0.7600, T12 = 0.2365)."""
+    import numpy as np
+    from napmo_b200 import cext
+    from napmo_b200.system import BOHR_TO_ANGSTROM, build_system
+    ms = build_system([('H', (0.0, 0.0, 0.0)), ('H', (0.0, 0.0, 1.4 * BOHR_TO_ANGSTROM))],
+                      'STO-3G')
+    b = ms['e-']['basis']
+    S = np.zeros((2, 2))
+    T = np.zeros((2, 2))
+    cext.checked(cext.lib.napmo_basis_one_body(b._this, S, T))
+    assert abs(S[0, 0] - 1.0) < 1e-12 and abs(S[0, 1] - 0.6593) < 5e-5
+    assert abs(T[0, 0] - 0.7600) < 5e-5 and abs(T[0, 1] - 0.2365) < 5e-5

@@ -44,7 +44,7 @@ def parse():
     p.add_argument('--cpu-points', type=int, default=4096)
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--no-scf', action='store_true', help='skip the SCF timing of the c4 line')
-    p.add_argument('--workload', default='c4', choices=['c4', 'c3', 'c5', 'c1'],
+    p.add_argument('--workload', default='c4', choices=['c4', 'c3', 'c5', 'c1', 'c2'],
                    help='c4: C20H42 single system (default); c3: batch of 64 random HCNO '
                         'chains with uneven per-atom grids, one CUDA-graph launch per batch')
     p.add_argument('--nmol', type=int, default=64)
@@ -452,6 +452,47 @@ def run_scf_c1(args, world, rank):
         print(json.dumps(line))
 
 
+# -------------------------------------------------------- C2: APMO SCF
+def run_scf_c2(args, world, rank):
+    """HCN (H at 0, C at 1.066 A, N at 2.222 A along z), electrons in
+    cc-pVDZ, the H nucleus as a quantum species (5s5p even-tempered, 4-64
+    bohr^-2), 100 x 302 Becke grid per atom (90,600 points) shared by both
+    species; electron-nucleus coupling by grid quadrature of the device
+    Poisson potentials, electron exchange from orbital-pair Poisson solves,
+    one DIIS (6) over both species, converged to 1e-8 Eh."""
+    from napmo_b200.scf import GridAPMO
+    from napmo_b200.system import build_system
+    atoms = [('H', (0.0, 0.0, 0.0)), ('C', (0.0, 0.0, 1.066)), ('N', (0.0, 0.0, 2.222))]
+    out = {}
+    for prec in ('fp64', 'int8x4'):
+        times, res = [], None
+        for k in range(args.warmup + args.steps):
+            ms = build_system(atoms, 'CC-PVDZ', quantum=(0,))
+            res = GridAPMO(ms, 'H_1', 100, 302, precision=prec).run(tol=1e-8)
+            if k >= args.warmup:
+                times.append(res['seconds'])
+        out[prec] = {'seconds': statistics.median(times), 'energy': res['energy'],
+                     'iterations': res['iterations'], 'converged': res['converged'],
+                     'poisson_solves': res['poisson_solves']}
+    dE = abs(out['int8x4']['energy'] - out['fp64']['energy'])
+    head = 'int8x4' if dE <= 1e-6 and out['int8x4']['converged'] else 'fp64'
+    t = out[head]['seconds']
+    line = {'metric': 'grid APMO-RHF SCF time, HCN with quantum H, 100x302 (C2)', 'value': t,
+            'unit': 's per SCF', 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': t * 1e3, 'higher_is_better': False, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'int8x4' if head == 'int8x4' else 'f64',
+            'data': 'synthetic',
+            'config': {'workload': 'C2: HCN, e- cc-pVDZ (35) + H nucleus 5s5p (20), 100x302 per '
+                                   'atom (90,600 points), lmax 14, DIIS(6), 1e-8 Eh',
+                       'parallelism': 'single GPU'},
+            'scf': out, 'energy_difference_eh': dE,
+            'e2e': {'value': t, 'unit': 's per SCF', 'h2d_bytes_per_step': 0,
+                    'd2h_bytes_per_step': 8},
+            'cpu_baseline': None}
+    if rank == 0:
+        print(json.dumps(line))
+
+
 # --------------------------------------------------------------------- main
 def main():
     args = parse()
@@ -493,8 +534,9 @@ def main():
     import napmo_b200 as nb
     from napmo_b200 import cext
 
-    if args.workload in ('c3', 'c5', 'c1'):
-        {'c3': run_batch, 'c5': run_gradients, 'c1': run_scf_c1}[args.workload](args, world, rank)
+    if args.workload in ('c3', 'c5', 'c1', 'c2'):
+        {'c3': run_batch, 'c5': run_gradients, 'c1': run_scf_c1,
+         'c2': run_scf_c2}[args.workload](args, world, rank)
         if dist:
             dist.barrier()
             dist.destroy_process_group()

@@ -31,6 +31,7 @@ from .grids import BeckeGrid, lebedev_get_order
 
 CX = -(3.0 / np.pi) ** (1.0 / 3.0)          # Slater: v_x = CX rho^(1/3)
 EX = 0.75 * CX                              # e_x = EX rho^(4/3)
+PROTON_MASS = 1836.15267247                 # electron masses (napmo/data/constants.py)
 
 
 def nuclear_repulsion(point_charges):
@@ -186,3 +187,195 @@ class GridRHF(object):
         return dict(energy=E, iterations=it, converged=converged, seconds=time.perf_counter() - t0,
                     fock_builds=self.fock_builds, poisson_solves=self.poisson_solves,
                     electrons=nel, history=history)
+
+
+def _diis_extrapolate(torch, Fs, errs):
+    m = len(Fs)
+    B = torch.empty((m + 1, m + 1), dtype=torch.float64, device='cuda')
+    for a in range(m):
+        for b in range(a + 1):
+            B[a, b] = B[b, a] = (errs[a] * errs[b]).sum()
+    B[m, :m] = -1.0
+    B[:m, m] = -1.0
+    B[m, m] = 0.0
+    rhs = torch.zeros(m + 1, dtype=torch.float64, device='cuda')
+    rhs[m] = -1.0
+    c = torch.linalg.solve(B, rhs)
+    return sum(c[a] * Fs[a] for a in range(m))
+
+
+class _Species(object):
+    """One species on the shared grid: its Fock plan, S, H = T / mass +
+    q V_nuc (classical charges), S^-1/2, occupation and DIIS history."""
+
+    def __init__(self, grid, sp, point_charges, lmax, mass, precision, ndiis, torch):
+        self.torch = torch
+        self.fb = FockBuilder(grid, sp['basis'], lmax)
+        n, N = self.fb.n, grid.size
+        self.n, self.N = n, N
+        self.q = float(sp['charge'])
+        self.eta = float(sp['eta'])
+        self.nocc = int(sp['occupation'])
+        S = np.zeros((n, n))
+        T = np.zeros((n, n))
+        checked(cext.lib.napmo_basis_one_body(sp['basis']._this, S, T))
+        dev = dict(device='cuda', dtype=torch.float64)
+        self.S = torch.as_tensor(S, **dev)
+        H = torch.as_tensor(T, **dev) / mass
+        if point_charges:
+            qc = np.array([[*pc['origin'], pc['atomic_number']] for pc in point_charges],
+                          dtype=np.float64).reshape(-1, 4)
+            x, y, z, _, _ = grid.device_arrays()
+            vn = torch.empty(N, **dev)
+            checked(cext.lib.napmo_gpu_nuclear_potential(
+                N, x, y, z, qc.shape[0], np.ascontiguousarray(qc), vn.data_ptr(),
+                torch.cuda.current_stream().cuda_stream))
+            H = H + self.fb.quadrature(self.q, vn)      # FP64, before any precision switch
+        self.H = H
+        self.fb.set_precision(precision)
+        s, U = torch.linalg.eigh(self.S)
+        self.X = U @ torch.diag(s.rsqrt()) @ U.T
+        self.ndiis = ndiis
+        self.Fs, self.errs = [], []
+
+    def diag(self, F):
+        e, Cp = self.torch.linalg.eigh(self.X.T @ F @ self.X)
+        C = self.X @ Cp
+        Cocc = C[:, :self.nocc]
+        return C, Cocc, self.eta * Cocc @ Cocc.T
+
+    def diis(self, F, D):
+        err = self.X.T @ (F @ D @ self.S - self.S @ D @ F) @ self.X
+        self.Fs.append(F)
+        self.errs.append(err)
+        if len(self.Fs) > self.ndiis:
+            self.Fs.pop(0)
+            self.errs.pop(0)
+        Fx = _diis_extrapolate(self.torch, self.Fs, self.errs) if len(self.Fs) > 1 else F
+        return Fx, float(err.abs().max())
+
+
+class GridAPMO(object):
+    """APMO closed-shell SCF of the electrons and one quantum-nucleus species
+    (nAPMO's multi-species drivers, scf.py:146-273 / psi_hybrid.py:81-110):
+    both species on one Becke grid over all atoms; the electron-nucleus
+    coupling is the grid Coulomb quadrature of the other species' density
+    (potential from the device Poisson solve); electron exchange from
+    orbital-pair Poisson solves; a single quantum nucleus has no self
+    interaction (J - K = 0); classical nuclei enter H of both species.
+
+    E = sum_s tr(D_s H_s) + 1/2 tr(D_e (J_e - K_e)) + q_e q_n <rho_e|V[rho_n]>
+        + E_nn(classical)
+    """
+
+    def __init__(self, ms, nuclear='H_1', nrad=100, nang=302, lmax=None, precision='fp64',
+                 diis=6, mass=PROTON_MASS):
+        torch = _torch()
+        self.torch = torch
+        self.ms = ms
+        self.grid = BeckeGrid(ms['e-'], nrad, nang)
+        if lmax is None:
+            lmax = 'per-atom' if isinstance(nang, (list, tuple)) else lebedev_get_order(nang) // 2
+        self.W = torch.as_tensor(self.grid.becke_weights * self.grid.weights, device='cuda',
+                                 dtype=torch.float64)
+        self.e = _Species(self.grid, ms['e-'], ms.point_charges, lmax, 1.0, precision, diis,
+                          torch)
+        self.nuc = _Species(self.grid, ms[nuclear], ms.point_charges, lmax, mass, precision,
+                            diis, torch)
+        if self.nuc.nocc != 1:
+            raise ValueError('one quantum nucleus of the species is supported')
+        self.Enn = nuclear_repulsion(ms.point_charges)
+        self._nuclear = nuclear
+        self.poisson_solves = 0
+
+    def _exchange(self, Cocc):
+        sp, t = self.e, self.torch
+        phi = sp.fb.phi()[:, :sp.N]
+        psi = Cocc.T @ phi
+        K = t.zeros((sp.n, sp.n), dtype=t.float64, device='cuda')
+        for i in range(psi.shape[0]):
+            wpsi = self.W * psi[i]
+            for nu in range(sp.n):
+                v = sp.fb.coulomb_potential(psi[i] * phi[nu])
+                self.poisson_solves += 1
+                K[:, nu] += phi @ (wpsi * v)
+        return 0.5 * (K + K.T)
+
+    def run(self, maxiter=100, tol=1e-8, verbose=False):
+        """SCF from a guess with the quantum nuclei as point charges (electrons)
+        and the nucleus in that electron density's field; one DIIS over both
+        species (concatenated error vectors, shared coefficients)."""
+        torch = self.torch
+        e, n = self.e, self.nuc
+        t0 = time.perf_counter()
+        qq = e.q * n.q
+        # guess: electrons with the quantum nuclei as classical charges
+        qpos = np.array([[*p['origin'], 1.0] for p in self.ms[self._nuclear]['particles']],
+                        dtype=np.float64).reshape(-1, 4)
+        x, y, z, _, _ = self.grid.device_arrays()
+        vq = torch.empty(self.grid.size, device='cuda', dtype=torch.float64)
+        checked(cext.lib.napmo_gpu_nuclear_potential(
+            self.grid.size, x, y, z, qpos.shape[0], np.ascontiguousarray(qpos), vq.data_ptr(),
+            torch.cuda.current_stream().cuda_stream))
+        prec = e.fb.precision
+        e.fb.set_precision('fp64')
+        Hg = e.H + e.fb.quadrature(e.q * n.q, vq)
+        e.fb.set_precision(prec)
+        Ce, _, De = e.diag(Hg)
+        v_e = e.fb.coulomb_potential(e.fb.density(De))
+        Cn, _, Dn = n.diag(n.H + n.fb.quadrature(qq, v_e))
+        self.poisson_solves += 1
+        Fs, errs = [], []
+        E_prev, history, converged = None, [], False
+        for it in range(1, maxiter + 1):
+            rho_e = e.fb.density(De)
+            rho_n = n.fb.density(Dn)
+            v_e = e.fb.coulomb_potential(rho_e)
+            v_n = e.fb.coulomb_potential(rho_n)
+            self.poisson_solves += 2
+            # electrons: J_e + q_e q_n J[rho_n] - K_e; nucleus: q_n q_e J[rho_e]
+            Ge = e.fb.quadrature(e.q * e.q, v_e, vext=qq * v_n)
+            Fe = e.H + Ge - self._exchange(Ce[:, :e.nocc])
+            Fn = n.H + n.fb.quadrature(qq, v_e)
+            # energy: one-body + electron two-body (1/2 of J - K) + coupling
+            coup = qq * float((self.W * rho_e * v_n).sum())
+            Ee = 0.5 * float((De * (e.H + Fe)).sum()) - 0.5 * coup
+            En = float((Dn * n.H).sum())
+            E = Ee + En + coup + self.Enn
+            err_e = e.X.T @ (Fe @ De @ e.S - e.S @ De @ Fe) @ e.X
+            err_n = n.X.T @ (Fn @ Dn @ n.S - n.S @ Dn @ Fn) @ n.X
+            Fs.append((Fe, Fn))
+            errs.append((err_e, err_n))
+            if len(Fs) > e.ndiis:
+                Fs.pop(0)
+                errs.pop(0)
+            emax = (float(err_e.abs().max()), float(err_n.abs().max()))
+            history.append((E,) + emax)
+            if verbose:
+                print('%3d %.12f %.2e %.2e' % ((it, E) + emax))
+            if E_prev is not None and abs(E - E_prev) < tol and max(emax) < 1e-4:
+                converged = True
+                break
+            E_prev = E
+            m = len(Fs)
+            if m > 1:
+                B = torch.empty((m + 1, m + 1), dtype=torch.float64, device='cuda')
+                for a in range(m):
+                    for b in range(a + 1):
+                        B[a, b] = B[b, a] = ((errs[a][0] * errs[b][0]).sum() +
+                                             (errs[a][1] * errs[b][1]).sum())
+                B[m, :m] = -1.0
+                B[:m, m] = -1.0
+                B[m, m] = 0.0
+                rhs = torch.zeros(m + 1, dtype=torch.float64, device='cuda')
+                rhs[m] = -1.0
+                c = torch.linalg.solve(B, rhs)
+                Fe = sum(c[a] * Fs[a][0] for a in range(m))
+                Fn = sum(c[a] * Fs[a][1] for a in range(m))
+            Ce, _, De = e.diag(Fe)
+            Cn, _, Dn = n.diag(Fn)
+        torch.cuda.synchronize()
+        return dict(energy=E, iterations=it, converged=converged,
+                    seconds=time.perf_counter() - t0, poisson_solves=self.poisson_solves,
+                    electrons=float((De * e.S).sum()), nuclei=float((Dn * n.S).sum()),
+                    history=history)

@@ -22,3 +22,19 @@ def test_grid_scf_h2o(exchange, lo, hi):
                  precision='int8x4').run(tol=1e-9)
     assert r8['converged']
     assert abs(r8['energy'] - r64['energy']) <= 1e-6
+
+
+def test_grid_apmo_hcn():
+    """Electrons + quantum H nucleus (5s5p), coupled through the grid."""
+    from helpers import HCN
+    from napmo_b200.scf import GridAPMO
+    from napmo_b200.system import build_system
+    res = {}
+    for prec in ('fp64', 'int8x4'):
+        ms = build_system(HCN, 'CC-PVDZ', quantum=(0,))
+        res[prec] = GridAPMO(ms, 'H_1', 50, 110, precision=prec).run(tol=1e-9)
+        assert res[prec]['converged'] and res[prec]['iterations'] <= 40
+        assert abs(res[prec]['electrons'] - 14.0) < 1e-8
+        assert abs(res[prec]['nuclei'] - 1.0) < 1e-8
+    assert -93.0 < res['fp64']['energy'] < -92.7
+    assert abs(res['int8x4']['energy'] - res['fp64']['energy']) <= 1e-6

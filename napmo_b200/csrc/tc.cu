@@ -459,57 +459,68 @@ gscale_kernel(int npoint, const double *__restrict__ wv, const double *__restric
 // Per call: the B image from the A image.  For each row and block,
 // x(p) = Y_A(p) gs(p) (|x| < 2^30); Y_B = rint(x 2^s) with s = 30 - e,
 // e = group exponent of max |x| over the block, so B keeps 31 bits of its own
-// block maximum; eb[row][b] = ea[row][b] + eg[b] - s.  CTA = (128-row tile,
-// block); thread = one 16-byte chunk position of a slice (row group, 16-point
-// column, row % 8) over the block's stages: pass 1 the row maxima (the four
-// chunks of a row are lanes c, c ^ 8, c ^ 16, c ^ 24), pass 2 the digits (the
-// block's 512 KB of A digits are re-read from L2).
-__global__ void __launch_bounds__(512, 1)
+// block maximum; eb[row][b] = ea[row][b] + eg[b] - s.  CTA = (8-row group,
+// block), 4 warps; in every stage the row group's 8 rows x 64 points of one
+// slice are 512 contiguous bytes, so lane c holds the 16-byte chunk of row
+// c & 7, points 16 (c >> 3) .. +15.  Warp w takes stages 4w .. 4w + 3 and keeps
+// their A digits in registers across both passes (row maxima: lanes c, c ^ 8,
+// c ^ 16, c ^ 24, then the four warps through shared memory; digits of B), so
+// A is read from memory once.
+__global__ void __launch_bounds__(128)
 scale_image_kernel(const int8_t *__restrict__ qa, int8_t *__restrict__ qb,
                    const double *__restrict__ gs, const int *__restrict__ ea,
                    const int *__restrict__ eg, int *__restrict__ eb, int nks, int nblk) {
-  const int c = threadIdx.x;                     // (c >> 5) row group, (c >> 3) & 3 column, c & 7 row
-  const int t = blockIdx.x, b = blockIdx.y;
-  const int kc = (c >> 3) & 3;
-  const int row = t * TM + (c >> 5) * 8 + (c & 7);
-  auto load = [&](int st, double *x) {
-    const int ks = b * QBLK_STAGES + st;
-    const long base = ((long)t * nks + ks) * stage_bytes(TM) + (long)c * 16;
-    uint4 q[NSL];
+  constexpr int SPW = QBLK_STAGES / 4;  // stages per warp
+  __shared__ double smax[4][8];
+  const int c = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int rg = blockIdx.x, b = blockIdx.y;
+  const int t = rg >> 4, r = c & 7, kc = c >> 3;
+  const int row = rg * 8 + r;
+  const long goff = (long)(rg & 15) * 512 + c * 16;
+  auto stage_base = [&](int st) {
+    return ((long)t * nks + b * QBLK_STAGES + w * SPW + st) * stage_bytes(TM) + goff;
+  };
+  uint4 q[SPW][NSL];
+#pragma unroll
+  for (int st = 0; st < SPW; ++st)
 #pragma unroll
     for (int s = 0; s < NSL; ++s)
-      q[s] = __ldg(reinterpret_cast<const uint4 *>(qa + base + (long)s * TM * KS));
-    const double *g = gs + (long)ks * KS + kc * 16;
+      q[st][s] = __ldg(reinterpret_cast<const uint4 *>(qa + stage_base(st) + (long)s * TM * KS));
+  auto values = [&](int st, double *x) {
+    const double *g = gs + ((long)b * QBLK_STAGES + w * SPW + st) * KS + kc * 16;
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       const int wq = i >> 2, bb = i & 3;
-      const int y = ((sbyte((&q[0].x)[wq], bb) * 256 + sbyte((&q[1].x)[wq], bb)) * 256 +
-                     sbyte((&q[2].x)[wq], bb)) * 256 + sbyte((&q[3].x)[wq], bb);
+      const int y = ((sbyte((&q[st][0].x)[wq], bb) * 256 + sbyte((&q[st][1].x)[wq], bb)) * 256 +
+                     sbyte((&q[st][2].x)[wq], bb)) * 256 + sbyte((&q[st][3].x)[wq], bb);
       x[i] = (double)y * __ldg(g + i);
     }
   };
   double mx = 0.0;
-  for (int st = 0; st < QBLK_STAGES; ++st) {
+#pragma unroll
+  for (int st = 0; st < SPW; ++st) {
     double x[16];
-    load(st, x);
+    values(st, x);
 #pragma unroll
     for (int i = 0; i < 16; ++i) mx = fmax(mx, fabs(x[i]));
   }
   mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 8));
   mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 16));
+  if (c < 8) smax[w][c] = mx;
+  __syncthreads();
+  mx = fmax(fmax(smax[0][r], smax[1][r]), fmax(smax[2][r], smax[3][r]));
   const int sh = 30 - group_exponent(mx);
-  if (kc == 0) eb[(long)row * nblk + b] = ea[(long)row * nblk + b] + eg[b] - sh;
+  if (w == 0 && c < 8) eb[(long)row * nblk + b] = ea[(long)row * nblk + b] + eg[b] - sh;
   const double scale = ldexp(1.0, sh);
-  for (int st = 0; st < QBLK_STAGES; ++st) {
+#pragma unroll
+  for (int st = 0; st < SPW; ++st) {
     double x[16];
-    load(st, x);
+    values(st, x);
     uint4 d[NSL];
     slice16(x, scale, d);
-    const long base =
-        ((long)t * nks + b * QBLK_STAGES + st) * stage_bytes(TM) + (long)c * 16;
 #pragma unroll
     for (int s = 0; s < NSL; ++s)
-      *reinterpret_cast<uint4 *>(qb + base + (long)s * TM * KS) = d[s];
+      *reinterpret_cast<uint4 *>(qb + stage_base(st) + (long)s * TM * KS) = d[s];
   }
 }
 
@@ -1039,8 +1050,7 @@ int int8_quadrature(Int8Plan *p, const double *phi, const double *wv, double *F,
   (void)phi;
   gscale_kernel<<<p->nblk, 256, 0, s>>>(p->npoint, wv, p->isc.p, p->gs.p, p->eg.p);
   NAPMO_TRY_CUDA(cudaGetLastError(), "block scales");
-  const int tiles_used = (p->n + TM - 1) / TM;
-  scale_image_kernel<<<dim3(tiles_used, p->nblk), 512, 0, s>>>(
+  scale_image_kernel<<<dim3((p->n + 7) / 8, p->nblk), 128, 0, s>>>(
       p->qa.p, p->qb.p, p->gs.p, p->qa_e.p, p->eg.p, p->qb_e.p, p->nks_q, p->nblk);
   NAPMO_TRY_CUDA(cudaGetLastError(), "wv phi image");
   QuadArgs g{p->qa.p, p->qb.p, p->qa_e.p, p->qb_e.p, p->nblk, p->nks_q,

@@ -613,7 +613,8 @@ def main():
              'int8_image_bytes': int(cext.lib.napmo_fock_plan_int8_bytes(fbld._plan)),
              'scheme': 'int8 slices (4 balanced base-256 digits per value, group exponents), '
                        'tcgen05 kind::i8 with exact int32 TMEM accumulation; 13 digit '
-                       'products per contraction; Poisson FP64'}
+                       'products per contraction; Poisson FP64, its evaluation skipping '
+                       'l-blocks bounded below 1e-10 a.u. per (atom, radial interval)'}
 
     # ---- per-kernel timings (same stream) for the roofline
     def time_it(fn, reps=3):
@@ -637,11 +638,14 @@ def main():
         tq = time_it(lambda: fbld.quadrature(1.0, v))
         kernels['density_' + prec] = {'ms': td * 1e3, 'tflops': flops / td / 1e12}
         kernels['quadrature_' + prec] = {'ms': tq * 1e3, 'tflops': flops / tq / 1e12}
-    t_poisson = time_it(lambda: fbld.coulomb_potential(rho))
-    kernels['poisson(project+radial+evaluate)'] = {'ms': t_poisson * 1e3}
+        # projection + radial solves + evaluation; int8x4 evaluates with the
+        # mode's truncation tolerance (l-blocks bounded below 1e-10 skipped)
+        tp = time_it(lambda: fbld.coulomb_potential(rho))
+        kernels['poisson_' + prec] = {'ms': tp * 1e3}
     fbld.set_precision(headline)
     t_density = kernels['density_' + headline]['ms'] / 1e3
     t_quad = kernels['quadrature_' + headline]['ms'] / 1e3
+    t_poisson_mode = kernels['poisson_' + headline]['ms'] / 1e3
 
     # ---- end-to-end through the C-ABI with host buffers
     Dh = torch.empty((n, n), dtype=torch.float64).pin_memory()
@@ -682,10 +686,13 @@ def main():
     if rank == 0:
         peaks, peak_kind = measured_peaks()
         fp64 = fp64_gemm_peak(torch)
-        t_poisson = kernels['poisson(project+radial+evaluate)']['ms'] / 1e3
-        stages = {'density': t_density, 'quadrature': t_quad, 'poisson': t_poisson}
+        stages = {'density': t_density, 'quadrature': t_quad, 'poisson': t_poisson_mode}
         dom = max(stages, key=stages.get)
         td = stages[dom]
+        if dom == 'poisson':
+            # the roofline is the kernel's: the untruncated evaluation, whose
+            # work is the full (l, m) count below
+            td = kernels['poisson_fp64']['ms'] / 1e3
         issued = None
         if dom == 'poisson':
             # potential evaluation dominates: FP64 ALU bound.  Algorithmic count:

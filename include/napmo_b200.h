@@ -263,6 +263,12 @@ int napmo_gpu_combine_weights(int npoint, const double *wb, const double *w, dou
 int napmo_gpu_poisson(void *grid, const double *rho, int lmax, double *v, int accumulate,
                       double *raw_y, double *raw_dt, void *stream);
 long napmo_poisson_raw_size(void *grid, int lmax);
+/* Truncation tolerance (a.u.) of the grid's potential evaluation.  No
+ * counterpart in nAPMO, whose evaluate.cpp:129-220 sums every (l, m) <= lmax:
+ * 0 (the default) does the same; tol > 0 lets each (atom, radial interval)
+ * drop its highest l-blocks while their bounded sum stays <= tol, so each
+ * point's potential moves by at most natom * tol. */
+int napmo_grid_set_poisson_tolerance(void *grid, double tol);
 /* sum_A Z_A / |r - R_A| at device points; replaces compute_nuclear (nnuclear.py:15-37). */
 int napmo_gpu_nuclear_potential(int npoint, const double *x, const double *y, const double *z,
                                 int nq, const double *charges, double *v, void *stream);
@@ -292,6 +298,9 @@ int napmo_fock_plan_quadrature(void *plan, double q, const double *v, const doub
                                double *F, void *stream);
 int napmo_fock_plan_build(void *plan, const double *D, double q, const double *vext, double *F,
                           double *rho_out, double *v_out, void *stream);
+/* v = V_H[rho] on the plan's grid with the plan's lmax and Poisson tolerance;
+ * replaces compute_coulomb (ntwobody.py:15-46) inside an SCF iteration. */
+int napmo_fock_plan_poisson(void *plan, const double *rho, double *v, void *stream);
 /* Host-buffer twin of napmo_fock_plan_build (copies inside the call). */
 int napmo_fock_plan_build_host(void *plan, const double *D, double q, const double *vext,
                                double *F, void *stream);
@@ -300,6 +309,12 @@ int napmo_fock_plan_build_host(void *plan, const double *D, double q, const doub
  * against a group exponent, exact int32 accumulation).  No counterpart in
  * nAPMO (its quadratures are FP64 only, src/wavefunction/nwavefunction.cpp). */
 int napmo_fock_plan_set_precision(void *plan, int mode);
+/* Truncation tolerance (a.u.) of the plan's Poisson potential evaluation: per
+ * (atom, radial interval), the highest l-blocks whose bounded contribution
+ * sums to at most tol are skipped.  No counterpart in nAPMO (evaluate.cpp:
+ * 129-220 sums every (l, m)).  set_precision resets it: 0 for mode 0 (every
+ * (l, m), as nAPMO), 1e-10 for mode 1. */
+int napmo_fock_plan_set_poisson_tolerance(void *plan, double tol);
 /* Device bytes of the plan's int8 operand images and scratch. */
 long napmo_fock_plan_int8_bytes(void *plan);
 /* Batched Fock builds of many plans (molecules of uneven size) by one CUDA

@@ -196,6 +196,7 @@ _SIGS = [
     ('napmo_gpu_poisson', c_int,
      [c_void_p, c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     ('napmo_poisson_raw_size', c_long, [c_void_p, c_int]),
+    ('napmo_grid_set_poisson_tolerance', c_int, [c_void_p, c_double]),
     ('napmo_gpu_nuclear_potential', c_int,
      [c_int, c_void_p, c_void_p, c_void_p, c_int, a2df, c_void_p, c_void_p]),
     ('napmo_fock_plan_new', c_void_p, [c_void_p, c_void_p, c_int, c_void_p]),
@@ -210,6 +211,8 @@ _SIGS = [
     ('napmo_fock_plan_build_host', c_int,
      [c_void_p, a2df, c_double, c_void_p, a2df, c_void_p]),
     ('napmo_fock_plan_set_precision', c_int, [c_void_p, c_int]),
+    ('napmo_fock_plan_set_poisson_tolerance', c_int, [c_void_p, c_double]),
+    ('napmo_fock_plan_poisson', c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ('napmo_fock_plan_int8_bytes', c_long, [c_void_p]),
     ('napmo_fock_batch_new', c_void_p, [c_void_p, c_int, c_double]),
     ('napmo_fock_batch_free', None, [c_void_p]),

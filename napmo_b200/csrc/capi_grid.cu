@@ -45,6 +45,7 @@ struct PoissonPlan {
   DevBuf<int> pairs;
   DevBuf<EvalItem> items;
   DevBuf<double> pair_v;
+  DevBuf<int> lcut;  // per bucket, for truncated evaluations
 };
 
 void free_poisson_plan(PoissonPlan *p) { delete p; }
@@ -237,6 +238,7 @@ int build_pair_lists(PoissonPlan *plan, const double *x, const double *y, const 
                  "pair scatter");
   NAPMO_TRY_CUDA(plan->items.upload(items, s), "pair lists");
   NAPMO_TRY_CUDA(plan->pair_v.alloc(d.npair), "pair lists");
+  NAPMO_TRY_CUDA(plan->lcut.alloc(nb), "pair lists");
   NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "pair lists");
   d.items = plan->items.p;
   d.nitems = (int)items.size();
@@ -290,7 +292,9 @@ int grid_poisson_plan(BeckeGrid *g, int lmax, cudaStream_t s, PoissonPlan **out)
 }
 
 int run_poisson(BeckeGrid *g, PoissonPlan *p, const double *rho_dev, double *v_dev,
-                bool accumulate, cudaStream_t s) {
+                bool accumulate, cudaStream_t s, double tol) {
+  p->d.eval_tol = tol;
+  p->d.lcut = tol > 0.0 ? p->lcut.p : nullptr;
   NAPMO_TRY_CUDA(launch_poisson_project(p->d, rho_dev, g->dev.wb, g->dev.w, s), "project");
   NAPMO_TRY_CUDA(launch_poisson_radial(p->d, s), "radial solve");
   NAPMO_TRY_CUDA(launch_poisson_evaluate(p->d, g->size, g->dev.x, g->dev.y, g->dev.z,
@@ -1095,7 +1099,7 @@ int napmo_gpu_poisson(BeckeGrid *g, const double *rho_dev, int lmax, double *v_d
     PoissonPlan *p = nullptr;
     int st = grid_poisson_plan(g, lmax, s, &p);
     if (st) return st;
-    st = run_poisson(g, p, rho_dev, v_dev, accumulate != 0, s);
+    st = run_poisson(g, p, rho_dev, v_dev, accumulate != 0, s, g->poisson_tol);
     if (st) return st;
     if (raw_y)
       NAPMO_TRY_CUDA(cudaMemcpyAsync(raw_y, p->raw_y.p, p->raw_y.n * sizeof(double),
@@ -1105,6 +1109,22 @@ int napmo_gpu_poisson(BeckeGrid *g, const double *rho_dev, int lmax, double *v_d
       NAPMO_TRY_CUDA(cudaMemcpyAsync(raw_dt, p->raw_dt.p, p->raw_dt.n * sizeof(double),
                                      cudaMemcpyDeviceToDevice, s),
                      "poisson raw");
+    return kOk;
+  });
+}
+
+// Truncation tolerance (a.u., >= 0) of the grid's Poisson potential
+// evaluation.  0 (the default) evaluates every (l, m) up to lmax at every
+// pair, as nAPMO's evaluation does (src/horton/evaluate.cpp:129-220).  tol > 0
+// lets each (atom, radial interval) bucket drop its highest l-blocks when the
+// sum of their bounds (Racah-normalised harmonics: |sum_m c_lm S_lm| <=
+// ||c_l||) is at most tol, so every pair's potential changes by at most tol.
+// Applies to later builds; a batch graph keeps the tolerance it was
+// captured with.
+int napmo_grid_set_poisson_tolerance(BeckeGrid *g, double tol) {
+  return guarded([&] {
+    NAPMO_REQUIRE(tol >= 0.0 && tol < 1.0, "Poisson tolerance must be in [0, 1)");
+    g->poisson_tol = tol;
     return kOk;
   });
 }

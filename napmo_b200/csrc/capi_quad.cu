@@ -15,7 +15,13 @@ namespace napmo {
 struct PoissonPlan;
 int grid_poisson_plan(BeckeGrid *g, int lmax, cudaStream_t s, PoissonPlan **out);
 int run_poisson(BeckeGrid *g, PoissonPlan *p, const double *rho_dev, double *v_dev,
-                bool accumulate, cudaStream_t s);
+                bool accumulate, cudaStream_t s, double tol);
+
+// Truncation tolerance (a.u.) of the Poisson potential evaluation that
+// precision 1 selects: each (atom, radial interval) drops l-blocks whose
+// bounded contribution sums to at most this, so every point's potential moves
+// by at most natom x 1e-10, well inside that mode's 1e-6 Eh energy budget.
+constexpr double kMixedPoissonTol = 1e-10;
 int basis_device(BasisSet *b, cudaStream_t s, const DeviceBasis **out);
 
 // ---------------------------------------------------------------- helpers
@@ -66,6 +72,7 @@ struct FockPlan {
   BasisSet *basis = nullptr;
   int n = 0, lmax = 0;
   int mode = 0;  // 0 FP64, 1 int8 slices on the tensor cores
+  double poisson_tol = 0.0;  // truncation tolerance of the potential evaluation
   long ld = 0;
   DevBuf<double> phi, rho, v, wv, work, D, F, vext;
   Int8Plan *i8 = nullptr;
@@ -102,7 +109,7 @@ int fock_build(FockPlan *p, const double *D_dev, double q, const double *vext_de
   PoissonPlan *pp = nullptr;
   e = grid_poisson_plan(g, p->lmax, s, &pp);
   if (e) return e;
-  e = run_poisson(g, pp, rho, v, false, s);
+  e = run_poisson(g, pp, rho, v, false, s, p->poisson_tol);
   if (e) return e;
   NAPMO_TRY_CUDA(launch_combine_weights(g->size, g->dev.wb, g->dev.w, q, v, vext_dev, p->wv.p, s),
                  "weights");
@@ -298,6 +305,18 @@ int napmo_fock_plan_quadrature(FockPlan *p, double q, const double *v_dev,
   });
 }
 
+// v (device) = V_H[rho] (device) on the plan's grid, with the plan's lmax
+// and Poisson tolerance (stream-ordered).
+int napmo_fock_plan_poisson(FockPlan *p, const double *rho_dev, double *v_dev, void *stream) {
+  return guarded([&] {
+    cudaStream_t s = (cudaStream_t)stream;
+    PoissonPlan *pp = nullptr;
+    int e = grid_poisson_plan(p->grid, p->lmax, s, &pp);
+    if (e) return e;
+    return run_poisson(p->grid, pp, rho_dev, v_dev, false, s, p->poisson_tol);
+  });
+}
+
 // One grid Fock build of a species with its own density:
 //   rho = density(D), v = q * V_H[rho] (Becke-Dickson Poisson), and
 //   F = phi diag(wb w (v + vext)) phi^T.
@@ -380,8 +399,10 @@ extern "C" {
 // Precision of a plan's contractions: 0 = FP64 (CUDA cores, default),
 // 1 = int8 slices on the tensor cores (four balanced base-256 digits per
 // value against a group exponent, exact int32 accumulation in TMEM).  The
-// Poisson solve stays FP64 in both modes.  Switching to 1 builds phi's
-// operand images (device-synchronous, once per plan).
+// Poisson solve stays FP64 in both modes; mode 1 also sets the plan's Poisson
+// truncation tolerance to 1e-10 a.u. (mode 0 to 0, every (l, m) evaluated).
+// Switching to 1 builds phi's operand images (device-synchronous, once per
+// plan).
 int napmo_fock_plan_set_precision(FockPlan *p, int mode) {
   return napmo::guarded([&] {
     NAPMO_REQUIRE(mode == 0 || mode == 1, "precision mode must be 0 (fp64) or 1 (int8x4)");
@@ -395,6 +416,18 @@ int napmo_fock_plan_set_precision(FockPlan *p, int mode) {
       NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "int8 operand images");
     }
     p->mode = mode;
+    p->poisson_tol = mode == 1 ? napmo::kMixedPoissonTol : 0.0;
+    return napmo::kOk;
+  });
+}
+
+// Truncation tolerance (a.u., >= 0) of the plan's Poisson potential
+// evaluation; napmo_fock_plan_set_precision resets it to the mode's default
+// (0 for FP64, which sums every (l, m) as nAPMO does; 1e-10 for int8 slices).
+int napmo_fock_plan_set_poisson_tolerance(FockPlan *p, double tol) {
+  return napmo::guarded([&] {
+    NAPMO_REQUIRE(tol >= 0.0 && tol < 1.0, "Poisson tolerance must be in [0, 1)");
+    p->poisson_tol = tol;
     return napmo::kOk;
   });
 }

@@ -192,6 +192,7 @@ struct BeckeGrid {
   std::vector<AtomLayout> layout;     // empty for grids read from points
   DeviceGrid dev;                     // device mirror (points SoA, weights)
   PoissonPlan *poisson = nullptr;     // cached for the last lmax used
+  double poisson_tol = 0.0;           // truncation tolerance of the potential evaluation
   BeckeGrid() = default;
   ~BeckeGrid();
 };

@@ -634,6 +634,48 @@ __device__ __forceinline__ void pair_values(const double *cf, int lmaxA, const d
 }
 
 
+// Truncation of the expansion per (atom, bucket) when P.eval_tol > 0.  With
+// Racah-normalised harmonics sum_m S_lm(r_hat)^2 = 1, so by Cauchy-Schwarz the
+// l-block adds at most bound_l = sqrt(sum_m c_lm^2) to the potential of any
+// pair of the bucket, with c_lm = sum_k |c_k,lm| inside the grid (0 <= u <= 1),
+// |a_lm| first_x^l below the first radial point (d^l <= first_x^l) and
+// |a_lm| last_x^-(l+1) beyond the last.  The bucket keeps l <= L, the smallest
+// L whose dropped blocks sum to at most eval_tol.  Grid (max nrad + 1, natom),
+// one warp: lane l bounds block l.
+__global__ void __launch_bounds__(32) bucket_lcut_kernel(PoissonDev P) {
+  __shared__ double bound[32];
+  const PoissonAtom &at = P.atoms[blockIdx.y];
+  const int b = blockIdx.x, l = threadIdx.x;
+  if (b > at.nrad) return;
+  const int lmaxA = at.lmax;
+  const int lsize = (lmaxA + 1) * (lmaxA + 1);
+  const int region = (b == 0) ? 1 : (b == at.nrad ? 2 : 0);
+  if (l <= lmaxA) {
+    double s2 = 0.0;
+    for (int lm = l * l; lm < (l + 1) * (l + 1); ++lm) {
+      double c;
+      if (region == 0) {
+        const double *cf = P.spl + at.spl_off + ((long)(b - 1) * lsize + lm) * 4;
+        c = fabs(cf[0]) + fabs(cf[1]) + fabs(cf[2]) + fabs(cf[3]);
+      } else {
+        c = fabs(P.amp[at.amp_off + lm * 2 + (region == 1 ? 0 : 1)]);
+      }
+      s2 = fma(c, c, s2);
+    }
+    const double g = region == 0 ? 1.0
+                                 : (region == 1 ? pow(at.first_x, (double)l)
+                                                : pow(at.last_x, -(double)(l + 1)));
+    bound[l] = sqrt(s2) * g;
+  }
+  __syncwarp();
+  if (l == 0) {
+    double dropped = 0.0;
+    int L = lmaxA;
+    while (L > 0 && dropped + bound[L] <= P.eval_tol) dropped += bound[L--];
+    P.lcut[at.bucket_off + b] = L;
+  }
+}
+
 template <int LMAX>
 __global__ void __launch_bounds__(kEvalChunk / kEvalPerThread)
 eval_pairs_kernel(PoissonDev P, const double *__restrict__ gx,
@@ -644,15 +686,17 @@ eval_pairs_kernel(PoissonDev P, const double *__restrict__ gx,
   const int lmaxA = at.lmax;
   const int lsize = (lmaxA + 1) * (lmaxA + 1);
   const int region = (it.bucket == 0) ? 1 : (it.bucket == at.nrad ? 2 : 0);
+  // l-blocks kept for this bucket (all unless a truncation tolerance is set)
+  const int lcut = P.lcut ? P.lcut[at.bucket_off + it.bucket] : lmaxA;
+  const int lkeep = (lcut + 1) * (lcut + 1);
   if (region == 0) {
     const double *src = P.spl + at.spl_off + (long)(it.bucket - 1) * lsize * 4;
-    for (int e = threadIdx.x; e < lsize * 4; e += blockDim.x) cf[e] = src[e];
+    for (int e = threadIdx.x; e < lkeep * 4; e += blockDim.x) cf[e] = src[e];
   } else {
     const double *src = P.amp + at.amp_off;
-    for (int e = threadIdx.x; e < lsize; e += blockDim.x)
+    for (int e = threadIdx.x; e < lkeep; e += blockDim.x)
       cf[e] = src[2 * e + (region == 1 ? 0 : 1)];
   }
-  __syncthreads();
   // thread t evaluates the pairs t and t + blockDim.x of the item (the
   // second may be absent: it then repeats the first and is not stored)
   const int t = threadIdx.x;
@@ -674,11 +718,11 @@ eval_pairs_kernel(PoissonDev P, const double *__restrict__ gx,
     u[j] = region == 0 ? rt_inv(at.rt, d[j]) - (it.bucket - 1) : 0.0;
   }
   if (region == 0)
-    pair_values<LMAX, 0, kEvalPerThread>(cf, lmaxA, x, y, z, d, inv, u, v);
+    pair_values<LMAX, 0, kEvalPerThread>(cf, lcut, x, y, z, d, inv, u, v);
   else if (region == 1)
-    pair_values<LMAX, 1, kEvalPerThread>(cf, lmaxA, x, y, z, d, inv, u, v);
+    pair_values<LMAX, 1, kEvalPerThread>(cf, lcut, x, y, z, d, inv, u, v);
   else
-    pair_values<LMAX, 2, kEvalPerThread>(cf, lmaxA, x, y, z, d, inv, u, v);
+    pair_values<LMAX, 2, kEvalPerThread>(cf, lcut, x, y, z, d, inv, u, v);
 #pragma unroll
   for (int j = 0; j < kEvalPerThread; ++j) {
     const int e = t + j * (int)blockDim.x;
@@ -714,6 +758,11 @@ cudaError_t launch_eval_l(const PoissonDev &P, int npoint, const double *x,
                           const double *y, const double *z, double *out, int acc,
                           cudaStream_t s) {
   if (P.items && P.nitems > 0) {
+    if (P.lcut) {
+      bucket_lcut_kernel<<<dim3(P.max_nrad + 1, P.natom), 32, 0, s>>>(P);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+    }
     const size_t smem = (size_t)(L + 1) * (L + 1) * 4 * sizeof(double);
     eval_pairs_kernel<L><<<P.nitems, kEvalChunk / kEvalPerThread, smem, s>>>(P, x, y, z);
     cudaError_t e = cudaGetLastError();

@@ -82,6 +82,12 @@ struct PoissonDev {
   int *pairs = nullptr;        // point index, bucket-sorted per atom
   EvalItem *items = nullptr;
   double *pair_v = nullptr;    // [atom][molecule point] contribution
+  // Truncation of the bucketed evaluation: with lcut null every (l, m) <=
+  // lmax is evaluated, as the reference does; with lcut set (one int per
+  // bucket) each bucket drops its highest l-blocks whose bounded contribution
+  // to any pair's potential sums to at most eval_tol (a.u.).
+  double eval_tol = 0.0;
+  int *lcut = nullptr;
 };
 
 // Uploads the Hermite FEM integral tables and solid-harmonic norms to

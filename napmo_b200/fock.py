@@ -61,11 +61,21 @@ class FockBuilder(object):
         self.n, self.npoint, self.ld, self._phi_ptr = n.value, npt.value, ld.value, phi.value
         self.set_precision(precision)
 
-    def set_precision(self, precision):
+    def set_precision(self, precision, poisson_tol=None):
         """'fp64' (CUDA cores) or 'int8x4' (int8 slices on the tensor cores) for
-        rho and F; the Poisson solve is FP64 in both."""
+        rho and F; the Poisson solve is FP64 in both.  The Poisson truncation
+        tolerance follows the mode (0: every (l, m) as nAPMO; 1e-10 a.u. for
+        'int8x4') unless `poisson_tol` is given."""
         checked(cext.lib.napmo_fock_plan_set_precision(self._plan, self.PRECISIONS[precision]))
         self.precision = precision
+        if poisson_tol is not None:
+            self.set_poisson_tolerance(poisson_tol)
+
+    def set_poisson_tolerance(self, tol):
+        """Truncation tolerance (a.u.) of the potential evaluation: per atom and
+        radial interval, l-blocks whose bounded contribution to any point sums
+        to at most `tol` are skipped (0: none)."""
+        checked(cext.lib.napmo_fock_plan_set_poisson_tolerance(self._plan, float(tol)))
 
     def tc_status(self, reset=True, stream=None):
         """Error word of the tensor-core kernels (0: none); synchronises the stream."""
@@ -115,8 +125,8 @@ class FockBuilder(object):
         t = self.torch
         rho = self._dev(rho, (self.npoint,))
         v = t.empty(self.npoint, dtype=t.float64, device='cuda')
-        checked(cext.lib.napmo_gpu_poisson(self.grid._this, rho.data_ptr(), self.lmax,
-                                           v.data_ptr(), 0, None, None, _stream(t, stream)))
+        checked(cext.lib.napmo_fock_plan_poisson(self._plan, rho.data_ptr(), v.data_ptr(),
+                                                 _stream(t, stream)))
         return v
 
     def build(self, D, q=1.0, vext=None, stream=None, out=None):

@@ -381,6 +381,13 @@ class BeckeGrid(object):
         _lib().napmo_grid_device_arrays(self._this, *[byref(p) for p in ptrs])
         return [p.value for p in ptrs]
 
+    def set_poisson_tolerance(self, tol):
+        """Truncation tolerance (a.u.) of the potential evaluation of this
+        grid's Poisson solves: 0 (default) sums every (l, m) <= lmax as nAPMO
+        does; tol > 0 drops, per atom and radial interval, the highest
+        l-blocks whose bounded contribution to any point stays <= tol."""
+        cext.checked(_lib().napmo_grid_set_poisson_tolerance(self._this, float(tol)))
+
     def show(self):
         print('\nGrid Information:', self._symbol)
         print('-' * (18 + len(self._symbol)))

@@ -187,8 +187,10 @@ int napmo_fock_batch_build(FockBatch *b, void *stream) {
   });
 }
 
-// Autotuner of the batch's launch shape (see the file comment).  Returns the
-// chosen nstream, budget (CTAs) and the time of one batch build in ms.
+// Autotuner of the batch's launch shape (see the file comment), timed on the
+// densities currently in the batch's D buffers (the cost of a truncated
+// Poisson evaluation depends on them).  Returns the chosen nstream, budget
+// (CTAs) and the time of one batch build in ms.
 int napmo_fock_batch_tune(FockBatch *b, void *stream, int reps, int *nstream_out,
                           int *budget_out, double *ms_out) {
   return guarded([&] {

@@ -737,6 +737,31 @@ __global__ void quad_i8_reduce_kernel(int n, int nchunk, int npair, int ntj,
 }
 
 // ---------------------------------------------------------------- density
+// First 64-wide stage of nu that block m (functions 96 m .. 96 m + 95) of the
+// density accumulates: the stage holding function 96 m.
+__host__ __device__ constexpr int dens_first_stage(int m) { return m * DN / KS; }
+
+// D' = the density matrix folded onto block-upper-triangular form, so that
+// sum_{mu,nu} D'[mu][nu] phi_mu phi_nu = sum_{mu,nu} D[mu][nu] phi_mu phi_nu
+// while block m needs only nu >= c(mu) = 64 dens_first_stage(mu / 96):
+//   D'[mu][nu] = 0                        nu < c(mu)
+//              = D[mu][nu] + D[nu][mu]    nu >= c(mu), mu < c(nu) (the mirror
+//                                         entry is skipped by its block)
+//              = D[mu][nu]                otherwise
+// (for a symmetric D the sum is 2 D[mu][nu], exact).
+__global__ void dsym_kernel(const double *__restrict__ D, int n, double *__restrict__ out) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long)n * n) return;
+  const int mu = (int)(i / n), nu = (int)(i % n);
+  const int cmu = dens_first_stage(mu / DN) * KS, cnu = dens_first_stage(nu / DN) * KS;
+  double v = 0.0;
+  if (nu >= cmu) {
+    v = D[i];
+    if (mu < cnu) v += D[(long)nu * n + mu];
+  }
+  out[i] = v;
+}
+
 struct DensArgs {
   const int8_t *a;        // phi^T image [point tile][nks][slices][128 x 64]
   const int *ea;          // exponent per point
@@ -747,9 +772,10 @@ struct DensArgs {
 };
 
 // Persistent: CTA c handles point tiles c, c + gridDim.x, ...  Pass (tile,
-// m): T[p][mu] = sum_nu phi[nu][p] D[mu][nu] for the 128 points and the 96
-// functions of block m, accumulated over all nu in TMEM; the drain adds
-// phi[mu][p] T[p][mu] into rho[p] (thread = point, 48 functions each).
+// m): T[p][mu] = sum_nu phi[nu][p] D'[mu][nu] for the 128 points and the 96
+// functions of block m, accumulated in TMEM over nu >= 64 dens_first_stage(m)
+// (D' is zero below, see dsym_kernel); the drain adds phi[mu][p] T[p][mu]
+// into rho[p] (thread = point, 48 functions each).
 __global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ __align__(8) uint64_t full[NSTAGE], empty[NSTAGE], accfull, accempty, done;
@@ -789,7 +815,7 @@ __global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
       bool ok = true;
       for (int pt = blockIdx.x; pt < g.npt && ok; pt += gridDim.x)
         for (int m = 0; m < g.nmt && ok; ++m)
-          for (int ks = 0; ks < g.nks; ++ks) {
+          for (int ks = dens_first_stage(m); ks < g.nks; ++ks) {
             const int slot = it % NSTAGE;
             if (!wait_phase(&empty[slot], ((it / NSTAGE) & 1) ^ 1, abort)) {
               ok = false;
@@ -815,7 +841,8 @@ __global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
             break;
           }
           fence_after_sync();
-          for (int ks = 0; ks < g.nks; ++ks, ++it) {
+          const int ks0 = dens_first_stage(m);
+          for (int ks = ks0; ks < g.nks; ++ks, ++it) {
             const int slot = it % NSTAGE;
             if (!wait_phase(&full[slot], (it / NSTAGE) & 1, abort)) {
               ok = false;
@@ -823,7 +850,7 @@ __global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
             }
             fence_after_sync();
             const uint32_t sa = smem_u32(smem + slot * STAGE);
-            issue_stage<DN, kDensProducts, true>(tmem, sa, sa + A_BYTES, ks == 0);
+            issue_stage<DN, kDensProducts, true>(tmem, sa, sa + A_BYTES, ks == ks0);
             umma_commit(&empty[slot]);
           }
           if (ok) umma_commit(&accfull);
@@ -943,6 +970,7 @@ struct Int8Plan {
   DevBuf<int8_t> qa, qb, da, dd;
   DevBuf<int> qa_e, qb_e, eg, da_e, dd_e;
   DevBuf<double> sc, isc, gs, work;
+  DevBuf<double> dsym;  // D folded to block-upper-triangular form (density)
 };
 
 // Sizes the kernels for `ctas` resident CTAs (<= 0: the SM count): the
@@ -1008,6 +1036,7 @@ int int8_plan_create(Int8Plan **out, int n, int npoint, const double *phi, long 
   NAPMO_TRY_CUDA(p->da_e.alloc((size_t)p->npt * TM), "alloc");
   NAPMO_TRY_CUDA(p->dd.alloc((size_t)p->nmt * p->nks_d * NSL_D * DN * KS), "alloc int8 D image");
   NAPMO_TRY_CUDA(p->dd_e.alloc((size_t)p->nmt * DN), "alloc");
+  NAPMO_TRY_CUDA(p->dsym.alloc((size_t)n * n), "alloc folded D");
 
   int e = int8_set_budget(p.get(), 0);
   if (e) return e;
@@ -1027,11 +1056,14 @@ void int8_plan_destroy(Int8Plan *p) { delete p; }
 size_t int8_plan_device_bytes(const Int8Plan *p) {
   return p->qa.n + p->qb.n + p->da.n + p->dd.n +
          4 * (p->qa_e.n + p->qb_e.n + p->eg.n + p->da_e.n + p->dd_e.n) +
-         8 * (p->sc.n + p->isc.n + p->gs.n + p->work.n);
+         8 * (p->sc.n + p->isc.n + p->gs.n + p->work.n + p->dsym.n);
 }
 
 int int8_density(Int8Plan *p, const double *D, double *rho, cudaStream_t s) {
-  NAPMO_TRY_CUDA(launch_slice_rows(D, p->n, p->n, p->nmt * DN, p->n, nullptr, nullptr,
+  const long nn = (long)p->n * p->n;
+  dsym_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(D, p->n, p->dsym.p);
+  NAPMO_TRY_CUDA(cudaGetLastError(), "fold D");
+  NAPMO_TRY_CUDA(launch_slice_rows(p->dsym.p, p->n, p->n, p->nmt * DN, p->n, nullptr, nullptr,
                                    p->nks_d * KS, 1, DN, p->nks_d, p->dd.p, p->dd_e.p, s, NSL_D),
                  "slice D");
   DensArgs g{p->da.p, p->da_e.p, p->dd.p, p->dd_e.p, p->nks_d, p->nmt, p->npt, p->npoint, rho};

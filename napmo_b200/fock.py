@@ -220,7 +220,9 @@ class FockBatch(object):
         return self._F
 
     def tune(self, reps=3, stream=None):
-        """Times candidate launch shapes and keeps the fastest; returns
+        """Times candidate launch shapes on the batch's current densities (load
+        representative ones first: the Poisson truncation of the int8 mode
+        makes the cost depend on them) and keeps the fastest; returns
         {'nstream', 'budget', 'ms'}."""
         ns, bud, ms = c_int(), c_int(), c_double()
         checked(cext.lib.napmo_fock_batch_tune(self._this, _stream(self.torch, stream), int(reps),

@@ -102,12 +102,29 @@ def quadrature(phi, wv, wb, w, block=BLOCK):
     return np.triu(F) + np.triu(F, 1).T
 
 
+DENS_BLOCK, DENS_STAGE = 96, 64
+
+
+def fold_density_matrix(D):
+    """D' with sum D' phi phi = sum D phi phi and zeros below each block's
+    first stage: function block m = mu // 96 accumulates nu >= c(mu) =
+    64 ((96 m) // 64); D'[mu][nu] = D[mu][nu] + D[nu][mu] where the mirror
+    entry lies below its own block's cut (mu < c(nu)), D[mu][nu] otherwise."""
+    D = np.asarray(D, np.float64)
+    n = D.shape[0]
+    idx = np.arange(n)
+    c = (idx // DENS_BLOCK) * DENS_BLOCK // DENS_STAGE * DENS_STAGE
+    keep = idx[None, :] >= c[:, None]                  # nu >= c(mu)
+    mirror = keep & (idx[:, None] < c[None, :])        # mu < c(nu)
+    return np.where(keep, D + np.where(mirror, D.T, 0.0), 0.0)
+
+
 def density(phi, D):
     """rho[p] = sum_{mu,nu} D[mu][nu] phi[mu][p] phi[nu][p], int8 slices
-    (phi 4 digits per point, D 5 digits per row), i + j <= 4.  phi [n][N],
-    D [n][n] (symmetric)."""
+    (phi 4 digits per point, D' = fold_density_matrix(D) 5 digits per row),
+    i + j <= 4.  phi [n][N], D [n][n]."""
     phi = np.asarray(phi, np.float64)
-    D = np.asarray(D, np.float64)
+    D = fold_density_matrix(D)
     ep = group_exponent(np.abs(phi).max(axis=0))      # per point
     eD = group_exponent(np.abs(D).max(axis=1))        # per row of D
     dp = digits(phi, ep[None, :])

@@ -315,6 +315,11 @@ int napmo_fock_plan_set_precision(void *plan, int mode);
  * 129-220 sums every (l, m)).  set_precision resets it: 0 for mode 0 (every
  * (l, m), as nAPMO), 1e-10 for mode 1. */
 int napmo_fock_plan_set_poisson_tolerance(void *plan, double tol);
+/* Point screening of the plan's current mode (mode 1 keeps the points with
+ * |w_becke w| max_mu phi_mu(p)^2 >= 1e-24; rho and v are 0 at the others).
+ * *keep: device flags, one int per grid point (null when all points are used);
+ * *nkeep: kept points.  No counterpart in nAPMO (every point is used). */
+int napmo_fock_plan_screening(void *plan, const int **keep, int *nkeep);
 /* Device bytes of the plan's int8 operand images and scratch. */
 long napmo_fock_plan_int8_bytes(void *plan);
 /* Batched Fock builds of many plans (molecules of uneven size) by one CUDA

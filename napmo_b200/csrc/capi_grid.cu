@@ -44,8 +44,15 @@ struct PoissonPlan {
   DevBuf<int> lpiv;
   DevBuf<int> pairs;
   DevBuf<EvalItem> items;
+  int nitems = 0;
   DevBuf<double> pair_v;
   DevBuf<int> lcut;  // per bucket, for truncated evaluations
+  // pair lists of the points kept by a screening mask (built for the last
+  // mask used; the mask is owned by the caller's int8 plan)
+  DevBuf<int> pairs_s;
+  DevBuf<EvalItem> items_s;
+  int nitems_s = 0;
+  const int *screen_key = nullptr;
 };
 
 void free_poisson_plan(PoissonPlan *p) { delete p; }
@@ -200,9 +207,11 @@ int build_poisson_plan(const std::vector<const AtomLayout *> &atoms,
 }
 
 // Bucket-sorted (atom, point) pair lists for the evaluation of the potential
-// at the points (x, y, z) (device, all molecules concatenated).  Built once
-// per grid; about 12 bytes per pair.
+// at the points (x, y, z) (device, all molecules concatenated), into pairs /
+// items; with `keep` only the points whose flag is set.  Built once per grid
+// (and once per screening mask); about 12 bytes per pair.  Synchronises `s`.
 int build_pair_lists(PoissonPlan *plan, const double *x, const double *y, const double *z,
+                     const int *keep, DevBuf<int> &pairs, DevBuf<EvalItem> &items, int &nitems,
                      cudaStream_t s) {
   PoissonDev &d = plan->d;
   const std::vector<PoissonAtom> &ha = plan->h_atoms;
@@ -212,7 +221,8 @@ int build_pair_lists(PoissonPlan *plan, const double *x, const double *y, const 
   NAPMO_TRY_CUDA(bucket_of.alloc(d.npair), "pair lists");
   NAPMO_TRY_CUDA(count.alloc(nb), "pair lists");
   NAPMO_TRY_CUDA(cudaMemsetAsync(count.p, 0, nb * sizeof(int), s), "pair lists");
-  NAPMO_TRY_CUDA(launch_pair_buckets(d, plan->max_mol_npoint, x, y, z, bucket_of.p, count.p, s),
+  NAPMO_TRY_CUDA(launch_pair_buckets(d, plan->max_mol_npoint, x, y, z, keep, bucket_of.p,
+                                     count.p, s),
                  "pair buckets");
   std::vector<int> hc(nb);
   NAPMO_TRY_CUDA(cudaMemcpyAsync(hc.data(), count.p, nb * sizeof(int), cudaMemcpyDeviceToHost, s),
@@ -220,29 +230,45 @@ int build_pair_lists(PoissonPlan *plan, const double *x, const double *y, const 
   NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "pair lists");
   // exclusive scan per atom -> bucket starts (relative to the atom's slice)
   std::vector<int> start(nb);
-  std::vector<EvalItem> items;
+  std::vector<EvalItem> hitems;
   for (int a = 0; a < (int)ha.size(); ++a) {
     int acc = 0;
     for (int b = 0; b <= ha[a].nrad; ++b) {
       const int k = ha[a].bucket_off + b;
       start[k] = acc;
       for (int c = 0; c < hc[k]; c += kEvalChunk)
-        items.push_back(EvalItem{a, b, acc + c, std::min(kEvalChunk, hc[k] - c)});
+        hitems.push_back(EvalItem{a, b, acc + c, std::min(kEvalChunk, hc[k] - c)});
       acc += hc[k];
     }
   }
   NAPMO_TRY_CUDA(count.upload(start, s), "pair lists");  // reused as the cursor
-  NAPMO_TRY_CUDA(plan->pairs.alloc(d.npair), "pair lists");
-  d.pairs = plan->pairs.p;
+  NAPMO_TRY_CUDA(pairs.alloc(d.npair), "pair lists");
+  d.pairs = pairs.p;
   NAPMO_TRY_CUDA(launch_pair_scatter(d, plan->max_mol_npoint, bucket_of.p, count.p, s),
                  "pair scatter");
-  NAPMO_TRY_CUDA(plan->items.upload(items, s), "pair lists");
-  NAPMO_TRY_CUDA(plan->pair_v.alloc(d.npair), "pair lists");
-  NAPMO_TRY_CUDA(plan->lcut.alloc(nb), "pair lists");
+  NAPMO_TRY_CUDA(items.upload(hitems, s), "pair lists");
+  if (!plan->pair_v.p) NAPMO_TRY_CUDA(plan->pair_v.alloc(d.npair), "pair lists");
+  if (!plan->lcut.p) NAPMO_TRY_CUDA(plan->lcut.alloc(nb), "pair lists");
   NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "pair lists");
-  d.items = plan->items.p;
-  d.nitems = (int)items.size();
+  nitems = (int)hitems.size();
   d.pair_v = plan->pair_v.p;
+  return kOk;
+}
+
+// Points the evaluation runs on: all (keep null) or the screened ones.
+static int select_pair_lists(PoissonPlan *p, BeckeGrid *g, const int *keep, cudaStream_t s) {
+  PoissonDev &d = p->d;
+  if (keep && keep != p->screen_key) {
+    p->screen_key = nullptr;
+    const int st = build_pair_lists(p, g->dev.x, g->dev.y, g->dev.z, keep, p->pairs_s,
+                                    p->items_s, p->nitems_s, s);
+    if (st) return st;
+    p->screen_key = keep;
+  }
+  d.keep = keep;
+  d.pairs = keep ? p->pairs_s.p : p->pairs.p;
+  d.items = keep ? p->items_s.p : p->items.p;
+  d.nitems = keep ? p->nitems_s : p->nitems;
   return kOk;
 }
 
@@ -280,19 +306,28 @@ int grid_poisson_plan(BeckeGrid *g, int lmax, cudaStream_t s, PoissonPlan **out)
     delete p;
     return st;
   }
-  st = build_pair_lists(p, g->dev.x, g->dev.y, g->dev.z, s);
+  st = build_pair_lists(p, g->dev.x, g->dev.y, g->dev.z, nullptr, p->pairs, p->items,
+                        p->nitems, s);
   if (st != kOk) {
     delete p;
     return st;
   }
+  p->d.items = p->items.p;
+  p->d.nitems = p->nitems;
   p->lmax = lmax;
   g->poisson = p;
   *out = p;
   return kOk;
 }
 
+// One Poisson solve on the grid's plan: v (=, += with accumulate) = V_H[rho].
+// tol > 0 truncates the evaluation (see eval_tol); keep (grid flags, or null)
+// restricts the evaluation to the flagged points, v = 0 elsewhere (its pair
+// lists are built, synchronously, the first time a mask is used).
 int run_poisson(BeckeGrid *g, PoissonPlan *p, const double *rho_dev, double *v_dev,
-                bool accumulate, cudaStream_t s, double tol) {
+                bool accumulate, cudaStream_t s, double tol, const int *keep) {
+  int st = select_pair_lists(p, g, keep, s);
+  if (st) return st;
   p->d.eval_tol = tol;
   p->d.lcut = tol > 0.0 ? p->lcut.p : nullptr;
   NAPMO_TRY_CUDA(launch_poisson_project(p->d, rho_dev, g->dev.wb, g->dev.w, s), "project");
@@ -1099,7 +1134,7 @@ int napmo_gpu_poisson(BeckeGrid *g, const double *rho_dev, int lmax, double *v_d
     PoissonPlan *p = nullptr;
     int st = grid_poisson_plan(g, lmax, s, &p);
     if (st) return st;
-    st = run_poisson(g, p, rho_dev, v_dev, accumulate != 0, s, g->poisson_tol);
+    st = run_poisson(g, p, rho_dev, v_dev, accumulate != 0, s, g->poisson_tol, nullptr);
     if (st) return st;
     if (raw_y)
       NAPMO_TRY_CUDA(cudaMemcpyAsync(raw_y, p->raw_y.p, p->raw_y.n * sizeof(double),

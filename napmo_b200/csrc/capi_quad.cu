@@ -15,13 +15,20 @@ namespace napmo {
 struct PoissonPlan;
 int grid_poisson_plan(BeckeGrid *g, int lmax, cudaStream_t s, PoissonPlan **out);
 int run_poisson(BeckeGrid *g, PoissonPlan *p, const double *rho_dev, double *v_dev,
-                bool accumulate, cudaStream_t s, double tol);
+                bool accumulate, cudaStream_t s, double tol, const int *keep);
 
 // Truncation tolerance (a.u.) of the Poisson potential evaluation that
 // precision 1 selects: each (atom, radial interval) drops l-blocks whose
 // bounded contribution sums to at most this, so every point's potential moves
 // by at most natom x 1e-10, well inside that mode's 1e-6 Eh energy budget.
 constexpr double kMixedPoissonTol = 1e-10;
+
+// Point screening of precision 1: points with |wb w| max_mu phi_mu(p)^2 below
+// this carry no weight that matters (each changes an element of F by at most
+// 1e-24 |v(p)|); about a fifth of a Becke grid's points (the outer radial
+// shells and points deep in other atoms' cells), skipped by the density, the
+// quadrature and the potential evaluation.
+constexpr double kMixedScreenTol = 1e-24;
 int basis_device(BasisSet *b, cudaStream_t s, const DeviceBasis **out);
 
 // ---------------------------------------------------------------- helpers
@@ -97,6 +104,11 @@ int plan_quadrature(FockPlan *p, double *F, cudaStream_t s) {
   return kOk;
 }
 
+// Screening flags of the plan's grid points in precision 1 (null otherwise).
+const int *plan_keep(const FockPlan *p) {
+  return p->mode == 1 && p->i8 ? int8_plan_keep(p->i8) : nullptr;
+}
+
 // The build chain of napmo_fock_plan_build (stream-ordered, no host
 // synchronisation, no allocation once the grid's Poisson plan exists).
 int fock_build(FockPlan *p, const double *D_dev, double q, const double *vext_dev, double *F_dev,
@@ -109,7 +121,7 @@ int fock_build(FockPlan *p, const double *D_dev, double q, const double *vext_de
   PoissonPlan *pp = nullptr;
   e = grid_poisson_plan(g, p->lmax, s, &pp);
   if (e) return e;
-  e = run_poisson(g, pp, rho, v, false, s, p->poisson_tol);
+  e = run_poisson(g, pp, rho, v, false, s, p->poisson_tol, plan_keep(p));
   if (e) return e;
   NAPMO_TRY_CUDA(launch_combine_weights(g->size, g->dev.wb, g->dev.w, q, v, vext_dev, p->wv.p, s),
                  "weights");
@@ -313,7 +325,7 @@ int napmo_fock_plan_poisson(FockPlan *p, const double *rho_dev, double *v_dev, v
     PoissonPlan *pp = nullptr;
     int e = grid_poisson_plan(p->grid, p->lmax, s, &pp);
     if (e) return e;
-    return run_poisson(p->grid, pp, rho_dev, v_dev, false, s, p->poisson_tol);
+    return run_poisson(p->grid, pp, rho_dev, v_dev, false, s, p->poisson_tol, plan_keep(p));
   });
 }
 
@@ -411,7 +423,7 @@ int napmo_fock_plan_set_precision(FockPlan *p, int mode) {
       cudaStream_t s = napmo::host_api_stream();
       BeckeGrid *g = p->grid;
       int e = napmo::int8_plan_create(&p->i8, p->n, g->size, p->phi.p, p->ld, g->dev.wb,
-                                      g->dev.w, s);
+                                      g->dev.w, napmo::kMixedScreenTol, s);
       if (e) return e;
       NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "int8 operand images");
     }
@@ -428,6 +440,18 @@ int napmo_fock_plan_set_poisson_tolerance(FockPlan *p, double tol) {
   return napmo::guarded([&] {
     NAPMO_REQUIRE(tol >= 0.0 && tol < 1.0, "Poisson tolerance must be in [0, 1)");
     p->poisson_tol = tol;
+    return napmo::kOk;
+  });
+}
+
+// Point screening of the plan's current mode: *keep receives the device flags
+// (one int per grid point, 1 = kept; null when every point is used) and
+// *nkeep the number of kept points.
+int napmo_fock_plan_screening(FockPlan *p, const int **keep, int *nkeep) {
+  return napmo::guarded([&] {
+    const int *k = napmo::plan_keep(p);
+    *keep = k;
+    *nkeep = k ? napmo::int8_plan_npoint(p->i8) : p->grid->size;
     return napmo::kOk;
   });
 }

@@ -49,9 +49,14 @@ cudaError_t launch_quadrature_reduce(int n, int nchunk, const double *work, doub
 // images (built once from phi, wb and w) and the per-call scratch; the calls
 // return library status codes and record g_tc_error on a device timeout.
 struct Int8Plan;
+// screen_tol > 0 keeps only the points with |wb w| max_mu phi_mu^2 >= screen_tol
+// (rho is 0 at the others, which the quadrature skips).
 int int8_plan_create(Int8Plan **out, int n, int npoint, const double *phi, long ld,
-                     const double *wb, const double *w, cudaStream_t s);
+                     const double *wb, const double *w, double screen_tol, cudaStream_t s);
 void int8_plan_destroy(Int8Plan *p);
+// Points the plan keeps, and their flags over the grid (null without screening).
+int int8_plan_npoint(const Int8Plan *p);
+const int *int8_plan_keep(const Int8Plan *p);
 // CTA budget the int8 kernels are sized for (<= 0: the SM count).
 int int8_set_budget(Int8Plan *p, int ctas);
 size_t int8_plan_device_bytes(const Int8Plan *p);

@@ -511,12 +511,16 @@ __device__ __forceinline__ int pair_bucket(const PoissonAtom &at, double px, dou
 
 __global__ void pair_bucket_kernel(PoissonDev P, const double *__restrict__ gx,
                                    const double *__restrict__ gy,
-                                   const double *__restrict__ gz, int *__restrict__ bucket_of,
-                                   int *__restrict__ count) {
+                                   const double *__restrict__ gz, const int *__restrict__ keep,
+                                   int *__restrict__ bucket_of, int *__restrict__ count) {
   const PoissonAtom &at = P.atoms[blockIdx.y];
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= at.mol_npoint) return;
   const int p = at.mol_point_start + q;
+  if (keep && !keep[p]) {  // screened-out point: no pair
+    bucket_of[at.pair_off + q] = -1;
+    return;
+  }
   const int b = pair_bucket(at, gx[p], gy[p], gz[p]);
   bucket_of[at.pair_off + q] = b;
   atomicAdd(&count[at.bucket_off + b], 1);
@@ -528,6 +532,7 @@ __global__ void pair_scatter_kernel(PoissonDev P, const int *__restrict__ bucket
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= at.mol_npoint) return;
   const int b = bucket_of[at.pair_off + q];
+  if (b < 0) return;
   const int pos = atomicAdd(&cursor[at.bucket_off + b], 1);
   P.pairs[at.pair_off + pos] = at.mol_point_start + q;
 }
@@ -735,6 +740,10 @@ __global__ void pairs_reduce_kernel(PoissonDev P, int npoint, double *__restrict
                                     int accumulate) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npoint) return;
+  if (P.keep && !P.keep[p]) {  // screened-out point: no potential evaluated
+    if (!accumulate) out[p] = 0.0;
+    return;
+  }
   int mol = 0;
   if (P.nmol > 1) {
     int lo = 0, hi = P.nmol - 1;
@@ -871,10 +880,10 @@ cudaError_t launch_poisson_radial(const PoissonDev &P, cudaStream_t s) {
 }
 
 cudaError_t launch_pair_buckets(const PoissonDev &P, int max_mol_npoint, const double *x,
-                                const double *y, const double *z, int *bucket_of, int *count,
-                                cudaStream_t s) {
+                                const double *y, const double *z, const int *keep,
+                                int *bucket_of, int *count, cudaStream_t s) {
   dim3 grid((max_mol_npoint + 255) / 256, P.natom);
-  pair_bucket_kernel<<<grid, 256, 0, s>>>(P, x, y, z, bucket_of, count);
+  pair_bucket_kernel<<<grid, 256, 0, s>>>(P, x, y, z, keep, bucket_of, count);
   return cudaGetLastError();
 }
 

@@ -88,6 +88,9 @@ struct PoissonDev {
   // to any pair's potential sums to at most eval_tol (a.u.).
   double eval_tol = 0.0;
   int *lcut = nullptr;
+  // Point screening: with keep set, only points with keep[p] != 0 have pairs
+  // (the pair lists were built with the same flags) and the others get v = 0.
+  const int *keep = nullptr;
 };
 
 // Uploads the Hermite FEM integral tables and solid-harmonic norms to
@@ -106,9 +109,10 @@ cudaError_t launch_poisson_radial(const PoissonDev &P, cudaStream_t s);
 // populations (count[atom.bucket_off + b], atomics on integers), then the
 // bucket-sorted point lists (order inside a bucket is irrelevant: each pair
 // writes its own slot of pair_v).
+// With keep non-null, points whose flag is 0 get no pair (bucket -1).
 cudaError_t launch_pair_buckets(const PoissonDev &P, int max_mol_npoint, const double *x,
-                                const double *y, const double *z, int *bucket_of, int *count,
-                                cudaStream_t s);
+                                const double *y, const double *z, const int *keep,
+                                int *bucket_of, int *count, cudaStream_t s);
 cudaError_t launch_pair_scatter(const PoissonDev &P, int max_mol_npoint, const int *bucket_of,
                                 int *cursor, cudaStream_t s);
 // spline tables -> potential at every grid point (out = or += ).  Uses the

@@ -31,12 +31,23 @@
 // images are built once per grid; wv phi (quadrature) and D (density) are
 // sliced on every call.
 //
+// Point screening.  A plan may keep only the points whose weight can matter:
+// |wb w| max_mu phi_mu(p)^2 >= screen_tol.  Every term of the density's
+// Poisson projection and of the quadrature carries wb w and a product of two
+// basis functions at the point, so a dropped point changes F by at most
+// screen_tol |v(p)| per matrix element.  The images then hold the kept points
+// only (idx[k] = grid index of compacted point k); rho is scattered back and
+// is 0 at dropped points.
+//
 // Kernels: warp 8 (one thread) streams stages into a 3-slot ring
 // (cp.async.bulk + mbarrier transaction counts), warp 9 (one thread) issues
 // the MMAs and owns TMEM, warps 0-7 drain TMEM.  Every mbarrier wait is
 // bounded (2 s of globaltimer, or another role's abort): on timeout the kernel
 // records an error in g_tc_error, the roles stop, copies and MMAs in flight
 // are waited for (bounded) and TMEM is freed before the CTA exits.
+#include <cub/device/device_select.cuh>
+#include <cub/iterator/counting_input_iterator.cuh>
+
 #include <cstdint>
 #include <memory>
 
@@ -291,7 +302,8 @@ template <int NS>
 __global__ void __launch_bounds__(256)
 slice_rows_kernel(const double *__restrict__ src, long ld, int nrows, int ncols,
                   const double *__restrict__ m1, const double *__restrict__ m2, int kb, int nblk,
-                  int TR, int nks, int8_t *__restrict__ img, int *__restrict__ eout) {
+                  int TR, int nks, int8_t *__restrict__ img, int *__restrict__ eout,
+                  const int *__restrict__ cidx) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row = blockIdx.x * 8 + warp;
   const int b = blockIdx.y;
@@ -302,7 +314,10 @@ slice_rows_kernel(const double *__restrict__ src, long ld, int nrows, int ncols,
     const long k = k0 + (long)c * 16;
     if (row < nrows && k + 16 <= ncols) {
       const double *p = src + (long)row * ld + k;
-      if (vec) {
+      if (cidx) {  // column k is source column cidx[k]
+#pragma unroll
+        for (int i = 0; i < 16; ++i) x[i] = __ldg(src + (long)row * ld + __ldg(cidx + k + i));
+      } else if (vec) {
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
           const double2 v = __ldg(reinterpret_cast<const double2 *>(p) + q);
@@ -334,7 +349,7 @@ slice_rows_kernel(const double *__restrict__ src, long ld, int nrows, int ncols,
       for (int i = 0; i < 16; ++i) {
         double v = 0.0;
         if (row < nrows && k + i < ncols) {
-          v = __ldg(src + (long)row * ld + k + i);
+          v = __ldg(src + (long)row * ld + (cidx ? __ldg(cidx + k + i) : k + i));
           if (m1) v *= __ldg(m1 + k + i);
           if (m2) v *= __ldg(m2 + k + i);
         }
@@ -377,15 +392,17 @@ slice_rows_kernel(const double *__restrict__ src, long ld, int nrows, int ncols,
 // thread per point, grid = padded points / 128.
 __global__ void __launch_bounds__(TM)
 slice_points_kernel(const double *__restrict__ phi, long ld, int n, int npoint, int nks,
-                    int8_t *__restrict__ img, int *__restrict__ eout) {
+                    int8_t *__restrict__ img, int *__restrict__ eout,
+                    const int *__restrict__ pidx) {
   const int r = threadIdx.x;
-  const long p = (long)blockIdx.x * TM + r;
-  const bool valid = p < npoint;
+  const long pk = (long)blockIdx.x * TM + r;
+  const bool valid = pk < npoint;
+  const long p = valid && pidx ? __ldg(pidx + pk) : pk;  // grid index of the point
   double mx = 0.0;
   if (valid)
     for (int nu = 0; nu < n; ++nu) mx = fmax(mx, fabs(__ldg(phi + (long)nu * ld + p)));
   const int e = group_exponent(mx);
-  eout[p] = e;
+  eout[pk] = e;
   const double scale = ldexp(1.0, 30 - e);
   const long tile = (long)NSL * TM * KS;
   for (int ks = 0; ks < nks; ++ks) {
@@ -409,11 +426,12 @@ slice_points_kernel(const double *__restrict__ phi, long ld, int n, int npoint, 
 // weight is zero).  Some Lebedev rules have negative weights: the magnitude is
 // split, the sign stays with wv.
 __global__ void balance_kernel(int npoint, const double *__restrict__ wb,
-                               const double *__restrict__ w, double *__restrict__ sc,
-                               double *__restrict__ isc) {
+                               const double *__restrict__ w, const int *__restrict__ pidx,
+                               double *__restrict__ sc, double *__restrict__ isc) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npoint) return;
-  const double t = fabs(wb[p] * w[p]);
+  const int q = pidx ? pidx[p] : p;
+  const double t = fabs(wb[q] * w[q]);
   int c = 0;
   if (t > 0.0 && t < 1e300) {
     int ex;
@@ -430,7 +448,7 @@ __global__ void balance_kernel(int npoint, const double *__restrict__ wb,
 // gs(p) = g(p) 2^-eg[b] (|gs| < 1; exact scaling).
 __global__ void __launch_bounds__(256)
 gscale_kernel(int npoint, const double *__restrict__ wv, const double *__restrict__ isc,
-              double *__restrict__ gs, int *__restrict__ eg) {
+              const int *__restrict__ pidx, double *__restrict__ gs, int *__restrict__ eg) {
   constexpr int PER = QKB / 256;
   __shared__ double red[8];
   const int t = threadIdx.x;
@@ -439,7 +457,7 @@ gscale_kernel(int npoint, const double *__restrict__ wv, const double *__restric
 #pragma unroll
   for (int i = 0; i < PER; ++i) {
     const long p = p0 + i;
-    g[i] = p < npoint ? wv[p] * isc[p] * isc[p] : 0.0;
+    g[i] = p < npoint ? wv[pidx ? pidx[p] : p] * isc[p] * isc[p] : 0.0;
     mx = fmax(mx, fabs(g[i]));
   }
 #pragma unroll
@@ -769,6 +787,7 @@ struct DensArgs {
   const int *ed;          // exponent per row of D
   int nks, nmt, npt, npoint;
   double *rho;
+  const int *pidx;        // grid index of each (kept) point, or null
 };
 
 // Persistent: CTA c handles point tiles c, c + gridDim.x, ...  Pass (tile,
@@ -918,7 +937,8 @@ __global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
       named_sync(1, NEPI);
       if (h == 0 && p < g.npoint) {
         const int ep = __ldg(g.ea + p);
-        g.rho[p] = (red[0][row] + red[1][row]) * pow2(ep - 37) * pow2(ep - 37);
+        g.rho[g.pidx ? __ldg(g.pidx + p) : p] =
+            (red[0][row] + red[1][row]) * pow2(ep - 37) * pow2(ep - 37);
       }
       named_sync(1, NEPI);
     }
@@ -945,21 +965,40 @@ int num_sms() {
 // slices (4 or 5).
 cudaError_t launch_slice_rows(const double *src, long ld, int nrows, int rows_pad, int ncols,
                               const double *m1, const double *m2, int kb, int nblk, int TR,
-                              int nks, int8_t *img, int *e, cudaStream_t s, int ns = NSL) {
+                              int nks, int8_t *img, int *e, cudaStream_t s, int ns = NSL,
+                              const int *cidx = nullptr) {
   if (ns == 5)
-    slice_rows_kernel<5><<<dim3(rows_pad / 8, nblk), 256, 0, s>>>(src, ld, nrows, ncols, m1, m2,
-                                                                  kb, nblk, TR, nks, img, e);
+    slice_rows_kernel<5><<<dim3(rows_pad / 8, nblk), 256, 0, s>>>(
+        src, ld, nrows, ncols, m1, m2, kb, nblk, TR, nks, img, e, cidx);
   else
-    slice_rows_kernel<4><<<dim3(rows_pad / 8, nblk), 256, 0, s>>>(src, ld, nrows, ncols, m1, m2,
-                                                                  kb, nblk, TR, nks, img, e);
+    slice_rows_kernel<4><<<dim3(rows_pad / 8, nblk), 256, 0, s>>>(
+        src, ld, nrows, ncols, m1, m2, kb, nblk, TR, nks, img, e, cidx);
   return cudaGetLastError();
+}
+
+// keep[p] = |wb w| max_mu phi[mu][p]^2 >= tol (1 for every point when
+// tol <= 0); one thread per grid point, phi read once (coalesced over p).
+__global__ void screen_kernel(const double *__restrict__ phi, long ld, int n, int npoint,
+                              const double *__restrict__ wb, const double *__restrict__ w,
+                              double tol, int *__restrict__ keep) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npoint) return;
+  if (!(tol > 0.0)) {
+    keep[p] = 1;
+    return;
+  }
+  double mx = 0.0;
+  for (int mu = 0; mu < n; ++mu) mx = fmax(mx, fabs(__ldg(phi + (long)mu * ld + p)));
+  const double t = fabs(wb[p] * w[p]);
+  keep[p] = (t * mx) * mx >= tol ? 1 : 0;
 }
 
 }  // namespace
 
 // ------------------------------------------------------------------- plan
 struct Int8Plan {
-  int n = 0, npoint = 0;
+  int n = 0, npoint = 0;  // npoint: kept points (all of the grid's without screening)
+  int npoint_grid = 0;    // points of the grid
   long ld = 0;
   // quadrature: A and B images share 128-row tiles (nimg of them, enough for
   // the 96-row B tiles too)
@@ -971,6 +1010,9 @@ struct Int8Plan {
   DevBuf<int> qa_e, qb_e, eg, da_e, dd_e;
   DevBuf<double> sc, isc, gs, work;
   DevBuf<double> dsym;  // D folded to block-upper-triangular form (density)
+  DevBuf<int> keep;     // [npoint_grid] 1 for a kept point
+  DevBuf<int> idx;      // [npoint] grid index of each kept point (screened plans)
+  bool screened = false;
 };
 
 // Sizes the kernels for `ctas` resident CTAs (<= 0: the SM count): the
@@ -1001,14 +1043,48 @@ int int8_set_budget(Int8Plan *p, int ctas) {
 }
 
 int int8_plan_create(Int8Plan **out, int n, int npoint, const double *phi, long ld,
-                     const double *wb, const double *w, cudaStream_t s) {
+                     const double *wb, const double *w, double screen_tol, cudaStream_t s) {
   *out = nullptr;
   NAPMO_REQUIRE(n >= 1 && n <= 8192, "int8 contractions need 1 <= n <= 8192 basis functions");
   NAPMO_REQUIRE(npoint >= 1, "empty grid");
   std::unique_ptr<Int8Plan> p(new Int8Plan);
   p->n = n;
-  p->npoint = npoint;
+  p->npoint_grid = npoint;
   p->ld = ld;
+  // point screening: keep flags, then the kept points' grid indices
+  NAPMO_TRY_CUDA(p->keep.alloc(npoint), "alloc screening flags");
+  screen_kernel<<<(npoint + 255) / 256, 256, 0, s>>>(phi, ld, n, npoint, wb, w, screen_tol,
+                                                      p->keep.p);
+  NAPMO_TRY_CUDA(cudaGetLastError(), "screen points");
+  if (screen_tol > 0.0) {
+    DevBuf<int> sel, cnt;
+    DevBuf<uint8_t> tmp;
+    NAPMO_TRY_CUDA(sel.alloc(npoint), "alloc screening");
+    NAPMO_TRY_CUDA(cnt.alloc(1), "alloc screening");
+    cub::CountingInputIterator<int> first(0);
+    size_t tb = 0;
+    NAPMO_TRY_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, first, p->keep.p, sel.p, cnt.p,
+                                              npoint, s),
+                   "screening scan size");
+    NAPMO_TRY_CUDA(tmp.alloc(tb + 1), "alloc screening");
+    NAPMO_TRY_CUDA(cub::DeviceSelect::Flagged(tmp.p, tb, first, p->keep.p, sel.p, cnt.p,
+                                              npoint, s),
+                   "screening scan");
+    int nkeep = 0;
+    NAPMO_TRY_CUDA(cudaMemcpyAsync(&nkeep, cnt.p, sizeof(int), cudaMemcpyDeviceToHost, s),
+                   "screening count");
+    NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "screening");
+    NAPMO_REQUIRE(nkeep >= 1, "point screening left no points");
+    NAPMO_TRY_CUDA(p->idx.alloc(nkeep), "alloc kept points");
+    NAPMO_TRY_CUDA(cudaMemcpyAsync(p->idx.p, sel.p, nkeep * sizeof(int),
+                                   cudaMemcpyDeviceToDevice, s),
+                   "kept points");
+    NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "screening");
+    npoint = nkeep;
+    p->screened = true;
+  }
+  const int *pidx = p->screened ? p->idx.p : nullptr;
+  p->npoint = npoint;
   p->nblk = (npoint + QKB - 1) / QKB;
   p->nks_q = p->nblk * QBLK_STAGES;
   p->nti = (n + TM - 1) / TM;
@@ -1040,12 +1116,13 @@ int int8_plan_create(Int8Plan **out, int n, int npoint, const double *phi, long 
 
   int e = int8_set_budget(p.get(), 0);
   if (e) return e;
-  balance_kernel<<<(npoint + 255) / 256, 256, 0, s>>>(npoint, wb, w, p->sc.p, p->isc.p);
+  balance_kernel<<<(npoint + 255) / 256, 256, 0, s>>>(npoint, wb, w, pidx, p->sc.p, p->isc.p);
   NAPMO_TRY_CUDA(cudaGetLastError(), "balance");
   NAPMO_TRY_CUDA(launch_slice_rows(phi, ld, n, p->nimg * TM, npoint, p->sc.p, nullptr, QKB,
-                                   p->nblk, TM, p->nks_q, p->qa.p, p->qa_e.p, s),
+                                   p->nblk, TM, p->nks_q, p->qa.p, p->qa_e.p, s, NSL, pidx),
                  "slice phi (quadrature)");
-  slice_points_kernel<<<p->npt, TM, 0, s>>>(phi, ld, n, npoint, p->nks_d, p->da.p, p->da_e.p);
+  slice_points_kernel<<<p->npt, TM, 0, s>>>(phi, ld, n, npoint, p->nks_d, p->da.p, p->da_e.p,
+                                             pidx);
   NAPMO_TRY_CUDA(cudaGetLastError(), "slice phi (density)");
   *out = p.release();
   return kOk;
@@ -1056,8 +1133,13 @@ void int8_plan_destroy(Int8Plan *p) { delete p; }
 size_t int8_plan_device_bytes(const Int8Plan *p) {
   return p->qa.n + p->qb.n + p->da.n + p->dd.n +
          4 * (p->qa_e.n + p->qb_e.n + p->eg.n + p->da_e.n + p->dd_e.n) +
+         4 * (p->keep.n + p->idx.n) +
          8 * (p->sc.n + p->isc.n + p->gs.n + p->work.n + p->dsym.n);
 }
+
+int int8_plan_npoint(const Int8Plan *p) { return p->npoint; }
+
+const int *int8_plan_keep(const Int8Plan *p) { return p->screened ? p->keep.p : nullptr; }
 
 int int8_density(Int8Plan *p, const double *D, double *rho, cudaStream_t s) {
   const long nn = (long)p->n * p->n;
@@ -1066,7 +1148,10 @@ int int8_density(Int8Plan *p, const double *D, double *rho, cudaStream_t s) {
   NAPMO_TRY_CUDA(launch_slice_rows(p->dsym.p, p->n, p->n, p->nmt * DN, p->n, nullptr, nullptr,
                                    p->nks_d * KS, 1, DN, p->nks_d, p->dd.p, p->dd_e.p, s, NSL_D),
                  "slice D");
-  DensArgs g{p->da.p, p->da_e.p, p->dd.p, p->dd_e.p, p->nks_d, p->nmt, p->npt, p->npoint, rho};
+  if (p->screened)  // dropped points get rho = 0
+    NAPMO_TRY_CUDA(cudaMemsetAsync(rho, 0, (size_t)p->npoint_grid * sizeof(double), s), "rho");
+  DensArgs g{p->da.p, p->da_e.p, p->dd.p, p->dd_e.p, p->nks_d, p->nmt, p->npt, p->npoint, rho,
+             p->screened ? p->idx.p : nullptr};
   const int smem = NSTAGE * (stage_bytes(TM) + NSL_D * DN * KS);
   NAPMO_TRY_CUDA(cudaFuncSetAttribute(density_i8_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
@@ -1080,7 +1165,8 @@ int int8_density(Int8Plan *p, const double *D, double *rho, cudaStream_t s) {
 int int8_quadrature(Int8Plan *p, const double *phi, const double *wv, double *F,
                     cudaStream_t s) {
   (void)phi;
-  gscale_kernel<<<p->nblk, 256, 0, s>>>(p->npoint, wv, p->isc.p, p->gs.p, p->eg.p);
+  gscale_kernel<<<p->nblk, 256, 0, s>>>(p->npoint, wv, p->isc.p,
+                                        p->screened ? p->idx.p : nullptr, p->gs.p, p->eg.p);
   NAPMO_TRY_CUDA(cudaGetLastError(), "block scales");
   scale_image_kernel<<<dim3((p->n + 7) / 8, p->nblk), 128, 0, s>>>(
       p->qa.p, p->qb.p, p->gs.p, p->qa_e.p, p->eg.p, p->qb_e.p, p->nks_q, p->nblk);

@@ -77,6 +77,16 @@ class FockBuilder(object):
         to at most `tol` are skipped (0: none)."""
         checked(cext.lib.napmo_fock_plan_set_poisson_tolerance(self._plan, float(tol)))
 
+    def kept_points(self):
+        """Boolean tensor of the grid points the current mode uses, or None
+        when it uses all ('int8x4' screens out the points with
+        |w_becke w| max_mu phi_mu^2 < 1e-24; rho and v are 0 there)."""
+        keep, nkeep = c_void_p(), c_int()
+        checked(cext.lib.napmo_fock_plan_screening(self._plan, byref(keep), byref(nkeep)))
+        if not keep.value:
+            return None
+        return _view(self.torch, keep.value, (self.npoint,), '<i4') != 0
+
     def tc_status(self, reset=True, stream=None):
         """Error word of the tensor-core kernels (0: none); synchronises the stream."""
         return cext.lib.napmo_tc_status(_stream(self.torch, stream), 1 if reset else 0)
@@ -160,13 +170,13 @@ class FockBuilder(object):
         return _view(self.torch, self._phi_ptr, (self.n, self.ld))
 
 
-def _view(torch, ptr, shape):
+def _view(torch, ptr, shape, typestr='<f8'):
     """A torch tensor aliasing libnapmo device memory (read-only use)."""
     n = int(np.prod(shape))
 
     class _Holder(object):
         __cuda_array_interface__ = {
-            'shape': (n,), 'typestr': '<f8', 'data': (ptr, False), 'version': 2}
+            'shape': (n,), 'typestr': typestr, 'data': (ptr, False), 'version': 2}
 
     return torch.as_tensor(_Holder(), device='cuda').view(*shape)
 

@@ -5,6 +5,10 @@ compute exactly this scheme (integer parts exact, FP64 sums reordered) and,
 separately, how far the scheme is from the FP64 path.  nAPMO has no mixed
 precision, so this file restates the library's own scheme, not nAPMO code.
 
+Point screening (screen()): the int8 mode keeps only the points whose
+weight can matter and runs both contractions on those points, compacted in
+grid order; rho is 0 at the others.
+
 Scheme: the values x of a group (one basis function over 1024 points for the
 quadrature; all basis functions at one point, and one row of D, for the
 density) share e = frexp exponent of max |x| (clamped at -960); each value is
@@ -103,6 +107,15 @@ def quadrature(phi, wv, wb, w, block=BLOCK):
 
 
 DENS_BLOCK, DENS_STAGE = 96, 64
+SCREEN_TOL = 1e-24
+
+
+def screen(phi, wb, w, tol=SCREEN_TOL):
+    """Points kept by the int8 mode's screening: (|wb w| max_mu |phi_mu|)
+    max_mu |phi_mu| >= tol, in that order of products (boolean [N])."""
+    mx = np.abs(np.asarray(phi, np.float64)).max(axis=0)
+    t = np.abs(np.asarray(wb, np.float64) * np.asarray(w, np.float64))
+    return (t * mx) * mx >= tol
 
 
 def fold_density_matrix(D):

@@ -1,10 +1,11 @@
 """Int8-slice tensor-core contractions (tcgen05 kind::i8) on the GPU.
 
 Two checks per result: (1) the kernels compute exactly the scheme restated in
-oracle/ozaki.py (integer parts exact; only the order of the final FP64 sums
-differs, so agreement to 1e-12 relative), and (2) the scheme's distance from
-the FP64 path: rho within 1e-7 of max|rho|, F within 1e-8 of max|F|, and the
-Fock-build energy 1/2 tr(D F) within 1e-6 Eh.
+oracle/ozaki.py (the same screened points; integer parts exact; only the
+order of the final FP64 sums differs, so agreement to 1e-12 relative), and
+(2) the scheme's distance from the FP64 path: rho within 1e-7 of max|rho| at
+the kept points (and wb w rho negligible at the others), F within 1e-8 of
+max|F|, and the Fock-build energy 1/2 tr(D F) within 1e-6 Eh.
 """
 import numpy as np
 import pytest
@@ -26,6 +27,27 @@ def _phi_host(fb):
     return fb.phi().cpu().numpy()[:, :fb.npoint].copy()
 
 
+def _screened_scheme(tc, phi, grid):
+    """Kept points of the int8 plan, checked against the oracle's screen."""
+    import ozaki
+    keep = tc.kept_points().cpu().numpy()
+    assert np.array_equal(keep, ozaki.screen(phi, grid.becke_weights, grid.weights))
+    assert 0 < keep.sum() <= keep.size
+    return keep
+
+
+def _scheme_density(phi, D, keep):
+    import ozaki
+    rs = np.zeros(phi.shape[1])
+    rs[keep] = ozaki.density(phi[:, keep], D)
+    return rs
+
+
+def _scheme_quadrature(phi, wv, wb, w, keep):
+    import ozaki
+    return ozaki.quadrature(phi[:, keep], wv[keep], wb[keep], w[keep])
+
+
 @pytest.mark.parametrize('atoms,nrad,nang', [(H2O, 50, 110), (BUTANE, 40, 110)])
 def test_int8_matches_scheme_and_fp64(atoms, nrad, nang):
     import napmo_b200 as nb
@@ -39,19 +61,24 @@ def test_int8_matches_scheme_and_fp64(atoms, nrad, nang):
     f64 = nb.FockBuilder(grid, basis, -1)
     tc = nb.FockBuilder(grid, basis, -1, precision='int8x4')
     phi = _phi_host(f64)
+    wb, w = grid.becke_weights, grid.weights
+    keep = _screened_scheme(tc, phi, grid)
+    assert f64.kept_points() is None
     r64 = f64.density(D).cpu().numpy()
     r8 = tc.density(D).cpu().numpy()
     assert tc.tc_status() == 0
-    rs = ozaki.density(phi, D)
+    rs = _scheme_density(phi, D, keep)
     assert np.abs(r8 - rs).max() <= 1e-12 * np.abs(rs).max()
-    assert np.abs(r8 - r64).max() <= 1e-7 * np.abs(r64).max()
+    assert np.abs(r8 - r64)[keep].max() <= 1e-7 * np.abs(r64).max()
+    assert np.all(r8[~keep] == 0.0)
+    # |rho(p)| <= sum |D| max phi^2 and |wb w| max phi^2 < 1e-24 at a dropped point
+    assert np.abs(wb * w * r64)[~keep].sum() <= (~keep).sum() * 1e-24 * np.abs(D).sum()
 
-    wb, w = grid.becke_weights, grid.weights
     F64 = f64.quadrature(1.0, v).cpu().numpy()
     F8 = tc.quadrature(1.0, v).cpu().numpy()
     assert tc.tc_status() == 0
     assert np.array_equal(F8, F8.T)
-    Fs = ozaki.quadrature(phi, (wb * w) * v, wb, w)
+    Fs = _scheme_quadrature(phi, (wb * w) * v, wb, w, keep)
     assert np.abs(F8 - Fs).max() <= 1e-12 * np.abs(Fs).max()
     assert np.abs(F8 - F64).max() <= 1e-8 * np.abs(F64).max()
     # determinism: same bits on a second call
@@ -75,7 +102,9 @@ def test_int8_uneven_grid_and_signed_potential():
     F8 = tc.quadrature(1.0, v).cpu().numpy()
     F64 = f64.quadrature(1.0, v).cpu().numpy()
     wb, w = grid.becke_weights, grid.weights
-    Fs = ozaki.quadrature(_phi_host(f64), (wb * w) * v, wb, w)
+    phi = _phi_host(f64)
+    keep = _screened_scheme(tc, phi, grid)
+    Fs = _scheme_quadrature(phi, (wb * w) * v, wb, w, keep)
     assert tc.tc_status() == 0
     assert np.abs(F8 - Fs).max() <= 1e-12 * np.abs(Fs).max()
     assert np.abs(F8 - F64).max() <= 1e-8 * np.abs(F64).max()

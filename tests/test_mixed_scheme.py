@@ -66,3 +66,24 @@ def test_scheme_density_accuracy(h2o_case):
     r8 = ozaki.density(phi, D)
     assert np.abs(r8 - rho).max() <= 1e-7 * np.abs(rho).max()
     assert abs(g.integrate(r8) - g.integrate(rho)) <= 1e-8
+
+
+def test_screened_scheme_matches_fp64(h2o_case):
+    """The int8 mode's point screening: the dropped points carry
+    |wb w| max phi^2 < 1e-24, so the screened quadrature and the screened
+    density's integral match the full FP64 ones as closely as the unscreened
+    scheme does."""
+    import ozaki
+    g, phi, D, rho, v = h2o_case
+    keep = ozaki.screen(phi, g.becke, g.weights)
+    mx = np.abs(phi).max(axis=0)
+    assert np.array_equal(keep, (np.abs(g.becke * g.weights) * mx) * mx >= 1e-24)
+    assert 0 < keep.sum() < keep.size       # this grid has points to drop
+    wv = g.becke * g.weights * v
+    F64 = (phi * wv) @ phi.T
+    F8 = ozaki.quadrature(phi[:, keep], wv[keep], g.becke[keep], g.weights[keep])
+    assert np.abs(F8 - F64).max() <= 1e-8 * np.abs(F64).max()
+    r8 = np.zeros_like(rho)
+    r8[keep] = ozaki.density(phi[:, keep], D)
+    assert abs(g.integrate(r8) - g.integrate(rho)) <= 1e-8
+    assert np.abs(g.becke * g.weights * rho)[~keep].sum() <= 1e-20

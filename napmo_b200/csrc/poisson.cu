@@ -117,7 +117,8 @@ project_kernel(PoissonDev P, const double *__restrict__ rho,
     double acc[kProjShells];
 #pragma unroll
     for (int s = 0; s < kProjShells; ++s) acc[s] = 0.0;
-    for (int j = 0; j < nang; ++j) {
+#pragma unroll 4
+    for (int j = 0; j < nang; ++j) {  // unrolled: several table loads in flight
       const double y = __ldg(Y + (long)j * lsize + lm);
 #pragma unroll
       for (int s = 0; s < kProjShells; ++s) acc[s] = fma(y, g[s * nang + j], acc[s]);
@@ -240,6 +241,8 @@ __global__ void radial_factor_kernel(PoissonDev P) {
   for (int e = tid; e < n2 * kW; e += nt) lu[e] = band[e];
 }
 
+// CTA = (system (atom, l), chunk of ncol of its 2l + 1 columns m); the columns
+// are independent once the atom's radial tables are staged.
 __global__ void radial_kernel(PoissonDev P, int ncol) {
   extern __shared__ double sm[];
   const int sys = blockIdx.x;
@@ -247,7 +250,9 @@ __global__ void radial_kernel(PoissonDev P, int ncol) {
   const int l = P.sys_l[sys];
   const int n = at.nrad, n2 = 2 * n;
   const int lsize = (at.lmax + 1) * (at.lmax + 1);
-  const int nm = 2 * l + 1;
+  const int c0 = blockIdx.y * ncol;  // first column (m index) of this chunk
+  if (c0 >= 2 * l + 1) return;
+  const int nm = min(ncol, 2 * l + 1 - c0);  // columns of this chunk
   const int tid = threadIdx.x, nt = blockDim.x;
   double *R = sm;                    // n2 * ncol  (row-major, column = m)
   double *buf = R + n2 * ncol;       // n * ncol   (spline t-derivatives)
@@ -274,7 +279,7 @@ __global__ void radial_kernel(PoissonDev P, int ncol) {
       rl[i] = pow(r[i], (double)l);
       rm[i] = pow(r[i], (double)(-l - 1));
     }
-    const double *proj = P.proj + at.proj_off + l * l;
+    const double *proj = P.proj + at.proj_off + l * l + c0;
     for (int e = tid; e < n * nm; e += nt) {
       const int i = e / nm, c = e - i * nm;
       Y[i * ncol + c] = proj[(long)i * lsize + c];
@@ -312,6 +317,9 @@ __global__ void radial_kernel(PoissonDev P, int ncol) {
     long lo = 2 * (row / 2 - 1), hi = 2 * (row / 2 + 2);
     if (lo < 0) lo = 0;
     if (hi > n2) hi = n2;
+    double ov[6];  // the row's Hermite overlaps, shared by all columns
+#pragma unroll
+    for (int t = 0; t < 6; ++t) ov[t] = lo + t < hi ? ov2_d(xmax, row, 0, lo + t, 0) : 0.0;
     for (int c = 0; c < nm; ++c) {
       double acc = 0.0;
       if (row == 0) {
@@ -319,7 +327,10 @@ __global__ void radial_kernel(PoissonDev P, int ncol) {
       } else if (row == n2 - 2) {
         acc = bc[ncol + c];
       } else {
-        for (long k = lo; k < hi; ++k) {
+#pragma unroll
+        for (int t = 0; t < 6; ++t) {
+          const long k = lo + t;
+          if (k >= hi) break;
           const int i = (int)(k / 2);
           const double fy = -kPI4 * Y[i * ncol + c];
           const double jsq = j1[i] * j1[i];
@@ -330,18 +341,27 @@ __global__ void radial_kernel(PoissonDev P, int ncol) {
             const double fdx = -kPI4 * (buf[i * ncol + c] / j1[i]);
             fk = (fdx * jsq + 2 * fy * j2[i]) * j1[i];
           }
-          if (fk != 0) acc += fk * ov2_d(xmax, row, 0, k, 0);
+          if (fk != 0) acc += fk * ov[t];
         }
       }
       R[row * ncol + c] = acc;
     }
   }
   __syncthreads();
+  // -- 1c. the system's LU factors into shared memory, over buf and Y (no
+  // longer needed): the substitutions below are chains of dependent steps
+  double *sband = buf;                 // [n2][kW]
+  double *smult = sband + n2 * kW;     // [n2][kKL]
+  int *spiv = reinterpret_cast<int *>(smult + n2 * kKL);
+  for (int e = tid; e < n2 * kW; e += nt) sband[e] = band[e];
+  for (int e = tid; e < n2 * kKL; e += nt) smult[e] = mult[e];
+  for (int e = tid; e < n2; e += nt) spiv[e] = piv[e];
+  __syncthreads();
   // -- 2. forward elimination with the stored factors, one column (m) per
   // thread (the same operations, in the same order, as during the factoring)
   for (int c = tid; c < nm; c += nt) {
     for (int k = 0; k < n2; ++k) {
-      const int p = piv[k];
+      const int p = spiv[k];
       if (p != k) {
         const double t = R[k * ncol + c];
         R[k * ncol + c] = R[p * ncol + c];
@@ -349,7 +369,7 @@ __global__ void radial_kernel(PoissonDev P, int ncol) {
       }
       const int im = min(k + kKL, n2 - 1);
       const double rk = R[k * ncol + c];
-      for (int i = k + 1; i <= im; ++i) R[i * ncol + c] -= mult[k * kKL + (i - k - 1)] * rk;
+      for (int i = k + 1; i <= im; ++i) R[i * ncol + c] -= smult[k * kKL + (i - k - 1)] * rk;
     }
   }
   // -- 3. back substitution, one column (m) per thread
@@ -357,8 +377,8 @@ __global__ void radial_kernel(PoissonDev P, int ncol) {
     for (int i = n2 - 1; i >= 0; --i) {
       double x = R[i * ncol + c];
       const int je = min(i + kKL + kKU, n2 - 1);
-      for (int j = i + 1; j <= je; ++j) x -= ABc(band, i, j) * R[j * ncol + c];
-      R[i * ncol + c] = x / ABc(band, i, i);
+      for (int j = i + 1; j <= je; ++j) x -= AB(sband, i, j) * R[j * ncol + c];
+      R[i * ncol + c] = x / AB(sband, i, i);
     }
   }
   __syncthreads();
@@ -366,7 +386,7 @@ __global__ void radial_kernel(PoissonDev P, int ncol) {
   const double fl = sqrt((double)(2 * l + 1)) * kInvSqrt4Pi;
   for (int e = tid; e < n * nm; e += nt) {
     const int c = e / n, i = e - c * n;
-    const long o = at.raw_off + (long)(l * l + c) * n + i;
+    const long o = at.raw_off + (long)(l * l + c0 + c) * n + i;
     P.raw_y[o] = R[(2 * i) * ncol + c];
     P.raw_dt[o] = (R[(2 * i + 1) * ncol + c] / j1[i]) * j1[i];
   }
@@ -376,14 +396,14 @@ __global__ void radial_kernel(PoissonDev P, int ncol) {
     const double d0 = (R[(2 * j + 1) * ncol + c] / j1[j]) * j1[j];
     const double d1 = (R[(2 * j + 3) * ncol + c] / j1[j + 1]) * j1[j + 1];
     const double z = y1 - y0;
-    double *cf = P.spl + at.spl_off + ((long)j * lsize + l * l + c) * 4;
+    double *cf = P.spl + at.spl_off + ((long)j * lsize + l * l + c0 + c) * 4;
     cf[0] = y0 * fl;
     cf[1] = d0 * fl;
     cf[2] = (3 * z - 2 * d0 - d1) * fl;
     cf[3] = (-2 * z + d0 + d1) * fl;
   }
   for (int c = tid; c < nm; c += nt) {
-    const int lm = l * l + c;
+    const int lm = l * l + c0 + c;
     P.amp[at.amp_off + lm * 2 + 0] = R[c] / pow(at.first_x, (double)l) * fl;
     P.amp[at.amp_off + lm * 2 + 1] = R[(2 * (n - 1)) * ncol + c] * pow(at.last_x, (double)(l + 1)) * fl;
   }
@@ -843,7 +863,11 @@ cudaError_t launch_poisson_project(const PoissonDev &P, const double *rho,
   return cudaGetLastError();
 }
 
-int poisson_radial_ncol(int max_lmax) { return ((2 * max_lmax + 1 + 31) / 32) * 32; }
+// Columns (m) per radial CTA: one warp; systems with 2l + 1 > 32 use several CTAs.
+int poisson_radial_ncol(int max_lmax) {
+  (void)max_lmax;
+  return 32;
+}
 
 size_t poisson_radial_smem(int max_nrad, int max_lmax) {
   const int ncol = poisson_radial_ncol(max_lmax);
@@ -875,7 +899,8 @@ cudaError_t launch_poisson_radial(const PoissonDev &P, cudaStream_t s) {
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
-  radial_kernel<<<P.nsys, ncol, smem, s>>>(P, ncol);
+  const int nchunk = (2 * P.max_lmax + 1 + ncol - 1) / ncol;
+  radial_kernel<<<dim3(P.nsys, nchunk), ncol, smem, s>>>(P, ncol);
   return cudaGetLastError();
 }
 

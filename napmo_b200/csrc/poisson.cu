@@ -242,7 +242,8 @@ __global__ void radial_factor_kernel(PoissonDev P) {
 }
 
 // CTA = (system (atom, l), chunk of ncol of its 2l + 1 columns m); the columns
-// are independent once the atom's radial tables are staged.
+// are independent once the atom's radial tables are staged.  Column loops run
+// one thread per column; row loops stride over the whole block.
 __global__ void radial_kernel(PoissonDev P, int ncol) {
   extern __shared__ double sm[];
   const int sys = blockIdx.x;
@@ -529,32 +530,42 @@ __device__ __forceinline__ int pair_bucket(const PoissonAtom &at, double px, dou
   return 1 + j;
 }
 
+// Neighbouring points mostly fall in the same bucket of an atom, so the
+// counters are bumped once per group of lanes with equal buckets (the lowest
+// lane adds the group's size): one atomic per group instead of per pair.
+__device__ __forceinline__ int lanes_below(unsigned m) {
+  return __popc(m & ((1u << (threadIdx.x & 31)) - 1u));
+}
+
 __global__ void pair_bucket_kernel(PoissonDev P, const double *__restrict__ gx,
                                    const double *__restrict__ gy,
                                    const double *__restrict__ gz, const int *__restrict__ keep,
                                    int *__restrict__ bucket_of, int *__restrict__ count) {
   const PoissonAtom &at = P.atoms[blockIdx.y];
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= at.mol_npoint) return;
-  const int p = at.mol_point_start + q;
-  if (keep && !keep[p]) {  // screened-out point: no pair
-    bucket_of[at.pair_off + q] = -1;
-    return;
+  const bool in = q < at.mol_npoint;
+  int b = -1;
+  if (in) {
+    const int p = at.mol_point_start + q;
+    if (!keep || keep[p]) b = pair_bucket(at, gx[p], gy[p], gz[p]);  // -1: screened out
+    bucket_of[at.pair_off + q] = b;
   }
-  const int b = pair_bucket(at, gx[p], gy[p], gz[p]);
-  bucket_of[at.pair_off + q] = b;
-  atomicAdd(&count[at.bucket_off + b], 1);
+  const unsigned group = __match_any_sync(0xffffffffu, b);
+  if (b >= 0 && lanes_below(group) == 0) atomicAdd(&count[at.bucket_off + b], __popc(group));
 }
 
 __global__ void pair_scatter_kernel(PoissonDev P, const int *__restrict__ bucket_of,
                                     int *__restrict__ cursor) {
   const PoissonAtom &at = P.atoms[blockIdx.y];
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= at.mol_npoint) return;
-  const int b = bucket_of[at.pair_off + q];
-  if (b < 0) return;
-  const int pos = atomicAdd(&cursor[at.bucket_off + b], 1);
-  P.pairs[at.pair_off + pos] = at.mol_point_start + q;
+  const int b = q < at.mol_npoint ? bucket_of[at.pair_off + q] : -1;
+  const unsigned group = __match_any_sync(0xffffffffu, b);
+  const int leader = __ffs(group) - 1;
+  int base = 0;
+  if (b >= 0 && (int)(threadIdx.x & 31) == leader)
+    base = atomicAdd(&cursor[at.bucket_off + b], __popc(group));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (b >= 0) P.pairs[at.pair_off + base + lanes_below(group)] = at.mol_point_start + q;
 }
 
 // One CTA per EvalItem: the coefficient block of the item's spline interval
@@ -900,7 +911,9 @@ cudaError_t launch_poisson_radial(const PoissonDev &P, cudaStream_t s) {
                                        (int)smem);
   if (e != cudaSuccess) return e;
   const int nchunk = (2 * P.max_lmax + 1 + ncol - 1) / ncol;
-  radial_kernel<<<dim3(P.nsys, nchunk), ncol, smem, s>>>(P, ncol);
+  // 4 warps: the per-column chains (spline, substitutions) use the first, the
+  // row-parallel stages (right-hand side, outputs, staging) all four
+  radial_kernel<<<dim3(P.nsys, nchunk), 4 * ncol, smem, s>>>(P, ncol);
   return cudaGetLastError();
 }
 

@@ -733,6 +733,7 @@ eval_pairs_kernel(PoissonDev P, const double *__restrict__ gx,
     for (int e = threadIdx.x; e < lkeep; e += blockDim.x)
       cf[e] = src[2 * e + (region == 1 ? 0 : 1)];
   }
+  __syncthreads();
   // thread t evaluates the pairs t and t + blockDim.x of the item (the
   // second may be absent: it then repeats the first and is not stored)
   const int t = threadIdx.x;

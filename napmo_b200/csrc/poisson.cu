@@ -32,10 +32,14 @@ namespace {
 __constant__ double c_ov2[5 * 2 * 5 * 2];
 __constant__ double c_ov3[5 * 2 * 5 * 2 * 5 * 2];
 __constant__ double c_shnorm[(kMaxLmax + 1) * (kMaxLmax + 1)];  // [l][m]
-// normalised solid-harmonic recursion along l at fixed m (evaluation kernel):
-// q_l = a_lm z q_(l-1) - b_lm q_(l-2), q_m = start_m
-__constant__ double c_rec_a[(kMaxLmax + 1) * (kMaxLmax + 1)];
-__constant__ double c_rec_b[(kMaxLmax + 1) * (kMaxLmax + 1)];
+// Normalised solid harmonics by a recursion along l at fixed m (evaluation
+// kernel).  With q_l = a_lm z q_(l-1) - b_lm q_(l-2) and q_m = start_m, the
+// rescaled q~_l = q_l / gamma_lm (gamma_m = gamma_(m+1) = 1, gamma_l =
+// b_lm gamma_(l-2)) obey q~_l = A_lm z q~_(l-1) - q~_(l-2) with
+// A_lm = a_lm gamma_(l-1) / gamma_l: one product and one FMA per step.  The
+// coefficients multiplying q_l are scaled by gamma_lm when staged.
+__constant__ double c_rec_a[(kMaxLmax + 1) * (kMaxLmax + 1)];      // A_lm at [l][m]
+__constant__ double c_rec_gamma[(kMaxLmax + 1) * (kMaxLmax + 1)];  // gamma at [lm]
 __constant__ double c_rec_start[kMaxLmax + 1];
 
 constexpr double kPI4 = 4.0 * M_PI;
@@ -617,10 +621,12 @@ __device__ __forceinline__ void pair_values(const double *cf, int lmaxA, const d
   // Normalised solid harmonics of the unit vector, m outer and l inner:
   // q_l^m = nrm_lm Pi_l^m with Pi_m^m = (2m-1)!!, Pi_(m+1)^m = (2m+1) z Pi_m^m,
   // Pi_l^m = ((2l-1) z Pi_(l-1)^m - (l+m-1) Pi_(l-2)^m) / (l-m) (|u| = 1);
-  // the normalisation is folded into the recursion constants (c_rec_a/b,
-  // c_rec_start).  S_l0 = q_l^0; S_lm (cos, sin) = q_l^m Re/Im (x + iy)^m at
-  // lm = l^2 + 2m - 1, l^2 + 2m: the values and lm order of solid_harmonics.h,
-  // evaluated column by column so that only a few are live.
+  // the normalisation is folded into the recursion constants (c_rec_a,
+  // c_rec_start) and the recursion runs on q~ = q / gamma (c_rec_gamma), whose
+  // scale the staged coefficients carry.  S_l0 = q_l^0; S_lm (cos, sin) =
+  // q_l^m Re/Im (x + iy)^m at lm = l^2 + 2m - 1, l^2 + 2m: the values and lm
+  // order of solid_harmonics.h, evaluated column by column so that only a few
+  // are live.
 #pragma unroll
   for (int m = 0; m <= LMAX; ++m) {
     if (m > lmaxA) break;
@@ -644,7 +650,7 @@ __device__ __forceinline__ void pair_values(const double *cf, int lmaxA, const d
         const int k = l * (kMaxLmax + 1) + m;
 #pragma unroll
         for (int j = 0; j < NP; ++j) {
-          const double qn = fma(c_rec_a[k], z[j] * q[j], -c_rec_b[k] * qprev[j]);
+          const double qn = fma(c_rec_a[k], z[j] * q[j], -qprev[j]);
           qprev[j] = q[j];
           q[j] = qn;
           gl[j] *= gstep[j];
@@ -725,13 +731,14 @@ eval_pairs_kernel(PoissonDev P, const double *__restrict__ gx,
   // l-blocks kept for this bucket (all unless a truncation tolerance is set)
   const int lcut = P.lcut ? P.lcut[at.bucket_off + it.bucket] : lmaxA;
   const int lkeep = (lcut + 1) * (lcut + 1);
+  // staged with the recursion's scale gamma_lm (see c_rec_gamma)
   if (region == 0) {
     const double *src = P.spl + at.spl_off + (long)(it.bucket - 1) * lsize * 4;
-    for (int e = threadIdx.x; e < lkeep * 4; e += blockDim.x) cf[e] = src[e];
+    for (int e = threadIdx.x; e < lkeep * 4; e += blockDim.x) cf[e] = src[e] * c_rec_gamma[e >> 2];
   } else {
     const double *src = P.amp + at.amp_off;
     for (int e = threadIdx.x; e < lkeep; e += blockDim.x)
-      cf[e] = src[2 * e + (region == 1 ? 0 : 1)];
+      cf[e] = src[2 * e + (region == 1 ? 0 : 1)] * c_rec_gamma[e];
   }
   __syncthreads();
   // thread t evaluates the pairs t and t + blockDim.x of the item (the
@@ -853,8 +860,22 @@ cudaError_t poisson_init_constants() {
         }
       }
     }
-    if ((e = cudaMemcpyToSymbol(c_rec_a, ra.data(), ra.size() * sizeof(double))) != cudaSuccess) return e;
-    if ((e = cudaMemcpyToSymbol(c_rec_b, rb.data(), rb.size() * sizeof(double))) != cudaSuccess) return e;
+    // rescaled recursion: gamma per (l, m), A = a gamma_(l-1) / gamma_l, and
+    // gamma laid out per lm (cos and sin columns share it)
+    std::vector<double> gam(K * K, 1.0), A(K * K, 0.0), gam_lm(K * K, 1.0);
+    for (int m = 0; m <= kMaxLmax; ++m)
+      for (int l = m; l <= kMaxLmax; ++l) {
+        if (l >= m + 2) gam[l * K + m] = rb[l * K + m] * gam[(l - 2) * K + m];
+        if (l > m) A[l * K + m] = ra[l * K + m] * gam[(l - 1) * K + m] / gam[l * K + m];
+        if (m == 0) {
+          gam_lm[l * l] = gam[l * K];
+        } else {
+          gam_lm[l * l + 2 * m - 1] = gam[l * K + m];
+          gam_lm[l * l + 2 * m] = gam[l * K + m];
+        }
+      }
+    if ((e = cudaMemcpyToSymbol(c_rec_a, A.data(), A.size() * sizeof(double))) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(c_rec_gamma, gam_lm.data(), gam_lm.size() * sizeof(double))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(c_rec_start, st.data(), st.size() * sizeof(double))) != cudaSuccess) return e;
   }
   done_dev = dev;

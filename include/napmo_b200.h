@@ -235,6 +235,11 @@ int AuxiliaryBasis_get_nao(void *a);
 
 /* ================================================== Part 2: device API */
 /* Device pointers of a grid's mirror: points (SoA), weights, Becke weights. */
+/* Moves the grid's centres (origin [ncenter][3], bohr): points rebuilt as at
+ * construction (atomic_grid.cpp:12-51), device mirror rewritten in place,
+ * Becke weights recomputed, Poisson tables dropped.  No counterpart in nAPMO
+ * (it builds a new grid per geometry). */
+int napmo_grid_set_centers(void *grid, const double *origin);
 int napmo_grid_device_arrays(void *grid, double **x, double **y, double **z, double **w,
                              double **wb);
 /* Becke weights of device points (SoA) owned by atoms through atom_offset
@@ -292,6 +297,10 @@ int napmo_gpu_quadrature_noalloc(int n, int npoint, const double *phi, const dou
  * (grids with different angular sizes per atom). */
 void *napmo_fock_plan_new(void *grid, void *basis, int lmax, void *stream);
 void napmo_fock_plan_free(void *plan);
+/* Re-evaluates the plan's basis values after its grid or basis moved, in its
+ * own buffers; rebuilds the int8 images and Poisson tables it holds.  No
+ * counterpart in nAPMO (new objects per geometry). */
+int napmo_fock_plan_refresh(void *plan, void *stream);
 int napmo_fock_plan_info(void *plan, int *n, int *npoint, long *ld, double **phi);
 int napmo_fock_plan_density(void *plan, const double *D, double *rho, void *stream);
 int napmo_fock_plan_quadrature(void *plan, double q, const double *v, const double *vext,
@@ -352,6 +361,11 @@ int napmo_grid_energy_gradient(void *grid, void *basis, const double *D, int nq,
 /* Analytic overlap and kinetic-energy matrices (host, [n][n]) of a basis
  * (Obara-Saika); nAPMO obtains them from libint (libint_iface.cpp:136-190). */
 int napmo_basis_one_body(void *basis, double *S, double *T);
+/* Origins [nfunc][3] of the basis functions; moving them (functions of one
+ * shell together) rewrites the device shell centres in place.  No
+ * counterpart in nAPMO (its basis is rebuilt per geometry). */
+int napmo_basis_get_origins(void *basis, double *out);
+int napmo_basis_set_origins(void *basis, const double *origins);
 
 /* Error word of the tensor-core kernels (0 none, 5 an mbarrier wait ran out);
  * synchronises the stream, `reset` nonzero clears it. */

@@ -201,6 +201,8 @@ _SIGS = [
      [c_int, c_void_p, c_void_p, c_void_p, c_int, a2df, c_void_p, c_void_p]),
     ('napmo_fock_plan_new', c_void_p, [c_void_p, c_void_p, c_int, c_void_p]),
     ('napmo_fock_plan_free', None, [c_void_p]),
+    ('napmo_fock_plan_refresh', c_int, [c_void_p, c_void_p]),
+    ('napmo_grid_set_centers', c_int, [c_void_p, a2df]),
     ('napmo_fock_plan_info', c_int,
      [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_long), POINTER(c_void_p)]),
     ('napmo_fock_plan_density', c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
@@ -222,6 +224,8 @@ _SIGS = [
     ('napmo_fock_batch_tune', c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     ('napmo_fock_batch_config', c_int, [c_void_p, c_void_p, c_void_p]),
     ('napmo_basis_one_body', c_int, [c_void_p, a2df, a2df]),
+    ('napmo_basis_get_origins', c_int, [c_void_p, a2df]),
+    ('napmo_basis_set_origins', c_int, [c_void_p, a2df]),
     ('napmo_grid_energy_gradient', c_int,
      [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ('napmo_tc_status', c_int, [c_void_p, c_int]),

@@ -240,6 +240,41 @@ int napmo_gpu_basis_values(BasisSet *b, int npoint, const double *x, const doubl
   });
 }
 
+// Origins [nfunc][3] (bohr) of the basis functions, in basis order.
+int napmo_basis_get_origins(BasisSet *b, double *out) {
+  return guarded([&] {
+    for (size_t k = 0; k < b->cont.size(); ++k)
+      for (int d = 0; d < 3; ++d) out[3 * k + d] = b->cont[k].origin[d];
+    return kOk;
+  });
+}
+
+// Moves the basis functions to origins [nfunc][3] (bohr; the functions of one
+// shell keep a common origin).  The device copy's shell centres are rewritten
+// in place (no allocation); plans built on this basis re-evaluate their basis
+// values with napmo_fock_plan_refresh.  No counterpart in nAPMO, which builds
+// a new basis per geometry.
+int napmo_basis_set_origins(BasisSet *b, const double *origins) {
+  return guarded([&] {
+    for (size_t k = 0; k < b->cont.size(); ++k) {
+      ContractedGaussian &c = b->cont[k];
+      for (int d = 0; d < 3; ++d) c.origin[d] = origins[3 * k + d];
+      for (auto &pg : c.prim)
+        for (int d = 0; d < 3; ++d) pg.origin[d] = origins[3 * k + d];
+    }
+    if (b->dev_valid) {
+      HostBasisPack pk;
+      pack_basis(b->cont, &pk);
+      NAPMO_REQUIRE(pk.nshell == b->dev.nshell,
+                    "moved functions no longer share their shell's origin");
+      NAPMO_TRY_CUDA(cudaMemcpy(b->dev.shell_center, pk.shell_center.data(),
+                                pk.shell_center.size() * sizeof(double), cudaMemcpyHostToDevice),
+                     "move basis");
+    }
+    return kOk;
+  });
+}
+
 // Overlap and kinetic-energy matrices (host out, [n][n] row-major) of the
 // normalised contracted basis, analytic (Obara-Saika); nAPMO takes them from
 // libint (libint_iface.cpp:136-190), not available here.

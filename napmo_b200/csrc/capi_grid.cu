@@ -923,6 +923,60 @@ double BeckeGrid_integrate(BeckeGrid *g, double *f) {
   return out;
 }
 
+// Moves the grid's centres to origin [ncenter][3] (bohr).  Each atomic grid's
+// points are rebuilt around its new centre with the expression of its
+// construction (atomic_grid.cpp:12-51, origin + r u), so the result equals a
+// grid built at the new geometry bit for bit; the device mirror is rewritten
+// in place (no allocation), the Becke weights recomputed and the Poisson
+// tables dropped (rebuilt on next use).  The quadrature weights do not depend
+// on the positions.  No counterpart in nAPMO, which builds a new grid per
+// geometry.  Synchronises the library's host stream.
+int napmo_grid_set_centers(BeckeGrid *g, const double *origin) {
+  return guarded([&] {
+    NAPMO_REQUIRE(!g->layout.empty() && (int)g->layout.size() == g->ncenter,
+                  "grid has no atomic structure (read from points)");
+    const int n = g->size;
+    std::vector<double> x(n), y(n), z(n);
+    for (int a = 0; a < g->ncenter; ++a) {
+      AtomLayout &L = g->layout[a];
+      AtomicGrid &ag = g->atgrid[a];
+      for (int d = 0; d < 3; ++d) {
+        g->origin[3 * a + d] = origin[3 * a + d];
+        L.center[d] = origin[3 * a + d];
+        ag.origin[d] = origin[3 * a + d];
+      }
+      for (int i = 0; i < L.nrad; ++i) {
+        const double rp = L.r[i];
+        for (int j = 0; j < L.nang; ++j) {
+          const int k = i * L.nang + j;
+          for (int d = 0; d < 3; ++d) ag.points[3 * k + d] = L.ang[3 * j + d] * rp + ag.origin[d];
+          const long q = (long)L.point_off + k;
+          for (int d = 0; d < 3; ++d) g->points[3 * q + d] = ag.points[3 * k + d];
+          x[q] = ag.points[3 * k];
+          y[q] = ag.points[3 * k + 1];
+          z[q] = ag.points[3 * k + 2];
+        }
+      }
+    }
+    cudaStream_t s = host_api_stream();
+    NAPMO_TRY_CUDA(cudaMemcpyAsync(g->dev.x, x.data(), n * sizeof(double), cudaMemcpyHostToDevice, s),
+                   "move grid");
+    NAPMO_TRY_CUDA(cudaMemcpyAsync(g->dev.y, y.data(), n * sizeof(double), cudaMemcpyHostToDevice, s),
+                   "move grid");
+    NAPMO_TRY_CUDA(cudaMemcpyAsync(g->dev.z, z.data(), n * sizeof(double), cudaMemcpyHostToDevice, s),
+                   "move grid");
+    NAPMO_TRY_CUDA(cudaMemcpyAsync(g->dev.origin, g->origin.data(), g->origin.size() * sizeof(double),
+                                   cudaMemcpyHostToDevice, s),
+                   "move grid");
+    if (g->poisson) {
+      NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "move grid");
+      delete g->poisson;
+      g->poisson = nullptr;
+    }
+    return compute_becke(g, s);  // synchronises s before the host vectors go
+  });
+}
+
 // Device pointers of the grid mirror: x, y, z, w, wb (each size long).
 int napmo_grid_device_arrays(BeckeGrid *g, double **x, double **y, double **z,
                              double **w, double **wb) {

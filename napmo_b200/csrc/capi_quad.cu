@@ -289,6 +289,41 @@ FockPlan *napmo_fock_plan_new(BeckeGrid *grid, BasisSet *basis, int lmax, void *
 
 void napmo_fock_plan_free(FockPlan *p) { delete p; }
 
+// After the plan's grid or basis moved (napmo_grid_set_centers,
+// napmo_basis_set_origins): re-evaluates the basis on the grid into the
+// plan's own buffer (no allocation) and rebuilds what derives from it (the
+// int8 operand images of precision 1, the Poisson tables).  Synchronises.
+int napmo_fock_plan_refresh(FockPlan *p, void *stream) {
+  return guarded([&] {
+    cudaStream_t s = (cudaStream_t)stream;
+    BeckeGrid *g = p->grid;
+    NAPMO_REQUIRE(padded_points(g->size) == p->ld && (int)p->basis->cont.size() == p->n,
+                  "plan no longer matches its grid or basis sizes");
+    const DeviceBasis *db = nullptr;
+    int e = basis_device(p->basis, s, &db);
+    if (e) return e;
+    NAPMO_TRY_CUDA(launch_basis_values(*db, g->size, g->dev.x, g->dev.y, g->dev.z, p->phi.p,
+                                       p->ld, nullptr, s),
+                   "basis");
+    if (p->lmax >= 0 || p->lmax == kLmaxPerAtom) {
+      PoissonPlan *pp = nullptr;
+      e = grid_poisson_plan(g, p->lmax, s, &pp);
+      if (e) return e;
+    }
+    NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "refresh");
+    if (p->i8) {
+      int8_plan_destroy(p->i8);
+      p->i8 = nullptr;
+      cudaStream_t hs = host_api_stream();
+      e = int8_plan_create(&p->i8, p->n, g->size, p->phi.p, p->ld, g->dev.wb, g->dev.w,
+                           kMixedScreenTol, hs);
+      if (e) return e;
+      NAPMO_TRY_CUDA(cudaStreamSynchronize(hs), "int8 operand images");
+    }
+    return kOk;
+  });
+}
+
 int napmo_fock_plan_info(FockPlan *p, int *n, int *npoint, long *ld, double **phi) {
   *n = p->n;
   *npoint = p->grid->size;

@@ -87,6 +87,11 @@ class FockBuilder(object):
             return None
         return _view(self.torch, keep.value, (self.npoint,), '<i4') != 0
 
+    def refresh(self, stream=None):
+        """Re-evaluates the basis on the grid after either moved
+        (BeckeGrid.set_centers, BasisSet.set_origins), in the plan's buffers."""
+        checked(cext.lib.napmo_fock_plan_refresh(self._plan, _stream(self.torch, stream)))
+
     def tc_status(self, reset=True, stream=None):
         """Error word of the tensor-core kernels (0: none); synchronises the stream."""
         return cext.lib.napmo_tc_status(_stream(self.torch, stream), 1 if reset else 0)

@@ -38,12 +38,18 @@ class GridChargeEnergy(object):
         quantum: indices of atoms whose nuclei are a quantum species (5s5p).
     """
 
-    def __init__(self, symbols, species='e-', basis='CC-PVDZ', quantum=(), nrad=75, nang=194):
+    def __init__(self, symbols, species='e-', basis='CC-PVDZ', quantum=(), nrad=75, nang=194,
+                 reuse=True):
         self.symbols = list(symbols)
         self.species = species
         self.basis_name = basis
         self.quantum = tuple(quantum)
         self.nrad, self.nang = int(nrad), int(nang)
+        # reuse: one grid, basis and plan, moved from geometry to geometry
+        # (napmo_grid_set_centers, napmo_basis_set_origins,
+        # napmo_fock_plan_refresh) instead of new objects per geometry
+        self.reuse = bool(reuse)
+        self._live = None
 
     def system(self, R):
         """MolecularSystem at positions R (natom x 3, bohr), with the atom
@@ -71,24 +77,54 @@ class GridChargeEnergy(object):
                        for k in range(len(charges))], dtype=np.float64).reshape(-1, 4)
         return ms, sp, grid, centres, charges, Zq
 
+    def _objects(self, R):
+        """(grid, basis, plan, centres, charges, Zq) at positions R."""
+        R = np.asarray(R, dtype=np.float64).reshape(-1, 3)
+        live = self._live
+        if live is None:
+            ms, sp, grid, centres, charges, Zq = self._setup(R)
+            fb = FockBuilder(grid, sp['basis'], -1)
+            obj = dict(ms=ms, grid=grid, basis=sp['basis'], fb=fb, centres=centres,
+                       charges=charges, Zq=Zq, R=R.copy())
+            if self.reuse:
+                # atom of every basis function: the centre its origin sits on
+                org = sp['basis'].origins()
+                cen = R[centres]
+                obj['func_centre'] = np.array(
+                    [int(np.flatnonzero((cen == o).all(axis=1))[0]) for o in org])
+                obj['qcharge'] = Zq[:, 3].copy()
+                self._live = obj
+            return obj
+        if not np.array_equal(live['R'], R):
+            cen = R[live['centres']]
+            live['grid'].set_centers(cen)
+            live['basis'].set_origins(cen[live['func_centre']])
+            live['fb'].refresh()
+            live['Zq'] = np.concatenate([R[live['charges']], live['qcharge'][:, None]], axis=1)
+            live['R'] = R.copy()
+        return live
+
     def quadrature_matrix(self, R):
         """(V, state): V = dE/dD on the device; state keeps the grid for the
         gradient."""
         torch = _torch()
-        ms, sp, grid, centres, charges, Zq = self._setup(R)
-        fb = FockBuilder(grid, sp['basis'], -1)
+        obj = self._objects(R)
+        grid, fb, centres, charges, Zq = (obj['grid'], obj['fb'], obj['centres'],
+                                          obj['charges'], obj['Zq'])
         x, y, z, _, _ = grid.device_arrays()
         v = torch.empty(grid.size, dtype=torch.float64, device='cuda')
         checked(cext.lib.napmo_gpu_nuclear_potential(
             grid.size, x, y, z, Zq.shape[0], np.ascontiguousarray(Zq), v.data_ptr(),
             torch.cuda.current_stream().cuda_stream))
         V = fb.quadrature(1.0, v)
-        return V, dict(grid=grid, basis=sp['basis'], centres=centres, charges=charges, Zq=Zq,
-                       natom=len(self.symbols), fb=fb)
+        return V, dict(grid=grid, basis=obj['basis'], centres=centres, charges=charges, Zq=Zq,
+                       natom=len(self.symbols), fb=fb, R=obj['R'].copy())
 
     def gradient(self, state, D):
         """(E, dE/dR [natom][3]) from the gradient kernel."""
         torch = _torch()
+        if self.reuse:  # the shared objects may have moved since the forward
+            self._objects(state['R'])
         D = torch.as_tensor(D, dtype=torch.float64, device='cuda').contiguous()
         nc = len(state['centres'])
         Zq = state['Zq']

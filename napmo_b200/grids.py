@@ -375,6 +375,13 @@ class BeckeGrid(object):
         out = _lib().BeckeGrid_integrate(self._this, f)
         return check(out)
 
+    def set_centers(self, origins):
+        """Moves the atomic grids to new centres (ncenter x 3, bohr) in place:
+        points rebuilt around each centre, Becke weights recomputed, device
+        buffers reused.  Plans on this grid need FockBuilder.refresh()."""
+        origins = np.ascontiguousarray(np.asarray(origins, dtype=np.float64).reshape(-1, 3))
+        checked(_lib().napmo_grid_set_centers(self._this, origins))
+
     def device_arrays(self):
         """Raw device pointers (x, y, z, w, becke weights) of the grid mirror."""
         ptrs = [c_void_p() for _ in range(5)]

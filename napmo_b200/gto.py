@@ -169,6 +169,19 @@ class BasisSet(dict):
         self['cont'] += other.get('cont')
         _lib().BasisSet_update(self._this, other._this)
 
+    def origins(self):
+        """Centre of every basis function (nbasis x 3, bohr)."""
+        out = np.zeros((self['nbasis'], 3))
+        cext.checked(_lib().napmo_basis_get_origins(self._this, out))
+        return out
+
+    def set_origins(self, origins):
+        """Moves the functions to new centres (nbasis x 3, bohr) in the library's
+        copy (the device copy is updated in place); plans on this basis need
+        FockBuilder.refresh()."""
+        origins = np.ascontiguousarray(np.asarray(origins, dtype=np.float64).reshape(-1, 3))
+        cext.checked(_lib().napmo_basis_set_origins(self._this, origins))
+
     def compute(self, coord=np.zeros([1, 3], dtype=np.float64)):
         """phi[p, mu] at points coord[p] (GPU)."""
         coord = np.ascontiguousarray(coord, dtype=np.float64)

@@ -410,6 +410,23 @@ def run_gradients(args, world, rank):
         fd[m.species] = {'max_abs_error_eh_per_bohr': float(np.abs(g - gf).max()),
                          'max_abs_gradient': float(np.abs(gf).max()),
                          'net_force': float(np.abs(g.sum(axis=0)).max())}
+    # int8 quadrature matrices (dE/dD) against FP64 over the geometries; the
+    # gradient kernel runs in FP64 in both modes
+    mixed = {}
+    for m in models:
+        m8 = GridChargeEnergy(sym, species=m.species, quantum=(1, 2), nrad=75, nang=194,
+                              precision='int8x4')
+        D = dens[m.species]
+        dV, dE, dg = 0.0, 0.0, 0.0
+        for R in geoms:
+            V, st = m.quadrature_matrix(R)
+            V8, st8 = m8.quadrature_matrix(R)
+            V, V8 = V.cpu().numpy(), V8.cpu().numpy()
+            dV = max(dV, float(np.abs(V8 - V).max() / np.abs(V).max()))
+            dE = max(dE, abs(float((D * (V8 - V)).sum())))
+            dg = max(dg, float(np.abs(m8.gradient(st8, D)[1] - m.gradient(st, D)[1]).max()))
+        mixed[m.species] = {'max_rel_dEdD_error': dV, 'max_energy_error_eh': dE,
+                            'max_gradient_error_eh_per_bohr': dg}
     nunit = len(geoms) * len(models)
     line = {
         'metric': 'grid energy gradients/s (H2O, both protons quantum, 75x194; C5)',
@@ -421,6 +438,7 @@ def run_gradients(args, world, rank):
                    'parallelism': 'single GPU'},
         'gradient_kernel': kern,
         'finite_differences': fd,
+        'mixed_int8x4': mixed,
         'e2e': {'value': nunit / t_step, 'unit': 'gradients/s',
                 'h2d_bytes_per_step': sum(8 * dens[m.species].size for m in models) * len(geoms),
                 'd2h_bytes_per_step': 8 * 10 * nunit},

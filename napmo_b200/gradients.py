@@ -39,7 +39,7 @@ class GridChargeEnergy(object):
     """
 
     def __init__(self, symbols, species='e-', basis='CC-PVDZ', quantum=(), nrad=75, nang=194,
-                 reuse=True):
+                 reuse=True, precision='fp64'):
         self.symbols = list(symbols)
         self.species = species
         self.basis_name = basis
@@ -50,6 +50,9 @@ class GridChargeEnergy(object):
         # napmo_fock_plan_refresh) instead of new objects per geometry
         self.reuse = bool(reuse)
         self._live = None
+        # precision of the quadrature matrix V = dE/dD ('fp64' or 'int8x4');
+        # the gradient kernel is FP64 in both
+        self.precision = precision
 
     def system(self, R):
         """MolecularSystem at positions R (natom x 3, bohr), with the atom
@@ -83,7 +86,7 @@ class GridChargeEnergy(object):
         live = self._live
         if live is None:
             ms, sp, grid, centres, charges, Zq = self._setup(R)
-            fb = FockBuilder(grid, sp['basis'], -1)
+            fb = FockBuilder(grid, sp['basis'], -1, precision=self.precision)
             obj = dict(ms=ms, grid=grid, basis=sp['basis'], fb=fb, centres=centres,
                        charges=charges, Zq=Zq, R=R.copy())
             if self.reuse:

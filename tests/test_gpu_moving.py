@@ -95,3 +95,19 @@ def test_grid_charge_energy_reuse_matches_fresh_objects(species):
         Eb, gb = fresh.gradient(sb, D)
         assert Ea == Eb
         assert np.array_equal(ga, gb)
+
+
+def test_grid_charge_energy_int8_quadrature_matrix():
+    """precision='int8x4': V = dE/dD from the int8 tensor-core quadrature
+    (also after moves, which rebuild the int8 images) within 1e-8 of max|V| of
+    the FP64 one; the gradient kernel is FP64 in both modes."""
+    from napmo_b200.gradients import GridChargeEnergy
+    kw = dict(species='e-', quantum=(1, 2), nrad=40, nang=110)
+    m64 = GridChargeEnergy(SYM, **kw)
+    m8 = GridChargeEnergy(SYM, precision='int8x4', **kw)
+    for R in _geoms(2, seed=13):
+        V, st = m64.quadrature_matrix(R)
+        V8, st8 = m8.quadrature_matrix(R)
+        V, V8 = V.cpu().numpy(), V8.cpu().numpy()
+        assert np.abs(V8 - V).max() <= 1e-8 * np.abs(V).max()
+        assert st8['fb'].tc_status() == 0

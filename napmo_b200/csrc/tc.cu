@@ -236,31 +236,66 @@ __device__ __forceinline__ double pow2(int e) {
   return e < -1022 ? 0.0 : __longlong_as_double((long long)(e + 1023) << 52);
 }
 
+// Balanced base-256 digits by byte arithmetic.  For |Y| < 2^31 - 2^24, the
+// balanced digits Y = d0 2^24 + d1 2^16 + d2 2^8 + d3 (-128 <= d1..d3 <= 127)
+// are the bytes of U = Y + 0x808080: bytes 0..2 of U are d3 + 128, d2 + 128,
+// d1 + 128 (no carries by construction) and byte 3 is d0.  So the int8 digit
+// bytes (d & 255) of one element are the bytes of U ^ 0x808080, and the
+// element is (W ^ 0x808080) - 0x808080 for its digit bytes W.  Four elements
+// and four slices are a 4 x 4 byte transpose (8 byte permutations).
+__device__ __forceinline__ void bytes_transpose4(uint32_t a, uint32_t b, uint32_t c, uint32_t d,
+                                                 uint32_t *o) {
+  // o[k] byte j = byte k of input j (inputs a, b, c, d = j 0..3)
+  const uint32_t lo01 = __byte_perm(a, b, 0x5140), lo23 = __byte_perm(c, d, 0x5140);
+  const uint32_t hi01 = __byte_perm(a, b, 0x7362), hi23 = __byte_perm(c, d, 0x7362);
+  o[0] = __byte_perm(lo01, lo23, 0x5410);
+  o[1] = __byte_perm(lo01, lo23, 0x7632);
+  o[2] = __byte_perm(hi01, hi23, 0x5410);
+  o[3] = __byte_perm(hi01, hi23, 0x7632);
+}
+
+// Four slices (d0 .. d3 words, byte e = element e) of four integers.
+__device__ __forceinline__ void digits4(const int *y, uint32_t *w) {
+  uint32_t t[4];
+  bytes_transpose4(((uint32_t)y[0] + 0x808080u) ^ 0x808080u, ((uint32_t)y[1] + 0x808080u) ^ 0x808080u,
+                   ((uint32_t)y[2] + 0x808080u) ^ 0x808080u, ((uint32_t)y[3] + 0x808080u) ^ 0x808080u,
+                   t);
+  // t[k] holds byte k of every element: k = 0 is d3 ... k = 3 is d0
+  w[0] = t[3];
+  w[1] = t[2];
+  w[2] = t[1];
+  w[3] = t[0];
+}
+
+// The four integers of four slice words (inverse of digits4).
+__device__ __forceinline__ void undigits4(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3,
+                                          int *y) {
+  uint32_t t[4];
+  bytes_transpose4(w3, w2, w1, w0, t);  // t[e] bytes: d3, d2, d1, d0 of element e
+#pragma unroll
+  for (int e = 0; e < 4; ++e) y[e] = (int)(t[e] ^ 0x808080u) - 0x808080;
+}
+
 // Four balanced base-256 digit slices of rint(x[i] * scale), i < 16, packed
 // one byte per element (slice s in out[s]).
 __device__ __forceinline__ void slice16(const double *x, double scale, uint4 *out) {
-  uint32_t w[NSL][4];
+  uint32_t w[4][4];  // [element group][slice]
 #pragma unroll
-  for (int s = 0; s < NSL; ++s)
+  for (int q = 0; q < 4; ++q) {
+    int y[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) w[s][q] = 0u;
-#pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    int y = __double2int_rn(x[i] * scale);
-    const int d3 = ((y + 128) & 255) - 128;
-    y = (y - d3) >> 8;
-    const int d2 = ((y + 128) & 255) - 128;
-    y = (y - d2) >> 8;
-    const int d1 = ((y + 128) & 255) - 128;
-    const int d0 = (y - d1) >> 8;
-    const int q = i >> 2, sh = (i & 3) * 8;
-    w[0][q] |= (uint32_t)(d0 & 255) << sh;
-    w[1][q] |= (uint32_t)(d1 & 255) << sh;
-    w[2][q] |= (uint32_t)(d2 & 255) << sh;
-    w[3][q] |= (uint32_t)(d3 & 255) << sh;
+    for (int e = 0; e < 4; ++e) y[e] = __double2int_rn(x[4 * q + e] * scale);
+    digits4(y, w[q]);
   }
 #pragma unroll
-  for (int s = 0; s < NSL; ++s) out[s] = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+  for (int s = 0; s < NSL; ++s) out[s] = make_uint4(w[0][s], w[1][s], w[2][s], w[3][s]);
+}
+
+// The 16 integers of four digit slices (inverse of slice16's packing).
+__device__ __forceinline__ void unslice16(const uint4 *q, int *y) {
+#pragma unroll
+  for (int g = 0; g < 4; ++g)
+    undigits4((&q[0].x)[g], (&q[1].x)[g], (&q[2].x)[g], (&q[3].x)[g], y + 4 * g);
 }
 
 // Five balanced base-256 digit slices of rint(x[i] * scale) (|.| <= 2^38;
@@ -289,8 +324,6 @@ __device__ __forceinline__ void slice16_5(const double *x, double scale, uint4 *
   for (int s = 0; s < 5; ++s) out[s] = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
 }
 
-// signed byte b (0..3) of a word
-__device__ __forceinline__ int sbyte(uint32_t w, int b) { return ((int)(w << (24 - 8 * b))) >> 24; }
 
 // Row-grouped slices of X[row][k] = src[row * ld + k] * m1[k] * m2[k]
 // (m1, m2 optional; X = 0 for row >= nrows or k >= ncols): exponent per
@@ -481,9 +514,9 @@ gscale_kernel(int npoint, const double *__restrict__ wv, const double *__restric
 // block), 4 warps; in every stage the row group's 8 rows x 64 points of one
 // slice are 512 contiguous bytes, so lane c holds the 16-byte chunk of row
 // c & 7, points 16 (c >> 3) .. +15.  Warp w takes stages 4w .. 4w + 3 and keeps
-// their A digits in registers across both passes (row maxima: lanes c, c ^ 8,
-// c ^ 16, c ^ 24, then the four warps through shared memory; digits of B), so
-// A is read from memory once.
+// their Y_A, decoded once from the digits, in registers across both passes
+// (row maxima: lanes c, c ^ 8, c ^ 16, c ^ 24, then the four warps through
+// shared memory; digits of B), so A is read from memory once.
 __global__ void __launch_bounds__(128)
 scale_image_kernel(const int8_t *__restrict__ qa, int8_t *__restrict__ qb,
                    const double *__restrict__ gs, const int *__restrict__ ea,
@@ -498,21 +531,20 @@ scale_image_kernel(const int8_t *__restrict__ qa, int8_t *__restrict__ qb,
   auto stage_base = [&](int st) {
     return ((long)t * nks + b * QBLK_STAGES + w * SPW + st) * stage_bytes(TM) + goff;
   };
-  uint4 q[SPW][NSL];
+  // Y_A of the thread's 64 elements, decoded once from the four digit slices
+  int ya[SPW][16];
 #pragma unroll
-  for (int st = 0; st < SPW; ++st)
+  for (int st = 0; st < SPW; ++st) {
+    uint4 q[NSL];
 #pragma unroll
     for (int s = 0; s < NSL; ++s)
-      q[st][s] = __ldg(reinterpret_cast<const uint4 *>(qa + stage_base(st) + (long)s * TM * KS));
+      q[s] = __ldg(reinterpret_cast<const uint4 *>(qa + stage_base(st) + (long)s * TM * KS));
+    unslice16(q, ya[st]);
+  }
   auto values = [&](int st, double *x) {
     const double *g = gs + ((long)b * QBLK_STAGES + w * SPW + st) * KS + kc * 16;
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      const int wq = i >> 2, bb = i & 3;
-      const int y = ((sbyte((&q[st][0].x)[wq], bb) * 256 + sbyte((&q[st][1].x)[wq], bb)) * 256 +
-                     sbyte((&q[st][2].x)[wq], bb)) * 256 + sbyte((&q[st][3].x)[wq], bb);
-      x[i] = (double)y * __ldg(g + i);
-    }
+    for (int i = 0; i < 16; ++i) x[i] = (double)ya[st][i] * __ldg(g + i);
   };
   double mx = 0.0;
 #pragma unroll
@@ -915,13 +947,11 @@ __global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
             for (int s = 0; s < NSL; ++s)
               q[s] = __ldg(reinterpret_cast<const uint4 *>(pa + (long)s * TM * KS));
             const int *ed = g.ed + mu0;
+            int yv[16];
+            unslice16(q, yv);
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
-              const int wq = i >> 2, b = i & 3;
-              const uint32_t w0 = (&q[0].x)[wq], w1 = (&q[1].x)[wq], w2 = (&q[2].x)[wq],
-                             w3 = (&q[3].x)[wq];
-              const int y = ((sbyte(w0, b) * 256 + sbyte(w1, b)) * 256 + sbyte(w2, b)) * 256 +
-                            sbyte(w3, b);
+              const int y = yv[i];
               const long long comb =
                   (((((long long)v[0][i] * 256 + v[1][i]) * 256 + v[2][i]) * 256 + v[3][i]) *
                    256) + v[4][i];

@@ -327,6 +327,8 @@ def run_batch(args, world, rank, dist=None):
                   'energy_error_eh_max': dEmax, 'energy_error_eh_mean': sum(dE) / len(dE),
                   'energy_error_eh_per_molecule': dE},
         'algorithmic_tflops': flops / t_dev / 1e12,
+        'grid_points_per_s': sum(sum(r * a for r, a in zip(m['nrad'], m['nang']))
+                                 for m in all_mols) / t_dev,
         'setup_s': t_setup,
         'clocks': clk8 if ok else clk64,
         'cpu_baseline': None,
@@ -771,6 +773,7 @@ def main():
                          'traffic': None, 'peak_source': peak_source,
                          'algorithmic_flops_per_launch': flops_alg, 'issued': issued},
             'stages_ms': {k: v * 1e3 for k, v in stages.items()},
+            'grid_points_per_s': world * args.steps / t_dev * N,
             'fp64': {'builds_per_s': world * args.steps / t_f64,
                      'ms_per_build': t_f64 / args.steps * 1e3, 'fp64_gemm_tflops': fp64},
             'mixed': mixed,

@@ -510,7 +510,8 @@ gscale_kernel(int npoint, const double *__restrict__ wv, const double *__restric
 // Per call: the B image from the A image.  For each row and block,
 // x(p) = Y_A(p) gs(p) (|x| < 2^30); Y_B = rint(x 2^s) with s = 30 - e,
 // e = group exponent of max |x| over the block, so B keeps 31 bits of its own
-// block maximum; eb[row][b] = ea[row][b] + eg[b] - s.  CTA = (8-row group,
+// block maximum; eb[b][row] = ea[row][b] + eg[b] - s (block-major, ebld rows
+// per block, so a drain thread's columns are contiguous).  CTA = (8-row group,
 // block), 4 warps; in every stage the row group's 8 rows x 64 points of one
 // slice are 512 contiguous bytes, so lane c holds the 16-byte chunk of row
 // c & 7, points 16 (c >> 3) .. +15.  Warp w takes stages 4w .. 4w + 3 and keeps
@@ -520,7 +521,8 @@ gscale_kernel(int npoint, const double *__restrict__ wv, const double *__restric
 __global__ void __launch_bounds__(128)
 scale_image_kernel(const int8_t *__restrict__ qa, int8_t *__restrict__ qb,
                    const double *__restrict__ gs, const int *__restrict__ ea,
-                   const int *__restrict__ eg, int *__restrict__ eb, int nks, int nblk) {
+                   const int *__restrict__ eg, int *__restrict__ eb, int nks, int nblk,
+                   int ebld) {
   constexpr int SPW = QBLK_STAGES / 4;  // stages per warp
   __shared__ double smax[4][8];
   const int c = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -560,7 +562,7 @@ scale_image_kernel(const int8_t *__restrict__ qa, int8_t *__restrict__ qb,
   __syncthreads();
   mx = fmax(fmax(smax[0][r], smax[1][r]), fmax(smax[2][r], smax[3][r]));
   const int sh = 30 - group_exponent(mx);
-  if (w == 0 && c < 8) eb[(long)row * nblk + b] = ea[(long)row * nblk + b] + eg[b] - sh;
+  if (w == 0 && c < 8) eb[(long)b * ebld + row] = ea[(long)row * nblk + b] + eg[b] - sh;
   const double scale = ldexp(1.0, sh);
 #pragma unroll
   for (int st = 0; st < SPW; ++st) {
@@ -595,8 +597,9 @@ __device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t sa, uint32_t
 // ------------------------------------------------------------- quadrature
 struct QuadArgs {
   const int8_t *a, *b;    // images of A and B, both in 128-row tiles
-  const int *ea, *eb;     // exponents of A and B [row][nblk]
+  const int *ea, *eb;     // exponents of A [row][nblk] and B [nblk][ebld]
   int nblk, nks;          // exponent blocks; stages per row tile (nblk * 64)
+  int ebld;               // rows per block of eb
   int ntj;                // 96-column tiles
   int bpc;                // blocks per chunk
   int npair;
@@ -730,7 +733,7 @@ __global__ void __launch_bounds__(NTHR, 1) quad_i8_kernel(QuadArgs g) {
       fence_after_sync();
       const int blk = b0 + bi;
       const int ea = __ldg(g.ea + mu * g.nblk + blk);
-      const int *eb = g.eb + ((long)J * QN + col0) * g.nblk + blk;
+      const int *eb = g.eb + (long)blk * g.ebld + J * QN + col0;  // 48 contiguous
 #pragma unroll
       for (int c = 0; c < 48; c += 8) {
         int32_t v[5][8];
@@ -739,12 +742,15 @@ __global__ void __launch_bounds__(NTHR, 1) quad_i8_kernel(QuadArgs g) {
         tmem_wait_ld();
 #pragma unroll
         for (int d = 0; d < 5; ++d) tie8(v[d]);
+        const int4 eb0 = __ldg(reinterpret_cast<const int4 *>(eb + c));
+        const int4 eb1 = __ldg(reinterpret_cast<const int4 *>(eb + c + 4));
+        const int ebv[8] = {eb0.x, eb0.y, eb0.z, eb0.w, eb1.x, eb1.y, eb1.z, eb1.w};
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
           const long long comb =
               (((((long long)v[0][i] * 256 + v[1][i]) * 256 + v[2][i]) * 256 + v[3][i]) * 256) +
               v[4][i];
-          part[c + i] += (double)comb * pow2(ea + __ldg(eb + (long)(c + i) * g.nblk) - 44);
+          part[c + i] += (double)comb * pow2(ea + ebv[i] - 44);
         }
       }
       fence_before_sync();
@@ -946,7 +952,16 @@ __global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
 #pragma unroll
             for (int s = 0; s < NSL; ++s)
               q[s] = __ldg(reinterpret_cast<const uint4 *>(pa + (long)s * TM * KS));
-            const int *ed = g.ed + mu0;
+            // exponents of D's rows mu0 .. mu0 + 15 (64-byte aligned)
+            int edv[16];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const int4 t4 = __ldg(reinterpret_cast<const int4 *>(g.ed + mu0) + k);
+              edv[4 * k] = t4.x;
+              edv[4 * k + 1] = t4.y;
+              edv[4 * k + 2] = t4.z;
+              edv[4 * k + 3] = t4.w;
+            }
             int yv[16];
             unslice16(q, yv);
 #pragma unroll
@@ -955,7 +970,7 @@ __global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
               const long long comb =
                   (((((long long)v[0][i] * 256 + v[1][i]) * 256 + v[2][i]) * 256 + v[3][i]) *
                    256) + v[4][i];
-              acc = fma((double)y * pow2(__ldg(ed + i)), (double)comb, acc);
+              acc = fma((double)y * pow2(edv[i]), (double)comb, acc);
             }
           }
         }
@@ -1199,9 +1214,10 @@ int int8_quadrature(Int8Plan *p, const double *phi, const double *wv, double *F,
                                         p->screened ? p->idx.p : nullptr, p->gs.p, p->eg.p);
   NAPMO_TRY_CUDA(cudaGetLastError(), "block scales");
   scale_image_kernel<<<dim3((p->n + 7) / 8, p->nblk), 128, 0, s>>>(
-      p->qa.p, p->qb.p, p->gs.p, p->qa_e.p, p->eg.p, p->qb_e.p, p->nks_q, p->nblk);
+      p->qa.p, p->qb.p, p->gs.p, p->qa_e.p, p->eg.p, p->qb_e.p, p->nks_q, p->nblk,
+      p->nimg * TM);
   NAPMO_TRY_CUDA(cudaGetLastError(), "wv phi image");
-  QuadArgs g{p->qa.p, p->qb.p, p->qa_e.p, p->qb_e.p, p->nblk, p->nks_q,
+  QuadArgs g{p->qa.p, p->qb.p, p->qa_e.p, p->qb_e.p, p->nblk, p->nks_q, p->nimg * TM,
              p->ntj,  p->bpc,  p->npair, p->work.p};
   const int smem = NSTAGE * (stage_bytes(TM) + stage_bytes(QN));
   NAPMO_TRY_CUDA(cudaFuncSetAttribute(quad_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <map>
 #include <stdexcept>
+#include <algorithm>
 #include <vector>
 
 #include "capi_common.cuh"
@@ -44,14 +45,14 @@ struct PoissonPlan {
   DevBuf<int> lpiv;
   DevBuf<int> pairs;
   DevBuf<EvalItem> items;
-  int nitems = 0;
+  int nitems = 0, nitems_in = 0;  // items, of which the first nitems_in are interior
   DevBuf<double> pair_v;
   DevBuf<int> lcut;  // per bucket, for truncated evaluations
   // pair lists of the points kept by a screening mask (built for the last
   // mask used; the mask is owned by the caller's int8 plan)
   DevBuf<int> pairs_s;
   DevBuf<EvalItem> items_s;
-  int nitems_s = 0;
+  int nitems_s = 0, nitems_in_s = 0;
   const int *screen_key = nullptr;
 };
 
@@ -212,7 +213,7 @@ int build_poisson_plan(const std::vector<const AtomLayout *> &atoms,
 // (and once per screening mask); about 12 bytes per pair.  Synchronises `s`.
 int build_pair_lists(PoissonPlan *plan, const double *x, const double *y, const double *z,
                      const int *keep, DevBuf<int> &pairs, DevBuf<EvalItem> &items, int &nitems,
-                     cudaStream_t s) {
+                     int &nitems_in, cudaStream_t s) {
   PoissonDev &d = plan->d;
   const std::vector<PoissonAtom> &ha = plan->h_atoms;
   int nb = 0;
@@ -246,6 +247,13 @@ int build_pair_lists(PoissonPlan *plan, const double *x, const double *y, const 
   d.pairs = pairs.p;
   NAPMO_TRY_CUDA(launch_pair_scatter(d, plan->max_mol_npoint, bucket_of.p, count.p, s),
                  "pair scatter");
+  // interior buckets first, the tails after them: the evaluation runs them as
+  // two kernels, each with the code of its own region only
+  std::stable_partition(hitems.begin(), hitems.end(), [&](const EvalItem &it) {
+    return it.bucket > 0 && it.bucket < ha[it.atom].nrad;
+  });
+  nitems_in = 0;
+  for (const EvalItem &it : hitems) nitems_in += (it.bucket > 0 && it.bucket < ha[it.atom].nrad);
   NAPMO_TRY_CUDA(items.upload(hitems, s), "pair lists");
   if (!plan->pair_v.p) NAPMO_TRY_CUDA(plan->pair_v.alloc(d.npair), "pair lists");
   if (!plan->lcut.p) NAPMO_TRY_CUDA(plan->lcut.alloc(nb), "pair lists");
@@ -261,7 +269,7 @@ static int select_pair_lists(PoissonPlan *p, BeckeGrid *g, const int *keep, cuda
   if (keep && keep != p->screen_key) {
     p->screen_key = nullptr;
     const int st = build_pair_lists(p, g->dev.x, g->dev.y, g->dev.z, keep, p->pairs_s,
-                                    p->items_s, p->nitems_s, s);
+                                    p->items_s, p->nitems_s, p->nitems_in_s, s);
     if (st) return st;
     p->screen_key = keep;
   }
@@ -269,6 +277,7 @@ static int select_pair_lists(PoissonPlan *p, BeckeGrid *g, const int *keep, cuda
   d.pairs = keep ? p->pairs_s.p : p->pairs.p;
   d.items = keep ? p->items_s.p : p->items.p;
   d.nitems = keep ? p->nitems_s : p->nitems;
+  d.nitems_inner = keep ? p->nitems_in_s : p->nitems_in;
   return kOk;
 }
 
@@ -307,13 +316,14 @@ int grid_poisson_plan(BeckeGrid *g, int lmax, cudaStream_t s, PoissonPlan **out)
     return st;
   }
   st = build_pair_lists(p, g->dev.x, g->dev.y, g->dev.z, nullptr, p->pairs, p->items,
-                        p->nitems, s);
+                        p->nitems, p->nitems_in, s);
   if (st != kOk) {
     delete p;
     return st;
   }
   p->d.items = p->items.p;
   p->d.nitems = p->nitems;
+  p->d.nitems_inner = p->nitems_in;
   p->lmax = lmax;
   g->poisson = p;
   *out = p;

@@ -718,16 +718,18 @@ __global__ void __launch_bounds__(32) bucket_lcut_kernel(PoissonDev P) {
   }
 }
 
-template <int LMAX>
+// TAILS = false: the interior items [0, nitems_inner) (region 0 only, so the
+// kernel carries that region's code alone); true: the others.
+template <int LMAX, bool TAILS>
 __global__ void __launch_bounds__(kEvalChunk / kEvalPerThread)
 eval_pairs_kernel(PoissonDev P, const double *__restrict__ gx,
                   const double *__restrict__ gy, const double *__restrict__ gz) {
   extern __shared__ double cf[];
-  const EvalItem it = P.items[blockIdx.x];
+  const EvalItem it = P.items[blockIdx.x + (TAILS ? P.nitems_inner : 0)];
   const PoissonAtom &at = P.atoms[it.atom];
   const int lmaxA = at.lmax;
   const int lsize = (lmaxA + 1) * (lmaxA + 1);
-  const int region = (it.bucket == 0) ? 1 : (it.bucket == at.nrad ? 2 : 0);
+  const int region = TAILS ? (it.bucket == 0 ? 1 : 2) : 0;
   // l-blocks kept for this bucket (all unless a truncation tolerance is set)
   const int lcut = P.lcut ? P.lcut[at.bucket_off + it.bucket] : lmaxA;
   const int lkeep = (lcut + 1) * (lcut + 1);
@@ -761,7 +763,7 @@ eval_pairs_kernel(PoissonDev P, const double *__restrict__ gx,
     z[j] = dz * inv[j];
     u[j] = region == 0 ? rt_inv(at.rt, d[j]) - (it.bucket - 1) : 0.0;
   }
-  if (region == 0)
+  if (!TAILS)
     pair_values<LMAX, 0, kEvalPerThread>(cf, lcut, x, y, z, d, inv, u, v);
   else if (region == 1)
     pair_values<LMAX, 1, kEvalPerThread>(cf, lcut, x, y, z, d, inv, u, v);
@@ -812,7 +814,12 @@ cudaError_t launch_eval_l(const PoissonDev &P, int npoint, const double *x,
       if (e != cudaSuccess) return e;
     }
     const size_t smem = (size_t)(L + 1) * (L + 1) * 4 * sizeof(double);
-    eval_pairs_kernel<L><<<P.nitems, kEvalChunk / kEvalPerThread, smem, s>>>(P, x, y, z);
+    if (P.nitems_inner > 0)
+      eval_pairs_kernel<L, false><<<P.nitems_inner, kEvalChunk / kEvalPerThread, smem, s>>>(
+          P, x, y, z);
+    if (P.nitems > P.nitems_inner)
+      eval_pairs_kernel<L, true>
+          <<<P.nitems - P.nitems_inner, kEvalChunk / kEvalPerThread, smem, s>>>(P, x, y, z);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     pairs_reduce_kernel<<<(npoint + 255) / 256, 256, 0, s>>>(P, npoint, out, acc);

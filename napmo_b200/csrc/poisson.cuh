@@ -79,6 +79,7 @@ struct PoissonDev {
   // its molecule sorted by spline interval, and a partial potential per pair
   long npair = 0;
   int nitems = 0;
+  int nitems_inner = 0;        // items [0, nitems_inner) lie inside their atom's grid
   int *pairs = nullptr;        // point index, bucket-sorted per atom
   EvalItem *items = nullptr;
   double *pair_v = nullptr;    // [atom][molecule point] contribution

@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(kGradThreads) grad_kernel(GradArgs g) {
         for (int l = 0; l < nc; ++l) {
           if (l == k) continue;
           // product of the other cell functions of k (recomputed: no division by s)
-          double excl = 1.0, s_kl = 0.0, ds_kl = 0.0, mu_kl = 0.0, R = 0.0;
+          double excl = 1.0, ds_kl = 0.0, mu_kl = 0.0, R = 0.0;
           for (int m = 0; m < nc; ++m) {
             if (m == k) continue;
             const int o = (k < m) ? m * (m + 1) / 2 + k : k * (k + 1) / 2 + m;
@@ -226,7 +226,6 @@ __global__ void __launch_bounds__(kGradThreads) grad_kernel(GradArgs g) {
             double s, ds;
             cell(mu + as * (1.0 - mu * mu), s, ds);
             if (m == l) {
-              s_kl = s;
               ds_kl = ds * (1.0 - 2.0 * as * mu);
               mu_kl = mu;
               R = g.Rt[o];
@@ -234,7 +233,6 @@ __global__ void __launch_bounds__(kGradThreads) grad_kernel(GradArgs g) {
               excl *= s;
             }
           }
-          (void)s_kl;
           const double t = alpha * excl * ds_kl / R;
           double e_kl[3];
           for (int d = 0; d < 3; ++d) e_kl[d] = (g.origin[3 * k + d] - g.origin[3 * l + d]) / R;

@@ -141,9 +141,6 @@ project_kernel(PoissonDev P, const double *__restrict__ rho,
 __device__ __forceinline__ double &AB(double *band, int i, int j) {
   return band[j * kW + (kKL + kKU) + i - j];
 }
-__device__ __forceinline__ double ABc(const double *band, int i, int j) {
-  return __ldg(band + j * kW + (kKL + kKU) + i - j);
-}
 
 // The FEM band matrix of a system depends on the atom's radial grid and l
 // only: it is assembled and LU-factored (partial pivoting, kl = ku = 3) once

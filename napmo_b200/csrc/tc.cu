@@ -46,7 +46,7 @@
 // records an error in g_tc_error, the roles stop, copies and MMAs in flight
 // are waited for (bounded) and TMEM is freed before the CTA exits.
 #include <cub/device/device_select.cuh>
-#include <cub/iterator/counting_input_iterator.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include <cstdint>
 #include <memory>
@@ -1106,7 +1106,7 @@ int int8_plan_create(Int8Plan **out, int n, int npoint, const double *phi, long 
     DevBuf<uint8_t> tmp;
     NAPMO_TRY_CUDA(sel.alloc(npoint), "alloc screening");
     NAPMO_TRY_CUDA(cnt.alloc(1), "alloc screening");
-    cub::CountingInputIterator<int> first(0);
+    thrust::counting_iterator<int> first(0);
     size_t tb = 0;
     NAPMO_TRY_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, first, p->keep.p, sel.p, cnt.p,
                                               npoint, s),

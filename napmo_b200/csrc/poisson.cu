@@ -96,41 +96,80 @@ __device__ __forceinline__ double rt_inv(const RTParams &rt, double r) {
 }
 
 // ------------------------------------------------------------------ project
-constexpr int kProjShells = 8;
-constexpr int kProjThreads = 128;
+// proj[s][lm] = sum_j g[s][j] Y[j][lm] / sigma[s] * sqrt(4 pi (2l + 1)) per atom,
+// g[s][j] = rho wb w at the atom's point (shell s, direction j): a small GEMM
+// (nrad x nang) x (nang x lsize).  CTA = (64 lm, 64 shells, atom), 256
+// threads each holding a 4 x 4 tile of the result; j runs in chunks of 32
+// staged in shared memory (g transposed, Y as is).  Every output is one FMA
+// chain over j in increasing order, as in a plain loop.
+constexpr int kProjTile = 64, kProjK = 32, kProjThreads = 256;
 
 __global__ void __launch_bounds__(kProjThreads)
 project_kernel(PoissonDev P, const double *__restrict__ rho,
                const double *__restrict__ wb, const double *__restrict__ w) {
-  extern __shared__ double g[];  // [kProjShells][nang]
-  const PoissonAtom at = P.atoms[blockIdx.y];
-  const int s0 = blockIdx.x * kProjShells;
-  if (s0 >= at.nrad) return;
-  const int ns = min(kProjShells, at.nrad - s0);
-  const int nang = at.nang;
+  __shared__ double gs[kProjK][kProjTile + 1];  // [j][shell]
+  __shared__ __align__(16) double ys[kProjK][kProjTile];  // [j][lm]
+  const PoissonAtom at = P.atoms[blockIdx.z];
   const int lsize = (at.lmax + 1) * (at.lmax + 1);
-  for (int idx = threadIdx.x; idx < ns * nang; idx += blockDim.x) {
-    const int s = idx / nang, j = idx % nang;
-    const long p = at.point_off + (long)(s0 + s) * nang + j;
-    g[s * nang + j] = rho[p] * wb[p] * w[p];
-  }
-  __syncthreads();
+  const int lm0 = blockIdx.x * kProjTile, s0 = blockIdx.y * kProjTile;
+  if (lm0 >= lsize || s0 >= at.nrad) return;
+  const int nang = at.nang;
+  const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
   const double *Y = P.ytab + at.ytab_off;
-  const double *sigma = P.rad + at.rad_off + kRadSigma * at.nrad;
-  for (int lm = threadIdx.x; lm < lsize; lm += blockDim.x) {
-    double acc[kProjShells];
+  double acc[4][4];
 #pragma unroll
-    for (int s = 0; s < kProjShells; ++s) acc[s] = 0.0;
-#pragma unroll 4
-    for (int j = 0; j < nang; ++j) {  // unrolled: several table loads in flight
-      const double y = __ldg(Y + (long)j * lsize + lm);
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int s = 0; s < kProjShells; ++s) acc[s] = fma(y, g[s * nang + j], acc[s]);
+    for (int k = 0; k < 4; ++k) acc[i][k] = 0.0;
+  for (int j0 = 0; j0 < nang; j0 += kProjK) {
+    // g tile: 64 shells x 32 directions (contiguous in j for each shell)
+    for (int e = t; e < kProjTile * kProjK; e += kProjThreads) {
+      const int sl = e / kProjK, jj = e % kProjK;
+      const int sh = s0 + sl, j = j0 + jj;
+      double v = 0.0;
+      if (sh < at.nrad && j < nang) {
+        const long p = at.point_off + (long)sh * nang + j;
+        v = rho[p] * wb[p] * w[p];
+      }
+      gs[jj][sl] = v;
     }
+    // Y tile: 32 directions x 64 lm (contiguous in lm)
+    for (int e = t; e < kProjK * kProjTile; e += kProjThreads) {
+      const int jj = e / kProjTile, ll = e % kProjTile;
+      const int j = j0 + jj, lm = lm0 + ll;
+      ys[jj][ll] = (j < nang && lm < lsize) ? __ldg(Y + (long)j * lsize + lm) : 0.0;
+    }
+    __syncthreads();
+    const int jn = min(kProjK, nang - j0);
+    for (int jj = 0; jj < jn; ++jj) {
+      double a[4], y[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = gs[jj][ty * 4 + i];
+      const double2 y01 = *reinterpret_cast<const double2 *>(&ys[jj][tx * 4]);
+      const double2 y23 = *reinterpret_cast<const double2 *>(&ys[jj][tx * 4 + 2]);
+      y[0] = y01.x;
+      y[1] = y01.y;
+      y[2] = y23.x;
+      y[3] = y23.y;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc[i][k] = fma(y[k], a[i], acc[i][k]);
+    }
+    __syncthreads();
+  }
+  const double *sigma = P.rad + at.rad_off + kRadSigma * at.nrad;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int lm = lm0 + tx * 4 + k;
+    if (lm >= lsize) continue;
     const int l = (int)sqrt((double)lm + 0.5);
     const double fac = sqrt(4.0 * M_PI * (2.0 * l + 1));
-    for (int s = 0; s < ns; ++s)
-      P.proj[at.proj_off + (long)(s0 + s) * lsize + lm] = acc[s] / sigma[s0 + s] * fac;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int sh = s0 + ty * 4 + i;
+      if (sh < at.nrad) P.proj[at.proj_off + (long)sh * lsize + lm] = acc[i][k] / sigma[sh] * fac;
+    }
   }
 }
 
@@ -890,13 +929,10 @@ cudaError_t launch_poisson_project(const PoissonDev &P, const double *rho,
                                    const double *wb, const double *w,
                                    cudaStream_t s) {
   if (P.natom == 0) return cudaSuccess;
-  dim3 grid((P.max_nrad + kProjShells - 1) / kProjShells, P.natom);
-  const size_t smem = (size_t)kProjShells * P.max_nang * sizeof(double);
-  cudaError_t e = cudaFuncSetAttribute(project_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
-  if (e != cudaSuccess) return e;
-  project_kernel<<<grid, kProjThreads, smem, s>>>(P, rho, wb, w);
+  const int lsize = (P.max_lmax + 1) * (P.max_lmax + 1);
+  dim3 grid((lsize + kProjTile - 1) / kProjTile, (P.max_nrad + kProjTile - 1) / kProjTile,
+            P.natom);
+  project_kernel<<<grid, kProjThreads, 0, s>>>(P, rho, wb, w);
   return cudaGetLastError();
 }
 

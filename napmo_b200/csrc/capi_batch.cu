@@ -4,7 +4,8 @@
 // The batch holds one Fock plan per molecule (napmo_fock_plan_new) and owns
 // a device D and F per molecule.  On first use it runs every build once
 // eagerly (lazy set-up: Poisson plans, kernel attributes, constant tables),
-// then captures the builds into a graph: the molecules are spread over
+// then captures the builds into a graph (again after any plan changed:
+// precision, Poisson tolerance, a refresh or a moved grid): the molecules are spread over
 // `nstream` capture streams forked from and joined back into the batch's
 // origin stream, so the graph holds nstream independent chains and small
 // molecules' kernels run side by side.  A build of the whole batch is then one
@@ -32,6 +33,7 @@ int fock_build(FockPlan *p, const double *D_dev, double q, const double *vext_de
                double *rho_out, double *v_out, cudaStream_t s);
 int fock_plan_nbasis(const FockPlan *p);
 Int8Plan *fock_plan_int8(FockPlan *p);
+unsigned long long fock_plan_state(const FockPlan *p);
 
 struct FockBatch {
   std::vector<FockPlan *> plans;  // not owned
@@ -45,6 +47,7 @@ struct FockBatch {
   int nstream = 8, budget = 0;
   bool warm = false;
   float tuned_ms = 0.0f;
+  std::vector<unsigned long long> state;  // fock_plan_state of every plan at warm-up
 
   ~FockBatch() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -69,14 +72,29 @@ int set_budgets(FockBatch *b, int budget) {
   return kOk;
 }
 
+// True when a plan changed since the warm-up (precision, tolerance, refresh,
+// moved grid): the captured graph would run on freed or stale state.
+bool stale(const FockBatch *b) {
+  if (b->state.size() != b->plans.size()) return true;
+  for (size_t i = 0; i < b->plans.size(); ++i)
+    if (fock_plan_state(b->plans[i]) != b->state[i]) return true;
+  return false;
+}
+
 // Every build once, outside any capture (creates the lazily built state).
 int warm_up(FockBatch *b, cudaStream_t s) {
+  if (b->exec) {  // captured against the previous state
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+  }
   for (size_t i = 0; i < b->plans.size(); ++i) {
     const int e = fock_build(b->plans[i], b->D[i]->p, b->q, nullptr, b->F[i]->p, nullptr,
                              nullptr, s);
     if (e) return e;
   }
   NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "batch warm-up");
+  b->state.clear();
+  for (auto *p : b->plans) b->state.push_back(fock_plan_state(p));
   b->warm = true;
   return kOk;
 }
@@ -174,7 +192,7 @@ int napmo_fock_batch_buffers(FockBatch *b, int i, double **D, double **F) {
 int napmo_fock_batch_build(FockBatch *b, void *stream) {
   return guarded([&] {
     cudaStream_t s = (cudaStream_t)stream;
-    if (!b->warm) {
+    if (!b->warm || stale(b)) {
       const int e = warm_up(b, s);
       if (e) return e;
     }
@@ -199,7 +217,7 @@ int napmo_fock_batch_tune(FockBatch *b, void *stream, int reps, int *nstream_out
     int dev = 0, sms = 148;
     NAPMO_TRY_CUDA(cudaGetDevice(&dev), "device");
     NAPMO_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SMs");
-    if (!b->warm) {
+    if (!b->warm || stale(b)) {
       const int e = warm_up(b, s);
       if (e) return e;
     }

@@ -983,6 +983,7 @@ int napmo_grid_set_centers(BeckeGrid *g, const double *origin) {
       delete g->poisson;
       g->poisson = nullptr;
     }
+    ++g->generation;
     return compute_becke(g, s);  // synchronises s before the host vectors go
   });
 }

@@ -80,6 +80,7 @@ struct FockPlan {
   int n = 0, lmax = 0;
   int mode = 0;  // 0 FP64, 1 int8 slices on the tensor cores
   double poisson_tol = 0.0;  // truncation tolerance of the potential evaluation
+  unsigned generation = 0;   // bumped by every change that captured builds depend on
   long ld = 0;
   DevBuf<double> phi, rho, v, wv, work, D, F, vext;
   Int8Plan *i8 = nullptr;
@@ -130,6 +131,12 @@ int fock_build(FockPlan *p, const double *D_dev, double q, const double *vext_de
 
 int fock_plan_nbasis(const FockPlan *p) { return p->n; }
 Int8Plan *fock_plan_int8(FockPlan *p) { return p->mode == 1 ? p->i8 : nullptr; }
+
+// State a captured build depends on: the plan's own changes (precision,
+// Poisson tolerance, refresh) and its grid's moves.
+unsigned long long fock_plan_state(const FockPlan *p) {
+  return ((unsigned long long)p->generation << 32) | p->grid->generation;
+}
 
 }  // namespace napmo
 
@@ -311,6 +318,7 @@ int napmo_fock_plan_refresh(FockPlan *p, void *stream) {
       if (e) return e;
     }
     NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "refresh");
+    ++p->generation;
     if (p->i8) {
       int8_plan_destroy(p->i8);
       p->i8 = nullptr;
@@ -464,6 +472,7 @@ int napmo_fock_plan_set_precision(FockPlan *p, int mode) {
     }
     p->mode = mode;
     p->poisson_tol = mode == 1 ? napmo::kMixedPoissonTol : 0.0;
+    ++p->generation;
     return napmo::kOk;
   });
 }
@@ -475,6 +484,7 @@ int napmo_fock_plan_set_poisson_tolerance(FockPlan *p, double tol) {
   return napmo::guarded([&] {
     NAPMO_REQUIRE(tol >= 0.0 && tol < 1.0, "Poisson tolerance must be in [0, 1)");
     p->poisson_tol = tol;
+    ++p->generation;
     return napmo::kOk;
   });
 }

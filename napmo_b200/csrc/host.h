@@ -193,6 +193,7 @@ struct BeckeGrid {
   DeviceGrid dev;                     // device mirror (points SoA, weights)
   PoissonPlan *poisson = nullptr;     // cached for the last lmax used
   double poisson_tol = 0.0;           // truncation tolerance of the potential evaluation
+  unsigned generation = 0;            // bumped when the centres move (napmo_grid_set_centers)
   BeckeGrid() = default;
   ~BeckeGrid();
 };

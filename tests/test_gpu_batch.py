@@ -53,3 +53,32 @@ def test_batch_equals_single_builds_fp64_and_int8():
         # the tuned split-K chunking only reorders FP64 partial sums
         assert np.abs(F - R).max() <= 1e-12 * np.abs(R).max()
         assert abs(0.5 * float((F * D).sum()) - 0.5 * float((R64 * D).sum())) <= 1e-6
+
+
+def test_batch_recaptures_after_plans_change():
+    """A captured batch holds the device state of its plans.  Moving one
+    molecule (grid + basis + refresh) and switching another to int8 must make
+    the next batch build run on the new state: equal to fresh single builds."""
+    import torch
+    import napmo_b200 as nb
+    mols = _molecules(nmol=3, seed=21)
+    builders = [nb.FockBuilder(g, e['basis'], 'per-atom') for e, g in mols]
+    Ds = [random_density(b.n, max(1, e['occupation']), seed=200 + i)
+          for i, ((e, g), b) in enumerate(zip(mols, builders))]
+    batch = nb.FockBatch(builders)
+    batch.build(Ds)
+    torch.cuda.synchronize()
+    # move molecule 0 by a rigid shift
+    e0, g0 = mols[0]
+    shift = np.array([0.31, -0.17, 0.23])
+    org = e0['basis'].origins()
+    centres = np.array([p['origin'] for p in e0['particles']], dtype=np.float64)
+    g0.set_centers(centres + shift)
+    e0['basis'].set_origins(org + shift)
+    builders[0].refresh()
+    builders[1].set_precision('int8x4')
+    Fs = [F.cpu().numpy() for F in batch.build()]
+    assert builders[1].tc_status() == 0
+    for F, b, D in zip(Fs, builders, Ds):
+        R = b.build(D)[0].cpu().numpy()
+        assert np.abs(F - R).max() <= 1e-12 * np.abs(R).max()

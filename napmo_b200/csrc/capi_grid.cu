@@ -53,7 +53,7 @@ struct PoissonPlan {
   DevBuf<int> pairs_s;
   DevBuf<EvalItem> items_s;
   int nitems_s = 0, nitems_in_s = 0;
-  const int *screen_key = nullptr;
+  unsigned long long screen_key = 0;  // serial of the mask's int8 plan (0: none)
 };
 
 void free_poisson_plan(PoissonPlan *p) { delete p; }
@@ -264,14 +264,15 @@ int build_pair_lists(PoissonPlan *plan, const double *x, const double *y, const 
 }
 
 // Points the evaluation runs on: all (keep null) or the screened ones.
-static int select_pair_lists(PoissonPlan *p, BeckeGrid *g, const int *keep, cudaStream_t s) {
+static int select_pair_lists(PoissonPlan *p, BeckeGrid *g, const int *keep,
+                             unsigned long long key, cudaStream_t s) {
   PoissonDev &d = p->d;
-  if (keep && keep != p->screen_key) {
-    p->screen_key = nullptr;
+  if (keep && key != p->screen_key) {
+    p->screen_key = 0;
     const int st = build_pair_lists(p, g->dev.x, g->dev.y, g->dev.z, keep, p->pairs_s,
                                     p->items_s, p->nitems_s, p->nitems_in_s, s);
     if (st) return st;
-    p->screen_key = keep;
+    p->screen_key = key;
   }
   d.keep = keep;
   d.pairs = keep ? p->pairs_s.p : p->pairs.p;
@@ -333,10 +334,12 @@ int grid_poisson_plan(BeckeGrid *g, int lmax, cudaStream_t s, PoissonPlan **out)
 // One Poisson solve on the grid's plan: v (=, += with accumulate) = V_H[rho].
 // tol > 0 truncates the evaluation (see eval_tol); keep (grid flags, or null)
 // restricts the evaluation to the flagged points, v = 0 elsewhere (its pair
-// lists are built, synchronously, the first time a mask is used).
+// lists are built, synchronously, the first time a mask is used; key names
+// the mask, which an address could not: a freed mask's address is reused).
 int run_poisson(BeckeGrid *g, PoissonPlan *p, const double *rho_dev, double *v_dev,
-                bool accumulate, cudaStream_t s, double tol, const int *keep) {
-  int st = select_pair_lists(p, g, keep, s);
+                bool accumulate, cudaStream_t s, double tol, const int *keep,
+                unsigned long long key) {
+  int st = select_pair_lists(p, g, keep, key, s);
   if (st) return st;
   p->d.eval_tol = tol;
   p->d.lcut = tol > 0.0 ? p->lcut.p : nullptr;
@@ -1199,7 +1202,7 @@ int napmo_gpu_poisson(BeckeGrid *g, const double *rho_dev, int lmax, double *v_d
     PoissonPlan *p = nullptr;
     int st = grid_poisson_plan(g, lmax, s, &p);
     if (st) return st;
-    st = run_poisson(g, p, rho_dev, v_dev, accumulate != 0, s, g->poisson_tol, nullptr);
+    st = run_poisson(g, p, rho_dev, v_dev, accumulate != 0, s, g->poisson_tol, nullptr, 0);
     if (st) return st;
     if (raw_y)
       NAPMO_TRY_CUDA(cudaMemcpyAsync(raw_y, p->raw_y.p, p->raw_y.n * sizeof(double),

@@ -15,7 +15,8 @@ namespace napmo {
 struct PoissonPlan;
 int grid_poisson_plan(BeckeGrid *g, int lmax, cudaStream_t s, PoissonPlan **out);
 int run_poisson(BeckeGrid *g, PoissonPlan *p, const double *rho_dev, double *v_dev,
-                bool accumulate, cudaStream_t s, double tol, const int *keep);
+                bool accumulate, cudaStream_t s, double tol, const int *keep,
+                unsigned long long key);
 
 // Truncation tolerance (a.u.) of the Poisson potential evaluation that
 // precision 1 selects: each (atom, radial interval) drops l-blocks whose
@@ -109,6 +110,9 @@ int plan_quadrature(FockPlan *p, double *F, cudaStream_t s) {
 const int *plan_keep(const FockPlan *p) {
   return p->mode == 1 && p->i8 ? int8_plan_keep(p->i8) : nullptr;
 }
+static unsigned long long plan_keep_key(const FockPlan *p) {
+  return p->mode == 1 && p->i8 ? int8_plan_serial(p->i8) : 0;
+}
 
 // The build chain of napmo_fock_plan_build (stream-ordered, no host
 // synchronisation, no allocation once the grid's Poisson plan exists).
@@ -122,7 +126,7 @@ int fock_build(FockPlan *p, const double *D_dev, double q, const double *vext_de
   PoissonPlan *pp = nullptr;
   e = grid_poisson_plan(g, p->lmax, s, &pp);
   if (e) return e;
-  e = run_poisson(g, pp, rho, v, false, s, p->poisson_tol, plan_keep(p));
+  e = run_poisson(g, pp, rho, v, false, s, p->poisson_tol, plan_keep(p), plan_keep_key(p));
   if (e) return e;
   NAPMO_TRY_CUDA(launch_combine_weights(g->size, g->dev.wb, g->dev.w, q, v, vext_dev, p->wv.p, s),
                  "weights");
@@ -368,7 +372,8 @@ int napmo_fock_plan_poisson(FockPlan *p, const double *rho_dev, double *v_dev, v
     PoissonPlan *pp = nullptr;
     int e = grid_poisson_plan(p->grid, p->lmax, s, &pp);
     if (e) return e;
-    return run_poisson(p->grid, pp, rho_dev, v_dev, false, s, p->poisson_tol, plan_keep(p));
+    return run_poisson(p->grid, pp, rho_dev, v_dev, false, s, p->poisson_tol, plan_keep(p),
+                       plan_keep_key(p));
   });
 }
 

@@ -57,6 +57,8 @@ void int8_plan_destroy(Int8Plan *p);
 // Points the plan keeps, and their flags over the grid (null without screening).
 int int8_plan_npoint(const Int8Plan *p);
 const int *int8_plan_keep(const Int8Plan *p);
+// Unique, never reused number of the plan (names its screening mask).
+unsigned long long int8_plan_serial(const Int8Plan *p);
 // CTA budget the int8 kernels are sized for (<= 0: the SM count).
 int int8_set_budget(Int8Plan *p, int ctas);
 size_t int8_plan_device_bytes(const Int8Plan *p);

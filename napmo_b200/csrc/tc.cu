@@ -48,6 +48,7 @@
 #include <cub/device/device_select.cuh>
 #include <thrust/iterator/counting_iterator.h>
 
+#include <atomic>
 #include <cstdint>
 #include <memory>
 
@@ -1058,6 +1059,7 @@ struct Int8Plan {
   DevBuf<int> keep;     // [npoint_grid] 1 for a kept point
   DevBuf<int> idx;      // [npoint] grid index of each kept point (screened plans)
   bool screened = false;
+  unsigned long long serial = 0;  // unique per plan
 };
 
 // Sizes the kernels for `ctas` resident CTAs (<= 0: the SM count): the
@@ -1092,7 +1094,9 @@ int int8_plan_create(Int8Plan **out, int n, int npoint, const double *phi, long 
   *out = nullptr;
   NAPMO_REQUIRE(n >= 1 && n <= 8192, "int8 contractions need 1 <= n <= 8192 basis functions");
   NAPMO_REQUIRE(npoint >= 1, "empty grid");
+  static std::atomic<unsigned long long> next_serial{1};
   std::unique_ptr<Int8Plan> p(new Int8Plan);
+  p->serial = next_serial++;
   p->n = n;
   p->npoint_grid = npoint;
   p->ld = ld;
@@ -1185,6 +1189,8 @@ size_t int8_plan_device_bytes(const Int8Plan *p) {
 int int8_plan_npoint(const Int8Plan *p) { return p->npoint; }
 
 const int *int8_plan_keep(const Int8Plan *p) { return p->screened ? p->keep.p : nullptr; }
+
+unsigned long long int8_plan_serial(const Int8Plan *p) { return p->serial; }
 
 int int8_density(Int8Plan *p, const double *D, double *rho, cudaStream_t s) {
   const long nn = (long)p->n * p->n;

@@ -111,3 +111,35 @@ def test_grid_charge_energy_int8_quadrature_matrix():
         V, V8 = V.cpu().numpy(), V8.cpu().numpy()
         assert np.abs(V8 - V).max() <= 1e-8 * np.abs(V).max()
         assert st8['fb'].tc_status() == 0
+
+
+def test_screened_pair_lists_follow_their_mask():
+    """Two int8 plans on one grid screen different points (different bases);
+    the grid's Poisson plan keeps one set of screened pair lists and must
+    rebuild it for the second plan's mask (keyed by the plan, not by the
+    mask's address, which a freed plan's successor may reuse)."""
+    import torch
+    import napmo_b200 as nb
+    from napmo_b200.system import MolecularSystem
+
+    def system(basis):
+        ms = MolecularSystem()
+        for s, xyz in zip(SYM, R0):
+            ms.add_atom(s, xyz, units='BOHR', basis_name=basis)
+        return ms['e-']
+
+    eA, eB, eB2 = system('CC-PVDZ'), system('STO-3G'), system('STO-3G')
+    g = nb.BeckeGrid(eA, 40, 110)
+    fA = nb.FockBuilder(g, eA['basis'], 6, precision='int8x4')
+    DA = np.eye(fA.n) * 0.2
+    fA.coulomb_potential(fA.density(DA))
+    keepA = fA.kept_points()
+    del fA
+    fB = nb.FockBuilder(g, eB['basis'], 6, precision='int8x4')
+    g2 = nb.BeckeGrid(eB2, 40, 110)
+    fB2 = nb.FockBuilder(g2, eB2['basis'], 6, precision='int8x4')
+    assert not torch.equal(keepA, fB.kept_points())
+    DB = np.eye(fB.n) * 0.3
+    vB = fB.coulomb_potential(fB.density(DB))
+    vB2 = fB2.coulomb_potential(fB2.density(DB))
+    assert torch.equal(vB, vB2)

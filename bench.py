@@ -149,13 +149,39 @@ def build_workload(args):
 
 
 # ------------------------------------------------------------- CPU baseline
+def _ref_evaluation(r, centers, radii, nrad, lmax, y, dt, pts, v):
+    """nAPMO's own multipole evaluation (horton/evaluate.cpp compiled from its
+    sources into oracle/_ref, OpenMP as nAPMO builds it): per atom the lsize
+    cubic splines of the decomposition on the atom's Chebyshev radial grid with
+    nAPMO's potential extrapolation, evaluated at every sample point."""
+    from ctypes import c_void_p
+    for c, radius in zip(centers, radii):
+        rt = r.ChebyshevRTransform_new(radius, nrad)
+        splines, keep = [], []
+        k = 0
+        for l in range(lmax + 1):
+            for _m in range(2 * l + 1):
+                ext = r.PotentialExtrapolation_new(l)
+                yy, dd = np.ascontiguousarray(y[k]), np.ascontiguousarray(dt[k])
+                keep += [yy, dd]
+                splines.append(r.CubicSpline_new(yy, dd, ext, rt, nrad))
+                k += 1
+        cell = r.Cell_new(None, 0)
+        r.eval_decomposition_grid(np.array(splines, dtype=c_void_p), np.ascontiguousarray(c), v,
+                                  pts, cell, len(splines), pts.shape[0])
+
+
 def cpu_baseline(args, atoms, grid, D, lmax):
-    """The oracle (C restatement of nAPMO's path, OpenMP on every host core)
-    on a bounded sample of one build: density, quadrature and multipole
-    evaluation on `cpu_points` grid points (scaled by N / sample), plus the
-    projection and radial ODE solves of one C and one H atom (scaled by the
-    atom counts).  The reference's own quadrature materialises all orbital
-    products (1.95 TB here), so the streamed restatement is timed."""
+    """nAPMO's path on the host cores, on a bounded sample of one build:
+    density, multipole evaluation and quadrature on `cpu_points` grid points
+    (scaled by N / sample), plus the projection and radial ODE solves of one
+    C and one H atom (scaled by the atom counts).  Where nAPMO's own code runs
+    here it is what is timed: the density by its numpy expression
+    (psi_hybrid.py / psi_analytic.py: phi * D.dot(phi) per point, summed), the
+    multipole evaluation by its compiled evaluate.cpp (oracle/_ref, when
+    built).  The quadrature is the oracle's streamed C restatement (nAPMO's
+    materialises all orbital products, 1.95 TB here, and needs Eigen), and
+    so are the projection and radial solves (scipy, as poisson_solver.py)."""
     sys.path.insert(0, os.path.join(ROOT, 'oracle'))
     import oracle as O
     lib = json.load(open(os.path.join(ROOT, 'napmo_b200', 'data', 'basis.json')))
@@ -171,18 +197,27 @@ def cpu_baseline(args, atoms, grid, D, lmax):
     w = np.ascontiguousarray(grid.weights[idx])
     phi = np.ascontiguousarray(O.basis_compute(fb, pts).T)
     t0 = time.perf_counter()
-    rho = O.density(phi, D)
+    Dgrid = np.array([p * D.dot(p) for p in phi.T]).T
+    rho = Dgrid.sum(axis=0)
     t1 = time.perf_counter()
     v = np.zeros(args.cpu_points)
     # multipole evaluation: every atom's lsize splines at every sample point
     lsize = (lmax + 1) ** 2
     spl_y = np.ascontiguousarray(rng.normal(size=(lsize, args.nrad)))
     spl_dt = np.ascontiguousarray(rng.normal(size=(lsize, args.nrad)))
+    radii = [el[s]['atomic_radii'] for s in syms]
+    # nAPMO's library sets OpenMP's thread count from OMP_NUM_THREADS when it
+    # loads (one thread if unset; utils/omp_helper.h): give it every core, as a
+    # user of nAPMO would
+    os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count() or 1))
+    r = O.ref_lib()
     t2 = time.perf_counter()
-    for a, c in enumerate(centers):
-        O.lib.orc_eval_decomposition(0, el[syms[a]]['atomic_radii'], 0.0, args.nrad, lsize,
-                                     spl_y, spl_dt, np.ascontiguousarray(c), args.cpu_points,
-                                     pts, v)
+    if r is not None:
+        _ref_evaluation(r, centers, radii, args.nrad, lmax, spl_y, spl_dt, pts, v)
+    else:
+        for c, radius in zip(centers, radii):
+            O.lib.orc_eval_decomposition(0, radius, 0.0, args.nrad, lsize, spl_y, spl_dt,
+                                         np.ascontiguousarray(c), args.cpu_points, pts, v)
     t3 = time.perf_counter()
     F = O.quadrature(phi, v, bw, w)
     t4 = time.perf_counter()
@@ -194,17 +229,25 @@ def cpu_baseline(args, atoms, grid, D, lmax):
     t5 = time.perf_counter()
     O.poisson_solver(og, dens, lmax)
     t6 = time.perf_counter()
+    del rho, F
     ncar = syms.count('C')
     nh = syms.count('H')
-    per_point = (t1 - t0) + (t3 - t2) + (t4 - t3)
-    t_build = per_point * N / args.cpu_points + (t6 - t5) * (ncar + nh) / 2.0
-    return {'value': 1.0 / t_build, 'unit': UNIT, 'cores': O.threads(), 'kind': 'port',
-            'sample': ('oracle C restatement (nAPMO order of operations, -O2, OpenMP): density, '
-                       'multipole evaluation (62 atoms x %d splines) and streamed quadrature '
-                       'on %d of %d points, scaled x%.0f; projection + radial FEM solves '
-                       '(scipy spsolve) of 2 of 62 atoms, scaled x31; sample wall %.1f s'
-                       % (lsize, args.cpu_points, N, N / args.cpu_points, t6 - t0)),
-            'seconds_per_build': t_build}
+    scale = N / args.cpu_points
+    parts = {'density': (t1 - t0) * scale, 'evaluation': (t3 - t2) * scale,
+             'quadrature': (t4 - t3) * scale,
+             'projection_radial': (t6 - t5) * (ncar + nh) / 2.0}
+    t_build = sum(parts.values())
+    return {'value': 1.0 / t_build, 'unit': UNIT, 'cores': O.threads(),
+            'kind': 'reference' if r is not None else 'port',
+            'sample': ('%d of %d points, scaled x%.0f: density by nAPMO\'s numpy expression, '
+                       'multipole evaluation (62 atoms x %d splines) by %s, quadrature by the '
+                       'oracle\'s streamed C restatement (OpenMP); projection + radial FEM solves '
+                       '(oracle, scipy spsolve) of 2 of 62 atoms, scaled x31; sample wall %.1f s'
+                       % (args.cpu_points, N, scale, lsize,
+                          "nAPMO's evaluate.cpp compiled from its sources (OpenMP, "
+                          "OMP_NUM_THREADS = host cores)"
+                          if r is not None else 'the oracle C restatement (OpenMP)', t6 - t0)),
+            'seconds_per_build': t_build, 'seconds_per_part': parts}
 
 
 # ------------------------------------------------------------ C3: batches

@@ -274,6 +274,17 @@ long napmo_poisson_raw_size(void *grid, int lmax);
  * drop its highest l-blocks while their bounded sum stays <= tol, so each
  * point's potential moves by at most natom * tol. */
 int napmo_grid_set_poisson_tolerance(void *grid, double tol);
+/* LDA exchange (Dirac-Slater) and VWN5 correlation of rho (device, n values):
+ * energies per particle and potentials, any output may be null; replaces
+ * Functional('lda').compute_exchange / compute_correlation
+ * (napmo/functional/xc_interface.py:62-90, LibXC lda_x / lda_c_vwn). */
+int napmo_gpu_lda_xc(long n, const double *rho, double *x_zk, double *x_vrho, double *c_zk,
+                     double *c_vrho, void *stream);
+/* epc17-2 electron-proton correlation at n common points (device): energy per
+ * electron and both species' potentials; replaces epc17_2
+ * (napmo/functional/interspecies_correlation.py:36-68). */
+int napmo_gpu_epc17_2(long n, const double *rho_e, const double *rho_n, double *ene,
+                      double *pot_e, double *pot_n, void *stream);
 /* sum_A Z_A / |r - R_A| at device points; replaces compute_nuclear (nnuclear.py:15-37). */
 int napmo_gpu_nuclear_potential(int npoint, const double *x, const double *y, const double *z,
                                 int nq, const double *charges, double *v, void *stream);

@@ -17,5 +17,6 @@ from .gto import BasisSet, ContractedGaussian, PrimitiveGaussian
 from .system import BOHR_TO_ANGSTROM, MolecularSystem
 from .wavefunction import WaveFunction, compute_coulomb, compute_nuclear
 from .fock import FockBatch, FockBuilder
+from .functional import Functional, epc17_2, isc_functional_selector
 
 ANGSTROM_TO_BOHR = 1.889726133921252

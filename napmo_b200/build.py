@@ -23,7 +23,8 @@ CUDA_FLAGS = ARCH + ['-O3', '-lineinfo', '-std=c++17', '--expt-relaxed-constexpr
                      '-Xcompiler', '-fPIC,-ffp-contract=off', '-Xptxas', '-warn-spills']
 HOST_SOURCES = ['host.cpp']
 CUDA_SOURCES = ['becke.cu', 'gto.cu', 'quad.cu', 'tc.cu', 'poisson.cu', 'capi_grid.cu',
-                'capi_basis.cu', 'capi_quad.cu', 'capi_batch.cu', 'capi_scf.cu', 'grad.cu']
+                'capi_basis.cu', 'capi_quad.cu', 'capi_batch.cu', 'capi_scf.cu', 'grad.cu',
+                'xc.cu']
 EXTRA_CUDA = {'becke.cu': ['--fmad=false']}
 LIBS = ['-lcusolver', '-lcublas']
 

@@ -197,6 +197,10 @@ _SIGS = [
      [c_void_p, c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     ('napmo_poisson_raw_size', c_long, [c_void_p, c_int]),
     ('napmo_grid_set_poisson_tolerance', c_int, [c_void_p, c_double]),
+    ('napmo_gpu_lda_xc', c_int,
+     [c_long, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ('napmo_gpu_epc17_2', c_int,
+     [c_long, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ('napmo_gpu_nuclear_potential', c_int,
      [c_int, c_void_p, c_void_p, c_void_p, c_int, a2df, c_void_p, c_void_p]),
     ('napmo_fock_plan_new', c_void_p, [c_void_p, c_void_p, c_int, c_void_p]),

@@ -1,0 +1,69 @@
+"""CPU restatement of the local functionals of nAPMO's grid path (test
+infrastructure only).
+
+nAPMO takes its electronic functionals from LibXC through pylibxc
+(napmo/functional/xc_interface.py:29-90: 'lda' = lda_x + lda_c_vwn,
+unpolarised), a third-party library absent here; its published forms are
+restated: Dirac-Slater exchange and the Vosko-Wilk-Nusair paramagnetic
+correlation fit (VWN5, Can. J. Phys. 58, 1200 (1980)), which is what LibXC's
+lda_c_vwn evaluates.  Pinned against nAPMO's own fixtures
+(napmo/functional/test/*.txt, subsampled into tests/golden/xc_lda.npz).
+The electron-proton correlation epc17-2 restates
+napmo/functional/interspecies_correlation.py:36-68.
+"""
+import numpy as np
+
+# densities below this give zk = vrho = 0 (nAPMO's fixtures, produced through
+# LibXC, place the cut between 3.1e-25 and 1.2e-22)
+DENS_CUT = 1e-24
+
+CX = -(3.0 / np.pi) ** (1.0 / 3.0)       # v_x = CX rho^(1/3)
+VWN_A, VWN_B, VWN_C, VWN_X0 = 0.0310907, 3.72744, 12.9352, -0.10498
+
+
+def lda_x(rho):
+    """(zk, vrho) of Dirac-Slater exchange, per particle and its derivative."""
+    rho = np.asarray(rho, np.float64)
+    m = rho >= DENS_CUT
+    r13 = np.cbrt(np.where(m, rho, 0.0))
+    return np.where(m, 0.75 * CX * r13, 0.0), np.where(m, CX * r13, 0.0)
+
+
+def lda_c_vwn(rho):
+    """(zk, vrho) of VWN5 correlation (paramagnetic)."""
+    rho = np.asarray(rho, np.float64)
+    m = rho >= DENS_CUT
+    r = np.where(m, rho, 1.0)
+    A, b, c, x0 = VWN_A, VWN_B, VWN_C, VWN_X0
+    x = np.sqrt(np.cbrt(3.0 / (4.0 * np.pi * r)))      # sqrt(r_s)
+    X = x * x + b * x + c
+    X0 = x0 * x0 + b * x0 + c
+    Q = np.sqrt(4.0 * c - b * b)
+    at = np.arctan(Q / (2.0 * x + b))
+    ec = A * (np.log(x * x / X) + 2.0 * b / Q * at
+              - b * x0 / X0 * (np.log((x - x0) ** 2 / X) + 2.0 * (b + 2.0 * x0) / Q * at))
+    dX = 2.0 * x + b
+    den = dX * dX + Q * Q
+    dec = A * (2.0 / x - dX / X - 4.0 * b / den
+               - b * x0 / X0 * (2.0 / (x - x0) - dX / X - 4.0 * (b + 2.0 * x0) / den))
+    vc = ec - x / 6.0 * dec                              # v = e - (r_s / 3) de/dr_s
+    return np.where(m, ec, 0.0), np.where(m, vc, 0.0)
+
+
+def epc17_2(rhoE, rhoN):
+    """(energy per electron, potential of the electrons, of the nuclei) of
+    epc17-2 at common points; if any density is below 1e-200 every point
+    uses the alternative potentials, as nAPMO does."""
+    rhoE = np.asarray(rhoE, np.float64)
+    rhoN = np.asarray(rhoN, np.float64)
+    a, b, c = 2.35, 2.4, 6.6
+    den = a - b * np.sqrt(rhoE * rhoN) + c * rhoE * rhoN
+    ene = -rhoN / den
+    if np.any(np.abs(rhoE) < 1.0e-200) or np.any(np.abs(rhoN) < 1.0e-200):
+        pa = (b * np.sqrt(rhoE) * rhoN ** 1.5 - 2.0 * a * rhoN) / den ** 2 / 2.0
+        pb = (b * np.sqrt(rhoN) * rhoE ** 1.5 - 2.0 * a * rhoE) / den ** 2 / 2.0
+    else:
+        s = np.sqrt(rhoE * rhoN)
+        pa = (rhoE * rhoN * (c * rhoN - b * rhoN / (2.0 * s)) - rhoN * den) / den ** 2
+        pb = (rhoN * rhoE * (c * rhoE - b * rhoE / (2.0 * s)) - rhoE * den) / den ** 2
+    return ene, pa, pb

@@ -1,0 +1,51 @@
+"""The local functionals' CPU restatement (oracle/xc.py) against nAPMO's own
+LDA fixtures (napmo/functional/test, produced through LibXC; subsampled into
+tests/golden/xc_lda.npz by tests/golden/make_xc_golden.py)."""
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden', 'xc_lda.npz')
+
+
+def test_lda_restatement_matches_napmo_fixtures():
+    import xc
+    g = np.load(GOLDEN)
+    zx, vx = xc.lda_x(g['rho'])
+    zc, vc = xc.lda_c_vwn(g['rho'])
+    assert np.abs(zx - g['x_zk']).max() <= 1e-15 * np.abs(g['x_zk']).max()
+    assert np.abs(vx - g['x_vrho']).max() <= 1e-15 * np.abs(g['x_vrho']).max()
+    assert np.abs(zc - g['c_zk']).max() <= 1e-15
+    assert np.abs(vc - g['c_vrho']).max() <= 1e-15
+    # the cut of the smallest densities: zero below, nonzero from 1.2e-22 up
+    assert np.all(g['x_zk'][g['rho'] < 1e-24] == 0.0)
+    assert np.all(zx[g['rho'] < 1e-24] == 0.0)
+
+
+def test_lda_potentials_are_derivatives_of_the_energy_density():
+    import xc
+    rho = np.geomspace(1e-8, 50.0, 200)
+    h = 1e-6 * rho
+    for f in (xc.lda_x, xc.lda_c_vwn):
+        zk, v = f(rho)
+        ep = f(rho + h)[0] * (rho + h)
+        em = f(rho - h)[0] * (rho - h)
+        assert np.abs((ep - em) / (2 * h) - v).max() <= 1e-7 * np.abs(v).max()
+
+
+def test_epc17_2_branches():
+    import xc
+    rng = np.random.default_rng(3)
+    e, n = rng.random(50) + 0.1, rng.random(50) + 0.1
+    ene, pa, pb = xc.epc17_2(e, n)
+    den = 2.35 - 2.4 * np.sqrt(e * n) + 6.6 * e * n
+    assert np.allclose(ene, -n / den, rtol=1e-15, atol=0)
+    # pa is d(e * ene)/d(rho_E) in the regular branch
+    h = 1e-7
+    f = lambda x: x * xc.epc17_2(x, n)[0]
+    assert np.allclose((f(e + h) - f(e - h)) / (2 * h), pa, rtol=1e-6)
+    e2 = e.copy()
+    e2[0] = 0.0                       # a zero density switches every point
+    _, pa2, _ = xc.epc17_2(e2, n)
+    den2 = 2.35 - 2.4 * np.sqrt(e2 * n) + 6.6 * e2 * n
+    assert np.allclose(pa2, (2.4 * np.sqrt(e2) * n ** 1.5 - 2 * 2.35 * n) / den2 ** 2 / 2)

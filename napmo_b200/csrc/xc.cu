@@ -19,7 +19,8 @@
 //   -rho_N / den, den = a - b sqrt(rho_E rho_N) + c rho_E rho_N with
 //   (a, b, c) = (2.35, 2.4, 6.6), and the potentials of both species; when any
 //   density of the call is below 1e-200 every point uses the alternative
-//   potentials, as nAPMO does (a device flag set by a first pass).
+//   potentials, as nAPMO does (a device flag set by a first pass).  Negative
+//   densities (rounding) count as zero.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -76,7 +77,7 @@ __global__ void epc_reset_kernel() { g_epc_tiny = 0; }
 __global__ void epc_flag_kernel(long n, const double *__restrict__ rE,
                                 const double *__restrict__ rN) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool tiny = i < n && (fabs(rE[i]) < 1.0e-200 || fabs(rN[i]) < 1.0e-200);
+  const bool tiny = i < n && (fmax(rE[i], 0.0) < 1.0e-200 || fmax(rN[i], 0.0) < 1.0e-200);
   if (__any_sync(0xffffffffu, tiny) && (threadIdx.x & 31) == 0) atomicOr(&g_epc_tiny, 1);
 }
 
@@ -86,7 +87,9 @@ __global__ void epc17_2_kernel(long n, const double *__restrict__ rE,
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double a = 2.35, b = 2.4, c = 6.6;
-  const double e = rE[i], q = rN[i];
+  // densities below zero (rounding far from every centre) count as zero; the
+  // square roots would give NaN (nAPMO's numpy restatement returns NaN there)
+  const double e = fmax(rE[i], 0.0), q = fmax(rN[i], 0.0);
   const double den = a - b * sqrt(e * q) + c * e * q;
   if (ene) ene[i] = -q / den;
   double pa, pb;

@@ -13,6 +13,8 @@ convergence.py:35-65; wavefunction.cpp:64-116) on top of the grid Fock build:
                         does in the orbital basis; small systems)
                'lda-x': Slater exchange v_x = -(3 rho / pi)^(1/3) folded into
                         the quadrature (any size)
+               'lda':   Slater exchange + VWN5 correlation (nAPMO's
+                        Functional 'lda', napmo_gpu_lda_xc)
                'none':  Hartree
       F = H + J - K (or H + J + V_x), Pulay DIIS on FDS - SDF (6 vectors),
       F C = S C e by the generalised eigensolver, D = 2 C_occ C_occ^T.
@@ -34,6 +36,27 @@ EX = 0.75 * CX                              # e_x = EX rho^(4/3)
 PROTON_MASS = 1836.15267247                 # electron masses (napmo/data/constants.py)
 
 
+def lda_xc(torch, rho):
+    """(v_xc, e_xc per particle) of LDA exchange + VWN5 correlation of rho
+    (device tensor), by napmo_gpu_lda_xc."""
+    n = rho.numel()
+    out = [torch.empty(n, dtype=torch.float64, device='cuda') for _ in range(4)]
+    checked(cext.lib.napmo_gpu_lda_xc(n, rho.data_ptr(), *[o.data_ptr() for o in out],
+                                      torch.cuda.current_stream().cuda_stream))
+    xzk, xv, czk, cv = out
+    return xv + cv, xzk + czk
+
+
+def epc17_2_device(torch, rho_e, rho_n):
+    """(energy per electron, v_e, v_n) of epc17-2 (device tensors)."""
+    n = rho_e.numel()
+    out = [torch.empty(n, dtype=torch.float64, device='cuda') for _ in range(3)]
+    checked(cext.lib.napmo_gpu_epc17_2(n, rho_e.data_ptr(), rho_n.data_ptr(),
+                                       *[o.data_ptr() for o in out],
+                                       torch.cuda.current_stream().cuda_stream))
+    return tuple(out)
+
+
 def nuclear_repulsion(point_charges):
     E = 0.0
     for i, a in enumerate(point_charges):
@@ -49,7 +72,7 @@ class GridRHF(object):
     Args:
         ms: MolecularSystem (all nuclei classical).
         nrad, nang: grid per atom (lists allowed).
-        exchange: 'hf', 'lda-x' or 'none'.
+        exchange: 'hf', 'lda-x', 'lda' (exchange + VWN5 correlation) or 'none'.
         precision: 'fp64' or 'int8x4' for rho and the quadratures.
         diis: number of DIIS vectors.
     """
@@ -118,6 +141,12 @@ class GridRHF(object):
         vH = self.fb.coulomb_potential(rho)
         self.fock_builds += 1
         self.poisson_solves += 1
+        if self.exchange == 'lda':
+            vxc, exc = lda_xc(t, rho)
+            G = self.fb.quadrature(1.0, vH, vext=vxc)
+            EJ = 0.5 * float((self.W * rho * vH).sum())
+            Exc = float((self.W * rho * exc).sum())
+            return self.H + G, float((D * self.H).sum()) + EJ + Exc
         if self.exchange == 'lda-x':
             r13 = t.clamp(rho, min=0.0) ** (1.0 / 3.0)
             G = self.fb.quadrature(1.0, vH, vext=CX * r13)
@@ -266,12 +295,22 @@ class GridAPMO(object):
 
     E = sum_s tr(D_s H_s) + 1/2 tr(D_e (J_e - K_e)) + q_e q_n <rho_e|V[rho_n]>
         + E_nn(classical)
+
+    exchange='lda' replaces the electrons' HF exchange by LDA exchange +
+    VWN5 correlation (nAPMO's Functional 'lda'); correlation='epc17-2' adds
+    the electron-proton correlation functional of the two densities.
     """
 
     def __init__(self, ms, nuclear='H_1', nrad=100, nang=302, lmax=None, precision='fp64',
-                 diis=6, mass=PROTON_MASS):
+                 diis=6, mass=PROTON_MASS, exchange='hf', correlation=None):
         torch = _torch()
         self.torch = torch
+        if exchange not in ('hf', 'lda'):
+            raise ValueError("exchange must be 'hf' or 'lda'")
+        if correlation not in (None, 'epc17-2'):
+            raise NotImplementedError(str(correlation) + ' Functional NOT available!')
+        self.exchange = exchange            # electrons: HF exchange or LDA (x + VWN5 c)
+        self.correlation = correlation      # electron-nucleus: None or epc17-2
         self.ms = ms
         self.grid = BeckeGrid(ms['e-'], nrad, nang)
         if lmax is None:
@@ -301,6 +340,44 @@ class GridAPMO(object):
                 K[:, nu] += phi @ (wpsi * v)
         return 0.5 * (K + K.T)
 
+    def fock(self, De, Dn, Ce=None):
+        """(F_e, F_n, E) for densities De, Dn (Ce: electron orbitals, for HF
+        exchange).  Both species share the grid, so the electron-nucleus
+        functional (epc17-2, interspecies_correlation.py:36-68) is evaluated
+        point by point and its energy sum_p W rho_e e_epc enters once, its
+        potentials the Fock matrices of both species (psi_analytic.py:219-258)."""
+        e, n, t = self.e, self.nuc, self.torch
+        qq = e.q * n.q
+        rho_e = e.fb.density(De)
+        rho_n = n.fb.density(Dn)
+        v_e = e.fb.coulomb_potential(rho_e)
+        v_n = e.fb.coulomb_potential(rho_n)
+        self.poisson_solves += 2
+        ext_e, ext_n, E_xc = qq * v_n, None, 0.0
+        if self.exchange == 'lda':
+            vxc, exc = lda_xc(t, rho_e)
+            ext_e = ext_e + vxc
+            E_xc += float((self.W * rho_e * exc).sum())
+        if self.correlation == 'epc17-2':
+            ene, pe, pn = epc17_2_device(t, rho_e, rho_n)
+            ext_e = ext_e + pe
+            ext_n = pn
+            E_xc += float((self.W * rho_e * ene).sum())
+        # electrons: q_e^2 J_e + q_e q_n J[rho_n] (+ v_xc, epc) - K_e;
+        # nucleus: q_n q_e J[rho_e] (+ epc)
+        Fe = e.H + e.fb.quadrature(e.q * e.q, v_e, vext=ext_e)
+        E_K = 0.0
+        if self.exchange == 'hf':
+            K = self._exchange(Ce[:, :e.nocc])
+            Fe = Fe - K
+            E_K = -0.5 * float((De * K).sum())
+        Fn = n.H + n.fb.quadrature(qq, v_e, vext=ext_n)
+        coup = qq * float((self.W * rho_e * v_n).sum())
+        E_J = 0.5 * e.q * e.q * float((self.W * rho_e * v_e).sum())
+        E = (float((De * e.H).sum()) + E_J + E_K + E_xc + float((Dn * n.H).sum()) + coup +
+             self.Enn)
+        return Fe, Fn, E
+
     def run(self, maxiter=100, tol=1e-8, verbose=False):
         """SCF from a guess with the quantum nuclei as point charges (electrons)
         and the nucleus in that electron density's field; one DIIS over both
@@ -328,20 +405,7 @@ class GridAPMO(object):
         Fs, errs = [], []
         E_prev, history, converged = None, [], False
         for it in range(1, maxiter + 1):
-            rho_e = e.fb.density(De)
-            rho_n = n.fb.density(Dn)
-            v_e = e.fb.coulomb_potential(rho_e)
-            v_n = e.fb.coulomb_potential(rho_n)
-            self.poisson_solves += 2
-            # electrons: J_e + q_e q_n J[rho_n] - K_e; nucleus: q_n q_e J[rho_e]
-            Ge = e.fb.quadrature(e.q * e.q, v_e, vext=qq * v_n)
-            Fe = e.H + Ge - self._exchange(Ce[:, :e.nocc])
-            Fn = n.H + n.fb.quadrature(qq, v_e)
-            # energy: one-body + electron two-body (1/2 of J - K) + coupling
-            coup = qq * float((self.W * rho_e * v_n).sum())
-            Ee = 0.5 * float((De * (e.H + Fe)).sum()) - 0.5 * coup
-            En = float((Dn * n.H).sum())
-            E = Ee + En + coup + self.Enn
+            Fe, Fn, E = self.fock(De, Dn, Ce)
             err_e = e.X.T @ (Fe @ De @ e.S - e.S @ De @ Fe) @ e.X
             err_n = n.X.T @ (Fn @ Dn @ n.S - n.S @ Dn @ Fn) @ n.X
             Fs.append((Fe, Fn))

@@ -54,8 +54,10 @@ def epc17_2(rhoE, rhoN):
     """(energy per electron, potential of the electrons, of the nuclei) of
     epc17-2 at common points; if any density is below 1e-200 every point
     uses the alternative potentials, as nAPMO does."""
-    rhoE = np.asarray(rhoE, np.float64)
-    rhoN = np.asarray(rhoN, np.float64)
+    # negative densities (rounding) count as zero, as in the library's kernel
+    # (nAPMO's own numpy code returns NaN there)
+    rhoE = np.maximum(np.asarray(rhoE, np.float64), 0.0)
+    rhoN = np.maximum(np.asarray(rhoN, np.float64), 0.0)
     a, b, c = 2.35, 2.4, 6.6
     den = a - b * np.sqrt(rhoE * rhoN) + c * rhoE * rhoN
     ene = -rhoN / den

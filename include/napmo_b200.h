@@ -83,7 +83,7 @@ double *AngularGrid_get_weights(void *g);                        /* angular.h:13
 void *RadialGrid_new(void *rtf, double rad);                     /* radial.h:53 */
 void RadialGrid_del(void *g);                                    /* radial.h:55 */
 double RadialGrid_integrate(void *g, int segments, double *f);   /* radial.h:57 */
-double *RadialGrid_deriv2(void *g, double *f);  /* radial.h:59; out of path: sets error */
+double *RadialGrid_deriv2(void *g, double *f);  /* radial.h:59, radial.cpp:51-192; new[] array, free with napmo_free_array */
 int RadialGrid_get_size(void *g);                                /* radial.h:61 */
 double RadialGrid_get_radii(void *g);                            /* radial.h:63 */
 double *RadialGrid_get_points(void *g);                          /* radial.h:65 */
@@ -285,6 +285,21 @@ int napmo_gpu_lda_xc(long n, const double *rho, double *x_zk, double *x_vrho, do
  * (napmo/functional/interspecies_correlation.py:36-68). */
 int napmo_gpu_epc17_2(long n, const double *rho_e, const double *rho_n, double *ene,
                       double *pot_e, double *pot_n, void *stream);
+/* Numerical-orbital operators on the grid (device rows of ld >= grid size).
+ * Kinetic: out[k] = scale * (-1/2 laplacian psi[k]); replaces compute_kinetic
+ * (napmo/wavefunction/nkinetic.py:15-73, RadialGrid::deriv2 of
+ * src/grid/radial.cpp:51-192).  Chebyshev radial grids of >= 8 points. */
+int napmo_gpu_kinetic(void *grid, int lmax, int nfunc, const double *psi, long ld, double scale,
+                      double *out, void *stream);
+/* Becke-Dickson orbital corrections of nfunc orbitals; replaces compute_dpsi
+ * (napmo/wavefunction/ndpsi.py:15-89).  doi, oi: host arrays of nfunc. */
+int napmo_gpu_dpsi(void *grid, int lmax, int nfunc, const double *phi, const double *resid,
+                   const double *vtot, long ld, const double *doi, const double *oi,
+                   double mass_inv, double *out, void *stream);
+/* M[i][j] = integral A_i B_j over the grid (n x m, device); replaces
+ * get_operator_matrix (napmo/wavefunction/psi_numeric.py:406-424). */
+int napmo_gpu_operator_matrix(void *grid, int n, int m, const double *A, long lda,
+                              const double *B, long ldb, double *M, void *stream);
 /* sum_A Z_A / |r - R_A| at device points; replaces compute_nuclear (nnuclear.py:15-37). */
 int napmo_gpu_nuclear_potential(int npoint, const double *x, const double *y, const double *z,
                                 int nq, const double *charges, double *v, void *stream);

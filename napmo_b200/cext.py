@@ -101,6 +101,7 @@ _SIGS = [
     ('RadialGrid_new', c_void_p, [c_void_p, c_double]),
     ('RadialGrid_del', None, [c_void_p]),
     ('RadialGrid_integrate', c_double, [c_void_p, c_int, a1df]),
+    ('RadialGrid_deriv2', PD, [c_void_p, a1df]),
     ('RadialGrid_get_size', c_int, [c_void_p]),
     ('RadialGrid_get_radii', c_double, [c_void_p]),
     ('RadialGrid_get_points', PD, [c_void_p]),
@@ -201,6 +202,13 @@ _SIGS = [
      [c_long, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ('napmo_gpu_epc17_2', c_int,
      [c_long, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ('napmo_gpu_kinetic', c_int,
+     [c_void_p, c_int, c_int, c_void_p, c_long, c_double, c_void_p, c_void_p]),
+    ('napmo_gpu_dpsi', c_int,
+     [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_long, a1df, a1df, c_double,
+      c_void_p, c_void_p]),
+    ('napmo_gpu_operator_matrix', c_int,
+     [c_void_p, c_int, c_int, c_void_p, c_long, c_void_p, c_long, c_void_p, c_void_p]),
     ('napmo_gpu_nuclear_potential', c_int,
      [c_int, c_void_p, c_void_p, c_void_p, c_int, a2df, c_void_p, c_void_p]),
     ('napmo_fock_plan_new', c_void_p, [c_void_p, c_void_p, c_int, c_void_p]),

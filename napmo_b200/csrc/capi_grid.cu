@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <stdexcept>
 #include <algorithm>
 #include <vector>
@@ -349,6 +350,64 @@ int run_poisson(BeckeGrid *g, PoissonPlan *p, const double *rho_dev, double *v_d
                                          v_dev, accumulate, s),
                  "evaluate");
   return kOk;
+}
+
+// The grid's Poisson tables for `lmax`, set up for an operator evaluation:
+// every point, no truncation, no raw spline output.
+static int operator_dev(BeckeGrid *g, int lmax, cudaStream_t s, PoissonDev *out) {
+  PoissonPlan *p = nullptr;
+  int st = grid_poisson_plan(g, lmax, s, &p);
+  if (st) return st;
+  st = select_pair_lists(p, g, nullptr, 0, s);
+  if (st) return st;
+  *out = p->d;
+  out->eval_tol = 0.0;
+  out->lcut = nullptr;
+  out->raw_y = nullptr;
+  out->raw_dt = nullptr;
+  return kOk;
+}
+
+// src = phi doi - resid (ndpsi.py:29)
+__global__ void dpsi_source_kernel(int n, const double *__restrict__ phi,
+                                   const double *__restrict__ resid, double doi,
+                                   double *__restrict__ src) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) src[p] = phi[p] * doi - resid[p];
+}
+
+static cudaError_t launch_dpsi_source(int n, const double *phi, const double *resid, double doi,
+                                      double *src, cudaStream_t s) {
+  dpsi_source_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, phi, resid, doi, src);
+  return cudaGetLastError();
+}
+
+// One CTA per (i, j): a fixed strided partition of the points and a fixed
+// reduction tree, so every entry is reproducible.
+__global__ void __launch_bounds__(256)
+operator_matrix_kernel(int npoint, const double *__restrict__ A, long lda,
+                       const double *__restrict__ B, long ldb, const double *__restrict__ wb,
+                       const double *__restrict__ w, double *__restrict__ M, int m) {
+  const int i = blockIdx.y, j = blockIdx.x;
+  const double *a = A + (long)i * lda, *b = B + (long)j * ldb;
+  double acc = 0.0;
+  for (int p = threadIdx.x; p < npoint; p += 256) acc += a[p] * b[p] * wb[p] * w[p];
+  __shared__ double red[256];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) M[(long)i * m + j] = red[0];
+}
+
+static cudaError_t launch_operator_matrix(int npoint, int n, int m, const double *A, long lda,
+                                          const double *B, long ldb, const double *wb,
+                                          const double *w, double *M, cudaStream_t s) {
+  if (n > 65535) return cudaErrorInvalidValue;
+  operator_matrix_kernel<<<dim3(m, n), 256, 0, s>>>(npoint, A, lda, B, ldb, wb, w, M, m);
+  return cudaGetLastError();
 }
 
 BeckeGrid::~BeckeGrid() {
@@ -747,11 +806,15 @@ void RadialGrid_del(RadialGrid *g) { delete g; }
 double RadialGrid_integrate(RadialGrid *g, int segments, double *f) {
   return g->integrate(segments, f);
 }
-double *RadialGrid_deriv2(RadialGrid *, double *) {
-  set_error(kNotSupported,
-            "RadialGrid.deriv2 belongs to the numerical-orbital kinetic operator, "
-            "which is outside the grid-quadrature path");
-  return nullptr;
+// (1/r) d^2/dr^2 (r f) at the grid's points (radial.cpp:51-192); returns a
+// new[] array of size() values released by napmo_free_array.
+double *RadialGrid_deriv2(RadialGrid *g, double *f) {
+  return make_or_null<double>([&] {
+    const int n = (int)g->points.size();
+    std::unique_ptr<double[]> out(new double[n]);
+    radial_deriv2(g->points.data(), n, g->radii, f, out.get());
+    return out.release();
+  });
 }
 int RadialGrid_get_size(RadialGrid *g) { return (int)g->points.size(); }
 double RadialGrid_get_radii(RadialGrid *g) { return g->radii; }
@@ -1212,6 +1275,112 @@ int napmo_gpu_poisson(BeckeGrid *g, const double *rho_dev, int lmax, double *v_d
       NAPMO_TRY_CUDA(cudaMemcpyAsync(raw_dt, p->raw_dt.p, p->raw_dt.n * sizeof(double),
                                      cudaMemcpyDeviceToDevice, s),
                      "poisson raw");
+    return kOk;
+  });
+}
+
+// ------------------------------------------- numerical-orbital operators
+// Kinetic operator of nAPMO's numerical orbitals (compute_kinetic,
+// napmo/wavefunction/nkinetic.py:15-73): out[k] = scale * (-1/2 laplacian
+// psi[k]) at the grid's points for nfunc functions (device, rows of ld >=
+// size doubles), through the Lebedev projection of psi wb, the radial
+// operator (1/r d2/dr2 r - l(l+1)/r^2) by finite differences
+// (src/grid/radial.cpp:51-192) and the multipole evaluation.  Every atom must
+// use the Chebyshev radial transform (nAPMO's default) with >= 8 points.
+int napmo_gpu_kinetic(BeckeGrid *g, int lmax, int nfunc, const double *psi, long ld,
+                      double scale, double *out, void *stream) {
+  return guarded([&] {
+    NAPMO_REQUIRE(nfunc >= 0 && ld >= g->size, "nfunc < 0 or ld < grid size");
+    if (nfunc == 0) return kOk;
+    for (auto &L : g->layout)
+      if (L.rt.kind != kRTChebyshev || L.nrad < 8)
+        return set_error(kNotSupported,
+                         "the kinetic operator needs Chebyshev radial grids of >= 8 points");
+    cudaStream_t s = (cudaStream_t)stream;
+    PoissonDev P;
+    int st = operator_dev(g, lmax, s, &P);
+    if (st) return st;
+    for (int k = 0; k < nfunc; ++k) {
+      NAPMO_TRY_CUDA(launch_poisson_project(P, psi + (long)k * ld, g->dev.wb, g->dev.w, s),
+                     "project");
+      NAPMO_TRY_CUDA(launch_kinetic_radial(P, -0.5 * scale, s), "kinetic radial");
+      NAPMO_TRY_CUDA(launch_poisson_evaluate(P, g->size, g->dev.x, g->dev.y, g->dev.z,
+                                             out + (long)k * ld, false, s),
+                     "evaluate");
+    }
+    return kOk;
+  });
+}
+
+// Becke-Dickson orbital corrections (compute_dpsi,
+// napmo/wavefunction/ndpsi.py:15-89) of nfunc orbitals: for orbital k the
+// source (phi doi - R) wb is projected per atom, every (l, m) solves
+//   u'' + 2/r u' - 2/m_inv (l(l+1)/r^2 + <V_k wb>(r) - oi - doi) u
+//       = -2/m_inv src_lm,   u = 0 at both ends,
+// (<.> the spherical average over each radial shell) and out[k] is the sum
+// of the solutions over atoms at every point.  phi, resid, vtot, out: device
+// rows of ld doubles; doi, oi: host arrays of nfunc.
+int napmo_gpu_dpsi(BeckeGrid *g, int lmax, int nfunc, const double *phi, const double *resid,
+                   const double *vtot, long ld, const double *doi, const double *oi,
+                   double mass_inv, double *out, void *stream) {
+  return guarded([&] {
+    NAPMO_REQUIRE(nfunc >= 0 && ld >= g->size, "nfunc < 0 or ld < grid size");
+    NAPMO_REQUIRE(mass_inv != 0.0, "mass_inv must be nonzero");
+    if (nfunc == 0) return kOk;
+    cudaStream_t s = (cudaStream_t)stream;
+    PoissonDev P;
+    int st = operator_dev(g, lmax, s, &P);
+    if (st) return st;
+    long nshell = 0;
+    for (auto &L : g->layout) nshell += L.nrad;
+    const size_t rows = (size_t)P.nsys * P.lu_stride;
+    void *ws = nullptr;
+    const size_t bytes = (g->size + nshell + rows * (kW + kKL)) * sizeof(double) +
+                         rows * sizeof(int);
+    NAPMO_TRY_CUDA(cudaMallocAsync(&ws, bytes, s), "Becke-Dickson workspace");
+    double *src = (double *)ws;
+    double *vsph = src + g->size;
+    P.lu = vsph + nshell;
+    P.lmul = P.lu + rows * kW;
+    P.lpiv = (int *)(P.lmul + rows * kKL);
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < nfunc && e == cudaSuccess; ++k) {
+      RadialOp op;
+      op.fscale = -2.0 / mass_inv;
+      op.ascale = -2.0 / mass_inv;
+      op.vsph = vsph;
+      op.e = oi[k];
+      op.de = doi[k];
+      op.zero_bc = true;
+      e = launch_dpsi_source(g->size, phi + (long)k * ld, resid + (long)k * ld, doi[k], src, s);
+      if (e == cudaSuccess) e = launch_poisson_project(P, src, g->dev.wb, g->dev.w, s);
+      if (e == cudaSuccess)
+        e = launch_shell_average(P, vtot + (long)k * ld, g->dev.wb, g->dev.w, vsph, s);
+      if (e == cudaSuccess) e = launch_radial_factor(P, op, s);
+      if (e == cudaSuccess) e = launch_radial_solve(P, op, s);
+      if (e == cudaSuccess)
+        e = launch_poisson_evaluate(P, g->size, g->dev.x, g->dev.y, g->dev.z,
+                                    out + (long)k * ld, false, s);
+    }
+    cudaFreeAsync(ws, s);
+    NAPMO_TRY_CUDA(e, "Becke-Dickson correction");
+    return kOk;
+  });
+}
+
+// M[i][j] = sum_p A[i][p] B[j][p] wb[p] w[p] for i < n, j < m: nAPMO's
+// get_operator_matrix (napmo/wavefunction/psi_numeric.py:406-424, each entry
+// a BeckeGrid::integrate of psi_i O psi_j).  A, B device rows (lda, ldb), M
+// device [n][m].
+int napmo_gpu_operator_matrix(BeckeGrid *g, int n, int m, const double *A, long lda,
+                              const double *B, long ldb, double *M, void *stream) {
+  return guarded([&] {
+    NAPMO_REQUIRE(n >= 0 && m >= 0 && lda >= g->size && ldb >= g->size,
+                  "negative size or leading dimension < grid size");
+    if (n == 0 || m == 0) return kOk;
+    NAPMO_TRY_CUDA(launch_operator_matrix(g->size, n, m, A, lda, B, ldb, g->dev.wb, g->dev.w,
+                                          M, (cudaStream_t)stream),
+                   "operator matrix");
     return kOk;
   });
 }

@@ -3,6 +3,7 @@
 #include "host.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <stdexcept>
@@ -540,6 +541,104 @@ void cubic_spline_dt(const double *y, double *dt, int n) {
   mid[n - 1] = 2.0;
   rhs[n - 1] = 3.0 * (y[n - 1] - y[n - 2]);
   tridiag_sym_solve(mid.data(), up.data(), rhs.data(), dt, n);
+}
+
+// ------------------------------------------------ radial second derivative
+// Fornberg's recursion: c[j * (m + 1) + k] = weight of node x[j] in the k-th
+// derivative at z (k <= m), nodes x[0..np-1].
+static void fornberg_weights(double z, const double *x, int np, int m, double *c) {
+  for (int e = 0; e < np * (m + 1); ++e) c[e] = 0.0;
+  double c1 = 1.0, c4 = x[0] - z;
+  c[0] = 1.0;
+  for (int i = 1; i < np; ++i) {
+    const int mn = i < m ? i : m;
+    double c2 = 1.0;
+    const double c5 = c4;
+    c4 = x[i] - z;
+    for (int j = 0; j < i; ++j) {
+      const double c3 = x[i] - x[j];
+      c2 *= c3;
+      if (j == i - 1) {
+        for (int k = mn; k >= 1; --k)
+          c[i * (m + 1) + k] =
+              c1 * (k * c[(i - 1) * (m + 1) + k - 1] - c5 * c[(i - 1) * (m + 1) + k]) / c2;
+        c[i * (m + 1)] = -c1 * c5 * c[(i - 1) * (m + 1)] / c2;
+      }
+      for (int k = mn; k >= 1; --k)
+        c[j * (m + 1) + k] = (c4 * c[j * (m + 1) + k] - k * c[j * (m + 1) + k - 1]) / c3;
+      c[j * (m + 1)] = c4 * c[j * (m + 1)] / c3;
+    }
+    c1 = c2;
+  }
+}
+
+const Deriv2Stencils &deriv2_stencils() {
+  static const Deriv2Stencils st = [] {
+    // common denominators of the weights: 7-point stencils are multiples of
+    // 1/720 (first derivative) and 1/360 (second), 9-point ones of 1/40320
+    // and 1/20160; scaled weights are exact integers
+    Deriv2Stencils s;
+    s.den_edge1 = 720.0;
+    s.den_edge2 = 360.0;
+    s.den_mid1 = 40320.0;
+    s.den_mid2 = 20160.0;
+    double x[9], c[9 * 3];
+    for (int k = 0; k < 9; ++k) x[k] = k;
+    for (int j = 0; j < 4; ++j) {
+      fornberg_weights((double)j, x, 7, 2, c);
+      for (int k = 0; k < 7; ++k) {
+        s.edge1[j][k] = std::nearbyint(c[k * 3 + 1] * s.den_edge1);
+        s.edge2[j][k] = std::nearbyint(c[k * 3 + 2] * s.den_edge2);
+      }
+    }
+    fornberg_weights(4.0, x, 9, 2, c);
+    for (int k = 0; k < 9; ++k) {
+      s.mid1[k] = std::nearbyint(c[k * 3 + 1] * s.den_mid1);
+      s.mid2[k] = std::nearbyint(c[k * 3 + 2] * s.den_mid2);
+    }
+    return s;
+  }();
+  return st;
+}
+
+void radial_deriv2(const double *r, int n, double radii, const double *f, double *out) {
+  if (n < 8) throw std::invalid_argument("radial second derivative needs >= 8 points");
+  const Deriv2Stencils &st = deriv2_stencils();
+  const double H = M_PI / (n + 1.0);
+  // g_k = f(w_k) = f[n - 1 - k]
+  auto g = [&](int k) { return f[n - 1 - k]; };
+  for (int i = 0; i < n; ++i) {
+    double d1 = 0.0, d2 = 0.0;
+    if (i < 4) {
+      for (int k = 0; k < 7; ++k) {
+        d1 += st.edge1[i][k] * g(k);
+        d2 += st.edge2[i][k] * g(k);
+      }
+      d1 /= st.den_edge1 * H;
+      d2 /= st.den_edge2 * H * H;
+    } else if (i >= n - 4) {
+      const int j = n - 1 - i;  // mirror of node j: first-derivative weights change sign
+      for (int k = 6; k >= 0; --k) {
+        d1 -= st.edge1[j][k] * g(n - 1 - k);
+        d2 += st.edge2[j][k] * g(n - 1 - k);
+      }
+      d1 /= st.den_edge1 * H;
+      d2 /= st.den_edge2 * H * H;
+    } else {
+      for (int k = 0; k < 9; ++k) {
+        d1 += st.mid1[k] * g(i - 4 + k);
+        d2 += st.mid2[k] * g(i - 4 + k);
+      }
+      d1 /= st.den_mid1 * H;
+      d2 /= st.den_mid2 * H * H;
+    }
+    // dw/dr and d2w/dr2 of r(w) = radii (1 + cos w) / (1 - cos w)
+    const double w = (i + 1) * H, X = cos(w), Y = sin(w), q = 1.0 - X;
+    const double wr = -q * q / (2.0 * radii * Y);
+    const double wrr = q * q * q * (2.0 * Y * Y - q * X) / (4.0 * radii * radii * Y * Y * Y);
+    const int idx = n - 1 - i;
+    out[idx] = wr * wr * d2 + (wrr + 2.0 * wr / r[idx]) * d1;
+  }
 }
 
 // ----------------------------------------------------- Hermite FEM integrals

@@ -317,6 +317,24 @@ void build_ode2_matrix(const double *b, const double *a, const double *f,
                        const double *bcs, double *coeffs, double *rhs,
                        long npoint);
 
+// Finite-difference stencils of the radial second derivative
+// (RadialGrid::deriv2, src/grid/radial.cpp:51-192): first and second
+// derivatives on a uniform axis, 7-point one-sided for the four points nearest
+// either end and 9-point centred inside.  Weights from Fornberg's recursion
+// (B. Fornberg, Math. Comp. 51, 699 (1988)), held as integers over a common
+// denominator (exact); the far end uses the mirror image.
+struct Deriv2Stencils {
+  double edge1[4][7], edge2[4][7];  // derivative at node j (0..3) from nodes 0..6
+  double mid1[9], mid2[9];          // derivative at node 4 from nodes 0..8
+  double den_edge1, den_edge2, den_mid1, den_mid2;
+};
+const Deriv2Stencils &deriv2_stencils();
+
+// (1/r) d^2/dr^2 (r f) = f'' + (2/r) f' on a Becke-Chebyshev radial grid
+// r = radii (1 + cos w) / (1 - cos w), w_k = (k + 1) pi / (n + 1), f sampled at
+// the n points r (ascending; r[n-1-k] belongs to w_k).  n >= 8.
+void radial_deriv2(const double *r, int n, double radii, const double *f, double *out);
+
 // Real solid harmonics of a 3-vector given as (z, x, y) in out[0..2]; fills
 // out[3..] for l = 2..lmax (horton ordering: m = 0, then cos/sin pairs).
 void pure_polynomials(double *out, long lmax);

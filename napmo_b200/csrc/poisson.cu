@@ -41,6 +41,12 @@ __constant__ double c_shnorm[(kMaxLmax + 1) * (kMaxLmax + 1)];  // [l][m]
 __constant__ double c_rec_a[(kMaxLmax + 1) * (kMaxLmax + 1)];      // A_lm at [l][m]
 __constant__ double c_rec_gamma[(kMaxLmax + 1) * (kMaxLmax + 1)];  // gamma at [lm]
 __constant__ double c_rec_start[kMaxLmax + 1];
+// Finite-difference weights of the radial second derivative (integers over
+// common denominators, host deriv2_stencils()): [0, 28) first derivative at
+// the four edge nodes (7 weights each), [28, 56) second derivative, [56, 65)
+// and [65, 74) the centred 9-point first and second derivative, [74, 78) the
+// denominators (edge first, edge second, centred first, centred second).
+__constant__ double c_fd[78];
 
 constexpr double kPI4 = 4.0 * M_PI;
 constexpr double kInvSqrt4Pi = 0.28209479177387814347;
@@ -185,14 +191,36 @@ __device__ __forceinline__ double &AB(double *band, int i, int j) {
 // only: it is assembled and LU-factored (partial pivoting, kl = ku = 3) once
 // per grid.  Outputs per system: the band with U (rows i, columns i..i+6), the
 // multipliers of step k in mult[k * kKL + i], the pivot row of step k.
-__global__ void radial_factor_kernel(PoissonDev P) {
+// Thomas sweep of the (2 1 / 1 4 1 / ... / 1 2) cubic-spline system with the
+// atom's precomputed denominators: t-derivatives dt of the spline through y
+// (strides ys, ds), the same operations as the Poisson radial kernel's.
+__device__ void spline_dt_col(const double *y, int ys, double *dt, int ds,
+                              const double *den, const double *upm, int n) {
+  double prev = (3.0 * (y[ys] - y[0])) / den[0];
+  dt[0] = prev;
+  for (int i = 1; i < n; ++i) {
+    const double rhs = (i < n - 1) ? 3.0 * (y[(i + 1) * ys] - y[(i - 1) * ys])
+                                   : 3.0 * (y[(n - 1) * ys] - y[(n - 2) * ys]);
+    prev = (rhs - prev * 1.0) / den[i];
+    dt[i * ds] = prev;
+  }
+  for (int i = n - 2; i >= 0; --i) dt[i * ds] = dt[i * ds] - upm[i] * dt[(i + 1) * ds];
+}
+
+// CTA = one radial system (atom, l): assembles the Hermite FEM band matrix of
+// u'' + b u' + a u and factors it.  Poisson: a = -l(l+1)/r^2 (analytic
+// derivative); Becke-Dickson (op.vsph set): a tabulated on the radial points
+// with its spline derivative (ndpsi.py:58-69).
+__global__ void radial_factor_kernel(PoissonDev P, RadialOp op) {
   extern __shared__ double sm[];
   const int sys = blockIdx.x;
   const PoissonAtom at = P.atoms[P.sys_atom[sys]];
   const int l = P.sys_l[sys];
   const int n = at.nrad, n2 = 2 * n;
   const int tid = threadIdx.x, nt = blockDim.x;
-  double *band = sm;  // n2 * kW
+  double *band = sm;          // n2 * kW
+  double *ay = band + n2 * kW;  // Becke-Dickson a(r_i) and its spline t-derivative
+  double *adt = ay + n;
   __shared__ double s_mult[kKL];
   __shared__ int s_piv;
   const double *rad = P.rad + at.rad_off;
@@ -204,8 +232,16 @@ __global__ void radial_factor_kernel(PoissonDev P) {
   int *piv = P.lpiv + (long)sys * P.lu_stride;
   // -- 2. band matrix (depends on l only)
   for (int e = tid; e < n2 * kW; e += nt) band[e] = 0.0;
-  __syncthreads();
   const double l2l = (double)(l * (l + 1));
+  const bool bd = op.vsph != nullptr;
+  if (bd) {
+    const double *vs = op.vsph + at.rad_off / kRadSlots;
+    for (int i = tid; i < n; i += nt)
+      ay[i] = op.ascale * (l2l * (1.0 / (r[i] * r[i])) + ((vs[i] - op.e) - op.de));
+    __syncthreads();
+    if (tid == 0) spline_dt_col(ay, 1, adt, 1, rad + kRadDen * n, rad + kRadUp * n, n);
+  }
+  __syncthreads();
   for (int row = tid; row < n2; row += nt) {
     if (row == 0 || row == n2 - 2) {
       AB(band, row, row) = 1.0;
@@ -222,7 +258,19 @@ __global__ void radial_factor_kernel(PoissonDev P) {
         const double ri = r[i], r2 = ri * ri;
         const double jsq = j1[i] * j1[i];
         double bk, ak;
-        if ((k & 1) == 0) {
+        if (bd) {
+          // b = (2 r^-1, -2 r^-2) as ndpsi.py:55 forms it
+          const double rinv = 1.0 / ri, r2inv = 1.0 / r2;
+          if ((k & 1) == 0) {
+            bk = j1[i] * (2.0 * rinv) - j2[i] / j1[i];
+            ak = ay[i] * jsq;
+          } else {
+            bk = j2[i] * (2.0 * rinv) + jsq * (-2.0 * r2inv) +
+                 (j2[i] * j2[i] - j1[i] * j3[i]) / jsq;
+            const double adx = adt[i] / j1[i];
+            ak = (adx * jsq + 2 * ay[i] * j2[i]) * j1[i];
+          }
+        } else if ((k & 1) == 0) {
           bk = j1[i] * (2 / ri) - j2[i] / j1[i];
           ak = (-l2l / r2) * jsq;
         } else {
@@ -284,7 +332,15 @@ __global__ void radial_factor_kernel(PoissonDev P) {
 // CTA = (system (atom, l), chunk of ncol of its 2l + 1 columns m); the columns
 // are independent once the atom's radial tables are staged.  Column loops run
 // one thread per column; row loops stride over the whole block.
-__global__ void radial_kernel(PoissonDev P, int ncol) {
+// Doubles of the region after R in the radial kernel's shared memory: the
+// spline derivatives and projected columns (n ncol each), later the system's
+// LU factors (band, multipliers, pivots as ints).
+__host__ __device__ __forceinline__ int radial_region_doubles(int n, int ncol) {
+  const int cols = 2 * n * ncol, lu = 2 * n * (kW + kKL) + n;
+  return cols > lu ? cols : lu;
+}
+
+__global__ void radial_kernel(PoissonDev P, int ncol, RadialOp op) {
   extern __shared__ double sm[];
   const int sys = blockIdx.x;
   const PoissonAtom at = P.atoms[P.sys_atom[sys]];
@@ -298,7 +354,7 @@ __global__ void radial_kernel(PoissonDev P, int ncol) {
   double *R = sm;                    // n2 * ncol  (row-major, column = m)
   double *buf = R + n2 * ncol;       // n * ncol   (spline t-derivatives)
   double *Y = buf + n * ncol;        // n * ncol   (projected density of this l)
-  double *r = Y + n * ncol;          // radial tables of the atom, n each
+  double *r = buf + radial_region_doubles(n, ncol);  // radial tables of the atom, n each
   double *wr = r + n, *j1 = wr + n, *j2 = j1 + n, *den = j2 + n, *upm = den + n;
   double *rl = upm + n, *rm = rl + n;  // r^l, r^-(l+1)
   double *bc = rm + n;                 // [2][ncol]: vmin, vmax per column
@@ -342,6 +398,11 @@ __global__ void radial_kernel(PoissonDev P, int ncol) {
     for (int i = n - 2; i >= 0; --i)
       buf[i * ncol + c] = buf[i * ncol + c] - upm[i] * buf[(i + 1) * ncol + c];
     // boundary values (Dirichlet) from radial moments
+    if (op.zero_bc) {
+      bc[ncol + c] = 0.0;
+      bc[c] = 0.0;
+      continue;
+    }
     double smax = 0.0, smin = 0.0;
     for (int i = 0; i < n; ++i) {
       const double yi = y[i * ncol];
@@ -373,13 +434,13 @@ __global__ void radial_kernel(PoissonDev P, int ncol) {
           const long k = lo + t;
           if (k >= hi) break;
           const int i = (int)(k / 2);
-          const double fy = -kPI4 * Y[i * ncol + c];
+          const double fy = op.fscale * Y[i * ncol + c];
           const double jsq = j1[i] * j1[i];
           double fk;
           if ((k & 1) == 0) {
             fk = fy * jsq;
           } else {
-            const double fdx = -kPI4 * (buf[i * ncol + c] / j1[i]);
+            const double fdx = op.fscale * (buf[i * ncol + c] / j1[i]);
             fk = (fdx * jsq + 2 * fy * j2[i]) * j1[i];
           }
           if (fk != 0) acc += fk * ov[t];
@@ -425,11 +486,13 @@ __global__ void radial_kernel(PoissonDev P, int ncol) {
   __syncthreads();
   // -- 4. output: raw splines, scaled cubic coefficients, extrapolation
   const double fl = sqrt((double)(2 * l + 1)) * kInvSqrt4Pi;
-  for (int e = tid; e < n * nm; e += nt) {
-    const int c = e / n, i = e - c * n;
-    const long o = at.raw_off + (long)(l * l + c0 + c) * n + i;
-    P.raw_y[o] = R[(2 * i) * ncol + c];
-    P.raw_dt[o] = (R[(2 * i + 1) * ncol + c] / j1[i]) * j1[i];
+  if (P.raw_y) {
+    for (int e = tid; e < n * nm; e += nt) {
+      const int c = e / n, i = e - c * n;
+      const long o = at.raw_off + (long)(l * l + c0 + c) * n + i;
+      P.raw_y[o] = R[(2 * i) * ncol + c];
+      P.raw_dt[o] = (R[(2 * i + 1) * ncol + c] / j1[i]) * j1[i];
+    }
   }
   for (int e = tid; e < (n - 1) * nm; e += nt) {
     const int j = e / nm, c = e - j * nm;
@@ -448,6 +511,118 @@ __global__ void radial_kernel(PoissonDev P, int ncol) {
     P.amp[at.amp_off + lm * 2 + 0] = R[c] / pow(at.first_x, (double)l) * fl;
     P.amp[at.amp_off + lm * 2 + 1] = R[(2 * (n - 1)) * ncol + c] * pow(at.last_x, (double)(l + 1)) * fl;
   }
+}
+
+// ------------------------------------------------------------------ kinetic
+// CTA = (system (atom, l), chunk of ncol columns m).  Per column: the radial
+// operator (1/r d2/dr2 r - l(l+1)/r^2) f_lm by finite differences in the
+// Chebyshev angle w (r = radii (1 + cos w)/(1 - cos w), w_i = (i + 1) pi /
+// (n + 1) belongs to radial point n - 1 - i), then the cubic spline of the
+// result with the potential extrapolation (nkinetic.py:48-61,
+// src/grid/radial.cpp:51-192), scaled by `scale` into the evaluation tables.
+__global__ void kinetic_radial_kernel(PoissonDev P, int ncol, double scale) {
+  extern __shared__ double sm[];
+  const int sys = blockIdx.x;
+  const PoissonAtom at = P.atoms[P.sys_atom[sys]];
+  const int l = P.sys_l[sys];
+  const int n = at.nrad;
+  const int lsize = (at.lmax + 1) * (at.lmax + 1);
+  const int c0 = blockIdx.y * ncol;
+  if (c0 >= 2 * l + 1) return;
+  const int nm = min(ncol, 2 * l + 1 - c0);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  double *Y = sm;            // n * ncol: projected function, then spline t-derivatives
+  double *V = Y + n * ncol;  // n * ncol: operator values
+  double *r = V + n * ncol, *den = r + n, *upm = den + n;
+  {
+    const double *rad = P.rad + at.rad_off;
+    for (int i = tid; i < n; i += nt) {
+      r[i] = rad[kRadR * n + i];
+      den[i] = rad[kRadDen * n + i];
+      upm[i] = rad[kRadUp * n + i];
+    }
+    const double *proj = P.proj + at.proj_off + l * l + c0;
+    for (int e = tid; e < n * nm; e += nt) {
+      const int i = e / nm, c = e - i * nm;
+      Y[i * ncol + c] = proj[(long)i * lsize + c];
+    }
+  }
+  __syncthreads();
+  const double radii = at.rt.p0, H = M_PI / (n + 1.0), l2l = (double)(l * (l + 1));
+  for (int e = tid; e < n * nm; e += nt) {
+    const int idx = e / nm, c = e - idx * nm;
+    const int i = n - 1 - idx;
+    const double *g = Y + c;  // g(k) = f(w_k) = g[(n - 1 - k) * ncol]
+    double d1 = 0.0, d2 = 0.0;
+    if (i < 4) {
+      for (int k = 0; k < 7; ++k) {
+        const double gk = g[(n - 1 - k) * ncol];
+        d1 += c_fd[i * 7 + k] * gk;
+        d2 += c_fd[28 + i * 7 + k] * gk;
+      }
+      d1 /= c_fd[74] * H;
+      d2 /= c_fd[75] * H * H;
+    } else if (i >= n - 4) {
+      const int j = n - 1 - i;  // mirror of edge node j: first-derivative weights change sign
+      for (int k = 6; k >= 0; --k) {
+        const double gk = g[k * ncol];  // f(w_(n-1-k))
+        d1 -= c_fd[j * 7 + k] * gk;
+        d2 += c_fd[28 + j * 7 + k] * gk;
+      }
+      d1 /= c_fd[74] * H;
+      d2 /= c_fd[75] * H * H;
+    } else {
+      for (int k = 0; k < 9; ++k) {
+        const double gk = g[(n - 1 - (i - 4 + k)) * ncol];
+        d1 += c_fd[56 + k] * gk;
+        d2 += c_fd[65 + k] * gk;
+      }
+      d1 /= c_fd[76] * H;
+      d2 /= c_fd[77] * H * H;
+    }
+    // dw/dr and d2w/dr2 of the Chebyshev map
+    const double w = (i + 1) * H, X = cos(w), Yw = sin(w), q = 1.0 - X;
+    const double wr = -q * q / (2.0 * radii * Yw);
+    const double wrr = q * q * q * (2.0 * Yw * Yw - q * X) / (4.0 * radii * radii * Yw * Yw * Yw);
+    const double ri = r[idx];
+    const double lap = wr * wr * d2 + (wrr + 2.0 * wr / ri) * d1;
+    V[idx * ncol + c] = lap - l2l * (1.0 / (ri * ri)) * Y[idx * ncol + c];
+  }
+  __syncthreads();
+  for (int c = tid; c < nm; c += nt) spline_dt_col(V + c, ncol, Y + c, ncol, den, upm, n);
+  __syncthreads();
+  const double fl = sqrt((double)(2 * l + 1)) * kInvSqrt4Pi * scale;
+  for (int e = tid; e < (n - 1) * nm; e += nt) {
+    const int j = e / nm, c = e - j * nm;
+    const double y0 = V[j * ncol + c], y1 = V[(j + 1) * ncol + c];
+    const double d0 = Y[j * ncol + c], d1 = Y[(j + 1) * ncol + c];
+    const double z = y1 - y0;
+    double *cf = P.spl + at.spl_off + ((long)j * lsize + l * l + c0 + c) * 4;
+    cf[0] = y0 * fl;
+    cf[1] = d0 * fl;
+    cf[2] = (3 * z - 2 * d0 - d1) * fl;
+    cf[3] = (-2 * z + d0 + d1) * fl;
+  }
+  for (int c = tid; c < nm; c += nt) {
+    const int lm = l * l + c0 + c;
+    P.amp[at.amp_off + lm * 2 + 0] = V[c] / pow(at.first_x, (double)l) * fl;
+    P.amp[at.amp_off + lm * 2 + 1] = V[(n - 1) * ncol + c] * pow(at.last_x, (double)(l + 1)) * fl;
+  }
+}
+
+// One warp per (radial shell, atom): sum_j f wb w / sum_j w over the shell.
+__global__ void __launch_bounds__(32)
+shell_average_kernel(PoissonDev P, const double *__restrict__ f, const double *__restrict__ wb,
+                     const double *__restrict__ w, double *__restrict__ out) {
+  const PoissonAtom at = P.atoms[blockIdx.y];
+  const int sh = blockIdx.x;
+  if (sh >= at.nrad) return;
+  const long base = at.point_off + (long)sh * at.nang;
+  double acc = 0.0;
+  for (int j = threadIdx.x; j < at.nang; j += 32) acc += f[base + j] * wb[base + j] * w[base + j];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (threadIdx.x == 0)
+    out[at.rad_off / kRadSlots + sh] = acc / P.rad[at.rad_off + kRadSigma * at.nrad + sh];
 }
 
 // ----------------------------------------------------------------- evaluate
@@ -921,6 +1096,24 @@ cudaError_t poisson_init_constants() {
     if ((e = cudaMemcpyToSymbol(c_rec_gamma, gam_lm.data(), gam_lm.size() * sizeof(double))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(c_rec_start, st.data(), st.size() * sizeof(double))) != cudaSuccess) return e;
   }
+  {
+    const Deriv2Stencils &st = deriv2_stencils();
+    double fd[78];
+    for (int j = 0; j < 4; ++j)
+      for (int k = 0; k < 7; ++k) {
+        fd[j * 7 + k] = st.edge1[j][k];
+        fd[28 + j * 7 + k] = st.edge2[j][k];
+      }
+    for (int k = 0; k < 9; ++k) {
+      fd[56 + k] = st.mid1[k];
+      fd[65 + k] = st.mid2[k];
+    }
+    fd[74] = st.den_edge1;
+    fd[75] = st.den_edge2;
+    fd[76] = st.den_mid1;
+    fd[77] = st.den_mid2;
+    if ((e = cudaMemcpyToSymbol(c_fd, fd, sizeof(fd))) != cudaSuccess) return e;
+  }
   done_dev = dev;
   return cudaSuccess;
 }
@@ -936,38 +1129,48 @@ cudaError_t launch_poisson_project(const PoissonDev &P, const double *rho,
   return cudaGetLastError();
 }
 
-// Columns (m) per radial CTA: one warp; systems with 2l + 1 > 32 use several CTAs.
-int poisson_radial_ncol(int max_lmax) {
-  (void)max_lmax;
-  return 32;
+constexpr size_t kMaxSmem = 227 * 1024;
+
+size_t poisson_radial_smem(int max_nrad, int ncol) {
+  const size_t n = (size_t)max_nrad;
+  return (2 * n * ncol + (size_t)radial_region_doubles(max_nrad, ncol) + 8 * n + 2 * (size_t)ncol) *
+         sizeof(double);
 }
 
-size_t poisson_radial_smem(int max_nrad, int max_lmax) {
-  const int ncol = poisson_radial_ncol(max_lmax);
-  const size_t n = (size_t)max_nrad;
-  return (2 * n * ncol + 2 * n * ncol + 8 * n + 2 * (size_t)ncol) * sizeof(double);
+// Columns (m) per radial CTA: 32, halved while the CTA's shared memory would
+// exceed the limit (long radial grids); systems with 2l + 1 > ncol use several
+// CTAs.  0 when even one column does not fit.
+int poisson_radial_ncol(int max_nrad) {
+  for (int ncol = 32; ncol >= 1; ncol /= 2)
+    if (poisson_radial_smem(max_nrad, ncol) <= kMaxSmem) return ncol;
+  return 0;
 }
 
 size_t poisson_factor_doubles(int nsys, int max_nrad) {
   return (size_t)nsys * 2 * max_nrad * (kW + kKL);
 }
 
-cudaError_t launch_poisson_factor(const PoissonDev &P, cudaStream_t s) {
+cudaError_t launch_radial_factor(const PoissonDev &P, const RadialOp &op, cudaStream_t s) {
   if (P.nsys == 0) return cudaSuccess;
-  const size_t smem = (size_t)2 * P.max_nrad * kW * sizeof(double);
-  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  const size_t smem =
+      ((size_t)2 * P.max_nrad * kW + (op.vsph ? 2 * (size_t)P.max_nrad : 0)) * sizeof(double);
+  if (smem > kMaxSmem) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(radial_factor_kernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  radial_factor_kernel<<<P.nsys, 32, smem, s>>>(P);
+  radial_factor_kernel<<<P.nsys, 32, smem, s>>>(P, op);
   return cudaGetLastError();
 }
 
-cudaError_t launch_poisson_radial(const PoissonDev &P, cudaStream_t s) {
+cudaError_t launch_poisson_factor(const PoissonDev &P, cudaStream_t s) {
+  return launch_radial_factor(P, RadialOp(), s);
+}
+
+cudaError_t launch_radial_solve(const PoissonDev &P, const RadialOp &op, cudaStream_t s) {
   if (P.nsys == 0) return cudaSuccess;
-  const int ncol = poisson_radial_ncol(P.max_lmax);
-  const size_t smem = poisson_radial_smem(P.max_nrad, P.max_lmax);
-  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  const int ncol = poisson_radial_ncol(P.max_nrad);
+  if (ncol == 0) return cudaErrorInvalidValue;
+  const size_t smem = poisson_radial_smem(P.max_nrad, ncol);
   cudaError_t e = cudaFuncSetAttribute(radial_kernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
@@ -975,7 +1178,33 @@ cudaError_t launch_poisson_radial(const PoissonDev &P, cudaStream_t s) {
   const int nchunk = (2 * P.max_lmax + 1 + ncol - 1) / ncol;
   // 4 warps: the per-column chains (spline, substitutions) use the first, the
   // row-parallel stages (right-hand side, outputs, staging) all four
-  radial_kernel<<<dim3(P.nsys, nchunk), 4 * ncol, smem, s>>>(P, ncol);
+  radial_kernel<<<dim3(P.nsys, nchunk), 128, smem, s>>>(P, ncol, op);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_poisson_radial(const PoissonDev &P, cudaStream_t s) {
+  return launch_radial_solve(P, RadialOp(), s);
+}
+
+cudaError_t launch_kinetic_radial(const PoissonDev &P, double scale, cudaStream_t s) {
+  if (P.nsys == 0) return cudaSuccess;
+  const size_t n = (size_t)P.max_nrad;
+  int ncol = 32;
+  while (ncol > 1 && (2 * n * ncol + 3 * n) * sizeof(double) > kMaxSmem) ncol /= 2;
+  const size_t smem = (2 * n * ncol + 3 * n) * sizeof(double);
+  if (smem > kMaxSmem) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(kinetic_radial_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int nchunk = (2 * P.max_lmax + 1 + ncol - 1) / ncol;
+  kinetic_radial_kernel<<<dim3(P.nsys, nchunk), 128, smem, s>>>(P, ncol, scale);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_shell_average(const PoissonDev &P, const double *f, const double *wb,
+                                 const double *w, double *out, cudaStream_t s) {
+  if (P.natom == 0) return cudaSuccess;
+  shell_average_kernel<<<dim3(P.max_nrad, P.natom), 32, 0, s>>>(P, f, wb, w, out);
   return cudaGetLastError();
 }
 

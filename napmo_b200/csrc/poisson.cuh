@@ -94,6 +94,19 @@ struct PoissonDev {
   const int *keep = nullptr;
 };
 
+// Radial stage of the pipeline.  The default is the Poisson equation
+// (u'' + 2/r u' - l(l+1)/r^2 u = -4 pi f_lm, Dirichlet values from the radial
+// moments).  With `vsph` set it is the Becke-Dickson orbital correction of
+// napmo/wavefunction/ndpsi.py:15-89: u'' + 2/r u' + a u = fscale f_lm with
+// a = ascale (l(l+1)/r^2 + (vsph - e) - de), u = 0 at both ends.
+struct RadialOp {
+  double fscale = -4.0 * 3.14159265358979323846;  // source factor
+  const double *vsph = nullptr;  // per shell, at atom offset rad_off / kRadSlots
+  double ascale = 0.0;           // -2 / mass_inv
+  double e = 0.0, de = 0.0;      // orbital energy and its correction
+  bool zero_bc = false;          // u = 0 at the first and last radial point
+};
+
 // Uploads the Hermite FEM integral tables and solid-harmonic norms to
 // constant memory (idempotent, per device).
 cudaError_t poisson_init_constants();
@@ -106,6 +119,20 @@ cudaError_t launch_poisson_project(const PoissonDev &P, const double *rho,
 cudaError_t launch_poisson_factor(const PoissonDev &P, cudaStream_t s);
 // projected density -> spline tables of the potential (one CTA per (atom, l)).
 cudaError_t launch_poisson_radial(const PoissonDev &P, cudaStream_t s);
+// The same two stages for another radial operator (factors into P.lu, P.lmul,
+// P.lpiv; raw spline output skipped when P.raw_y is null).
+cudaError_t launch_radial_factor(const PoissonDev &P, const RadialOp &op, cudaStream_t s);
+cudaError_t launch_radial_solve(const PoissonDev &P, const RadialOp &op, cudaStream_t s);
+// Kinetic operator of nAPMO's numerical orbitals (nkinetic.py:15-73):
+// projected function -> spline tables of scale * (1/r d2/dr2 r - l(l+1)/r^2)
+// f_lm (radial second derivative by finite differences in the Chebyshev angle,
+// src/grid/radial.cpp:51-192).  Every atom must use the Chebyshev transform
+// and >= 8 radial points.
+cudaError_t launch_kinetic_radial(const PoissonDev &P, double scale, cudaStream_t s);
+// Per atom and radial shell: sum_j f wb w / sum_j w over the shell's
+// directions (AtomicGrid.spherical_average of f wb); out at rad_off / kRadSlots.
+cudaError_t launch_shell_average(const PoissonDev &P, const double *f, const double *wb,
+                                 const double *w, double *out, cudaStream_t s);
 // Pair-list construction: bucket of every (atom, point) pair and the bucket
 // populations (count[atom.bucket_off + b], atomics on integers), then the
 // bucket-sorted point lists (order inside a bucket is irrelevant: each pair

@@ -173,6 +173,19 @@ class RadialGrid(object):
         f = np.ascontiguousarray(f, dtype=np.float64)
         return _lib().RadialGrid_integrate(self._this, segments, f)
 
+    def deriv2(self, f):
+        """(1/r) d2/dr2 (r f) by finite differences in the Chebyshev angle
+        (radial.py, src/grid/radial.cpp:51-192)."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        if f.shape[0] != self.size:
+            raise NapmoError('f must hold one value per radial point')
+        ptr = _lib().RadialGrid_deriv2(self._this, f)
+        if not ptr:
+            check()
+        out = cext.as_array(ptr, (self.size,)).copy()
+        _lib().napmo_free_array(ptr)
+        return out
+
     size = property(lambda self: _lib().RadialGrid_get_size(self._this))
     symbol = property(lambda self: self._symbol)
     radii = property(lambda self: _lib().RadialGrid_get_radii(self._this))

@@ -170,7 +170,7 @@ class GridRHF(object):
         t = self.torch
         torch = t
         t0 = time.perf_counter()
-        _, C = self._diag(self.H)                          # core guess
+        self.O, C = self._diag(self.H)                     # core guess
         Cocc = C[:, :self.nocc]
         D = 2.0 * Cocc @ Cocc.T
         Fs, errs, history = [], [], []
@@ -207,9 +207,10 @@ class GridRHF(object):
                 rhs[m] = -1.0
                 c = torch.linalg.solve(B, rhs)
                 F = sum(c[a] * Fs[a] for a in range(m))
-            _, C = self._diag(F)
+            e, C = self._diag(F)
             Cocc = C[:, :self.nocc]
             D = 2.0 * Cocc @ Cocc.T
+            self.O = e
         torch.cuda.synchronize()
         self.D, self.C = D, C
         nel = float((D * self.S).sum())

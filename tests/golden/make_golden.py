@@ -8,7 +8,7 @@
   values (H2O/cc-pVDZ, HCN/cc-pVDZ), spline derivatives, FEM assembly and
   the multipole evaluation of a decomposition.
 
-Usage: python tests/golden/make_golden.py [/path/to/nAPMO]
+Usage: python tests/golden/make_golden.py [/path/to/nAPMO] [--answers-only]
 """
 import json
 import os
@@ -60,6 +60,22 @@ def known_answers(ref):
         'radial_He_50_points': {
             'value': vec('napmo/wavefunction/test/test_kinetic.py', 'rdat'),
             'source': 'napmo/wavefunction/test/test_kinetic.py'},
+        'deriv2_He_50_input': {
+            'value': vec('napmo/wavefunction/test/test_kinetic.py', 'test'),
+            'source': 'napmo/wavefunction/test/test_kinetic.py'},
+        'deriv2_He_50': {
+            'value': vec('napmo/wavefunction/test/test_kinetic.py', 'gold'),
+            'source': 'napmo/wavefunction/test/test_kinetic.py'},
+        'becke_He_sto3g_300x110_energy': {
+            'value': grab('napmo/wavefunction/test/test_psi_numeric_becke_He.py',
+                          r'allclose\(E_tot, (-[0-9.]+), rtol=1e-5\)'),
+            'rtol': 1e-5,
+            'source': 'napmo/wavefunction/test/test_psi_numeric_becke_He.py'},
+        'becke_H2_sto3g_100x110_energy': {
+            'value': grab('napmo/wavefunction/test/test_psi_numeric_becke_H2.py',
+                          r'GRID: (-[0-9.]+) \(100x110\)'),
+            'rtol': 1e-2,
+            'source': 'napmo/wavefunction/test/test_psi_numeric_becke_H2.py'},
         'lebedev_110_order': {'value': 17, 'source': 'napmo/grids/test/test_lebedev.py'},
         'multigrid_common_points': {'value': 5500, 'source': 'napmo/grids/test/test_multi_grid.py'},
     }
@@ -159,8 +175,11 @@ def reference_vectors():
 
 
 if __name__ == '__main__':
-    ref = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+    args = [a for a in sys.argv[1:] if not a.startswith('--')]
+    ref = args[0] if args else '/root/reference'
     with open(os.path.join(HERE, 'known_answers.json'), 'w') as f:
         json.dump(known_answers(ref), f, indent=1)
-    np.savez_compressed(os.path.join(HERE, 'reference_vectors.npz'), **reference_vectors())
-    print('wrote known_answers.json and reference_vectors.npz')
+    if '--answers-only' not in sys.argv:
+        np.savez_compressed(os.path.join(HERE, 'reference_vectors.npz'), **reference_vectors())
+    print('wrote known_answers.json' +
+          ('' if '--answers-only' in sys.argv else ' and reference_vectors.npz'))

@@ -1,0 +1,131 @@
+"""Numerical-orbital operators on the device against the oracle, and nAPMO's
+Becke-Dickson known answers.
+
+* napmo_gpu_kinetic (compute_kinetic, nkinetic.py:15-73) against
+  oracle/numeric.py on HCN (40 x 110 per atom): pointwise within 1e-8 of the
+  largest value, <psi|T|psi> within 1e-11.  The finite-difference Laplacian
+  amplifies differences of its input by ~3e3 near the nuclei (1e-15 relative
+  noise on psi moves the oracle's own output by 3e-12 of its maximum), and
+  the device projection (FP64, another summation order) differs from the
+  oracle's at ~1e-13: measured 1e-9 pointwise.
+* napmo_gpu_dpsi (compute_dpsi, ndpsi.py:15-89): within 1e-9 of the largest
+  value (FEM solves, banded LU against scipy's sparse LU).
+* napmo_gpu_operator_matrix (get_operator_matrix) against numpy: 1e-12.
+* He/STO-3G 300 x 110 and H2/STO-3G 100 x 110 through PSIN + PSIO_BECKE
+  (test_psi_numeric_becke_He.py: E = -2.861679541872, rtol 1e-5;
+  test_psi_numeric_becke_H2.py: E = -1.13306385225865 in its docstring), the
+  grid one-body matrices of the basis-set orbital equal to the analytic ones
+  (the He test's np.allclose(psi_a.T, psi_n.T)).
+"""
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+from helpers import HCN, oracle_system, product_system
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not gpu_available(), reason='needs a CUDA device')]
+
+
+@pytest.fixture(scope='module')
+def hcn(oracle, basis_library, elements):
+    ms, grid = product_system(HCN, nrad=40, nang=110)
+    og, fb = oracle_system(oracle, basis_library, elements, HCN, nrad=40, nang=110)
+    assert np.array_equal(grid.points, og.points)
+    phi = oracle.basis_compute(fb, og.points).T.copy()
+    rng = np.random.default_rng(20261203)
+    psi = rng.normal(size=(3, phi.shape[0])) @ phi / np.sqrt(phi.shape[0])
+    return grid, og, psi
+
+
+def test_kinetic_matches_oracle(hcn):
+    import numeric as N
+    from napmo_b200.numeric import GridOperators, compute_kinetic
+    grid, og, psi = hcn
+    ops = GridOperators(grid, 8)
+    T = ops.kinetic(psi, 1.0).cpu().numpy()
+    for k in range(psi.shape[0]):
+        ref = N.compute_kinetic(og, psi[k], 8)
+        err = np.abs(T[k] - ref).max() / np.abs(ref).max()
+        assert err <= 1e-8, err
+        t_dev, t_ref = og.integrate(psi[k] * T[k]), og.integrate(psi[k] * ref)
+        assert abs(t_dev - t_ref) <= 1e-11 * abs(t_ref), (t_dev, t_ref)
+    # nAPMO's numpy-in, numpy-out call
+    one = compute_kinetic(grid, psi[0], 8)
+    assert isinstance(one, np.ndarray) and np.array_equal(one, T[0])
+    # scale multiplies (the species' inverse mass)
+    T2 = ops.kinetic(psi[:1], 0.25).cpu().numpy()
+    assert np.abs(T2[0] - 0.25 * T[0]).max() <= 1e-14 * np.abs(T[0]).max()
+
+
+def test_dpsi_matches_oracle(hcn):
+    import numeric as N
+    from napmo_b200.numeric import GridOperators
+    grid, og, psi = hcn
+    ops = GridOperators(grid, 8)
+    vnuc = np.zeros(og.size)
+    for c in og.origin:
+        vnuc += 1.0 / np.sqrt(((og.points - c) ** 2).sum(1))
+    phi, resid = psi[0], 0.1 * psi[1]
+    vtot = -phi * vnuc + 0.3 * psi[2]
+    doi, oi = [0.05, -0.02], [-0.7, -0.4]
+    out = ops.dpsi(np.stack([phi, psi[2]]), np.stack([resid, 0.2 * phi]),
+                   np.stack([vtot, vtot]), doi, oi, 1.0).cpu().numpy()
+    for k, (p, r) in enumerate(((phi, resid), (psi[2], 0.2 * phi))):
+        ref = N.compute_dpsi(og, 8, p, doi[k], oi[k], r, vtot, 1.0)
+        err = np.abs(out[k] - ref).max() / np.abs(ref).max()
+        assert err <= 1e-9, err
+
+
+def test_operator_matrix(hcn):
+    from napmo_b200.numeric import GridOperators
+    grid, og, psi = hcn
+    ops = GridOperators(grid, 8)
+    B = psi[:2] * np.linspace(0.5, 1.5, og.size)
+    M = ops.matrix(psi, B).cpu().numpy()
+    ref = (psi * og.becke * og.weights) @ B.T
+    assert M.shape == (3, 2)
+    assert np.abs(M - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def _becke(atoms, nrad, nang):
+    from napmo_b200.numeric import from_grid_rhf, optimize
+    from napmo_b200.scf import GridRHF
+    from napmo_b200.system import build_system
+    rhf = GridRHF(build_system(atoms, 'STO-3G'), nrad, nang, exchange='hf')
+    r = rhf.run(tol=1e-10)
+    assert r['converged']
+    psin = from_grid_rhf(rhf)
+    return rhf, r, psin, optimize(psin, tol=1e-8)
+
+
+def test_becke_he_known_answer(known):
+    rhf, r, psin, res = _becke([('He', (0.0, 0.0, 0.0))], 300, 110)
+    assert abs(r['energy'] - (-2.807784)) < 1e-5        # GTO start (CCCBDB, the test's docstring)
+    assert res['converged']
+    ref = known['becke_He_sto3g_300x110_energy']
+    assert abs(res['energy'] - ref) <= 1e-5 * abs(ref)
+
+
+def test_becke_he_one_body_equals_analytic():
+    """The basis-set orbital's grid T and V equal the analytic / quadrature
+    ones (the He test's np.allclose(psi_a.T, psi_n.T), rtol 1e-5)."""
+    from napmo_b200.numeric import from_grid_rhf
+    from napmo_b200.scf import GridRHF
+    from napmo_b200.system import build_system
+    rhf = GridRHF(build_system([('He', (0.0, 0.0, 0.0))], 'STO-3G'), 300, 110, exchange='hf')
+    rhf.run(tol=1e-10)
+    psin = from_grid_rhf(rhf)
+    C = rhf.C[:, :1]
+    T_an = float((C.T @ rhf.T @ C)[0, 0])
+    V_an = float((C.T @ rhf.V @ C)[0, 0])
+    assert abs(float(psin.T[0, 0]) - T_an) <= 1e-5 * abs(T_an)
+    assert abs(float(psin.V[0, 0]) - V_an) <= 1e-5 * abs(V_an)
+
+
+def test_becke_h2_known_answer(known):
+    rhf, r, psin, res = _becke([('H', (0.0, 0.0, 0.356)), ('H', (0.0, 0.0, -0.356))], 100, 110)
+    assert abs(r['energy'] - (-1.117506)) < 1e-4       # GTO start (CCCBDB, the test's docstring)
+    assert res['converged']
+    ref = known['becke_H2_sto3g_100x110_energy']
+    assert abs(res['energy'] - ref) <= 1e-4 * abs(ref)

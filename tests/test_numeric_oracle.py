@@ -1,0 +1,66 @@
+"""The numerical-orbital operators of the oracle (CPU): the radial second
+derivative against nAPMO's own vectors (napmo/wavefunction/test/
+test_kinetic.py), libnapmo's host RadialGrid.deriv2 against the same
+vectors, and the oracle's kinetic operator against the analytic Laplacian."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import napmo_b200 as nb
+from conftest import GOLDEN
+
+
+@pytest.fixture(scope='module')
+def deriv2_case():
+    with open(os.path.join(GOLDEN, 'known_answers.json')) as f:
+        k = json.load(f)
+    return np.array(k['deriv2_He_50_input']['value']), np.array(k['deriv2_He_50']['value'])
+
+
+def test_oracle_deriv2_matches_napmo_vectors(elements, deriv2_case):
+    import numeric as N
+    import oracle as O
+    R, gold = deriv2_case
+    r, _ = O.radial_grid(50, elements['He']['atomic_radii'])
+    res = N.deriv2(r, elements['He']['atomic_radii'], R)
+    # nAPMO's test: np.allclose(ref, res); the restatement agrees to 1e-11 of max
+    assert np.allclose(gold, res)
+    assert np.abs(res - gold).max() <= 1e-10 * np.abs(gold).max()
+
+
+def test_host_deriv2_matches_napmo_vectors(deriv2_case):
+    import numeric as N
+    R, gold = deriv2_case
+    g = nb.RadialGrid(50, 'He')
+    res = g.deriv2(R)
+    assert np.abs(res - gold).max() <= 1e-12 * np.abs(gold).max()
+    ora = N.deriv2(g.points, g.radii, R)
+    assert np.abs(res - ora).max() <= 1e-10 * np.abs(gold).max()
+
+
+def test_host_deriv2_rejects_short_grids():
+    g = nb.RadialGrid(6, 'He')
+    with pytest.raises(nb.NapmoError):
+        g.deriv2(np.ones(6))
+    g = nb.RadialGrid(50, 'He')
+    with pytest.raises(nb.NapmoError):
+        g.deriv2(np.ones(49))
+
+
+def test_oracle_kinetic_of_gaussians(elements):
+    """-1/2 laplacian of exp(-a r^2) and x exp(-a r^2) on one atom: the
+    expectation values agree with the analytic ones to 1e-6 relative on a
+    60-point radial grid (finite differences: 1e-5 at 40 points)."""
+    import numeric as N
+    import oracle as O
+    g = O.Grid([np.zeros(3)], [elements['He']['atomic_radii']], 60, 50)
+    a = 1.3
+    r2 = (g.points ** 2).sum(1)
+    f = np.exp(-a * r2)
+    for fn, lap in ((f, (4 * a * a * r2 - 6 * a) * f),
+                    (g.points[:, 0] * f, (4 * a * a * r2 - 10 * a) * g.points[:, 0] * f)):
+        T = N.compute_kinetic(g, fn, 5)
+        exact = g.integrate(fn * (-0.5 * lap))
+        assert abs(g.integrate(fn * T) - exact) <= 1e-6 * abs(exact)

@@ -142,3 +142,94 @@ def compute_dpsi(grid, lmax, phi, doi, oi, ri, V_tot, mass_inv):
         O.evaluate_decomposition(grid, a_i, (np.array(ys), np.array(dts)), out)
         off += atom.size
     return out
+
+
+def becke_scf(grid, phi0, e0, vnuc, lmax, nocc=1, eta=2.0, kappa=-1.0, charge=-1.0, mass_inv=1.0,
+              maxiter=100, tol=1e-8, pce=0.0, verbose=False):
+    """The Becke-Dickson SCF of nAPMO's numerical solver for a closed-shell
+    species whose occupied orbitals start as the rows of phi0 with energies
+    e0 (psi_numeric.py:23-424, psi_optimization.py:124-221, the loop of
+    test_psi_numeric_becke_He.py:100-130), with the oracle's operators and
+    numpy's generalised eigensolver.  Returns the energy history."""
+    import scipy.linalg
+    ndim = nocc
+    x_factor = kappa / eta
+    W = grid.becke * grid.weights
+
+    def mat(A, B):
+        return (A * W) @ B.T
+
+    def normalize(psi):
+        S = mat(psi, psi)
+        psi = psi / np.sqrt(S.diagonal())[:, None]
+        return psi, mat(psi, psi)
+
+    def one_body(psi):
+        Tg = np.array([compute_kinetic(grid, p, lmax) for p in psi]) * mass_inv
+        Vg = psi * vnuc * charge
+        return Tg, Vg, mat(psi, Tg) + mat(psi, Vg)
+
+    def coul(rho):
+        return O.compute_coulomb(grid, rho, lmax)
+
+    def two_body(psi, D):
+        Jpot = coul((psi * psi * eta).sum(axis=0))
+        G = mat(psi, psi * Jpot)
+        aux = {}
+        for s in range(ndim):
+            for v in range(s + 1):
+                aux[(s, v)] = coul(psi[s] * psi[v])
+        K = np.array([sum(psi[k] * aux[(max(l, j), min(l, j))] * D[k, l]
+                          for k in range(ndim) for l in range(ndim)) for j in range(ndim)])
+        E = mat(psi, K)
+        E = np.triu(E) + np.triu(E, 1).T
+        return Jpot, K, (G + x_factor * E) * charge ** 2
+
+    def iterate(S, F, H, G):
+        e, C = scipy.linalg.eigh(F, S)
+        D = eta * C[:, :nocc] @ C[:, :nocc].T
+        return e, C, D, float((D * (H + 0.5 * G)).sum())
+
+    psi, S = normalize(np.asarray(phi0, dtype=np.float64)[:ndim])
+    Tg, Vg, H = one_body(psi)
+    _, C = scipy.linalg.eigh(H, S)
+    D = eta * C[:, :nocc] @ C[:, :nocc].T
+    Jpot, K, G = two_body(psi, D)
+    O_, C, D, E = iterate(S, H + G, H, G)
+    prev_O = np.asarray(e0, dtype=np.float64)
+    history = [E + pce]
+    E_prev = 0.0
+    for it in range(maxiter):
+        # PSIO_BECKE.optimize
+        V_tot = Vg + psi * Jpot + K * x_factor
+        R = Tg + V_tot - prev_O[:ndim, None] * psi
+        de = np.array([float((R[i] * psi[i] * W).sum()) for i in range(ndim)])
+        dpsi = np.array([compute_dpsi(grid, lmax, psi[i], de[i], prev_O[i], R[i], V_tot[i],
+                                      mass_inv) for i in range(ndim)])
+        ext = np.vstack([psi, dpsi])
+        m = ext.shape[0]
+        Sx = mat(ext, ext)
+        Hg = np.array([compute_kinetic(grid, p, lmax) for p in ext]) * mass_inv + ext * vnuc * charge
+        pot = {}
+        for s in range(m):
+            for v in range(s + 1):
+                pot[(s, v)] = coul(ext[s] * ext[v])
+        Kg = np.array([sum(ext[s] * pot[(max(s, v), min(s, v))] for s in range(m))
+                       for v in range(m)])
+        Fx = mat(ext, Hg + ext * Jpot - Kg)
+        Fx = (Fx + Fx.T) / 2.0
+        ex, Cx = scipy.linalg.eigh(Fx, Sx)
+        prev_O = O_.copy()
+        psi = (Cx.T @ ext)[:ndim]
+        # PSIN: normalize, one-body, two-body, Fock, iterate
+        psi, S = normalize(psi)
+        Tg, Vg, H = one_body(psi)
+        Jpot, K, G = two_body(psi, D)
+        O_, C, D, E = iterate(S, H + G, H, G)
+        history.append(E + pce)
+        if verbose:
+            print(it + 1, E + pce, abs(E + pce - E_prev))
+        if abs(E + pce - E_prev) < tol:
+            break
+        E_prev = E + pce
+    return history

@@ -71,6 +71,11 @@ def known_answers(ref):
                           r'allclose\(E_tot, (-[0-9.]+), rtol=1e-5\)'),
             'rtol': 1e-5,
             'source': 'napmo/wavefunction/test/test_psi_numeric_becke_He.py'},
+        'becke_He_sto3g_300x110_grid_energy': {
+            'value': grab('napmo/wavefunction/test/test_psi_numeric_becke_He.py',
+                          r'GRID: (-[0-9.]+) \(300x110\)'),
+            'source': 'napmo/wavefunction/test/test_psi_numeric_becke_He.py (docstring: the '
+                      'grid energy of this algorithm on 300x110)'},
         'becke_H2_sto3g_100x110_energy': {
             'value': grab('napmo/wavefunction/test/test_psi_numeric_becke_H2.py',
                           r'GRID: (-[0-9.]+) \(100x110\)'),

@@ -11,10 +11,17 @@ Becke-Dickson known answers.
 * napmo_gpu_dpsi (compute_dpsi, ndpsi.py:15-89): within 1e-9 of the largest
   value (FEM solves, banded LU against scipy's sparse LU).
 * napmo_gpu_operator_matrix (get_operator_matrix) against numpy: 1e-12.
-* He/STO-3G 300 x 110 and H2/STO-3G 100 x 110 through PSIN + PSIO_BECKE
-  (test_psi_numeric_becke_He.py: E = -2.861679541872, rtol 1e-5;
-  test_psi_numeric_becke_H2.py: E = -1.13306385225865 in its docstring), the
-  grid one-body matrices of the basis-set orbital equal to the analytic ones
+* He/STO-3G 300 x 110 and H2/STO-3G 100 x 110 through PSIN + PSIO_BECKE.
+  He: the grid energy recorded in test_psi_numeric_becke_He.py's docstring,
+  -2.86165379510810, within 5e-7 Eh (the oracle's SCF reaches it to 1e-9;
+  measured 1.0e-7 on the device), and the test's assert (-2.861679541872,
+  rtol 1e-5).  The SCF energy of any FP64 implementation is reproducible to
+  ~1e-7 Eh only: the finite-difference Laplacian turns 1e-16 relative changes
+  of an orbital into 5e-6 of its maximum at the innermost radial point
+  (r = 1.4e-5 bohr), and the optimiser feeds that point back.
+  H2: test_psi_numeric_becke_H2.py's docstring value -1.13306385225865 within
+  1e-5 Eh (the oracle's SCF, stopped by the same 1e-8 rule: 4.4e-6).  The
+  grid one-body matrices of the basis-set orbital equal the analytic ones
   (the He test's np.allclose(psi_a.T, psi_n.T)).
 """
 import numpy as np
@@ -103,6 +110,8 @@ def test_becke_he_known_answer(known):
     rhf, r, psin, res = _becke([('He', (0.0, 0.0, 0.0))], 300, 110)
     assert abs(r['energy'] - (-2.807784)) < 1e-5        # GTO start (CCCBDB, the test's docstring)
     assert res['converged']
+    grid_value = known['becke_He_sto3g_300x110_grid_energy']
+    assert abs(res['energy'] - grid_value) <= 5e-7, (res['energy'], grid_value)
     ref = known['becke_He_sto3g_300x110_energy']
     assert abs(res['energy'] - ref) <= 1e-5 * abs(ref)
 
@@ -128,4 +137,4 @@ def test_becke_h2_known_answer(known):
     assert abs(r['energy'] - (-1.117506)) < 1e-4       # GTO start (CCCBDB, the test's docstring)
     assert res['converged']
     ref = known['becke_H2_sto3g_100x110_energy']
-    assert abs(res['energy'] - ref) <= 1e-4 * abs(ref)
+    assert abs(res['energy'] - ref) <= 1e-5, (res['energy'], ref)

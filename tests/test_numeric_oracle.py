@@ -64,3 +64,18 @@ def test_oracle_kinetic_of_gaussians(elements):
         T = N.compute_kinetic(g, fn, 5)
         exact = g.integrate(fn * (-0.5 * lap))
         assert abs(g.integrate(fn * T) - exact) <= 1e-6 * abs(exact)
+
+
+def test_oracle_becke_he_reproduces_napmo_grid_energy(elements, basis_library, known):
+    """The oracle's Becke-Dickson SCF (PSIN + PSIO_BECKE restated) from the
+    STO-3G orbital reaches the grid energy recorded in nAPMO's
+    test_psi_numeric_becke_He.py docstring (-2.86165379510810, 300 x 110) to
+    1e-8 Eh (measured 5e-10 to 1.2e-9 across OpenMP thread counts)."""
+    import numeric as N
+    import oracle as O
+    g = O.Grid([np.zeros(3)], [elements['He']['atomic_radii']], 300, 110)
+    fb = O.flat_basis([np.zeros(3)], ['He'], basis_library, 'STO-3G')
+    phi = O.basis_compute(fb, g.points).T.copy()
+    vnuc = 2.0 / np.sqrt((g.points ** 2).sum(1))
+    hist = N.becke_scf(g, phi, [-0.876036], vnuc, 8)
+    assert abs(hist[-1] - known['becke_He_sto3g_300x110_grid_energy']) <= 1e-8

@@ -215,10 +215,14 @@ void nwavefunction_compute_xc_matrix(void *psi, void *grid, double *phi,
 /* ---- analytic integrals / auxiliary basis (libint2, not on the grid
  * path): present so the ctypes layer binds, every call sets an error.
  * src/ints/libint_iface.h:106-148, src/grid/auxiliary_basis.h */
+/* One-body part of nAPMO's libint interface (libint_iface.cpp:41-190, 1318-1345),
+ * computed on the device (ints.cu): add the species' bases and point charges, then
+ * kind 1 = overlap, 2 = kinetic, 3 = nuclear attraction -sum Z <1/r_C> into a host
+ * [n][n] matrix of unit-normalised contracted functions. */
 void *LibintInterface_new(int id);
 void LibintInterface_del(void *l);
 void LibintInterface_add_basis(void *l, void *b);
-void LibintInterface_add_pointcharges(void *l, int n, double *q);
+void LibintInterface_add_pointcharges(void *l, int z, double *center);
 int LibintInterface_get_nbasis(void *l);
 void LibintInterface_compute_1body_ints(void *l, int kind, double *out);
 void LibintInterface_init_2body_ints(void *l);
@@ -300,6 +304,11 @@ int napmo_gpu_dpsi(void *grid, int lmax, int nfunc, const double *phi, const dou
  * get_operator_matrix (napmo/wavefunction/psi_numeric.py:406-424). */
 int napmo_gpu_operator_matrix(void *grid, int n, int m, const double *A, long lda,
                               const double *B, long ldb, double *M, void *stream);
+/* S, T, V = -sum_C Z_C <mu|1/r_C|nu> of a basis (device [n][n] outputs, any may be
+ * null; charges host [nq][4] = x, y, z, Z); replaces libint's one-body engines
+ * (libint_iface.cpp:136-190) and overlap.cpp:12-64. */
+int napmo_gpu_one_body(void *basis, int nq, const double *charges, double *S, double *T,
+                       double *V, void *stream);
 /* sum_A Z_A / |r - R_A| at device points; replaces compute_nuclear (nnuclear.py:15-37). */
 int napmo_gpu_nuclear_potential(int npoint, const double *x, const double *y, const double *z,
                                 int nq, const double *charges, double *v, void *stream);

@@ -24,7 +24,7 @@ CUDA_FLAGS = ARCH + ['-O3', '-lineinfo', '-std=c++17', '--expt-relaxed-constexpr
 HOST_SOURCES = ['host.cpp']
 CUDA_SOURCES = ['becke.cu', 'gto.cu', 'quad.cu', 'tc.cu', 'poisson.cu', 'capi_grid.cu',
                 'capi_basis.cu', 'capi_quad.cu', 'capi_batch.cu', 'capi_scf.cu', 'grad.cu',
-                'xc.cu']
+                'xc.cu', 'ints.cu']
 EXTRA_CUDA = {'becke.cu': ['--fmad=false']}
 LIBS = ['-lcusolver', '-lcublas']
 

@@ -209,6 +209,14 @@ _SIGS = [
       c_void_p, c_void_p]),
     ('napmo_gpu_operator_matrix', c_int,
      [c_void_p, c_int, c_int, c_void_p, c_long, c_void_p, c_long, c_void_p, c_void_p]),
+    ('napmo_gpu_one_body', c_int,
+     [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ('LibintInterface_new', c_void_p, [c_int]),
+    ('LibintInterface_del', None, [c_void_p]),
+    ('LibintInterface_add_basis', None, [c_void_p, c_void_p]),
+    ('LibintInterface_add_pointcharges', None, [c_void_p, c_int, a1df]),
+    ('LibintInterface_get_nbasis', c_int, [c_void_p]),
+    ('LibintInterface_compute_1body_ints', None, [c_void_p, c_int, a2df]),
     ('napmo_gpu_nuclear_potential', c_int,
      [c_int, c_void_p, c_void_p, c_void_p, c_int, a2df, c_void_p, c_void_p]),
     ('napmo_fock_plan_new', c_void_p, [c_void_p, c_void_p, c_int, c_void_p]),

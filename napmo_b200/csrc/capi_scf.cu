@@ -336,12 +336,6 @@ int MultiGrid_get_common_index_size(MultiGrid *m, int a, int b) {
                                    "the grid-quadrature path");                   \
     return val;                                                                   \
   }
-NAPMO_STUB(void *, LibintInterface_new, (int), nullptr)
-NAPMO_STUB(void, LibintInterface_del, (void *), )
-NAPMO_STUB(void, LibintInterface_add_basis, (void *, void *), )
-NAPMO_STUB(void, LibintInterface_add_pointcharges, (void *, int, double *), )
-NAPMO_STUB(int, LibintInterface_get_nbasis, (void *), 0)
-NAPMO_STUB(void, LibintInterface_compute_1body_ints, (void *, int, double *), )
 NAPMO_STUB(void, LibintInterface_init_2body_ints, (void *), )
 NAPMO_STUB(void *, LibintInterface_compute_2body_ints, (void *, double *), nullptr)
 NAPMO_STUB(void, LibintInterface_compute_2body_direct, (void *, double *, double *), )

@@ -75,10 +75,13 @@ class GridRHF(object):
         exchange: 'hf', 'lda-x', 'lda' (exchange + VWN5 correlation) or 'none'.
         precision: 'fp64' or 'int8x4' for rho and the quadratures.
         diis: number of DIIS vectors.
+        hcore: 'grid' (V_ne by grid quadrature, as nnuclear.py) or 'analytic'
+            (V_ne by the device one-electron integrals, as libint gives it to
+            nAPMO's analytic wave function).
     """
 
     def __init__(self, ms, nrad=50, nang=110, lmax=None, exchange='hf', precision='fp64',
-                 diis=6):
+                 diis=6, hcore='grid'):
         torch = _torch()
         self.torch = torch
         e = ms['e-']
@@ -103,7 +106,17 @@ class GridRHF(object):
         checked(cext.lib.napmo_gpu_nuclear_potential(N, x, y, z, q.shape[0],
                                                      np.ascontiguousarray(q), vne.data_ptr(),
                                                      torch.cuda.current_stream().cuda_stream))
-        self.V = self.fb.quadrature(-1.0, vne)          # FP64: built before any precision switch
+        if hcore == 'analytic':
+            # device McMurchie-Davidson integrals (libint's role in nAPMO)
+            self.V = torch.empty((n, n), **dev)
+            checked(cext.lib.napmo_gpu_one_body(e['basis']._this, q.shape[0],
+                                                np.ascontiguousarray(q).ctypes.data, None, None,
+                                                self.V.data_ptr(),
+                                                torch.cuda.current_stream().cuda_stream))
+        elif hcore == 'grid':
+            self.V = self.fb.quadrature(-1.0, vne)      # FP64: built before any precision switch
+        else:
+            raise ValueError("hcore must be 'grid' or 'analytic'")
         self.H = self.T + self.V
         self.Enn = nuclear_repulsion(ms.point_charges)
         self.W = torch.as_tensor(self.grid.becke_weights * self.grid.weights, **dev)

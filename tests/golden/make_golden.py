@@ -5,8 +5,8 @@
 * ``reference_vectors.npz``: outputs of nAPMO's own compiled sources
   (oracle/_ref/libnapmo_ref.so, built by oracle/Makefile) on small seeded
   inputs: Lebedev rules, Chebyshev/Power radial transforms, Cartesian GTO
-  values (H2O/cc-pVDZ, HCN/cc-pVDZ), spline derivatives, FEM assembly and
-  the multipole evaluation of a decomposition.
+  values and overlap matrices (H2O/cc-pVDZ, HCN/cc-pVDZ), spline derivatives,
+  FEM assembly and the multipole evaluation of a decomposition.
 
 Usage: python tests/golden/make_golden.py [/path/to/nAPMO] [--answers-only]
 """
@@ -139,6 +139,9 @@ def reference_vectors():
         r.BasisSet_compute(bs, pts, phi, 64)
         out['gto_%s_points' % tag] = pts
         out['gto_%s_phi' % tag] = phi
+        # overlap matrix by nAPMO's own contracted overlap (gto.cpp, ints/overlap.cpp)
+        out['ints_%s_S' % tag] = np.array([[r.ContractedGaussian_overlap(ci, cj) for cj in cont]
+                                           for ci in cont])
     # spline derivatives and FEM assembly on a random case
     y = np.ascontiguousarray(rng.normal(size=40))
     dt = np.zeros(40)

@@ -55,6 +55,10 @@ struct PoissonPlan {
   DevBuf<EvalItem> items_s;
   int nitems_s = 0, nitems_in_s = 0;
   unsigned long long screen_key = 0;  // serial of the mask's int8 plan (0: none)
+  // Becke-Dickson workspace (source, shell averages, LU factors), kept
+  // between calls: an allocation per call would return to the driver at
+  // every synchronisation of the caller's loop
+  DevBuf<char> bd_ws;
 };
 
 void free_poisson_plan(PoissonPlan *p) { delete p; }
@@ -354,10 +358,12 @@ int run_poisson(BeckeGrid *g, PoissonPlan *p, const double *rho_dev, double *v_d
 
 // The grid's Poisson tables for `lmax`, set up for an operator evaluation:
 // every point, no truncation, no raw spline output.
-static int operator_dev(BeckeGrid *g, int lmax, cudaStream_t s, PoissonDev *out) {
+static int operator_dev(BeckeGrid *g, int lmax, cudaStream_t s, PoissonDev *out,
+                        PoissonPlan **plan = nullptr) {
   PoissonPlan *p = nullptr;
   int st = grid_poisson_plan(g, lmax, s, &p);
   if (st) return st;
+  if (plan) *plan = p;
   st = select_pair_lists(p, g, nullptr, 0, s);
   if (st) return st;
   *out = p->d;
@@ -1329,16 +1335,19 @@ int napmo_gpu_dpsi(BeckeGrid *g, int lmax, int nfunc, const double *phi, const d
     if (nfunc == 0) return kOk;
     cudaStream_t s = (cudaStream_t)stream;
     PoissonDev P;
-    int st = operator_dev(g, lmax, s, &P);
+    PoissonPlan *plan = nullptr;
+    int st = operator_dev(g, lmax, s, &P, &plan);
     if (st) return st;
     long nshell = 0;
     for (auto &L : g->layout) nshell += L.nrad;
     const size_t rows = (size_t)P.nsys * P.lu_stride;
-    void *ws = nullptr;
     const size_t bytes = (g->size + nshell + rows * (kW + kKL)) * sizeof(double) +
                          rows * sizeof(int);
-    NAPMO_TRY_CUDA(cudaMallocAsync(&ws, bytes, s), "Becke-Dickson workspace");
-    double *src = (double *)ws;
+    if (plan->bd_ws.n < bytes) {
+      NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "Becke-Dickson workspace");
+      NAPMO_TRY_CUDA(plan->bd_ws.alloc(bytes), "Becke-Dickson workspace");
+    }
+    double *src = (double *)plan->bd_ws.p;
     double *vsph = src + g->size;
     P.lu = vsph + nshell;
     P.lmul = P.lu + rows * kW;
@@ -1362,7 +1371,6 @@ int napmo_gpu_dpsi(BeckeGrid *g, int lmax, int nfunc, const double *phi, const d
         e = launch_poisson_evaluate(P, g->size, g->dev.x, g->dev.y, g->dev.z,
                                     out + (long)k * ld, false, s);
     }
-    cudaFreeAsync(ws, s);
     NAPMO_TRY_CUDA(e, "Becke-Dickson correction");
     return kOk;
   });

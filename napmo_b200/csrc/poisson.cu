@@ -57,30 +57,35 @@ __device__ __forceinline__ int piece_d(long c, long k, long g) {
   return 4;
 }
 
-__device__ double ov2_d(long xmax, long i0, int d0, long i1, int d1) {
+// The Hermite tables are read through a pointer: constant memory (c_ov2,
+// c_ov3) where every lane of a warp reads the same entry, a shared-memory copy
+// where lanes read different entries (the FEM assembly; constant memory
+// would serve those one address at a time).
+__device__ double ov2_d(long xmax, long i0, int d0, long i1, int d1, const double *ov2 = c_ov2) {
   const long c0 = i0 / 2, k0 = i0 % 2, c1 = i1 / 2, k1 = i1 % 2;
   if (labs(c1 - c0) >= 2) return 0.0;
   double r = 0.0;
   if (c0 >= 1 && c0 <= xmax)
-    r += c_ov2[((piece_d(c0, k0, c0 - 1) * 2 + d0) * 5 + piece_d(c1, k1, c0 - 1)) * 2 + d1];
+    r += ov2[((piece_d(c0, k0, c0 - 1) * 2 + d0) * 5 + piece_d(c1, k1, c0 - 1)) * 2 + d1];
   if (c0 >= 0 && c0 <= xmax - 1)
-    r += c_ov2[((piece_d(c0, k0, c0) * 2 + d0) * 5 + piece_d(c1, k1, c0)) * 2 + d1];
+    r += ov2[((piece_d(c0, k0, c0) * 2 + d0) * 5 + piece_d(c1, k1, c0)) * 2 + d1];
   return r;
 }
 
-__device__ double ov3_d(long xmax, long i0, int d0, long i1, int d1, long i2, int d2) {
+__device__ double ov3_d(long xmax, long i0, int d0, long i1, int d1, long i2, int d2,
+                       const double *ov3 = c_ov3) {
   const long c0 = i0 / 2, k0 = i0 % 2, c1 = i1 / 2, k1 = i1 % 2, c2 = i2 / 2,
              k2 = i2 % 2;
   if (labs(c1 - c0) >= 2 || labs(c2 - c0) >= 2) return 0.0;
   double r = 0.0;
   if (c0 >= 1 && c0 <= xmax) {
     const long g = c0 - 1;
-    r += c_ov3[((((piece_d(c0, k0, g) * 2 + d0) * 5 + piece_d(c1, k1, g)) * 2 + d1) * 5 +
+    r += ov3[((((piece_d(c0, k0, g) * 2 + d0) * 5 + piece_d(c1, k1, g)) * 2 + d1) * 5 +
                 piece_d(c2, k2, g)) * 2 + d2];
   }
   if (c0 >= 0 && c0 <= xmax - 1) {
     const long g = c0;
-    r += c_ov3[((((piece_d(c0, k0, g) * 2 + d0) * 5 + piece_d(c1, k1, g)) * 2 + d1) * 5 +
+    r += ov3[((((piece_d(c0, k0, g) * 2 + d0) * 5 + piece_d(c1, k1, g)) * 2 + d1) * 5 +
                 piece_d(c2, k2, g)) * 2 + d2];
   }
   return r;
@@ -223,6 +228,9 @@ __global__ void radial_factor_kernel(PoissonDev P, RadialOp op) {
   double *adt = ay + n;
   __shared__ double s_mult[kKL];
   __shared__ int s_piv;
+  __shared__ double s_ov2[5 * 2 * 5 * 2], s_ov3[5 * 2 * 5 * 2 * 5 * 2];
+  for (int e = threadIdx.x; e < 100; e += blockDim.x) s_ov2[e] = c_ov2[e];
+  for (int e = threadIdx.x; e < 1000; e += blockDim.x) s_ov3[e] = c_ov3[e];
   const double *rad = P.rad + at.rad_off;
   const double *r = rad + kRadR * n, *j1 = rad + kRadJ1 * n, *j2 = rad + kRadJ2 * n,
                *j3 = rad + kRadJ3 * n;
@@ -252,7 +260,7 @@ __global__ void radial_factor_kernel(PoissonDev P, RadialOp op) {
     if (hi > n2) hi = n2;
     for (long col = lo; col < hi; ++col) {
       double cf = 0.0;
-      cf -= ov2_d(xmax, row, 1, col, 1);
+      cf -= ov2_d(xmax, row, 1, col, 1, s_ov2);
       for (long k = lo; k < hi; ++k) {
         const int i = (int)(k / 2);
         const double ri = r[i], r2 = ri * ri;
@@ -278,8 +286,8 @@ __global__ void radial_factor_kernel(PoissonDev P, RadialOp op) {
           const double ay = -l2l / r2, adx = 2 * l2l / (r2 * ri);
           ak = (adx * jsq + 2 * ay * j2[i]) * j1[i];
         }
-        if (bk != 0) cf += bk * ov3_d(xmax, row, 0, col, 1, k, 0);
-        if (ak != 0) cf += ak * ov3_d(xmax, row, 0, col, 0, k, 0);
+        if (bk != 0) cf += bk * ov3_d(xmax, row, 0, col, 1, k, 0, s_ov3);
+        if (ak != 0) cf += ak * ov3_d(xmax, row, 0, col, 0, k, 0, s_ov3);
       }
       cf += node_d(xmax, row / 2, row % 2, 0) * node_d(xmax, col / 2, col % 2, 1);
       cf -= node_d(0, row / 2, row % 2, 0) * node_d(0, col / 2, col % 2, 1);
@@ -1154,11 +1162,14 @@ cudaError_t launch_radial_factor(const PoissonDev &P, const RadialOp &op, cudaSt
   if (P.nsys == 0) return cudaSuccess;
   const size_t smem =
       ((size_t)2 * P.max_nrad * kW + (op.vsph ? 2 * (size_t)P.max_nrad : 0)) * sizeof(double);
-  if (smem > kMaxSmem) return cudaErrorInvalidValue;
+  // static part: the Hermite tables, multipliers and pivot
+  constexpr size_t kStatic = (100 + 1000 + kKL) * sizeof(double) + sizeof(int);
+  if (smem + kStatic > kMaxSmem) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(radial_factor_kernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  radial_factor_kernel<<<P.nsys, 32, smem, s>>>(P, op);
+  // 4 warps: rows of the assembly in parallel; the elimination is one chain
+  radial_factor_kernel<<<P.nsys, 128, smem, s>>>(P, op);
   return cudaGetLastError();
 }
 

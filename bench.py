@@ -44,7 +44,8 @@ def parse():
     p.add_argument('--cpu-points', type=int, default=4096)
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--no-scf', action='store_true', help='skip the SCF timing of the c4 line')
-    p.add_argument('--workload', default='c4', choices=['c4', 'c3', 'c5', 'c1', 'c2', 'c6'],
+    p.add_argument('--workload', default='c4',
+                   choices=['c4', 'c3', 'c5', 'c1', 'c2', 'c6', 'c7'],
                    help='c4: C20H42 single system (default); c3: batch of 64 random HCNO '
                         'chains with uneven per-atom grids, one CUDA-graph launch per batch')
     p.add_argument('--nmol', type=int, default=64)
@@ -672,6 +673,85 @@ def run_becke_c6(args, world, rank):
         print(json.dumps(line))
 
 
+# ----------------------------------------- C7: one-electron integrals on the GPU
+C7_WORKLOAD = ('C7: S, T and V = -sum Z <1/r_C> of C20H42/cc-pVDZ (510 Cartesian functions, '
+               '130,305 pairs, 62 point charges), nAPMO\'s libint one-body calls')
+
+
+def c7_cpu_baseline(ms):
+    """The host restatements: S and T by the product's host Obara-Saika code
+    (C++, one thread, all pairs); V by the oracle (McMurchie-Davidson in
+    Python) on a sample of 400 function pairs, scaled to all pairs."""
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import ints as OI
+    from napmo_b200 import cext
+    b = ms['e-']['basis']
+    n = b['nbasis']
+    S, T = np.zeros((n, n)), np.zeros((n, n))
+    t0 = time.perf_counter()
+    cext.checked(cext.lib.napmo_basis_one_body(b._this, S, T))
+    t_st = time.perf_counter() - t0
+    rng = np.random.default_rng(SEED)
+    pairs = rng.integers(0, n, size=(400, 2))
+    charges = [(pc['atomic_number'], np.asarray(pc['origin'])) for pc in ms.point_charges]
+    cont = b['cont']
+    t0 = time.perf_counter()
+    for i, j in pairs:
+        ci, cj = cont[i], cont[j]
+        li, lj, oi, oj = [int(x) for x in ci.l], [int(x) for x in cj.l], ci.origin, cj.origin
+        for pa in ci._primitives:
+            for pb in cj._primitives:
+                OI.primitive(li, oi, pa.exponent, lj, oj, pb.exponent, charges)
+    t_v = (time.perf_counter() - t0) * (n * (n + 1) / 2) / len(pairs)
+    return {'value': t_st + t_v, 'unit': 's per S,T,V', 'cores': 1, 'kind': 'port',
+            'sample': 'S, T: all pairs by the host C++ code (%.3f s); V: 400 seeded pairs by the '
+                      'oracle, scaled to 130,305 pairs (%.1f s)' % (t_st, t_v)}
+
+
+def run_ints_c7(args, world, rank):
+    import torch
+    from napmo_b200 import cext
+    from napmo_b200.system import alkane_geometry, build_system
+    ms = build_system(alkane_geometry(20), 'CC-PVDZ')
+    b = ms['e-']['basis']
+    n = b['nbasis']
+    q = np.ascontiguousarray(np.array([[*pc['origin'], pc['atomic_number']]
+                                       for pc in ms.point_charges], dtype=np.float64))
+    out = [torch.empty((n, n), dtype=torch.float64, device='cuda') for _ in range(3)]
+    stream = torch.cuda.current_stream()
+
+    def one():
+        cext.checked(cext.lib.napmo_gpu_one_body(b._this, q.shape[0], q.ctypes.data,
+                                                 *[o.data_ptr() for o in out],
+                                                 stream.cuda_stream))
+    for _ in range(args.warmup):
+        one()
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record()
+    for _ in range(args.steps):
+        one()
+    ev[1].record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    t = ev[0].elapsed_time(ev[1]) / 1e3 / args.steps
+    cb = c7_cpu_baseline(ms) if not args.no_cpu_baseline and rank == 0 else None
+    line = {'metric': 'one-electron integrals S, T, V of C20H42/cc-pVDZ (C7)', 'value': t,
+            'unit': 's per S,T,V', 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': t * 1e3, 'higher_is_better': False, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+            'config': {'workload': C7_WORKLOAD, 'parallelism': 'single GPU',
+                       'l2': 'inputs are the basis description (a few KB); outputs 6 MB'},
+            'clocks': clocks, 'gpu_launches': args.steps,
+            'e2e': {'value': t, 'unit': 's per S,T,V', 'h2d_bytes_per_step': 0,
+                    'd2h_bytes_per_step': 0},
+            'cpu_baseline': cb}
+    if rank == 0:
+        print(json.dumps(line))
+
+
 # --------------------------------------------------------------------- main
 def main():
     args = parse()
@@ -730,12 +810,12 @@ def main():
     import napmo_b200 as nb
     from napmo_b200 import cext
 
-    if args.workload in ('c3', 'c5', 'c1', 'c2', 'c6'):
+    if args.workload in ('c3', 'c5', 'c1', 'c2', 'c6', 'c7'):
         if args.workload == 'c3':
             run_batch(args, world, rank, dist)
         else:
             {'c5': run_gradients, 'c1': run_scf_c1, 'c2': run_scf_c2,
-             'c6': run_becke_c6}[args.workload](
+             'c6': run_becke_c6, 'c7': run_ints_c7}[args.workload](
                 args, world, rank)
         if dist:
             dist.barrier()

@@ -227,7 +227,6 @@ __global__ void radial_factor_kernel(PoissonDev P, RadialOp op) {
   double *ay = band + n2 * kW;  // Becke-Dickson a(r_i) and its spline t-derivative
   double *adt = ay + n;
   __shared__ double s_mult[kKL];
-  __shared__ int s_piv;
   __shared__ double s_ov2[5 * 2 * 5 * 2], s_ov3[5 * 2 * 5 * 2 * 5 * 2];
   for (int e = threadIdx.x; e < 100; e += blockDim.x) s_ov2[e] = c_ov2[e];
   for (int e = threadIdx.x; e < 1000; e += blockDim.x) s_ov3[e] = c_ov3[e];
@@ -295,45 +294,49 @@ __global__ void radial_factor_kernel(PoissonDev P, RadialOp op) {
     }
   }
   __syncthreads();
-  // -- 3. banded LU with partial pivoting
-  for (int k = 0; k < n2; ++k) {
-    const int im = min(k + kKL, n2 - 1);
-    const int ju = min(k + kKL + kKU, n2 - 1);
-    if (tid == 0) {
+  // -- 3. banded LU with partial pivoting.  A step updates at most 3 x 9
+  // entries, so warp 0 runs the elimination with warp-level synchronisation
+  // (a block barrier per step, 2 n times, cost more than the step itself).
+  if (tid < 32) {
+    const unsigned full = 0xffffffffu;
+    for (int k = 0; k < n2; ++k) {
+      const int im = min(k + kKL, n2 - 1);
+      const int ju = min(k + kKL + kKU, n2 - 1);
       int p = k;
-      double best = fabs(AB(band, k, k));
-      for (int i = k + 1; i <= im; ++i) {
-        const double v = fabs(AB(band, i, k));
-        if (v > best) {
-          best = v;
-          p = i;
+      if (tid == 0) {
+        double best = fabs(AB(band, k, k));
+        for (int i = k + 1; i <= im; ++i) {
+          const double v = fabs(AB(band, i, k));
+          if (v > best) {
+            best = v;
+            p = i;
+          }
         }
       }
-      s_piv = p;
-    }
-    __syncthreads();
-    const int p = s_piv;
-    if (p != k) {
-      for (int j = k + tid; j <= ju; j += nt) {
-        const double t = AB(band, k, j);
-        AB(band, k, j) = AB(band, p, j);
-        AB(band, p, j) = t;
+      p = __shfl_sync(full, p, 0);
+      if (p != k) {
+        for (int j = k + tid; j <= ju; j += 32) {
+          const double t = AB(band, k, j);
+          AB(band, k, j) = AB(band, p, j);
+          AB(band, p, j) = t;
+        }
+        __syncwarp();
       }
-      __syncthreads();
+      if (tid < im - k) s_mult[tid] = AB(band, k + 1 + tid, k) / AB(band, k, k);
+      __syncwarp();
+      const int nrow = im - k, ncolu = ju - k;
+      for (int e = tid; e < nrow * ncolu; e += 32) {
+        const int i = k + 1 + e / ncolu, j = k + 1 + e % ncolu;
+        AB(band, i, j) -= s_mult[i - k - 1] * AB(band, k, j);
+      }
+      if (tid == 0) {
+        piv[k] = p;
+        for (int i = 0; i < kKL; ++i) mult[k * kKL + i] = i < nrow ? s_mult[i] : 0.0;
+      }
+      __syncwarp();
     }
-    if (tid < im - k) s_mult[tid] = AB(band, k + 1 + tid, k) / AB(band, k, k);
-    __syncthreads();
-    const int nrow = im - k, ncolu = ju - k;
-    for (int e = tid; e < nrow * ncolu; e += nt) {
-      const int i = k + 1 + e / ncolu, j = k + 1 + e % ncolu;
-      AB(band, i, j) -= s_mult[i - k - 1] * AB(band, k, j);
-    }
-    if (tid == 0) {
-      piv[k] = p;
-      for (int i = 0; i < kKL; ++i) mult[k * kKL + i] = i < nrow ? s_mult[i] : 0.0;
-    }
-    __syncthreads();
   }
+  __syncthreads();
   for (int e = tid; e < n2 * kW; e += nt) lu[e] = band[e];
 }
 
@@ -1162,8 +1165,8 @@ cudaError_t launch_radial_factor(const PoissonDev &P, const RadialOp &op, cudaSt
   if (P.nsys == 0) return cudaSuccess;
   const size_t smem =
       ((size_t)2 * P.max_nrad * kW + (op.vsph ? 2 * (size_t)P.max_nrad : 0)) * sizeof(double);
-  // static part: the Hermite tables, multipliers and pivot
-  constexpr size_t kStatic = (100 + 1000 + kKL) * sizeof(double) + sizeof(int);
+  // static part: the Hermite tables and the multipliers
+  constexpr size_t kStatic = (100 + 1000 + kKL) * sizeof(double);
   if (smem + kStatic > kMaxSmem) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(radial_factor_kernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

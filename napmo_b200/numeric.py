@@ -273,6 +273,7 @@ class PSIO_BECKE(object):
         F = ops.matrix(ext, Fgrid)
         self.asymmetry = float((F - F.T).abs().max())
         F = (F + F.T) / 2.0
+        self.S_ext, self.F_ext = S, F
         z = np.zeros((m, m))
         for name, val in (('S', S.cpu().numpy()), ('F', F.cpu().numpy()), ('H', z), ('G', z),
                           ('J', z)):

@@ -145,12 +145,14 @@ def compute_dpsi(grid, lmax, phi, doi, oi, ri, V_tot, mass_inv):
 
 
 def becke_scf(grid, phi0, e0, vnuc, lmax, nocc=1, eta=2.0, kappa=-1.0, charge=-1.0, mass_inv=1.0,
-              maxiter=100, tol=1e-8, pce=0.0, verbose=False):
+              maxiter=100, tol=1e-8, pce=0.0, verbose=False, record=None):
     """The Becke-Dickson SCF of nAPMO's numerical solver for a closed-shell
     species whose occupied orbitals start as the rows of phi0 with energies
     e0 (psi_numeric.py:23-424, psi_optimization.py:124-221, the loop of
     test_psi_numeric_becke_He.py:100-130), with the oracle's operators and
-    numpy's generalised eigensolver.  Returns the energy history."""
+    numpy's generalised eigensolver.  Returns the energy history; with
+    `record` (a list) each optimiser step appends its (S, F) of the
+    orbitals-plus-corrections space."""
     import scipy.linalg
     ndim = nocc
     x_factor = kappa / eta
@@ -218,6 +220,8 @@ def becke_scf(grid, phi0, e0, vnuc, lmax, nocc=1, eta=2.0, kappa=-1.0, charge=-1
                        for v in range(m)])
         Fx = mat(ext, Hg + ext * Jpot - Kg)
         Fx = (Fx + Fx.T) / 2.0
+        if record is not None:
+            record.append((Sx.copy(), Fx.copy()))
         ex, Cx = scipy.linalg.eigh(Fx, Sx)
         prev_O = O_.copy()
         psi = (Cx.T @ ext)[:ndim]

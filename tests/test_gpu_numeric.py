@@ -138,3 +138,44 @@ def test_becke_h2_known_answer(known):
     assert res['converged']
     ref = known['becke_H2_sto3g_100x110_energy']
     assert abs(res['energy'] - ref) <= 1e-5, (res['energy'], ref)
+
+
+def test_becke_h2o_first_step_matches_oracle(basis_library, elements):
+    """Five occupied orbitals (H2O/STO-3G, 30 x 50 per atom) from the grid
+    RHF orbitals: the grid Fock step and the optimiser's overlap and Fock
+    matrices of the 10-function space (exchange pair potentials in INDEX
+    packing, five corrections in one call) equal the oracle's
+    (oracle/numeric.py: becke_scf) to 1e-10 of their largest entries.  Later
+    steps are compared by energy only loosely: the 10 x 10 overlap has
+    condition number ~6e5, so the generalised eigenproblem amplifies
+    1e-12 differences to ~1e-4 Eh after one step in any FP64
+    implementation (nAPMO's Becke tests cover one-orbital species only)."""
+    import numeric as N
+    import oracle as O
+    from helpers import H2O, BOHR
+    from napmo_b200.numeric import from_grid_rhf, optimize
+    from napmo_b200.scf import GridRHF, nuclear_repulsion
+    from napmo_b200.system import build_system
+    rhf = GridRHF(build_system(H2O, 'STO-3G'), 30, 50, exchange='hf')
+    assert rhf.run(tol=1e-10)['converged']
+    psin = from_grid_rhf(rhf)
+    assert psin.ndim == 5
+    dev = optimize(psin, maxiter=1, tol=0.0)['history']
+    Sd = psin.optimizer.S_ext.cpu().numpy()
+    Fd = psin.optimizer.F_ext.cpu().numpy()
+    cs = [np.array(x) / BOHR for _, x in H2O]
+    og = O.Grid(cs, [elements[s]['atomic_radii'] for s, _ in H2O], 30, 50)
+    fb = O.flat_basis(cs, [s for s, _ in H2O], basis_library, 'STO-3G')
+    phi = O.basis_compute(fb, og.points).T
+    C, e0 = rhf.C.cpu().numpy(), rhf.O.cpu().numpy()
+    Z = [8.0, 1.0, 1.0]
+    vnuc = sum(z / np.sqrt(((og.points - c) ** 2).sum(1)) for z, c in zip(Z, cs))
+    pce = nuclear_repulsion(build_system(H2O, 'STO-3G').point_charges)
+    rec = []
+    ora = N.becke_scf(og, (C.T @ phi)[:5], e0, vnuc, psin.lmax, nocc=5, maxiter=1, tol=0.0,
+                      pce=pce, record=rec)
+    assert abs(dev[0] - ora[0]) <= 1e-10
+    So, Fo = rec[0]
+    assert np.abs(Sd - So).max() <= 1e-10 * np.abs(So).max()
+    assert np.abs(Fd - Fo).max() <= 1e-10 * np.abs(Fo).max()
+    assert abs(dev[1] - ora[1]) <= 1e-3

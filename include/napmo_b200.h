@@ -296,7 +296,9 @@ int napmo_gpu_epc17_2(long n, const double *rho_e, const double *rho_n, double *
 int napmo_gpu_kinetic(void *grid, int lmax, int nfunc, const double *psi, long ld, double scale,
                       double *out, void *stream);
 /* Becke-Dickson orbital corrections of nfunc orbitals; replaces compute_dpsi
- * (napmo/wavefunction/ndpsi.py:15-89).  doi, oi: host arrays of nfunc. */
+ * (napmo/wavefunction/ndpsi.py:15-89).  doi, oi: host arrays of nfunc.  The
+ * workspace lives on the grid's Poisson tables: calls on one grid (and its
+ * Poisson solves) must not overlap on the device. */
 int napmo_gpu_dpsi(void *grid, int lmax, int nfunc, const double *phi, const double *resid,
                    const double *vtot, long ld, const double *doi, const double *oi,
                    double mass_inv, double *out, void *stream);

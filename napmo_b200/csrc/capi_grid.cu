@@ -1325,7 +1325,9 @@ int napmo_gpu_kinetic(BeckeGrid *g, int lmax, int nfunc, const double *psi, long
 //       = -2/m_inv src_lm,   u = 0 at both ends,
 // (<.> the spherical average over each radial shell) and out[k] is the sum
 // of the solutions over atoms at every point.  phi, resid, vtot, out: device
-// rows of ld doubles; doi, oi: host arrays of nfunc.
+// rows of ld doubles; doi, oi: host arrays of nfunc.  Uses the grid's Poisson
+// tables and a workspace kept with them: calls on one grid must not overlap
+// on the device.
 int napmo_gpu_dpsi(BeckeGrid *g, int lmax, int nfunc, const double *phi, const double *resid,
                    const double *vtot, long ld, const double *doi, const double *oi,
                    double mass_inv, double *out, void *stream) {

@@ -189,16 +189,18 @@ class PSIN(object):
         self.Jpot = self.ops.coulomb(self.Dgrid.sum(dim=0))
         G = self.ops.matrix(self.psi, self.psi * self.Jpot)
         if self.x_factor != 0.0:
-            aux = [None] * (n * (n + 1) // 2)
+            # K_j = sum_kl psi_k V[psi_l psi_j] D_kl = sum_l V[psi_l psi_j] chi_l with
+            # chi_l = sum_k D_kl psi_k; each pair potential (INDEX packing, s >= v)
+            # is used as soon as it is solved, so memory stays O(n N)
+            D = t.as_tensor(self.wf.D.copy(), device='cuda')
+            chi = D.T @ self.psi
+            K = t.zeros((n, self.N), dtype=t.float64, device='cuda')
             for s in range(n):
                 for v in range(s + 1):
-                    aux[INDEX(s, v)] = self.ops.coulomb(self.psi[s] * self.psi[v])
-            D = self.wf.D
-            K = t.zeros((n, self.N), dtype=t.float64, device='cuda')
-            for j in range(n):
-                for k in range(n):
-                    for l in range(n):
-                        K[j] += self.psi[k] * aux[INDEX(l, j)] * float(D[k, l])
+                    pot = self.ops.coulomb(self.psi[s] * self.psi[v])
+                    K[v] += pot * chi[s]
+                    if s != v:
+                        K[s] += pot * chi[v]
             self.Kpot = K
             E = self.ops.matrix(self.psi, self.Kpot)
             E = t.triu(E) + t.triu(E, 1).T
@@ -261,14 +263,15 @@ class PSIO_BECKE(object):
         Fgrid = Hgrid
         if psi.calculate_2body:
             Jgrid = ext * psi.Jpot
-            pot = {}
+            # K_v = sum_s ext_s V[ext_s ext_v], each pair potential solved once
+            # and used at once (memory O(m N))
+            Kgrid = t.zeros_like(ext)
             for s in range(m):
                 for v in range(s + 1):
-                    pot[(s, v)] = ops.coulomb(ext[s] * ext[v])
-            Kgrid = t.zeros_like(ext)
-            for v in range(m):
-                for s in range(m):
-                    Kgrid[v] += ext[s] * pot[(max(s, v), min(s, v))]
+                    pot = ops.coulomb(ext[s] * ext[v])
+                    Kgrid[v] += ext[s] * pot
+                    if s != v:
+                        Kgrid[s] += ext[v] * pot
             Fgrid = Hgrid + Jgrid - Kgrid
         F = ops.matrix(ext, Fgrid)
         self.asymmetry = float((F - F.T).abs().max())

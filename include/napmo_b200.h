@@ -272,6 +272,10 @@ int napmo_gpu_combine_weights(int npoint, const double *wb, const double *w, dou
 int napmo_gpu_poisson(void *grid, const double *rho, int lmax, double *v, int accumulate,
                       double *raw_y, double *raw_dt, void *stream);
 long napmo_poisson_raw_size(void *grid, int lmax);
+/* k solves in one call: v[j] = V_H[rho[j]], device rows of ld >= grid size (the
+ * orbital-pair densities of exchange, psi_numeric.py:186-215). */
+int napmo_gpu_poisson_many(void *grid, int k, const double *rho, long ld, int lmax, double *v,
+                           void *stream);
 /* Truncation tolerance (a.u.) of the grid's potential evaluation.  No
  * counterpart in nAPMO, whose evaluate.cpp:129-220 sums every (l, m) <= lmax:
  * 0 (the default) does the same; tol > 0 lets each (atom, radial interval)
@@ -347,6 +351,9 @@ int napmo_fock_plan_build(void *plan, const double *D, double q, const double *v
 /* v = V_H[rho] on the plan's grid with the plan's lmax and Poisson tolerance;
  * replaces compute_coulomb (ntwobody.py:15-46) inside an SCF iteration. */
 int napmo_fock_plan_poisson(void *plan, const double *rho, double *v, void *stream);
+/* k such solves in one call on device rows of ld >= npoint doubles. */
+int napmo_fock_plan_poisson_many(void *plan, int k, const double *rho, long ld, double *v,
+                                 void *stream);
 /* Host-buffer twin of napmo_fock_plan_build (copies inside the call). */
 int napmo_fock_plan_build_host(void *plan, const double *D, double q, const double *vext,
                                double *F, void *stream);

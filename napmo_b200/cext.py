@@ -235,6 +235,10 @@ _SIGS = [
     ('napmo_fock_plan_set_precision', c_int, [c_void_p, c_int]),
     ('napmo_fock_plan_set_poisson_tolerance', c_int, [c_void_p, c_double]),
     ('napmo_fock_plan_poisson', c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    ('napmo_fock_plan_poisson_many', c_int, [c_void_p, c_int, c_void_p, c_long, c_void_p,
+                                             c_void_p]),
+    ('napmo_gpu_poisson_many', c_int, [c_void_p, c_int, c_void_p, c_long, c_int, c_void_p,
+                                       c_void_p]),
     ('napmo_fock_plan_screening', c_int, [c_void_p, POINTER(c_void_p), POINTER(c_int)]),
     ('napmo_fock_plan_int8_bytes', c_long, [c_void_p]),
     ('napmo_fock_batch_new', c_void_p, [c_void_p, c_int, c_double]),

@@ -1395,6 +1395,25 @@ int napmo_gpu_operator_matrix(BeckeGrid *g, int n, int m, const double *A, long 
   });
 }
 
+// k Poisson solves on the grid: v[j] = V_H[rho[j]] for device rows of
+// ld >= size doubles, with the grid's truncation tolerance.
+int napmo_gpu_poisson_many(BeckeGrid *g, int k, const double *rho_dev, long ld, int lmax,
+                           double *v_dev, void *stream) {
+  return guarded([&] {
+    NAPMO_REQUIRE(k >= 0 && ld >= g->size, "k < 0 or ld < grid size");
+    cudaStream_t s = (cudaStream_t)stream;
+    PoissonPlan *p = nullptr;
+    int st = grid_poisson_plan(g, lmax, s, &p);
+    if (st) return st;
+    for (int j = 0; j < k; ++j) {
+      st = run_poisson(g, p, rho_dev + (long)j * ld, v_dev + (long)j * ld, false, s,
+                       g->poisson_tol, nullptr, 0);
+      if (st) return st;
+    }
+    return kOk;
+  });
+}
+
 // Truncation tolerance (a.u., >= 0) of the grid's Poisson potential
 // evaluation.  0 (the default) evaluates every (l, m) up to lmax at every
 // pair, as nAPMO's evaluation does (src/horton/evaluate.cpp:129-220).  tol > 0

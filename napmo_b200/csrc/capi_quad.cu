@@ -377,6 +377,27 @@ int napmo_fock_plan_poisson(FockPlan *p, const double *rho_dev, double *v_dev, v
   });
 }
 
+// k Poisson solves on the plan's grid: v[j] = V_H[rho[j]] for device rows of
+// ld >= npoint doubles (the exchange pair densities of an SCF step), in one
+// call: the same kernels as napmo_fock_plan_poisson, without a host round
+// trip per solve.
+int napmo_fock_plan_poisson_many(FockPlan *p, int k, const double *rho_dev, long ld,
+                                 double *v_dev, void *stream) {
+  return guarded([&] {
+    NAPMO_REQUIRE(k >= 0 && ld >= p->grid->size, "k < 0 or ld < grid size");
+    cudaStream_t s = (cudaStream_t)stream;
+    PoissonPlan *pp = nullptr;
+    int e = grid_poisson_plan(p->grid, p->lmax, s, &pp);
+    if (e) return e;
+    for (int j = 0; j < k; ++j) {
+      e = run_poisson(p->grid, pp, rho_dev + (long)j * ld, v_dev + (long)j * ld, false, s,
+                      p->poisson_tol, plan_keep(p), plan_keep_key(p));
+      if (e) return e;
+    }
+    return kOk;
+  });
+}
+
 // One grid Fock build of a species with its own density:
 //   rho = density(D), v = q * V_H[rho] (Becke-Dickson Poisson), and
 //   F = phi diag(wb w (v + vext)) phi^T.

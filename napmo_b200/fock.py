@@ -144,6 +144,16 @@ class FockBuilder(object):
                                                  _stream(t, stream)))
         return v
 
+    def coulomb_potentials(self, rho, stream=None):
+        """V_H of every row of rho (k x npoint) in one library call."""
+        t = self.torch
+        rho = self._dev(rho).reshape(-1, self.npoint).contiguous()
+        v = t.empty_like(rho)
+        checked(cext.lib.napmo_fock_plan_poisson_many(self._plan, rho.shape[0], rho.data_ptr(),
+                                                      self.npoint, v.data_ptr(),
+                                                      _stream(t, stream)))
+        return v
+
     def build(self, D, q=1.0, vext=None, stream=None, out=None):
         """One grid Fock build: returns (F, rho, v) with v = q V_H[rho]."""
         t = self.torch

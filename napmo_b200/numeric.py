@@ -89,6 +89,14 @@ class GridOperators(object):
         coulomb_potential_device(self.grid, rho, self.lmax, v)
         return v
 
+    def coulomb_many(self, rho):
+        """V_H of every row of rho, in one library call."""
+        rho = self.rows(rho)
+        v = self.t.empty_like(rho)
+        checked(cext.lib.napmo_gpu_poisson_many(self.grid._this, rho.shape[0], rho.data_ptr(),
+                                                self.N, self.lmax, v.data_ptr(), self._stream()))
+        return v
+
 
 def _like_input(x, out):
     t = _torch()
@@ -118,10 +126,11 @@ class PSIN(object):
         occupation: occupied orbitals; ndim defaults to it (1 when 0).
         point_charges: [(Z, (x, y, z))] in bohr; pce: their repulsion energy.
         eta, kappa, charge, mass: species constants (electrons 2, -1, -1, 1).
+        size: number of particles (default eta x occupation).
     """
 
     def __init__(self, grid, gbasis, C, O, occupation, point_charges, pce=0.0, ndim=None,
-                 lmax=None, eta=2.0, kappa=-1.0, charge=-1.0, mass=1.0):
+                 lmax=None, eta=2.0, kappa=-1.0, charge=-1.0, mass=1.0, size=None):
         t = self.t = _torch()
         self.ops = GridOperators(grid, lmax)
         self.grid, self.N, self.lmax = grid, grid.size, self.ops.lmax
@@ -142,7 +151,9 @@ class PSIN(object):
         gb = self.ops.rows(gbasis)
         Cd = t.as_tensor(np.asarray(C, dtype=np.float64), device='cuda')
         self.psi = Cd.T @ gb                      # compute_psi_from_cm: row j = sum_k C[k,j] phi_k
-        self.calculate_2body = 2 * self.occupation > 0
+        # two-body terms whenever the species has particles (psi_numeric.py:81-83)
+        size = self.eta * self.occupation if size is None else size
+        self.calculate_2body = size > 0
         self.Jpot = t.zeros(self.N, dtype=t.float64, device='cuda')
         self.Kpot = t.zeros((self.ndim, self.N), dtype=t.float64, device='cuda')
         self.initialize()
@@ -196,11 +207,11 @@ class PSIN(object):
             chi = D.T @ self.psi
             K = t.zeros((n, self.N), dtype=t.float64, device='cuda')
             for s in range(n):
+                pots = self.ops.coulomb_many(self.psi[s] * self.psi[:s + 1])
                 for v in range(s + 1):
-                    pot = self.ops.coulomb(self.psi[s] * self.psi[v])
-                    K[v] += pot * chi[s]
+                    K[v] += pots[v] * chi[s]
                     if s != v:
-                        K[s] += pot * chi[v]
+                        K[s] += pots[v] * chi[v]
             self.Kpot = K
             E = self.ops.matrix(self.psi, self.Kpot)
             E = t.triu(E) + t.triu(E, 1).T
@@ -267,11 +278,11 @@ class PSIO_BECKE(object):
             # and used at once (memory O(m N))
             Kgrid = t.zeros_like(ext)
             for s in range(m):
+                pots = ops.coulomb_many(ext[s] * ext[:s + 1])
                 for v in range(s + 1):
-                    pot = ops.coulomb(ext[s] * ext[v])
-                    Kgrid[v] += ext[s] * pot
+                    Kgrid[v] += ext[s] * pots[v]
                     if s != v:
-                        Kgrid[s] += ext[v] * pot
+                        Kgrid[s] += ext[v] * pots[v]
             Fgrid = Hgrid + Jgrid - Kgrid
         F = ops.matrix(ext, Fgrid)
         self.asymmetry = float((F - F.T).abs().max())

@@ -140,11 +140,10 @@ class GridRHF(object):
         psi = Cocc.T @ phi                                  # nocc x N
         K = t.zeros((self.n, self.n), dtype=t.float64, device='cuda')
         for i in range(psi.shape[0]):
-            wpsi = self.W * psi[i]
-            for nu in range(self.n):
-                v = self.fb.coulomb_potential(psi[i] * phi[nu])
-                self.poisson_solves += 1
-                K[:, nu] += phi @ (wpsi * v)
+            # the n pair densities psi_i phi_nu solved in one call
+            V = self.fb.coulomb_potentials(psi[i] * phi)
+            self.poisson_solves += self.n
+            K += (phi * (self.W * psi[i])) @ V.T
         return 0.5 * (K + K.T)
 
     def fock(self, D, Cocc):
@@ -347,11 +346,9 @@ class GridAPMO(object):
         psi = Cocc.T @ phi
         K = t.zeros((sp.n, sp.n), dtype=t.float64, device='cuda')
         for i in range(psi.shape[0]):
-            wpsi = self.W * psi[i]
-            for nu in range(sp.n):
-                v = sp.fb.coulomb_potential(psi[i] * phi[nu])
-                self.poisson_solves += 1
-                K[:, nu] += phi @ (wpsi * v)
+            V = sp.fb.coulomb_potentials(psi[i] * phi)
+            self.poisson_solves += sp.n
+            K += (phi * (self.W * psi[i])) @ V.T
         return 0.5 * (K + K.T)
 
     def fock(self, De, Dn, Ce=None):

@@ -59,6 +59,9 @@ struct PoissonPlan {
   // between calls: an allocation per call would return to the driver at
   // every synchronisation of the caller's loop
   DevBuf<char> bd_ws;
+  // per-solve tables (projection, splines, amplitudes, pair potentials,
+  // truncation) of batched solves
+  DevBuf<char> batch_ws;
 };
 
 void free_poisson_plan(PoissonPlan *p) { delete p; }
@@ -414,6 +417,63 @@ static cudaError_t launch_operator_matrix(int npoint, int n, int m, const double
   if (n > 65535) return cudaErrorInvalidValue;
   operator_matrix_kernel<<<dim3(m, n), 256, 0, s>>>(npoint, A, lda, B, ldb, wb, w, M, m);
   return cudaGetLastError();
+}
+
+// k solves on the plan's grid (v[j] = V_H[rho[j]], rows ld apart): the
+// projection, radial and evaluation launches each take a batch of solves, whose
+// per-solve tables live in the plan's batch workspace (at most 512 MB; larger
+// k runs in several batches).  Results equal k calls of run_poisson.
+int run_poisson_many(BeckeGrid *g, PoissonPlan *p, int k, const double *rho_dev, long ld,
+                     double *v_dev, cudaStream_t s, double tol, const int *keep,
+                     unsigned long long key) {
+  if (k <= 0) return kOk;
+  int st = select_pair_lists(p, g, keep, key, s);
+  if (st) return st;
+  const PoissonDev &d = p->d;
+  const size_t nd = p->proj.n + p->spl.n + p->amp.n + p->pair_v.n;
+  const size_t per = nd * sizeof(double) + p->lcut.n * sizeof(int);
+  // grid limits: the projection and truncation launches use natom x B blocks
+  // in y/z, the radial one (column chunks, at most 2 lmax + 1) x B
+  long B = std::min<long>(k, (long)((512ull << 20) / std::max<size_t>(per, 1)));
+  B = std::min<long>(B, 65535 / std::max(d.natom, 2 * d.max_lmax + 1));
+  if (B < 2 || !d.items) {
+    for (int j = 0; j < k; ++j) {
+      st = run_poisson(g, p, rho_dev + (long)j * ld, v_dev + (long)j * ld, false, s, tol, keep,
+                       key);
+      if (st) return st;
+    }
+    return kOk;
+  }
+  if (p->batch_ws.n < per * B) {
+    NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "batch workspace");
+    NAPMO_TRY_CUDA(p->batch_ws.alloc(per * B), "batch workspace");
+  }
+  PoissonDev P = d;
+  P.batch_ld = ld;
+  P.proj_stride = (long)p->proj.n;
+  P.spl_stride = (long)p->spl.n;
+  P.amp_stride = (long)p->amp.n;
+  P.pairv_stride = (long)p->pair_v.n;
+  P.lcut_stride = (long)p->lcut.n;
+  double *ws = (double *)p->batch_ws.p;
+  P.proj = ws;
+  P.spl = P.proj + P.proj_stride * B;
+  P.amp = P.spl + P.spl_stride * B;
+  P.pair_v = P.amp + P.amp_stride * B;
+  P.lcut = tol > 0.0 ? (int *)(P.pair_v + P.pairv_stride * B) : nullptr;
+  P.eval_tol = tol;
+  P.raw_y = nullptr;
+  P.raw_dt = nullptr;
+  for (long j0 = 0; j0 < k; j0 += B) {
+    P.nbatch = (int)std::min<long>(B, k - j0);
+    NAPMO_TRY_CUDA(launch_poisson_project(P, rho_dev + j0 * ld, g->dev.wb, g->dev.w, s),
+                   "project");
+    NAPMO_TRY_CUDA(launch_poisson_radial(P, s), "radial solve");
+    NAPMO_TRY_CUDA(launch_poisson_evaluate(P, g->size, g->dev.x, g->dev.y, g->dev.z,
+                                           v_dev + j0 * ld, false, s),
+                   "evaluate");
+  }
+  return kOk;
 }
 
 BeckeGrid::~BeckeGrid() {
@@ -1405,12 +1465,7 @@ int napmo_gpu_poisson_many(BeckeGrid *g, int k, const double *rho_dev, long ld, 
     PoissonPlan *p = nullptr;
     int st = grid_poisson_plan(g, lmax, s, &p);
     if (st) return st;
-    for (int j = 0; j < k; ++j) {
-      st = run_poisson(g, p, rho_dev + (long)j * ld, v_dev + (long)j * ld, false, s,
-                       g->poisson_tol, nullptr, 0);
-      if (st) return st;
-    }
-    return kOk;
+    return run_poisson_many(g, p, k, rho_dev, ld, v_dev, s, g->poisson_tol, nullptr, 0);
   });
 }
 

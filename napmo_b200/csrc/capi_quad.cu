@@ -17,6 +17,9 @@ int grid_poisson_plan(BeckeGrid *g, int lmax, cudaStream_t s, PoissonPlan **out)
 int run_poisson(BeckeGrid *g, PoissonPlan *p, const double *rho_dev, double *v_dev,
                 bool accumulate, cudaStream_t s, double tol, const int *keep,
                 unsigned long long key);
+int run_poisson_many(BeckeGrid *g, PoissonPlan *p, int k, const double *rho_dev, long ld,
+                     double *v_dev, cudaStream_t s, double tol, const int *keep,
+                     unsigned long long key);
 
 // Truncation tolerance (a.u.) of the Poisson potential evaluation that
 // precision 1 selects: each (atom, radial interval) drops l-blocks whose
@@ -379,8 +382,7 @@ int napmo_fock_plan_poisson(FockPlan *p, const double *rho_dev, double *v_dev, v
 
 // k Poisson solves on the plan's grid: v[j] = V_H[rho[j]] for device rows of
 // ld >= npoint doubles (the exchange pair densities of an SCF step), in one
-// call: the same kernels as napmo_fock_plan_poisson, without a host round
-// trip per solve.
+// call: each launch of the pipeline takes a batch of solves.
 int napmo_fock_plan_poisson_many(FockPlan *p, int k, const double *rho_dev, long ld,
                                  double *v_dev, void *stream) {
   return guarded([&] {
@@ -389,12 +391,8 @@ int napmo_fock_plan_poisson_many(FockPlan *p, int k, const double *rho_dev, long
     PoissonPlan *pp = nullptr;
     int e = grid_poisson_plan(p->grid, p->lmax, s, &pp);
     if (e) return e;
-    for (int j = 0; j < k; ++j) {
-      e = run_poisson(p->grid, pp, rho_dev + (long)j * ld, v_dev + (long)j * ld, false, s,
-                      p->poisson_tol, plan_keep(p), plan_keep_key(p));
-      if (e) return e;
-    }
-    return kOk;
+    return run_poisson_many(p->grid, pp, k, rho_dev, ld, v_dev, s, p->poisson_tol,
+                            plan_keep(p), plan_keep_key(p));
   });
 }
 

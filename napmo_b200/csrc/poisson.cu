@@ -120,7 +120,10 @@ project_kernel(PoissonDev P, const double *__restrict__ rho,
                const double *__restrict__ wb, const double *__restrict__ w) {
   __shared__ double gs[kProjK][kProjTile + 1];  // [j][shell]
   __shared__ __align__(16) double ys[kProjK][kProjTile];  // [j][lm]
-  const PoissonAtom at = P.atoms[blockIdx.z];
+  const int bat = blockIdx.z / P.natom;  // solve of a batch
+  const PoissonAtom at = P.atoms[blockIdx.z - bat * P.natom];
+  rho += bat * P.batch_ld;
+  double *proj = P.proj + bat * P.proj_stride;
   const int lsize = (at.lmax + 1) * (at.lmax + 1);
   const int lm0 = blockIdx.x * kProjTile, s0 = blockIdx.y * kProjTile;
   if (lm0 >= lsize || s0 >= at.nrad) return;
@@ -179,7 +182,7 @@ project_kernel(PoissonDev P, const double *__restrict__ rho,
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int sh = s0 + ty * 4 + i;
-      if (sh < at.nrad) P.proj[at.proj_off + (long)sh * lsize + lm] = acc[i][k] / sigma[sh] * fac;
+      if (sh < at.nrad) proj[at.proj_off + (long)sh * lsize + lm] = acc[i][k] / sigma[sh] * fac;
     }
   }
 }
@@ -358,7 +361,11 @@ __global__ void radial_kernel(PoissonDev P, int ncol, RadialOp op) {
   const int l = P.sys_l[sys];
   const int n = at.nrad, n2 = 2 * n;
   const int lsize = (at.lmax + 1) * (at.lmax + 1);
-  const int c0 = blockIdx.y * ncol;  // first column (m index) of this chunk
+  const int nchunk = gridDim.y / P.nbatch;
+  const int bat = blockIdx.y / nchunk;  // solve of a batch
+  const int c0 = (blockIdx.y - bat * nchunk) * ncol;  // first column (m index) of this chunk
+  double *const spl = P.spl + bat * P.spl_stride;
+  double *const amp = P.amp + bat * P.amp_stride;
   if (c0 >= 2 * l + 1) return;
   const int nm = min(ncol, 2 * l + 1 - c0);  // columns of this chunk
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -387,7 +394,7 @@ __global__ void radial_kernel(PoissonDev P, int ncol, RadialOp op) {
       rl[i] = pow(r[i], (double)l);
       rm[i] = pow(r[i], (double)(-l - 1));
     }
-    const double *proj = P.proj + at.proj_off + l * l + c0;
+    const double *proj = P.proj + bat * P.proj_stride + at.proj_off + l * l + c0;
     for (int e = tid; e < n * nm; e += nt) {
       const int i = e / nm, c = e - i * nm;
       Y[i * ncol + c] = proj[(long)i * lsize + c];
@@ -511,7 +518,7 @@ __global__ void radial_kernel(PoissonDev P, int ncol, RadialOp op) {
     const double d0 = (R[(2 * j + 1) * ncol + c] / j1[j]) * j1[j];
     const double d1 = (R[(2 * j + 3) * ncol + c] / j1[j + 1]) * j1[j + 1];
     const double z = y1 - y0;
-    double *cf = P.spl + at.spl_off + ((long)j * lsize + l * l + c0 + c) * 4;
+    double *cf = spl + at.spl_off + ((long)j * lsize + l * l + c0 + c) * 4;
     cf[0] = y0 * fl;
     cf[1] = d0 * fl;
     cf[2] = (3 * z - 2 * d0 - d1) * fl;
@@ -519,8 +526,8 @@ __global__ void radial_kernel(PoissonDev P, int ncol, RadialOp op) {
   }
   for (int c = tid; c < nm; c += nt) {
     const int lm = l * l + c0 + c;
-    P.amp[at.amp_off + lm * 2 + 0] = R[c] / pow(at.first_x, (double)l) * fl;
-    P.amp[at.amp_off + lm * 2 + 1] = R[(2 * (n - 1)) * ncol + c] * pow(at.last_x, (double)(l + 1)) * fl;
+    amp[at.amp_off + lm * 2 + 0] = R[c] / pow(at.first_x, (double)l) * fl;
+    amp[at.amp_off + lm * 2 + 1] = R[(2 * (n - 1)) * ncol + c] * pow(at.last_x, (double)(l + 1)) * fl;
   }
 }
 
@@ -908,7 +915,10 @@ __device__ __forceinline__ void pair_values(const double *cf, int lmaxA, const d
 // one warp: lane l bounds block l.
 __global__ void __launch_bounds__(32) bucket_lcut_kernel(PoissonDev P) {
   __shared__ double bound[32];
-  const PoissonAtom &at = P.atoms[blockIdx.y];
+  const int bat = blockIdx.y / P.natom;  // solve of a batch
+  const PoissonAtom &at = P.atoms[blockIdx.y - bat * P.natom];
+  const double *const spl = P.spl + bat * P.spl_stride;
+  const double *const amp = P.amp + bat * P.amp_stride;
   const int b = blockIdx.x, l = threadIdx.x;
   if (b > at.nrad) return;
   const int lmaxA = at.lmax;
@@ -919,10 +929,10 @@ __global__ void __launch_bounds__(32) bucket_lcut_kernel(PoissonDev P) {
     for (int lm = l * l; lm < (l + 1) * (l + 1); ++lm) {
       double c;
       if (region == 0) {
-        const double *cf = P.spl + at.spl_off + ((long)(b - 1) * lsize + lm) * 4;
+        const double *cf = spl + at.spl_off + ((long)(b - 1) * lsize + lm) * 4;
         c = fabs(cf[0]) + fabs(cf[1]) + fabs(cf[2]) + fabs(cf[3]);
       } else {
-        c = fabs(P.amp[at.amp_off + lm * 2 + (region == 1 ? 0 : 1)]);
+        c = fabs(amp[at.amp_off + lm * 2 + (region == 1 ? 0 : 1)]);
       }
       s2 = fma(c, c, s2);
     }
@@ -936,13 +946,16 @@ __global__ void __launch_bounds__(32) bucket_lcut_kernel(PoissonDev P) {
     double dropped = 0.0;
     int L = lmaxA;
     while (L > 0 && dropped + bound[L] <= P.eval_tol) dropped += bound[L--];
-    P.lcut[at.bucket_off + b] = L;
+    P.lcut[bat * P.lcut_stride + at.bucket_off + b] = L;
   }
 }
 
 // TAILS = false: the interior items [0, nitems_inner) (region 0 only, so the
 // kernel carries that region's code alone); true: the others.
-template <int LMAX, bool TAILS>
+// BATCH: the launch evaluates several solves (blockIdx.y); the single-solve
+// instance carries no batch offsets (its registers, and occupancy, stay those
+// the recursion was tuned at)
+template <int LMAX, bool TAILS, bool BATCH>
 __global__ void __launch_bounds__(kEvalChunk / kEvalPerThread)
 eval_pairs_kernel(PoissonDev P, const double *__restrict__ gx,
                   const double *__restrict__ gy, const double *__restrict__ gz) {
@@ -952,15 +965,17 @@ eval_pairs_kernel(PoissonDev P, const double *__restrict__ gx,
   const int lmaxA = at.lmax;
   const int lsize = (lmaxA + 1) * (lmaxA + 1);
   const int region = TAILS ? (it.bucket == 0 ? 1 : 2) : 0;
+  const long bat = BATCH ? (long)blockIdx.y : 0;  // solve of a batch
   // l-blocks kept for this bucket (all unless a truncation tolerance is set)
-  const int lcut = P.lcut ? P.lcut[at.bucket_off + it.bucket] : lmaxA;
+  const int lcut = P.lcut ? P.lcut[bat * P.lcut_stride + at.bucket_off + it.bucket] : lmaxA;
   const int lkeep = (lcut + 1) * (lcut + 1);
   // staged with the recursion's scale gamma_lm (see c_rec_gamma)
   if (region == 0) {
-    const double *src = P.spl + at.spl_off + (long)(it.bucket - 1) * lsize * 4;
+    const double *src =
+        P.spl + bat * P.spl_stride + at.spl_off + (long)(it.bucket - 1) * lsize * 4;
     for (int e = threadIdx.x; e < lkeep * 4; e += blockDim.x) cf[e] = src[e] * c_rec_gamma[e >> 2];
   } else {
-    const double *src = P.amp + at.amp_off;
+    const double *src = P.amp + bat * P.amp_stride + at.amp_off;
     for (int e = threadIdx.x; e < lkeep; e += blockDim.x)
       cf[e] = src[2 * e + (region == 1 ? 0 : 1)] * c_rec_gamma[e];
   }
@@ -994,7 +1009,8 @@ eval_pairs_kernel(PoissonDev P, const double *__restrict__ gx,
 #pragma unroll
   for (int j = 0; j < kEvalPerThread; ++j) {
     const int e = t + j * (int)blockDim.x;
-    if (e < it.count) P.pair_v[at.pair_off + (pidx[j] - at.mol_point_start)] = v[j];
+    if (e < it.count)
+      P.pair_v[bat * P.pairv_stride + at.pair_off + (pidx[j] - at.mol_point_start)] = v[j];
   }
 }
 
@@ -1003,6 +1019,9 @@ __global__ void pairs_reduce_kernel(PoissonDev P, int npoint, double *__restrict
                                     int accumulate) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npoint) return;
+  const int bat = blockIdx.y;  // solve of a batch
+  out += bat * P.batch_ld;
+  const double *pair_v = P.pair_v + bat * P.pairv_stride;
   if (P.keep && !P.keep[p]) {  // screened-out point: no potential evaluated
     if (!accumulate) out[p] = 0.0;
     return;
@@ -1020,7 +1039,7 @@ __global__ void pairs_reduce_kernel(PoissonDev P, int npoint, double *__restrict
   const int a1 = P.mol_atom_off[mol + 1];
   for (int A = P.mol_atom_off[mol]; A < a1; ++A) {
     const PoissonAtom &at = P.atoms[A];
-    v += P.pair_v[at.pair_off + (p - at.mol_point_start)];
+    v += pair_v[at.pair_off + (p - at.mol_point_start)];
   }
   out[p] = v;
 }
@@ -1031,22 +1050,32 @@ cudaError_t launch_eval_l(const PoissonDev &P, int npoint, const double *x,
                           cudaStream_t s) {
   if (P.items && P.nitems > 0) {
     if (P.lcut) {
-      bucket_lcut_kernel<<<dim3(P.max_nrad + 1, P.natom), 32, 0, s>>>(P);
+      bucket_lcut_kernel<<<dim3(P.max_nrad + 1, P.natom * P.nbatch), 32, 0, s>>>(P);
       cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) return e;
     }
     const size_t smem = (size_t)(L + 1) * (L + 1) * 4 * sizeof(double);
-    if (P.nitems_inner > 0)
-      eval_pairs_kernel<L, false><<<P.nitems_inner, kEvalChunk / kEvalPerThread, smem, s>>>(
-          P, x, y, z);
-    if (P.nitems > P.nitems_inner)
-      eval_pairs_kernel<L, true>
-          <<<P.nitems - P.nitems_inner, kEvalChunk / kEvalPerThread, smem, s>>>(P, x, y, z);
+    const dim3 gin(P.nitems_inner, P.nbatch), gtail(P.nitems - P.nitems_inner, P.nbatch);
+    constexpr int kT = kEvalChunk / kEvalPerThread;
+    if (P.nitems_inner > 0) {
+      if (P.nbatch > 1)
+        eval_pairs_kernel<L, false, true><<<gin, kT, smem, s>>>(P, x, y, z);
+      else
+        eval_pairs_kernel<L, false, false><<<gin, kT, smem, s>>>(P, x, y, z);
+    }
+    if (P.nitems > P.nitems_inner) {
+      if (P.nbatch > 1)
+        eval_pairs_kernel<L, true, true><<<gtail, kT, smem, s>>>(P, x, y, z);
+      else
+        eval_pairs_kernel<L, true, false><<<gtail, kT, smem, s>>>(P, x, y, z);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    pairs_reduce_kernel<<<(npoint + 255) / 256, 256, 0, s>>>(P, npoint, out, acc);
+    pairs_reduce_kernel<<<dim3((npoint + 255) / 256, P.nbatch), 256, 0, s>>>(P, npoint, out,
+                                                                             acc);
     return cudaGetLastError();
   }
+  if (P.nbatch != 1) return cudaErrorInvalidValue;  // batches need the pair lists
   evaluate_kernel<L><<<(npoint + 127) / 128, 128, 0, s>>>(P, npoint, x, y, z, out, acc);
   return cudaGetLastError();
 }
@@ -1135,7 +1164,7 @@ cudaError_t launch_poisson_project(const PoissonDev &P, const double *rho,
   if (P.natom == 0) return cudaSuccess;
   const int lsize = (P.max_lmax + 1) * (P.max_lmax + 1);
   dim3 grid((lsize + kProjTile - 1) / kProjTile, (P.max_nrad + kProjTile - 1) / kProjTile,
-            P.natom);
+            P.natom * P.nbatch);
   project_kernel<<<grid, kProjThreads, 0, s>>>(P, rho, wb, w);
   return cudaGetLastError();
 }
@@ -1192,7 +1221,7 @@ cudaError_t launch_radial_solve(const PoissonDev &P, const RadialOp &op, cudaStr
   const int nchunk = (2 * P.max_lmax + 1 + ncol - 1) / ncol;
   // 4 warps: the per-column chains (spline, substitutions) use the first, the
   // row-parallel stages (right-hand side, outputs, staging) all four
-  radial_kernel<<<dim3(P.nsys, nchunk), 128, smem, s>>>(P, ncol, op);
+  radial_kernel<<<dim3(P.nsys, nchunk * P.nbatch), 128, smem, s>>>(P, ncol, op);
   return cudaGetLastError();
 }
 

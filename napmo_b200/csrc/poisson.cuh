@@ -92,6 +92,12 @@ struct PoissonDev {
   // Point screening: with keep set, only points with keep[p] != 0 have pairs
   // (the pair lists were built with the same flags) and the others get v = 0.
   const int *keep = nullptr;
+  // Batched solves: nbatch densities batch_ld points apart, solved by the same
+  // launches (project, radial, evaluate); each solve's tables lie *_stride
+  // doubles (ints for lcut) apart.  nbatch = 1: one solve, strides unused.
+  int nbatch = 1;
+  long batch_ld = 0;
+  long proj_stride = 0, spl_stride = 0, amp_stride = 0, lcut_stride = 0, pairv_stride = 0;
 };
 
 // Radial stage of the pipeline.  The default is the Poisson equation

@@ -762,6 +762,34 @@ def main():
     if args.impl == 'reference':
         if rank != 0:
             return
+        why = {'c1': 'nAPMO runs this SCF only through libint (analytic drivers), absent here',
+               'c2': 'nAPMO runs this SCF only through libint (analytic drivers), absent here',
+               'c3': 'nAPMO has no batched multi-molecule build; its per-build CPU cost is the '
+                     'c4 reference arm',
+               'c5': 'nAPMO computes no nuclear-coordinate gradients'}
+        if args.workload in why:
+            print(json.dumps({'impl': 'reference', 'workload': args.workload,
+                              'unavailable': why[args.workload]}))
+            return
+        if args.workload == 'c7':
+            from napmo_b200.system import alkane_geometry, build_system
+            ms = build_system(alkane_geometry(20), 'CC-PVDZ')
+            vals, cb = [], None
+            for _ in range(args.warmup + args.steps):
+                cb = c7_cpu_baseline(ms)
+                vals.append(cb['value'])
+            v = statistics.median(vals[args.warmup:])
+            cb['value'] = v
+            print(json.dumps({
+                'impl': 'reference', 'metric': 'one-electron integrals S, T, V of C20H42/cc-pVDZ (C7)',
+                'value': v, 'unit': 's per S,T,V', 'n_gpus': 1, 'steps': args.steps,
+                'warmup': args.warmup, 'ms_per_step': v * 1e3, 'higher_is_better': False,
+                'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+                'config': {'workload': C7_WORKLOAD, 'parallelism': 'host, one thread'},
+                'cpu_baseline': cb,
+                'e2e': {'value': v, 'unit': 's per S,T,V', 'h2d_bytes_per_step': 0,
+                        'd2h_bytes_per_step': 0}}))
+            return
         if args.workload == 'c6':
             vals, cb = [], None
             for _ in range(args.warmup + args.steps):

@@ -35,6 +35,12 @@ struct FuncTable {
   const double *origin = nullptr; // [n][3]
 };
 
+// 1 / (2j + 1) for j < kInvOdd: the series and the downward recursion below
+// multiply by these instead of dividing (one FP64 division per series term
+// would dominate the kernel)
+constexpr int kInvOdd = 320;
+__device__ double g_inv_odd[kInvOdd];
+
 // Boys function F_m(T) for m = 0..mmax.  T < 35: the series at mmax,
 //   F_m(T) = e^-T sum_k (2T)^k / ((2m+1)(2m+3)...(2m+2k+1))
 // (all terms positive), then the downward recursion
@@ -44,14 +50,15 @@ struct FuncTable {
 __device__ void boys(int mmax, double T, double *F) {
   const double e = exp(-T);
   if (T < 35.0) {
-    double term = 1.0 / (2 * mmax + 1), sum = term;
-    for (int k = 1; k < 256; ++k) {
-      term *= 2.0 * T / (2 * mmax + 2 * k + 1);
+    const double t2 = 2.0 * T;
+    double term = __ldg(&g_inv_odd[mmax]), sum = term;
+    for (int k = 1; k < 256; ++k) {  // mmax + k < 8 + 256 <= kInvOdd
+      term *= t2 * __ldg(&g_inv_odd[mmax + k]);
       sum += term;
       if (term < 1e-17 * sum) break;
     }
     F[mmax] = e * sum;
-    for (int m = mmax - 1; m >= 0; --m) F[m] = (2.0 * T * F[m + 1] + e) / (2 * m + 1);
+    for (int m = mmax - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * __ldg(&g_inv_odd[m]);
   } else {
     F[0] = 0.5 * sqrt(M_PI / T) * erf(sqrt(T));
     for (int m = 0; m < mmax; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) / (2.0 * T);
@@ -201,6 +208,108 @@ one_body_kernel(FuncTable B, int nq, const double *__restrict__ q, double *__res
   if (V) V[mu * n + nu] = V[nu * n + mu] = v_acc;
 }
 
+// The same integrals with one warp per contracted pair: the primitive loops
+// run in step across the warp and the lanes share the point charges, then
+// one shuffle reduction (the thread-per-pair kernel diverges on the
+// primitive counts and angular momenta of neighbouring pairs; with many
+// charges this mapping keeps the lanes busy).
+template <int L>
+__global__ void __launch_bounds__(128)
+one_body_warp_kernel(FuncTable B, int nq, const double *__restrict__ q, double *__restrict__ S,
+                     double *__restrict__ T, double *__restrict__ V, long npair) {
+  const long e = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // one pair per warp
+  const int lane = threadIdx.x & 31;
+  if (e >= npair) return;
+  int mu = (int)((sqrt(8.0 * (double)e + 1.0) - 1.0) * 0.5);
+  while ((long)mu * (mu + 1) / 2 > e) --mu;
+  while ((long)(mu + 1) * (mu + 2) / 2 <= e) ++mu;
+  const int nu = (int)(e - (long)mu * (mu + 1) / 2);
+  int la[3], lb[3];
+  double A[3], Bc[3];
+  for (int d = 0; d < 3; ++d) {
+    la[d] = B.l[mu * 3 + d];
+    lb[d] = B.l[nu * 3 + d];
+    A[d] = B.origin[mu * 3 + d];
+    Bc[d] = B.origin[nu * 3 + d];
+  }
+  const int Lx = la[0] + lb[0], Ly = la[1] + lb[1], Lz = la[2] + lb[2];
+  const int Lt = Lx + Ly + Lz;
+  const int ny = Ly + 1, nz = Lz + 1, nxyz = (Lx + 1) * ny * nz;
+  const bool fits = (Lt + 1) * nxyz <= RSize<L>::value;
+  double s_acc = 0.0, t_acc = 0.0, v_acc = fits ? 0.0 : nan("");
+  double AB2 = 0.0;
+  for (int d = 0; d < 3; ++d) AB2 += (A[d] - Bc[d]) * (A[d] - Bc[d]);
+  for (int kp = B.start[mu]; kp < B.start[mu + 1]; ++kp) {
+    const double a = B.zeta[kp];
+    for (int lp = B.start[nu]; lp < B.start[nu + 1]; ++lp) {
+      const double b = B.zeta[lp];
+      const double p = a + b, oo2p = 0.5 / p;
+      const double cc = B.coef[kp] * B.coef[lp] * exp(-a * b / p * AB2);
+      const double sq = sqrt(M_PI / p);
+      double Et[3][2 * L + 1], P[3], Sd[3], Td[3];
+      for (int d = 0; d < 3; ++d) {
+        P[d] = (a * A[d] + b * Bc[d]) / p;
+        double s0, sp2, sm2;
+        hermite_dir<L>(la[d], lb[d], P[d] - A[d], P[d] - Bc[d], oo2p, Et[d], s0, sp2, sm2);
+        const int j = lb[d];
+        Sd[d] = sq * s0;
+        Td[d] = sq * (-2.0 * b * b * sp2 + b * (2 * j + 1) * s0 - 0.5 * j * (j - 1) * sm2);
+      }
+      s_acc += cc * Sd[0] * Sd[1] * Sd[2];
+      t_acc += cc * (Td[0] * Sd[1] * Sd[2] + Sd[0] * Td[1] * Sd[2] + Sd[0] * Sd[1] * Td[2]);
+      if (!V || !fits) continue;
+      double sum_c = 0.0;
+      for (int c = lane; c < nq; c += 32) {
+        const double X = P[0] - q[c * 4 + 0], Y = P[1] - q[c * 4 + 1], Z = P[2] - q[c * 4 + 2];
+        double F[2 * L + 1];
+        boys(Lt, p * (X * X + Y * Y + Z * Z), F);
+        double R[RSize<L>::value];
+        auto at = [&](int n, int t, int u, int v) { return ((n * (Lx + 1) + t) * ny + u) * nz + v; };
+        double m2p = 1.0;
+        for (int n = 0; n <= Lt; ++n) {
+          R[at(n, 0, 0, 0)] = m2p * F[n];
+          m2p *= -2.0 * p;
+        }
+        for (int sum = 1; sum <= Lt; ++sum)
+          for (int t = 0; t <= min(sum, Lx); ++t)
+            for (int u = 0; u <= min(sum - t, Ly); ++u) {
+              const int v = sum - t - u;
+              if (v > Lz) continue;
+              for (int n = 0; n <= Lt - sum; ++n) {
+                double r;
+                if (t > 0)
+                  r = X * R[at(n + 1, t - 1, u, v)] +
+                      (t > 1 ? (t - 1) * R[at(n + 1, t - 2, u, v)] : 0.0);
+                else if (u > 0)
+                  r = Y * R[at(n + 1, t, u - 1, v)] +
+                      (u > 1 ? (u - 1) * R[at(n + 1, t, u - 2, v)] : 0.0);
+                else
+                  r = Z * R[at(n + 1, t, u, v - 1)] +
+                      (v > 1 ? (v - 1) * R[at(n + 1, t, u, v - 2)] : 0.0);
+                R[at(n, t, u, v)] = r;
+              }
+            }
+        double acc = 0.0;
+        for (int t = 0; t <= Lx; ++t)
+          for (int u = 0; u <= Ly; ++u)
+            for (int v = 0; v <= Lz; ++v)
+              acc += Et[0][t] * Et[1][u] * Et[2][v] * R[at(0, t, u, v)];
+        sum_c += q[c * 4 + 3] * acc;
+      }
+      v_acc -= cc * (2.0 * M_PI / p) * sum_c;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) v_acc += __shfl_down_sync(0xffffffffu, v_acc, o);
+  if (lane != 0) return;
+  const long n = B.n;
+  if (S) S[mu * n + nu] = S[nu * n + mu] = s_acc;
+  if (T) T[mu * n + nu] = T[nu * n + mu] = t_acc;
+  if (V) V[mu * n + nu] = V[nu * n + mu] = v_acc;
+}
+
+// Point charges from which the warp-per-pair kernel is used.
+constexpr int kWarpCharges = 16;
+
 // Host image of a FuncTable.
 struct HostFuncs {
   std::vector<int> start{0}, l;
@@ -231,6 +340,17 @@ int one_body_device(const HostFuncs &h, int nq, const double *charges, double *S
   if (n == 0) return kOk;
   if (h.max_l > 3)
     return set_error(kNotSupported, "one-electron integrals support functions up to f");
+  {
+    static thread_local int done_dev = -1;
+    int dev = 0;
+    NAPMO_TRY_CUDA(cudaGetDevice(&dev), "device");
+    if (done_dev != dev) {
+      double inv[kInvOdd];
+      for (int j = 0; j < kInvOdd; ++j) inv[j] = 1.0 / (2 * j + 1);
+      NAPMO_TRY_CUDA(cudaMemcpyToSymbol(g_inv_odd, inv, sizeof(inv)), "Boys tables");
+      done_dev = dev;
+    }
+  }
   const size_t np = h.zeta.size();
   const size_t bytes = (h.start.size() + h.l.size()) * sizeof(int) +
                        (2 * np + h.origin.size() + 4 * (size_t)nq) * sizeof(double) + 64;
@@ -260,11 +380,19 @@ int one_body_device(const HostFuncs &h, int nq, const double *charges, double *S
     B.l = dl;
     B.origin = dor;
     const long npair = (long)n * (n + 1) / 2;
-    const unsigned grid = (unsigned)((npair + 127) / 128);
-    if (h.max_l <= 2)
-      one_body_kernel<2><<<grid, 128, 0, s>>>(B, nq, dq, S, T, V, npair);
-    else
-      one_body_kernel<3><<<grid, 128, 0, s>>>(B, nq, dq, S, T, V, npair);
+    if (V && nq >= kWarpCharges) {  // many charges: one warp per pair
+      const unsigned grid = (unsigned)((npair + 3) / 4);
+      if (h.max_l <= 2)
+        one_body_warp_kernel<2><<<grid, 128, 0, s>>>(B, nq, dq, S, T, V, npair);
+      else
+        one_body_warp_kernel<3><<<grid, 128, 0, s>>>(B, nq, dq, S, T, V, npair);
+    } else {
+      const unsigned grid = (unsigned)((npair + 127) / 128);
+      if (h.max_l <= 2)
+        one_body_kernel<2><<<grid, 128, 0, s>>>(B, nq, dq, S, T, V, npair);
+      else
+        one_body_kernel<3><<<grid, 128, 0, s>>>(B, nq, dq, S, T, V, npair);
+    }
     e = cudaGetLastError();
   }
   // the host images must outlive the copies

@@ -147,3 +147,22 @@ def test_f_functions_match_oracle():
     assert S.shape == (40, 40)
     for dev, ref in ((S, So), (T, To), (V, Vo)):
         assert np.abs(dev - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_many_charges_warp_kernel(library):
+    """40 point charges (the warp-per-pair instance, used from 16 charges):
+    V against the oracle to 1e-12 of its largest entry, S and T bit for bit
+    those of the thread-per-pair instance."""
+    import ints as I
+    import oracle as O
+    from napmo_b200.system import build_system
+    ms = build_system(H2O, 'CC-PVDZ')
+    rng = np.random.default_rng(11)
+    charges = [(float(rng.uniform(0.1, 1.0)), rng.normal(scale=2.0, size=3)) for _ in range(40)]
+    S, T, V = _device(ms['e-']['basis'], charges)
+    S3, T3, _ = _device(ms['e-']['basis'], charges[:3])
+    assert np.array_equal(S, S3) and np.array_equal(T, T3)
+    cs = [np.array(x) / BOHR for _, x in H2O]
+    fb = O.flat_basis(cs, [s for s, _ in H2O], library, 'CC-PVDZ')
+    _, _, Vo = I.one_body(fb, charges)
+    assert np.abs(V - Vo).max() <= 1e-12 * np.abs(Vo).max()

@@ -4,7 +4,10 @@ Drop-in for ``napmo.grids`` / ``napmo.gto`` and the grid quadrature entry
 points of ``libnapmo.so``: Becke partition weights, contracted GTOs and
 gradients on grid points, rho = phi^T D phi, F = phi^T diag(w v) phi, and the
 Lebedev-projected radial Poisson solve, all as sm_100a CUDA kernels behind
-nAPMO's C-ABI.  Loading fails if ``lib/libnapmo.so`` has not been built.
+nAPMO's C-ABI; with nAPMO's numerical-orbital operators (``compute_kinetic``,
+``compute_dpsi``, ``PSIN``, ``PSIO_BECKE``), local functionals and the
+one-electron integrals of its libint interface.  Loading fails if
+``lib/libnapmo.so`` has not been built.
 """
 from . import cext
 from .cext import NapmoError
@@ -18,5 +21,6 @@ from .system import BOHR_TO_ANGSTROM, MolecularSystem
 from .wavefunction import WaveFunction, compute_coulomb, compute_nuclear
 from .fock import FockBatch, FockBuilder
 from .functional import Functional, epc17_2, isc_functional_selector
+from .numeric import PSIN, PSIO_BECKE, GridOperators, compute_dpsi, compute_kinetic
 
 ANGSTROM_TO_BOHR = 1.889726133921252

@@ -76,3 +76,18 @@ def test_libint_interface_bookkeeping():
                                                  np.asarray(pc['origin'], np.float64))
     assert cext.lib.LibintInterface_get_nbasis(lint) == 25
     cext.lib.LibintInterface_del(lint)
+
+
+def test_oracle_translation_invariance(library):
+    """S and T of a molecule do not change when it moves; V does not change
+    when the charges move with it."""
+    import ints as I
+    import oracle as O
+    cs = [np.array(x) / BOHR for _, x in H2O]
+    shift = np.array([0.7, -1.3, 2.1])
+    out = []
+    for c in (cs, [x + shift for x in cs]):
+        fb = O.flat_basis(c, [s for s, _ in H2O], library, 'STO-3G')
+        out.append(I.one_body(fb, [(Z, x) for Z, x in zip([8.0, 1.0, 1.0], c)]))
+    for a, b in zip(*out):
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max()

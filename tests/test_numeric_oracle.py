@@ -79,3 +79,28 @@ def test_oracle_becke_he_reproduces_napmo_grid_energy(elements, basis_library, k
     vnuc = 2.0 / np.sqrt((g.points ** 2).sum(1))
     hist = N.becke_scf(g, phi, [-0.876036], vnuc, 8)
     assert abs(hist[-1] - known['becke_He_sto3g_300x110_grid_energy']) <= 1e-8
+
+
+def test_oracle_dpsi_and_kinetic_are_linear(elements):
+    """Size-independent properties of the restated operators: the kinetic
+    image is linear in psi, and with de = 0 the Becke-Dickson correction is
+    linear in the residual (the radial equation's operator depends on the
+    orbital energy and the potential only)."""
+    import numeric as N
+    import oracle as O
+    g = O.Grid([np.zeros(3), np.array([0.0, 0.0, 1.5])],
+               [elements['H']['atomic_radii']] * 2, 24, 26)
+    r2a = (g.points ** 2).sum(1)
+    r2b = ((g.points - np.array([0.0, 0.0, 1.5])) ** 2).sum(1)
+    f1, f2 = np.exp(-1.1 * r2a), g.points[:, 2] * np.exp(-0.7 * r2b)
+    k1, k2 = N.compute_kinetic(g, f1, 3), N.compute_kinetic(g, f2, 3)
+    k12 = N.compute_kinetic(g, 0.3 * f1 - 1.7 * f2, 3)
+    # the finite-difference Laplacian turns the rounding of the combination
+    # (1e-16) into ~1e-10 of the maximum at the innermost radial points
+    assert np.abs(k12 - (0.3 * k1 - 1.7 * k2)).max() <= 1e-9 * np.abs(k12).max()
+    phi = f1 + f2
+    vt = -phi * (1.0 / np.sqrt(r2a) + 1.0 / np.sqrt(r2b))
+    d1 = N.compute_dpsi(g, 3, phi, 0.0, -0.6, 0.2 * f1, vt, 1.0)
+    d2 = N.compute_dpsi(g, 3, phi, 0.0, -0.6, 0.5 * f2, vt, 1.0)
+    d12 = N.compute_dpsi(g, 3, phi, 0.0, -0.6, 0.2 * f1 + 0.5 * f2, vt, 1.0)
+    assert np.abs(d12 - (d1 + d2)).max() <= 1e-10 * np.abs(d12).max()

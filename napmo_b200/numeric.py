@@ -235,6 +235,16 @@ class PSIN(object):
     def energy(self):
         return self.wf.energy
 
+    def get_operator_matrix(self, Operator):
+        """M[i][j] = integral psi_i Operator_j over the grid, for the rows
+        Operator_j = O psi_j (psi_numeric.py:406-424)."""
+        return self.ops.matrix(self.psi, Operator)
+
+    def compute_overlap(self):
+        """S of the current orbitals (psi_numeric.py:125-133)."""
+        self.S = self.ops.matrix(self.psi, self.psi)
+        return self.S
+
     # ---------------------------------------------------------- optimiser
     def optimize_psi(self):
         self.psi = self.optimizer.optimize(self)[:self.ndim]

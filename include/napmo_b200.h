@@ -166,25 +166,25 @@ void eval_decomposition_grid(void **splines, double *center, double *output, dou
                              void *cell, long nspline, long npoint); /* evaluate.h:43 (GPU) */
 
 /* ---- Gaussian basis: src/system/{gto,basis_set}.h */
-void *PrimitiveGaussian_new(int *l, double *A, double zeta, double coeff); /* gto.h:99 */
+void *PrimitiveGaussian_new(int *l, double *A, double zeta, double coeff); /* gto.h:112 */
 void PrimitiveGaussian_del(void *p);
-void PrimitiveGaussian_get_l(void *p, int *l);                   /* gto.h:102 */
-void PrimitiveGaussian_get_origin(void *p, double *A);           /* gto.h:104 */
-void PrimitiveGaussian_compute(void *p, double *r, double *out, int size); /* gto.h:106 (GPU) */
-void PrimitiveGaussian_deriv(void *p, double *r, double *out, int size);   /* gto.h:109 (GPU) */
-double PrimitiveGaussian_overlap(void *p, void *q);              /* gto.h:112 */
-double PrimitiveGaussian_get_zeta(void *p);                      /* gto.h:114 */
-double PrimitiveGaussian_get_coeff(void *p);                     /* gto.h:116 */
-double PrimitiveGaussian_get_norma(void *p);                     /* gto.h:118 */
-void *ContractedGaussian_new(void **prims, int n);               /* gto.h:185 */
+void PrimitiveGaussian_get_l(void *p, int *l);                   /* gto.h:115 */
+void PrimitiveGaussian_get_origin(void *p, double *A);           /* gto.h:117 */
+void PrimitiveGaussian_compute(void *p, double *r, double *out, int size); /* gto.h:119 (GPU) */
+void PrimitiveGaussian_deriv(void *p, double *r, double *out, int size);   /* gto.h:122 (GPU) */
+double PrimitiveGaussian_overlap(void *p, void *q);              /* gto.h:125 */
+double PrimitiveGaussian_get_zeta(void *p);                      /* gto.h:127 */
+double PrimitiveGaussian_get_coeff(void *p);                     /* gto.h:129 */
+double PrimitiveGaussian_get_norma(void *p);                     /* gto.h:131 */
+void *ContractedGaussian_new(void **prims, int n);               /* gto.h:200 */
 void ContractedGaussian_del(void *c);
-int ContractedGaussian_get_nprim(void *c);                       /* gto.h:188 */
-void ContractedGaussian_get_l(void *c, int *l);                  /* gto.h:190 */
-void ContractedGaussian_get_origin(void *c, double *A);          /* gto.h:192 */
-void ContractedGaussian_compute(void *c, double *r, double *out, int size); /* gto.h:194 (GPU) */
-void ContractedGaussian_deriv(void *c, double *r, double *out, int size);   /* gto.h:197 (GPU) */
-double ContractedGaussian_overlap(void *c, void *o);             /* gto.h:200 */
-double ContractedGaussian_get_norma(void *c);                    /* gto.h:202 */
+int ContractedGaussian_get_nprim(void *c);                       /* gto.h:203 */
+void ContractedGaussian_get_l(void *c, int *l);                  /* gto.h:205 */
+void ContractedGaussian_get_origin(void *c, double *A);          /* gto.h:207 */
+void ContractedGaussian_compute(void *c, double *r, double *out, int size); /* gto.h:209 (GPU) */
+void ContractedGaussian_deriv(void *c, double *r, double *out, int size);   /* gto.h:212 (GPU) */
+double ContractedGaussian_overlap(void *c, void *o);             /* gto.h:215 */
+double ContractedGaussian_get_norma(void *c);                    /* gto.h:218 */
 void *BasisSet_new_empty(void);                                  /* basis_set.h:53 */
 void *BasisSet_new(void **contractions, int n);                  /* basis_set.h:55 */
 void BasisSet_del(void *b);
@@ -260,7 +260,9 @@ int napmo_gpu_basis_values(void *basis, int npoint, const double *x, const doubl
 int napmo_gpu_density(int n, int npoint, const double *phi, long ld, const double *D,
                       double *rho, void *stream);
 /* F = phi diag(wv) psi^T (psi = phi if null), upper triangle mirrored;
- * replaces nwavefunction_compute_coupling/_xc_matrix (nwavefunction.cpp:77-197). */
+ * replaces nwavefunction_compute_coupling/_xc_matrix (nwavefunction.cpp:77-197).
+ * phi, psi [n][ld] and wv are 16-byte aligned, ld even and >= npoint rounded up
+ * to 128, every array zero padded to that length; npoint = 0 gives F = 0. */
 int napmo_gpu_quadrature(int n, int npoint, const double *phi, const double *psi, long ld,
                          const double *wv, double *F, void *stream);
 /* wv = wb w (q v + vext), zero padded to the next multiple of 128. */
@@ -324,9 +326,13 @@ int napmo_gpu_nuclear_potential(int npoint, const double *x, const double *y, co
  * memory themselves; callers that must not let an allocation stall the
  * device).  No counterpart in nAPMO.  Split-K scratch is a fixed 16 MiB device
  * array inside the library (held by every GPU that loads it until exit), so
- * n <= 1920; larger n is refused with an error.  The first call on a device
- * resolves the array's address (make it before any stream capture).  Calls
- * share the array: overlapping calls on the GPU race. */
+ * n <= 1920; larger n is refused with an error.  Each call looks up the
+ * array's device address (no allocation); the first call on a device may load
+ * the library's device code, so make it before any stream capture.  Inputs as
+ * for napmo_gpu_quadrature: phi, psi, wv 16-byte aligned, ld even and >=
+ * npoint rounded up to 128, wv zero padded to that length (as
+ * napmo_gpu_combine_weights writes it); npoint = 0 gives F = 0.  Calls share
+ * the array: overlapping calls on the GPU race. */
 int napmo_gpu_quadrature_noalloc(int n, int npoint, const double *phi, const double *psi,
                                  long ld, const double *wv, double *F, void *stream);
 

@@ -232,8 +232,13 @@ int napmo_gpu_density(int n, int npoint, const double *phi, long ld, const doubl
 int napmo_gpu_quadrature(int n, int npoint, const double *phi, const double *psi, long ld,
                          const double *wv, double *F, void *stream) {
   return guarded([&] {
+    NAPMO_REQUIRE(n > 0 && npoint >= 0, "n must be positive, npoint >= 0");
     NAPMO_REQUIRE(ld >= padded_points(npoint) && ld % 2 == 0, "ld too small or odd");
     cudaStream_t s = (cudaStream_t)stream;
+    if (npoint == 0) {  // empty grid: F = 0
+      NAPMO_TRY_CUDA(cudaMemsetAsync(F, 0, (size_t)n * n * sizeof(double), s), "F");
+      return kOk;
+    }
     void *work = nullptr;
     const size_t bytes = quadrature_workspace_bytes(n, npoint);
     NAPMO_TRY_CUDA(cudaMallocAsync(&work, bytes, s), "quadrature workspace");

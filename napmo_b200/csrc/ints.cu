@@ -38,8 +38,17 @@ struct FuncTable {
 // 1 / (2j + 1) for j < kInvOdd: the series and the downward recursion below
 // multiply by these instead of dividing (one FP64 division per series term
 // would dominate the kernel)
+// (IEEE divisions folded at compile time; the table is part of the module
+// image, so it is in place whenever the module is loaded, with no upload).
 constexpr int kInvOdd = 320;
-__device__ double g_inv_odd[kInvOdd];
+struct InvOddTable {
+  double v[kInvOdd];
+  constexpr InvOddTable() : v() {
+    for (int j = 0; j < kInvOdd; ++j) v[j] = 1.0 / (2 * j + 1);
+  }
+};
+__device__ const InvOddTable g_inv_odd_table;
+#define g_inv_odd (g_inv_odd_table.v)
 
 // Boys function F_m(T) for m = 0..mmax.  T < 35: the series at mmax,
 //   F_m(T) = e^-T sum_k (2T)^k / ((2m+1)(2m+3)...(2m+2k+1))
@@ -340,17 +349,6 @@ int one_body_device(const HostFuncs &h, int nq, const double *charges, double *S
   if (n == 0) return kOk;
   if (h.max_l > 3)
     return set_error(kNotSupported, "one-electron integrals support functions up to f");
-  {
-    static thread_local int done_dev = -1;
-    int dev = 0;
-    NAPMO_TRY_CUDA(cudaGetDevice(&dev), "device");
-    if (done_dev != dev) {
-      double inv[kInvOdd];
-      for (int j = 0; j < kInvOdd; ++j) inv[j] = 1.0 / (2 * j + 1);
-      NAPMO_TRY_CUDA(cudaMemcpyToSymbol(g_inv_odd, inv, sizeof(inv)), "Boys tables");
-      done_dev = dev;
-    }
-  }
   const size_t np = h.zeta.size();
   const size_t bytes = (h.start.size() + h.l.size()) * sizeof(int) +
                        (2 * np + h.origin.size() + 4 * (size_t)nq) * sizeof(double) + 64;

@@ -1082,12 +1082,13 @@ cudaError_t launch_eval_l(const PoissonDev &P, int npoint, const double *x,
 
 }  // namespace
 
+// Uploads the constant tables to the current device.  Called by every Poisson
+// plan construction (which allocates and copies far more): uploading per plan
+// rather than once per device keeps the tables in place under any context and
+// after a device reset.  The bytes are the same every time, so an upload while
+// kernels of another plan read the tables changes nothing they see.
 cudaError_t poisson_init_constants() {
-  static thread_local int done_dev = -1;
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  if (done_dev == dev) return cudaSuccess;
+  cudaError_t e = cudaSuccess;
   std::vector<double> ov2(100), ov3(1000);
   hermite_tables_export(ov2.data(), ov3.data());
   std::vector<double> nrm((kMaxLmax + 1) * (kMaxLmax + 1), 0.0);
@@ -1154,7 +1155,6 @@ cudaError_t poisson_init_constants() {
     fd[77] = st.den_mid2;
     if ((e = cudaMemcpyToSymbol(c_fd, fd, sizeof(fd))) != cudaSuccess) return e;
   }
-  done_dev = dev;
   return cudaSuccess;
 }
 

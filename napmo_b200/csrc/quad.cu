@@ -21,7 +21,6 @@
 //
 // Tiles: 128x128 per CTA, 256 threads, 8x8 doubles per thread (two 4x4
 // quadrants 64 apart), K step 8, register-staged double buffering.
-#include <mutex>
 #include <string>
 
 #include "common.h"
@@ -365,14 +364,23 @@ cudaError_t launch_combine_weights(int npoint, const double *wb, const double *w
 // result can differ from napmo_gpu_quadrature in the last bits (different
 // summation grouping); it is deterministic from call to call.
 //
-// Set-up: the first call on a device looks up the device address of the
-// array with cudaGetSymbolAddress (with that device current) and caches it;
-// make that first call before any stream capture.  The array is shared by
-// all calls and keeps the previous call's contents; nothing in it needs to
-// start at zero (each chunk overwrites its own tiles before they are added).
-// Calls that overlap on the GPU (different streams, or different host
-// threads without ordering) race on the array and must be serialised by the
-// caller.
+// Address: every call looks up the device address of the array with
+// cudaGetSymbolAddress, with the caller's device current, and passes it to the
+// kernels (in host code the array's name is only a host-side stand-in).  The
+// lookup allocates nothing; doing it per call rather than caching it keeps the
+// address right under any context and after a device reset.  The first call
+// on a device may load the library's device code there: make it before any
+// stream capture.
+//
+// Inputs: phi, psi and wv are read with 16-byte loads up to npoint rounded up
+// to 128, so they must be 16-byte aligned, ld even, and wv zero padded to that
+// length (napmo_gpu_combine_weights writes it so).  npoint = 0 gives F = 0.
+//
+// Sharing: the array is shared by all calls and keeps the previous call's
+// contents; nothing in it needs to start at zero (each chunk overwrites its
+// own tiles before they are added).  Calls that overlap on the GPU (different
+// streams, or different host threads without ordering) race on the array and
+// must be serialised by the caller.
 // ===========================================================================
 namespace napmo {
 namespace {
@@ -380,24 +388,14 @@ namespace {
 constexpr size_t kNoAllocScratchDoubles = size_t(2) << 20;  // 16 MiB
 __device__ __align__(256) double g_quad_scratch[kNoAllocScratchDoubles];
 
-std::mutex g_scratch_mutex;
-double *g_scratch_ptr[64] = {nullptr};
-
+// Device address of g_quad_scratch in the current context.
 int scratch_address(double **out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return set_error(kCudaError, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= 64) return set_error(kNotSupported, "device index above 63");
-  std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (!g_scratch_ptr[dev]) {
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_quad_scratch);
-    if (e != cudaSuccess)
-      return set_error(kCudaError, std::string("cudaGetSymbolAddress(quadrature scratch): ") +
-                                       cudaGetErrorString(e));
-    g_scratch_ptr[dev] = static_cast<double *>(p);
-  }
-  *out = g_scratch_ptr[dev];
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_quad_scratch);
+  if (e != cudaSuccess)
+    return set_error(kCudaError, std::string("cudaGetSymbolAddress(quadrature scratch): ") +
+                                     cudaGetErrorString(e));
+  *out = static_cast<double *>(p);
   return kOk;
 }
 
@@ -409,7 +407,8 @@ extern "C" {
 // F[mu][nu] = sum_p phi[mu][p] wv[p] psi[nu][p] (psi = phi when null), upper
 // triangle mirrored, like napmo_gpu_quadrature, without allocating: the
 // split-K scratch lives in a fixed 16 MiB device array (n <= 1920).  See the
-// block comment above for the set-up call and the sharing rules.
+// block comment above for the address lookup, the input contract and the
+// sharing rules.
 int napmo_gpu_quadrature_noalloc(int n, int npoint, const double *phi, const double *psi,
                                  long ld, const double *wv, double *F, void *stream) {
   using namespace napmo;
@@ -425,10 +424,15 @@ int napmo_gpu_quadrature_noalloc(int n, int npoint, const double *phi, const dou
     return set_error(kInvalidArgument,
                      "napmo_gpu_quadrature_noalloc: n = " + std::to_string(n) +
                          " exceeds the 16 MiB fixed scratch (at most 1920 basis functions)");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (npoint == 0) {  // empty grid: F = 0 (a memset allocates nothing)
+    const cudaError_t e = cudaMemsetAsync(F, 0, (size_t)n * n * sizeof(double), s);
+    if (e != cudaSuccess) return set_error(kCudaError, std::string("memset F: ") + cudaGetErrorString(e));
+    return kOk;
+  }
   double *scratch = nullptr;
   int st = scratch_address(&scratch);
   if (st != kOk) return st;
-  cudaStream_t s = (cudaStream_t)stream;
   // as many chunks as the launch policy wants, capped by the fixed array
   int chunk;
   int nchunk = quad_chunks(n, npad, &chunk);

@@ -184,7 +184,10 @@ def reference_vectors():
 
 if __name__ == '__main__':
     args = [a for a in sys.argv[1:] if not a.startswith('--')]
-    ref = args[0] if args else '/root/reference'
+    ref = args[0] if args else os.environ.get('NAPMO_REFERENCE')
+    if not ref:
+        sys.exit('usage: make_golden.py <nAPMO source tree> [--answers-only] '
+                 '(or set NAPMO_REFERENCE)')
     with open(os.path.join(HERE, 'known_answers.json'), 'w') as f:
         json.dump(known_answers(ref), f, indent=1)
     if '--answers-only' not in sys.argv:

@@ -6,7 +6,7 @@ energies per particle (x_zk.txt, c_zk.txt) and potentials (x_vrho.txt,
 c_vrho.txt).  Kept: every 10th point, plus every point below 1e-10 (zeros,
 denormal-range values and the cut of the smallest densities).
 
-Usage: python tests/golden/make_xc_golden.py [/path/to/nAPMO]
+Usage: python tests/golden/make_xc_golden.py /path/to/nAPMO (or NAPMO_REFERENCE set)
 """
 import os
 import sys
@@ -31,4 +31,7 @@ def main(ref):
 
 
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('NAPMO_REFERENCE')
+    if not ref:
+        sys.exit('usage: make_xc_golden.py <nAPMO source tree> (or set NAPMO_REFERENCE)')
+    main(ref)

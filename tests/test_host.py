@@ -2,6 +2,7 @@
 reference, Hermite FEM tables, splines and extrapolations, GTO set-up, and
 the exported C-ABI."""
 import ctypes
+import json
 import os
 import re
 
@@ -216,3 +217,77 @@ def test_one_body_integrals_h2_sto3g():
     cext.checked(cext.lib.napmo_basis_one_body(b._this, S, T))
     assert abs(S[0, 0] - 1.0) < 1e-12 and abs(S[0, 1] - 0.6593) < 5e-5
     assert abs(T[0, 0] - 0.7600) < 5e-5 and abs(T[0, 1] - 0.2365) < 5e-5
+
+
+# C parameter spellings per ctypes type class of nAPMO's bindings
+_CTYPE_CLASS = {
+    'c_int': {'int'}, 'c_long': {'long'}, 'c_double': {'double'}, 'c_bool': {'bool', 'int'},
+    'c_void_p': {'void*', 'void**', 'double*', 'int*', 'long*', 'char*'},
+    'a1df': {'double*'}, 'a2df': {'double*'}, 'a3df': {'double*'},
+    'POINTER(c_double)': {'double*'}, 'POINTER(c_int)': {'int*'},
+    'a1di': {'int*'}, 'a1dli': {'long*'}, 'aptr': {'void**'}, 'None': {'void'},
+}
+# nAPMO's own C++ (angular.cpp:142-164, 189-193) takes and reads a fourth
+# argument s[] that its binding (napmo/__init__.py:296) does not pass; this
+# library keeps the C++ arity (s = NULL means s = 1), see INTEGRATION.md.
+_ARITY_EXCEPTIONS = {'AngularGrid_integrate': 4}
+# nAPMO's binding (napmo/__init__.py:203) says c_double, its C++ (gto.h:119)
+# returns void and primitive_gaussian.py:56 ignores the value; void is kept.
+_RESTYPE_EXCEPTIONS = {'PrimitiveGaussian_compute': 'void'}
+
+
+def _header_declarations():
+    with open(os.path.join(ROOT, 'include', 'napmo_b200.h')) as f:
+        text = re.sub(r'/\*.*?\*/', '', f.read(), flags=re.S)
+    text = re.sub(r'#[^\n]*', '', text)
+    decls = {}
+    for m in re.finditer(r'([A-Za-z_][A-Za-z0-9_ \*]*?)\b([A-Za-z_][A-Za-z0-9_]*)\s*\(([^)]*)\)\s*;',
+                         text):
+        ret, name, params = m.group(1), m.group(2), m.group(3).strip()
+        ret = re.sub(r'\bconst\b|\bextern\b|"C"', '', ret).replace(' ', '')
+        args = []
+        if params and params != 'void':
+            for p in params.split(','):
+                p = re.sub(r'\bconst\b|\bunsigned\b', '', p).strip()
+                stars = p.count('*')
+                base = re.sub(r'\*', ' ', p).split()[0]
+                args.append(base + '*' * stars)
+        decls[name] = (ret, args)
+    return decls
+
+
+def test_declarations_match_napmo_ctypes_bindings():
+    """Every C symbol nAPMO binds (napmo/__init__.py:106-585, recorded in
+    tests/golden/napmo_bindings.json by make_bindings.py) is declared in
+    include/napmo_b200.h with the same arity and compatible types, and is
+    exported by libnapmo.so."""
+    with open(os.path.join(ROOT, 'tests', 'golden', 'napmo_bindings.json')) as f:
+        ref = json.load(f)['bindings']
+    assert len(ref) == 140
+    decls = _header_declarations()
+    lib = ctypes.CDLL(cext.LIBPATH)
+    bad = []
+    for name, b in sorted(ref.items()):
+        if name not in decls:
+            bad.append((name, 'not declared'))
+            continue
+        if not hasattr(lib, name):
+            bad.append((name, 'not exported'))
+        ret, args = decls[name]
+        if 'argtypes' in b:
+            want = _ARITY_EXCEPTIONS.get(name, len(b['argtypes']))
+            if len(args) != want:
+                bad.append((name, 'arity %d != %d' % (len(args), want)))
+            for i, (t, a) in enumerate(zip(b['argtypes'], args)):
+                if a not in _CTYPE_CLASS[t]:
+                    bad.append((name, 'arg %d: %s vs %s' % (i, t, a)))
+        rt = b.get('restype', 'c_int')
+        if _RESTYPE_EXCEPTIONS.get(name) == ret:
+            continue
+        if rt != 'None' and ret not in _CTYPE_CLASS[rt] and not (
+                rt == 'c_void_p' and ret.endswith('*')) and not (
+                rt == 'POINTER(c_double)' and ret == 'double*'):
+            bad.append((name, 'restype %s vs %s' % (rt, ret)))
+        if rt == 'None' and ret != 'void':
+            bad.append((name, 'restype None vs %s' % ret))
+    assert not bad, bad

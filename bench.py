@@ -141,12 +141,15 @@ def build_workload(args):
     grid = nb.BeckeGrid(e, args.nrad, args.nang)
     lmax = nb.lebedev_get_order(args.nang) // 2
     basis = e['basis']
-    n = basis['nbasis']
-    nocc = e['occupation']
-    rng = np.random.default_rng(SEED)
-    C = rng.normal(size=(n, nocc)) / np.sqrt(n)
-    D = 2.0 * C @ C.T
+    D = c4_density(basis['nbasis'], e['occupation'])
     return atoms, ms, grid, basis, lmax, D
+
+
+def c4_config(world, n, N, lmax):
+    """Workload description shared by the device arm and the host arm."""
+    return {'workload': WORKLOAD, 'global_batch': world, 'n_basis': n, 'n_points': N,
+            'lmax': lmax, 'parallelism': 'replicas' if world > 1 else 'single GPU',
+            'l2': 'inputs larger than L2 (phi 7.6 GB)'}
 
 
 # ------------------------------------------------------------- CPU baseline
@@ -172,7 +175,74 @@ def _ref_evaluation(r, centers, radii, nrad, lmax, y, dt, pts, v):
                                   pts, cell, len(splines), pts.shape[0])
 
 
-def cpu_baseline(args, atoms, grid, D, lmax):
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import oracle as O
+    with open(os.path.join(ROOT, 'napmo_b200', 'data', 'basis.json')) as f:
+        lib = json.load(f)
+    with open(os.path.join(ROOT, 'napmo_b200', 'data', 'elements.json')) as f:
+        el = json.load(f)
+    return O, lib, el
+
+
+def c4_density(n, nocc):
+    """D = 2 C C^T, C ~ N(0, 1/n) of shape n x nocc (seed 20261203)."""
+    rng = np.random.default_rng(SEED)
+    C = rng.normal(size=(n, nocc)) / np.sqrt(n)
+    return 2.0 * C @ C.T
+
+
+class HostWorkload(object):
+    """The C20H42 build on the host, set up by the oracle alone (no
+    libnapmo.so in the process): grid points and weights (atomic_grid.cpp),
+    Becke weights of the sampled points and of two atoms' grids
+    (becke.cpp:79-176 per point), the basis at the sampled points, the
+    density of the two atoms' grids, and their Poisson splines
+    (poisson_solver.py) as the spline coefficients of every atom of the same
+    element."""
+
+    def __init__(self, args):
+        O, lib, el = _oracle()
+        import workloads
+        import scf as OS
+        self.O = O
+        atoms = workloads.alkane_geometry(args.ncarbon)
+        self.syms = [s for s, _ in atoms]
+        self.centers = [np.array(x) / 0.52917724924 for _, x in atoms]
+        self.radii = [el[s]['atomic_radii'] for s in self.syms]
+        self.grid = O.Grid(self.centers, self.radii, args.nrad, args.nang, becke=False)
+        self.N = self.grid.size
+        self.lmax = OS.lebedev_lmax(args.nang)
+        self.nrad = args.nrad
+        self.fb = O.flat_basis(self.centers, self.syms, lib, 'CC-PVDZ')
+        self.n = self.fb['nf']
+        nel = sum(el[s]['atomic_number'] for s in self.syms)
+        self.D = c4_density(self.n, nel // 2)
+        rng = np.random.default_rng(SEED)
+        self.idx = np.sort(rng.choice(self.N, size=args.cpu_points, replace=False))
+        self.pts = np.ascontiguousarray(self.grid.points[self.idx])
+        self.bw = self.grid.becke_sample(self.idx)
+        self.w = np.ascontiguousarray(self.grid.weights[self.idx])
+        self.phi = np.ascontiguousarray(O.basis_compute(self.fb, self.pts).T)
+        # one C and one H atom with their Becke weights in the molecule
+        self.sub = [self.syms.index('C'), self.syms.index('H')]
+        offs = self.grid.offsets
+        sub_idx = np.concatenate([np.arange(offs[a], offs[a + 1]) for a in self.sub])
+
+        class Sub(object):
+            pass
+        self.subgrid = Sub()
+        self.subgrid.atoms = [self.grid.atoms[a] for a in self.sub]
+        self.subgrid.becke = self.grid.becke_sample(sub_idx)
+        phis = O.basis_compute(self.fb, self.grid.points[sub_idx])
+        self.sub_rho = np.einsum('pi,pi->p', phis @ self.D, phis)
+        del phis
+        U = O.poisson_solver(self.subgrid, self.sub_rho, self.lmax)
+        by_sym = {self.syms[a]: U[k] for k, a in enumerate(self.sub)}
+        self.splines = [by_sym[s] for s in self.syms]
+
+
+def cpu_baseline(args, hw):
     """nAPMO's path on the host cores, on a bounded sample of one build:
     density, multipole evaluation and quadrature on `cpu_points` grid points
     (scaled by N / sample), plus the projection and radial ODE solves of one
@@ -180,75 +250,136 @@ def cpu_baseline(args, atoms, grid, D, lmax):
     here it is what is timed: the density by its numpy expression
     (psi_hybrid.py / psi_analytic.py: phi * D.dot(phi) per point, summed), the
     multipole evaluation by its compiled evaluate.cpp (oracle/_ref, when
-    built).  The quadrature is the oracle's streamed C restatement (nAPMO's
-    materialises all orbital products, 1.95 TB here, and needs Eigen), and
-    so are the projection and radial solves (scipy, as poisson_solver.py)."""
-    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
-    import oracle as O
-    lib = json.load(open(os.path.join(ROOT, 'napmo_b200', 'data', 'basis.json')))
-    el = json.load(open(os.path.join(ROOT, 'napmo_b200', 'data', 'elements.json')))
-    centers = [np.array(x) / 0.52917724924 for _, x in atoms]
-    syms = [s for s, _ in atoms]
-    fb = O.flat_basis(centers, syms, lib, 'CC-PVDZ')
-    N = grid.size
-    rng = np.random.default_rng(SEED)
-    idx = np.sort(rng.choice(N, size=args.cpu_points, replace=False))
-    pts = np.ascontiguousarray(grid.points[idx])
-    bw = np.ascontiguousarray(grid.becke_weights[idx])
-    w = np.ascontiguousarray(grid.weights[idx])
-    phi = np.ascontiguousarray(O.basis_compute(fb, pts).T)
+    built), with the spline coefficients of the real density.  The quadrature
+    is the oracle's streamed C restatement (nAPMO's materialises all orbital
+    products, 1.95 TB here, and needs Eigen), and so are the projection and
+    radial solves (scipy, as poisson_solver.py)."""
+    O = hw.O
+    N, D, phi = hw.N, hw.D, hw.phi
     t0 = time.perf_counter()
     Dgrid = np.array([p * D.dot(p) for p in phi.T]).T
     rho = Dgrid.sum(axis=0)
     t1 = time.perf_counter()
     v = np.zeros(args.cpu_points)
-    # multipole evaluation: every atom's lsize splines at every sample point
-    lsize = (lmax + 1) ** 2
-    spl_y = np.ascontiguousarray(rng.normal(size=(lsize, args.nrad)))
-    spl_dt = np.ascontiguousarray(rng.normal(size=(lsize, args.nrad)))
-    radii = [el[s]['atomic_radii'] for s in syms]
+    lsize = (hw.lmax + 1) ** 2
     # nAPMO's library sets OpenMP's thread count from OMP_NUM_THREADS when it
     # loads (one thread if unset; utils/omp_helper.h): give it every core, as a
     # user of nAPMO would
     os.environ.setdefault('OMP_NUM_THREADS', str(os.cpu_count() or 1))
     r = O.ref_lib()
     t2 = time.perf_counter()
-    if r is not None:
-        _ref_evaluation(r, centers, radii, args.nrad, lmax, spl_y, spl_dt, pts, v)
-    else:
-        for c, radius in zip(centers, radii):
-            O.lib.orc_eval_decomposition(0, radius, 0.0, args.nrad, lsize, spl_y, spl_dt,
-                                         np.ascontiguousarray(c), args.cpu_points, pts, v)
+    for c, radius, (y, dt) in zip(hw.centers, hw.radii, hw.splines):
+        if r is not None:
+            _ref_evaluation(r, [c], [radius], hw.nrad, hw.lmax, y, dt, hw.pts, v)
+        else:
+            O.lib.orc_eval_decomposition(0, radius, 0.0, hw.nrad, lsize,
+                                         np.ascontiguousarray(y), np.ascontiguousarray(dt),
+                                         np.ascontiguousarray(c), args.cpu_points, hw.pts, v)
     t3 = time.perf_counter()
-    F = O.quadrature(phi, v, bw, w)
+    F = O.quadrature(phi, v, hw.bw, hw.w)
     t4 = time.perf_counter()
-    # projection + radial solves for one C and one H atom (full atomic grids)
-    sub = [i for i in (0, syms.index('H'))]
-    og = O.Grid([centers[i] for i in sub], [el[syms[i]]['atomic_radii'] for i in sub],
-                args.nrad, args.nang)
-    dens = np.ones(og.size)
+    O.poisson_solver(hw.subgrid, hw.sub_rho, hw.lmax)
     t5 = time.perf_counter()
-    O.poisson_solver(og, dens, lmax)
-    t6 = time.perf_counter()
     del rho, F
-    ncar = syms.count('C')
-    nh = syms.count('H')
+    natom = len(hw.syms)
     scale = N / args.cpu_points
     parts = {'density': (t1 - t0) * scale, 'evaluation': (t3 - t2) * scale,
              'quadrature': (t4 - t3) * scale,
-             'projection_radial': (t6 - t5) * (ncar + nh) / 2.0}
+             'projection_radial': (t5 - t4) * natom / 2.0}
     t_build = sum(parts.values())
     return {'value': 1.0 / t_build, 'unit': UNIT, 'cores': O.threads(),
             'kind': 'reference' if r is not None else 'port',
             'sample': ('%d of %d points, scaled x%.0f: density by nAPMO\'s numpy expression, '
-                       'multipole evaluation (62 atoms x %d splines) by %s, quadrature by the '
-                       'oracle\'s streamed C restatement (OpenMP); projection + radial FEM solves '
-                       '(oracle, scipy spsolve) of 2 of 62 atoms, scaled x31; sample wall %.1f s'
-                       % (args.cpu_points, N, scale, lsize,
+                       'multipole evaluation (%d atoms x %d splines of the real density, per '
+                       'element) by %s, quadrature by the oracle\'s streamed C restatement '
+                       '(OpenMP); projection + radial FEM solves (oracle, scipy spsolve) of 2 '
+                       'of %d atoms, scaled x%.0f'
+                       % (args.cpu_points, N, scale, natom, lsize,
                           "nAPMO's evaluate.cpp compiled from its sources (OpenMP, "
                           "OMP_NUM_THREADS = host cores)"
-                          if r is not None else 'the oracle C restatement (OpenMP)', t6 - t0)),
-            'seconds_per_build': t_build, 'seconds_per_part': parts}
+                          if r is not None else 'the oracle C restatement (OpenMP)',
+                          natom, natom / 2.0)),
+            'sample_seconds': t5 - t0, 'seconds_per_build': t_build,
+            'seconds_per_part': parts}
+
+
+# ------------------------------------------------- C1/C2: host SCF arms
+# Iterations the oracle's SCFs take to converge (|dE| < 1e-9 Eh; the fixture
+# tests/golden/scf_oracle.json records them): a timed iteration scaled by
+# these is the host's time per SCF.
+ORACLE_SCF_ITERATIONS = {'c1': 11, 'c2': 13}
+
+
+def reference_scf(args, workload):
+    """The oracle's grid SCF on the host cores (oracle/scf.py: nAPMO's
+    arithmetic for the grid, the basis, the quadratures and the Poisson solves,
+    the drivers' SCF loop).  C1: every step is one SCF iteration of H2O 50 x
+    110 (J, orbital-pair exchange, DIIS, diagonalisation), continuing one SCF
+    from the core guess.  C2 (HCN + quantum H, 100 x 302): every step is one
+    iteration's Coulomb and coupling part (two densities, two Poisson solves,
+    the quadratures of both species) plus the exchange of one of the seven
+    occupied orbitals (n = 35 pair densities solved together), the exchange
+    scaled by 7.  Value = seconds per iteration x the oracle SCF's
+    iteration count."""
+    O, lib, el = _oracle()
+    import scf as OS
+    import workloads
+    niter = ORACLE_SCF_ITERATIONS[workload]
+    times = []
+    if workload == 'c1':
+        orc = OS.GridRHF(workloads.H2O, lib, el, 50, 110)
+        gen = orc.iterations(tol=1e-9)
+        for _ in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            try:
+                it, E, emax, conv, D = next(gen)
+            except StopIteration:
+                gen = orc.iterations(tol=1e-9)
+                it, E, emax, conv, D = next(gen)
+            times.append(time.perf_counter() - t0)
+        sample = ('one SCF iteration per step (J by one Poisson solve, exchange by 5 x 25 '
+                  'pair-density solves, DIIS, diagonalisation), x %d iterations' % niter)
+        cfg = {'workload': 'C1: H2O cc-pVDZ (25 Cartesian functions), 50x110 per atom '
+                           '(16,500 points), lmax 8, grid J and exchange, DIIS(6), 1e-8 Eh',
+               'parallelism': 'single GPU'}
+        metric = 'grid RHF SCF time, H2O / cc-pVDZ 50x110 (C1)'
+        iter_s = times[args.warmup:]
+    else:
+        orc = OS.GridAPMO(workloads.HCN, lib, el, (0,), 100, 302)
+        Ce, De, Cn, Dn = orc.guess()
+        e, nuc, g = orc.e, orc.nuc, orc.grid
+        qq = e.q * nuc.q
+        iter_s = []
+        for k in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            rho_e, rho_n = O.density(e.phi, De), O.density(nuc.phi, Dn)
+            V = OS.poisson_many(orc.plan, np.stack([rho_e, rho_n]))
+            O.quadrature(e.phi, e.q * e.q * V[0] + qq * V[1], g.becke, g.weights)
+            O.quadrature(nuc.phi, qq * V[0], g.becke, g.weights)
+            t1 = time.perf_counter()
+            psi = Ce[:, 0] @ e.phi
+            Vk = OS.poisson_many(orc.plan, psi * e.phi)
+            (e.phi * (orc.W * psi)) @ Vk.T
+            t2 = time.perf_counter()
+            if k >= args.warmup:
+                iter_s.append((t1 - t0) + e.nocc * (t2 - t1))
+        sample = ('per step one iteration\'s Coulomb + coupling part and the exchange of 1 '
+                  'of 7 occupied orbitals (x7), x %d iterations' % niter)
+        cfg = {'workload': 'C2: HCN, e- cc-pVDZ (35) + H nucleus 5s5p (20), 100x302 per '
+                           'atom (90,600 points), lmax 14, DIIS(6), 1e-8 Eh',
+               'parallelism': 'single GPU'}
+        metric = 'grid APMO-RHF SCF time, HCN with quantum H, 100x302 (C2)'
+    t_iter = statistics.median(iter_s)
+    v = t_iter * niter
+    cb = {'value': v, 'unit': 's per SCF', 'cores': O.threads(), 'kind': 'port',
+          'sample': sample, 'seconds_per_iteration': t_iter}
+    return {'impl': 'reference', 'metric': metric, 'value': v, 'unit': 's per SCF',
+            'n_gpus': 1, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': t_iter * 1e3, 'sample_scale_to_scf': niter,
+            'higher_is_better': False, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+            'data': 'synthetic', 'config': cfg, 'cpu_baseline': cb,
+            'e2e': {'value': v, 'unit': 's per SCF', 'h2d_bytes_per_step': 0,
+                    'd2h_bytes_per_step': 0}}
 
 
 # ------------------------------------------------------------ C3: batches
@@ -762,9 +893,10 @@ def main():
     if args.impl == 'reference':
         if rank != 0:
             return
-        why = {'c1': 'nAPMO runs this SCF only through libint (analytic drivers), absent here',
-               'c2': 'nAPMO runs this SCF only through libint (analytic drivers), absent here',
-               'c3': 'nAPMO has no batched multi-molecule build; its per-build CPU cost is the '
+        if args.workload in ('c1', 'c2'):
+            print(json.dumps(reference_scf(args, args.workload)))
+            return
+        why = {'c3': 'nAPMO has no batched multi-molecule build; its per-build CPU cost is the '
                      'c4 reference arm',
                'c5': 'nAPMO computes no nuclear-coordinate gradients'}
         if args.workload in why:
@@ -807,21 +939,26 @@ def main():
                 'e2e': {'value': v, 'unit': 's per SCF', 'h2d_bytes_per_step': 0,
                         'd2h_bytes_per_step': 0}}))
             return
-        import napmo_b200  # grid construction only; no GPU work is timed here
-        import torch
-        atoms, ms, grid, basis, lmax, D = build_workload(args)
+        # the host arm loads no part of this package's library: the oracle
+        # builds the grid, the sample and the density
+        hw = HostWorkload(args)
         steps = []
         for _ in range(args.warmup + args.steps):
-            cb = cpu_baseline(args, atoms, grid, D, lmax)
-            steps.append(cb['value'])
-        vals = steps[args.warmup:]
-        v = statistics.median(vals)
+            cb = cpu_baseline(args, hw)
+            steps.append(cb)
+        timed = steps[args.warmup:]
+        v = statistics.median([c['value'] for c in timed])
+        sample_s = statistics.median([c['sample_seconds'] for c in timed])
         cb['value'] = v
-        line = {'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': UNIT, 'n_gpus': 1,
-                'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 / v,
+        line = {'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': UNIT, 'n_gpus': world,
+                'steps': args.steps, 'warmup': args.warmup,
+                # what each step actually ran; value is that sample scaled to a build
+                'ms_per_step': sample_s * 1e3,
+                'sample_scale_to_build': (1.0 / v) / sample_s,
+                'extrapolated_ms_per_build': 1e3 / v,
                 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
                 'dtype': 'f64', 'data': 'synthetic',
-                'config': {'workload': WORKLOAD, 'parallelism': 'host cores'},
+                'config': c4_config(world, hw.n, hw.N, hw.lmax),
                 'cpu_baseline': cb,
                 'e2e': {'value': v, 'unit': UNIT, 'h2d_bytes_per_step': 0,
                         'd2h_bytes_per_step': 0}}
@@ -1025,16 +1162,13 @@ def main():
         value = world * args.steps / t_dev
         cb = None
         if not args.no_cpu_baseline and world == 1:
-            cb = cpu_baseline(args, atoms, grid, D, lmax)
+            cb = cpu_baseline(args, HostWorkload(args))
         line = {
             'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world,
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': t_dev / args.steps * 1e3,
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
             'dtype': 'int8x4' if headline == 'int8x4' else 'f64', 'data': 'synthetic',
-            'config': {'workload': WORKLOAD, 'global_batch': world, 'n_basis': n,
-                       'n_points': N, 'lmax': lmax,
-                       'parallelism': 'replicas' if world > 1 else 'single GPU',
-                       'l2': 'inputs larger than L2 (phi 7.6 GB)'},
+            'config': c4_config(world, n, N, lmax),
             'e2e': {'value': world * args.steps / t_e2e, 'unit': UNIT,
                     'h2d_bytes_per_step': n * n * 8, 'd2h_bytes_per_step': n * n * 8},
             'gpu_launches': launches_per_build * args.steps,

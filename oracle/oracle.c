@@ -507,6 +507,24 @@ void orc_spline_dt(const double *y, double *dt, int n) {
   free(mid); free(up); free(right);
 }
 
+/* orc_spherical_expansion of k functions f[c * ld + p] of one atom's points
+ * (same arithmetic per function), out [k][nrad][lsize]; OpenMP over functions. */
+void orc_spherical_expansion_many(int nrad, int nang, const double *points, const double *weights,
+                                  const double *center, int k, const double *f, long ld, int lmax,
+                                  double *out) {
+  const long lsize = (long)(lmax + 1) * (lmax + 1);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int c = 0; c < k; ++c)
+    orc_spherical_expansion(nrad, nang, points, weights, center, f + (long)c * ld, lmax,
+                            out + (long)c * nrad * lsize);
+}
+
+/* orc_spline_dt of ncol columns y[c * n + i]; OpenMP over columns. */
+void orc_spline_dt_many(const double *y, double *dt, int n, int ncol) {
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < ncol; ++c) orc_spline_dt(y + (long)c * n, dt + (long)c * n, n);
+}
+
 /* ----------------------------------------------------------- FEM (ODE) */
 /* Cubic Hermite FEM assembly (src/horton/ode2.cpp:232-321).  The segment
  * integrals of products of Hermite basis polynomials are evaluated exactly
@@ -664,6 +682,81 @@ void orc_eval_decomposition(int kind, double p0, double p1, int n, int nspline, 
       output[i] = acc;
     }
     free(work);
+  }
+  free(amp_l); free(amp_r); free(ls);
+}
+
+/* orc_eval_decomposition for k sets of splines on the same atom (y, dt:
+ * [k][nspline][n]; output row c at output + c * ldo): the point's distance,
+ * spline interval and harmonics are computed once and shared; each set's
+ * arithmetic is that of orc_eval_decomposition, so every row equals a
+ * separate call bit for bit. */
+void orc_eval_decomposition_many(int kind, double p0, double p1, int n, int nspline, int k,
+                                 const double *y, const double *dt, const double *center,
+                                 int npoint, const double *points, double *output, long ldo) {
+  long lmax = (long)sqrt((double)nspline) - 1;
+  double first_x, last_x;
+  if (kind == 0) { first_x = orc_cheb_radius(p0, n, 0); last_x = orc_cheb_radius(p0, n, n - 1); }
+  else { first_x = orc_power_radius(p0, p1, 0); last_x = orc_power_radius(p0, p1, n - 1); }
+  const long ks = (long)nspline * n;
+  double *amp_l = malloc(sizeof(double) * nspline * k), *amp_r = malloc(sizeof(double) * nspline * k);
+  int *ls = malloc(sizeof(int) * nspline);
+  for (int l = 0, c = 0; l <= lmax; ++l)
+    for (int m = -l; m <= l; ++m, ++c) ls[c] = l;
+  for (int b = 0; b < k; ++b)
+    for (int c = 0; c < nspline; ++c) {
+      amp_l[b * nspline + c] = y[b * ks + (long)c * n] / pow(first_x, ls[c]);
+      amp_r[b * nspline + c] = y[b * ks + (long)c * n + n - 1] * pow(last_x, ls[c] + 1);
+    }
+#pragma omp parallel
+  {
+    double *work = malloc(sizeof(double) * (nspline + 3));
+    double *sh = malloc(sizeof(double) * (nspline + 3));
+    double *fac = malloc(sizeof(double) * (nspline + 3));
+#pragma omp for schedule(static)
+    for (int i = 0; i < npoint; ++i) {
+      double x = points[3 * i] - center[0], yy = points[3 * i + 1] - center[1],
+             z = points[3 * i + 2] - center[2];
+      double d = sqrt(x * x + yy * yy + z * z);
+      double t = 0.0, u = 0.0;
+      int j = 0;
+      if (d >= first_x && d <= last_x) {
+        t = kind == 0 ? orc_cheb_inv(p0, n, d) : pow(d / p0, 1.0 / p1) - 1;
+        j = (int)floor(t);
+        if (j == n - 1) j = n - 2;
+        if (j < 0) j = 0;
+        u = t - j;
+      }
+      if (lmax > 0) {
+        sh[0] = z; sh[1] = x; sh[2] = yy;
+        if (lmax > 1) pure_poly(sh, lmax);
+        long counter = 0;
+        double dpowl = 1.0;
+        for (long l = 1; l <= lmax; l++) {
+          dpowl = dpowl / d;
+          double factor = sqrt(2 * l + 1);
+          for (long m = -l; m <= l; m++) fac[counter++] = factor * 0.28209479177387814347 * dpowl;
+        }
+      }
+      for (int b = 0; b < k; ++b) {
+        const double *yb = y + b * ks, *db = dt + b * ks;
+        for (int c = 0; c < nspline; ++c) {
+          double s;
+          if (d < first_x) s = amp_l[b * nspline + c] * pow(d, ls[c]);
+          else if (d <= last_x) {
+            const double *Y = yb + (long)c * n, *D = db + (long)c * n;
+            double zz = Y[j + 1] - Y[j];
+            s = Y[j] + u * (D[j] + u * (3 * zz - 2 * D[j] - D[j + 1] + u * (-2 * zz + D[j] + D[j + 1])));
+          } else s = amp_r[b * nspline + c] / pow(d, ls[c] + 1);
+          work[c] = s;
+        }
+        double acc = output[b * ldo + i];
+        acc += work[0] * 0.28209479177387814347;
+        for (long c = 0; c + 1 < nspline; ++c) acc += work[c + 1] * fac[c] * sh[c];
+        output[b * ldo + i] = acc;
+      }
+    }
+    free(work); free(sh); free(fac);
   }
   free(amp_l); free(amp_r); free(ls);
 }

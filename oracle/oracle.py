@@ -58,9 +58,14 @@ def _load_oracle():
         'orc_quadrature': (None, [c_int, c_int, a2d, a1d, a1d, a1d, a2d]),
         'orc_spherical_expansion': (None, [c_int, c_int, a2d, a1d, a1d, a1d, c_int, a2d]),
         'orc_spline_dt': (None, [a1d, a1d, c_int]),
+        'orc_spline_dt_many': (None, [a2d, a2d, c_int, c_int]),
+        'orc_spherical_expansion_many': (None, [c_int, c_int, a2d, a1d, a1d, c_int, a2d, c_long,
+                                                c_int, a2d]),
         'orc_build_ode2': (None, [a1d, a1d, a1d, a1d, a2d, a1d, c_long]),
         'orc_eval_decomposition': (None, [c_int, c_double, c_double, c_int, c_int, a2d, a2d,
                                           a1d, c_int, a2d, a1d]),
+        'orc_eval_decomposition_many': (None, [c_int, c_double, c_double, c_int, c_int, c_int,
+                                               a2d, a2d, a1d, c_int, a2d, a2d, c_long]),
         'orc_num_threads': (c_int, []),
     }
     for name, (res, args) in sig.items():
@@ -168,7 +173,7 @@ class Atom(object):
 class Grid(object):
     """Molecular grid: concatenated atoms plus Becke weights (becke.cpp:12-176)."""
 
-    def __init__(self, centers, radii, nrad, nang):
+    def __init__(self, centers, radii, nrad, nang, becke=True):
         nc = len(centers)
         nr = nrad if isinstance(nrad, (list, tuple)) else [nrad] * nc
         na = nang if isinstance(nang, (list, tuple)) else [nang] * nc
@@ -180,8 +185,24 @@ class Grid(object):
         self.size = self.points.shape[0]
         self.offsets = np.cumsum([0] + [a.size for a in self.atoms]).astype(np.int32)
         self.becke = np.zeros(self.size)
-        lib.orc_becke_weights(nc, self.size, self.radii, self.origin, self.points, self.offsets,
-                              self.becke)
+        if becke:
+            lib.orc_becke_weights(nc, self.size, self.radii, self.origin, self.points,
+                                  self.offsets, self.becke)
+
+    def becke_sample(self, index):
+        """Becke weights of the grid points `index` only (the per-point
+        computation of becke.cpp:128-171 with each point's owning atom)."""
+        index = np.asarray(index, dtype=np.int64)
+        owner = np.searchsorted(self.offsets, index, side='right') - 1
+        order = np.argsort(owner, kind='stable')
+        pts = np.ascontiguousarray(self.points[index[order]])
+        counts = np.bincount(owner, minlength=len(self.atoms))
+        offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
+        out = np.zeros(len(index))
+        lib.orc_becke_weights(len(self.atoms), len(index), self.radii, self.origin, pts, offs, out)
+        res = np.empty(len(index))
+        res[order] = out
+        return res
 
     def integrate(self, f):
         return float(np.sum(f * self.becke * self.weights))

@@ -29,9 +29,11 @@ def _fd(model, D, R, h=1e-4):
 
 
 @pytest.mark.parametrize('species,quantum', [('e-', ()), ('H_1', (1, 2))])
-def test_gradient_matches_finite_differences(species, quantum):
+@pytest.mark.parametrize('nrad,nang', [(30, 110), (75, 194)])
+def test_gradient_matches_finite_differences(species, quantum, nrad, nang):
+    """(75, 194) is the grid of the two-quantum-proton H2O configuration."""
     from napmo_b200.gradients import GridChargeEnergy
-    model = GridChargeEnergy(SYM, species=species, quantum=quantum, nrad=30, nang=110)
+    model = GridChargeEnergy(SYM, species=species, quantum=quantum, nrad=nrad, nang=nang)
     R = R0 + np.random.default_rng(3).uniform(-0.05, 0.05, size=R0.shape) / BOHR
     V, state = model.quadrature_matrix(R)
     n = V.shape[0]

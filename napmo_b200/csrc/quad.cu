@@ -1,4 +1,4 @@
-// FP64 grid quadratures on CUDA cores (the plain FP64 path):
+// FP64 grid quadratures (the plain FP64 path) on the FP64 tensor pipe:
 //
 //   density     rho[p]     = sum_{mu,nu} phi[mu][p] D[mu][nu] phi[nu][p]
 //   quadrature  F[mu][nu]  = sum_p phi[mu][p] wv[p] phi[nu][p]
@@ -8,19 +8,27 @@
 // nAPMO computes the density point by point in Python (psi_hybrid.py:144-150)
 // and the quadrature by materialising every orbital product
 // Psi[n(n+1)/2][N] (src/wavefunction/nwavefunction.cpp:77-107,161-197).  Here
-// both are register-tiled DFMA GEMMs over phi stored basis-major
-// [n][ld] (ld a multiple of 128, zero padded):
+// both are FP64 GEMMs over phi stored basis-major [n][ld] (ld a multiple of
+// 128, zero padded), issued as mma.sync m16n8k8 f64 (DMMA: 2048 flops per
+// warp instruction, FP64 accumulation) from operand tiles that cp.async
+// streams into a 4-stage shared-memory ring:
 //
-//   * density: a CTA owns 128 points, sweeps 128-row blocks of mu, forms
-//     T = D phi for the block in registers and folds it into the per-point
+//   * density: a CTA owns 128 points and sweeps 128-row blocks of mu.  D is
+//     folded onto block-upper-triangular form (block b of mu takes nu from
+//     its own first row on; entries right of the diagonal block count twice,
+//     exact for symmetric D), so the CTA forms T' = D' phi for each block
+//     (62 % of the full product at n = 510) and folds T' into the per-point
 //     sum with phi[mu][p] in the epilogue; deterministic, no atomics.
 //   * quadrature: split-K over points.  CTA (tile, chunk) accumulates one
 //     128x128 upper-triangle tile of F over one chunk of points into a
-//     workspace slot; a second kernel adds the chunks in fixed order and
-//     writes both triangles, so F is exactly symmetric and bit-reproducible.
+//     workspace slot (wv applied to the B fragments in registers); a second
+//     kernel adds the chunks in fixed order and writes both triangles, so F
+//     is exactly symmetric and bit-reproducible.
 //
-// Tiles: 128x128 per CTA, 256 threads, 8x8 doubles per thread (two 4x4
-// quadrants 64 apart), K step 8, register-staged double buffering.
+// Tiles: 128x128 per CTA, 8 warps as 2 x 4 of 64x32 (4 x 4 m16n8 tiles, 64
+// FP64 accumulators per thread), 16 points (quadrature) or 16 functions
+// (density) per stage.  Shared-memory rows are padded to a stride of 4 mod 16
+// doubles, so the fragment loads of each half-warp hit 16 distinct banks.
 #include <string>
 
 #include "common.h"
@@ -30,132 +38,224 @@ namespace napmo {
 
 namespace {
 
-constexpr int BM = 128, BN = 128, BK = 8, NT = 256;
+constexpr int BM = 128, BN = 128, NT = 256;
+constexpr int BK = 16;                 // points (quadrature) / functions (density) per stage
+constexpr int NS = 4;                  // stages of the cp.async ring
+constexpr int LDA = BK + 4;            // [row][k] tiles: stride 20 doubles
+constexpr int LDB = BN + 4;            // density phi tile [nu][p]: stride 132 doubles
 
-struct TileSmem {
-  double a[2][BK][BM];
-  double b[2][BK][BN];
+struct QuadSmem {
+  double a[NS][BM][LDA];               // phi rows mu0.. over the stage's points
+  double b[NS][BN][LDA];               // psi rows nu0..
+  double w[NS][BK];                    // wv over the stage's points
 };
 
-// acc[i][j] += sum_k As[k][row(i)] * Bs[k][col(j)] for one BK slice.
-__device__ __forceinline__ void mma_slice(const double (*As)[BM],
-                                          const double (*Bs)[BN], int tx, int ty,
-                                          double acc[8][8]) {
-#pragma unroll
-  for (int k = 0; k < BK; ++k) {
-    double a[8], b[8];
-    const double2 a0 = *reinterpret_cast<const double2 *>(&As[k][ty * 4]);
-    const double2 a1 = *reinterpret_cast<const double2 *>(&As[k][ty * 4 + 2]);
-    const double2 a2 = *reinterpret_cast<const double2 *>(&As[k][64 + ty * 4]);
-    const double2 a3 = *reinterpret_cast<const double2 *>(&As[k][64 + ty * 4 + 2]);
-    const double2 b0 = *reinterpret_cast<const double2 *>(&Bs[k][tx * 4]);
-    const double2 b1 = *reinterpret_cast<const double2 *>(&Bs[k][tx * 4 + 2]);
-    const double2 b2 = *reinterpret_cast<const double2 *>(&Bs[k][64 + tx * 4]);
-    const double2 b3 = *reinterpret_cast<const double2 *>(&Bs[k][64 + tx * 4 + 2]);
-    a[0] = a0.x; a[1] = a0.y; a[2] = a1.x; a[3] = a1.y;
-    a[4] = a2.x; a[5] = a2.y; a[6] = a3.x; a[7] = a3.y;
-    b[0] = b0.x; b[1] = b0.y; b[2] = b1.x; b[3] = b1.y;
-    b[4] = b2.x; b[5] = b2.y; b[6] = b3.x; b[7] = b3.y;
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-      for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-  }
+struct DensSmem {
+  double a[NS][BM][LDA];               // D' rows mu0.. over the stage's nu
+  double b[NS][BK][LDB];               // phi rows nu over the CTA's 128 points
+  double red[2][BN];                   // per-point sums of the two warp rows
+};
+
+constexpr size_t kQuadSmem = sizeof(QuadSmem);
+constexpr size_t kDensSmem = sizeof(DensSmem);
+
+// 16-byte / 8-byte asynchronous global -> shared copies; src_bytes = 0 fills
+// the destination with zeros (rows beyond n) without reading the source.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem),
+               "r"(valid ? 16 : 0));
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem),
+               "r"(valid ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-__device__ __forceinline__ int row_of(int ty, int i) {
-  return (i < 4) ? ty * 4 + i : 64 + ty * 4 + (i - 4);
+// d += a (16x8, row) * b (8x8, col), FP64.  Fragments (g = lane / 4,
+// q = lane % 4): a = {A[g][q], A[g+8][q], A[g][q+4], A[g+8][q+4]},
+// b = {B[q][g], B[q+4][g]}, d = {C[g][2q], C[g][2q+1], C[g+8][2q], C[g+8][2q+1]}.
+__device__ __forceinline__ void dmma(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+// acc[mt][nt] += A-tile rows (warp rows mt) x B-tile columns (warp columns nt)
+// over one stage: A fragments from a[row][k], B fragments from bf(col, k).
+template <typename BFrag>
+__device__ __forceinline__ void stage_mma(const double (*a)[LDA], int wrow, int g, int q,
+                                          double scale, BFrag bf, double (&acc)[4][4][4]) {
+#pragma unroll
+  for (int kk = 0; kk < BK; kk += 8) {
+    double b[4][2];
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) bf(nt, kk, b[nt]);
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt) {
+      const int r = wrow + mt * 16 + g;
+      double af[4] = {a[r][kk + q], a[r + 8][kk + q], a[r][kk + q + 4], a[r + 8][kk + q + 4]};
+      if (scale != 1.0) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) af[i] *= scale;
+      }
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) dmma(acc[mt][nt], af, b[nt]);
+    }
+  }
 }
 
 // ------------------------------------------------------------------ density
-// Loads of one K slice (rows nu0..nu0+7):
-//   A: As[k][m] = D[nu0+k][mu0+m]  (D symmetric, so rows of D are columns)
-//   B: Bs[k][c] = phi[nu0+k][p0+c]
-__global__ void __launch_bounds__(NT)
+// Stages of a CTA: block mb of mu takes nu from mb*BM to n (rounded up to BK),
+// the blocks one after the other.
+__device__ __forceinline__ void density_stage(int it, int nblk, int nk, int &mb, int &k0) {
+  mb = 0;
+  int left = it;
+  while (mb < nblk) {
+    const int cnt = nk - mb * (BM / BK);
+    if (left < cnt) break;
+    left -= cnt;
+    ++mb;
+  }
+  k0 = (mb * (BM / BK) + left) * BK;
+}
+
+__global__ void __launch_bounds__(NT, 1)
 density_kernel(int n, int npoint, const double *__restrict__ phi, long ld,
                const double *__restrict__ D, double *__restrict__ rho) {
-  __shared__ __align__(16) TileSmem sm;
-  __shared__ double red[16][BN];
-  const int t = threadIdx.x, tx = t % 16, ty = t / 16;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  DensSmem &sm = *reinterpret_cast<DensSmem *>(smem_raw);
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int wrow = (warp >> 2) * 64, wcol = (warp & 3) * 32;
   const int p0 = blockIdx.x * BN;
-  // load mapping: each thread loads 4 consecutive elements of one K row
-  const int lk = t / 32, lc = (t % 32) * 4;
-  double part[8];
-#pragma unroll
-  for (int j = 0; j < 8; ++j) part[j] = 0.0;
+  const int nblk = (n + BM - 1) / BM;
+  const int nk = (n + BK - 1) / BK;                 // stages of nu over the whole basis
+  int nstage = 0;
+  for (int mb = 0; mb < nblk; ++mb) nstage += nk - mb * (BM / BK);
 
-  const int nkb = (n + BK - 1) / BK;
-  for (int mu0 = 0; mu0 < n; mu0 += BM) {
-    double acc[8][8];
+  // copies of one stage: D' rows (8-byte copies, D rows need not be 16-byte
+  // aligned) and phi rows (16-byte copies; p0 + c is even, ld even)
+  auto load_stage = [&](int it) {
+    int mb, k0;
+    density_stage(it, nblk, nk, mb, k0);
+    const int slot = it % NS;
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < (BM * BK) / NT; ++i) {
+      const int e = t + NT * i, r = e / BK, c = e % BK;
+      const int mu = mb * BM + r, nu = k0 + c;
+      const bool v = mu < n && nu < n;
+      cp_async8(&sm.a[slot][r][c], D + (v ? (long)mu * n + nu : 0), v);
+    }
 #pragma unroll
-      for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+    for (int i = 0; i < (BK * BN / 2) / NT; ++i) {
+      const int e = t + NT * i, r = e / (BN / 2), c = (e % (BN / 2)) * 2;
+      const int nu = k0 + r;
+      const bool v = nu < n;
+      cp_async16(&sm.b[slot][r][c], phi + (v ? (long)nu * ld + p0 + c : 0), v);
+    }
+  };
 
-    double ra[4], rb[4];
-    auto gload = [&](int kb) {
-      const int nu = kb * BK + lk;
+  double part[4][2];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int mu = mu0 + lc + q;
-        ra[q] = (nu < n && mu < n) ? __ldg(D + (long)nu * n + mu) : 0.0;
-      }
-      if (nu < n) {
-        const double2 v0 = __ldg(reinterpret_cast<const double2 *>(phi + (long)nu * ld + p0 + lc));
-        const double2 v1 = __ldg(reinterpret_cast<const double2 *>(phi + (long)nu * ld + p0 + lc + 2));
-        rb[0] = v0.x; rb[1] = v0.y; rb[2] = v1.x; rb[3] = v1.y;
-      } else {
-        rb[0] = rb[1] = rb[2] = rb[3] = 0.0;
-      }
-    };
-    auto sstore = [&](int buf) {
+  for (int nt = 0; nt < 4; ++nt) part[nt][0] = part[nt][1] = 0.0;
+  double acc[4][4][4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        sm.a[buf][lk][lc + q] = ra[q];
-        sm.b[buf][lk][lc + q] = rb[q];
-      }
-    };
-    gload(0);
-    sstore(0);
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) acc[mt][nt][i] = 0.0;
+
+#pragma unroll
+  for (int i = 0; i < NS - 1; ++i) {
+    if (i < nstage) load_stage(i);
+    cp_async_commit();
+  }
+  for (int it = 0; it < nstage; ++it) {
+    cp_async_wait<NS - 2>();
     __syncthreads();
-    for (int kb = 0; kb < nkb; ++kb) {
-      const int cur = kb & 1;
-      if (kb + 1 < nkb) gload(kb + 1);
-      mma_slice(sm.a[cur], sm.b[cur], tx, ty, acc);
-      if (kb + 1 < nkb) sstore(cur ^ 1);
-      __syncthreads();
-    }
-    // epilogue: part[c] += sum_i T[mu_i][c] phi[mu_i][c]
+    if (it + NS - 1 < nstage) load_stage(it + NS - 1);
+    cp_async_commit();
+    int mb, k0;
+    density_stage(it, nblk, nk, mb, k0);
+    const int slot = it % NS;
+    // nu right of the diagonal block counts twice (D symmetric)
+    const double scale = (k0 >= (mb + 1) * BM) ? 2.0 : 1.0;
+    const double(*bt)[LDB] = sm.b[slot];
+    stage_mma(sm.a[slot], wrow, g, q, scale,
+              [&](int nt, int kk, double(&b)[2]) {
+                const int c = wcol + nt * 8 + g;
+                b[0] = bt[kk + q][c];
+                b[1] = bt[kk + q + 4][c];
+              },
+              acc);
+    // last stage of block mb: part[p] += sum_mu T'[mu][p] phi[mu][p]
+    if (k0 + BK >= nk * BK) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int mu = mu0 + row_of(ty, i);
-      if (mu < n) {
-        const double *prow = phi + (long)mu * ld + p0;
+      for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) part[j] = fma(acc[i][j], __ldg(prow + row_of(tx, j)), part[j]);
-      }
+        for (int h = 0; h < 2; ++h) {
+          const int mu = mb * BM + wrow + mt * 16 + g + 8 * h;
+          if (mu < n) {
+            const double *prow = phi + (long)mu * ld + p0 + wcol + 2 * q;
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+              const double2 f = __ldg(reinterpret_cast<const double2 *>(prow + nt * 8));
+              part[nt][0] = fma(acc[mt][nt][2 * h], f.x, part[nt][0]);
+              part[nt][1] = fma(acc[mt][nt][2 * h + 1], f.y, part[nt][1]);
+            }
+          }
+        }
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+          for (int i = 0; i < 4; ++i) acc[mt][nt][i] = 0.0;
     }
   }
-  // reduce the 16 row-groups (ty) sharing each column
+  cp_async_wait<0>();
+  // sum over the warp's rows (lanes of equal q), then over the two warp rows
 #pragma unroll
-  for (int j = 0; j < 8; ++j) red[ty][row_of(tx, j)] = part[j];
+  for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      double v = part[nt][j];
+      v += __shfl_xor_sync(0xffffffffu, v, 4);
+      v += __shfl_xor_sync(0xffffffffu, v, 8);
+      v += __shfl_xor_sync(0xffffffffu, v, 16);
+      part[nt][j] = v;
+    }
+  if (g == 0) {
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      sm.red[warp >> 2][wcol + nt * 8 + 2 * q] = part[nt][0];
+      sm.red[warp >> 2][wcol + nt * 8 + 2 * q + 1] = part[nt][1];
+    }
+  }
   __syncthreads();
-  if (t < BN) {
-    double s = 0.0;
-#pragma unroll
-    for (int r = 0; r < 16; ++r) s += red[r][t];
-    if (p0 + t < npoint) rho[p0 + t] = s;
-  }
+  if (t < BN && p0 + t < npoint) rho[p0 + t] = sm.red[0][t] + sm.red[1][t];
 }
 
 // --------------------------------------------------------------- quadrature
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 1)
 quadrature_kernel(int n, int npoint_pad, const double *__restrict__ phi,
                   const double *__restrict__ phib, long ld,
                   const double *__restrict__ wv, int nblk, int chunk,
                   double *__restrict__ work) {
-  __shared__ __align__(16) TileSmem sm;
-  const int t = threadIdx.x, tx = t % 16, ty = t / 16;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  QuadSmem &sm = *reinterpret_cast<QuadSmem *>(smem_raw);
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int wrow = (warp >> 2) * 64, wcol = (warp & 3) * 32;
   // upper-triangle tile index -> (mb, nb)
   int tile = blockIdx.x, mb = 0;
   {
@@ -170,66 +270,63 @@ quadrature_kernel(int n, int npoint_pad, const double *__restrict__ phi,
   const int mu0 = mb * BM, nu0 = nb * BN;
   const int k_begin = blockIdx.y * chunk;
   const int k_end = min(k_begin + chunk, npoint_pad);
-  // load mapping: thread loads 4 consecutive k of one row (rows t/2, k (t%2)*4)
-  const int lr = t / 2, lk = (t % 2) * 4;
-  const int mu_l = mu0 + lr, nu_l = nu0 + lr;
-  const double *arow = phi + (long)min(mu_l, n - 1) * ld;
-  const double *brow = phib + (long)min(nu_l, n - 1) * ld;
-  const bool aval = mu_l < n, bval = nu_l < n;
+  const int nstage = k_end > k_begin ? (k_end - k_begin) / BK : 0;
 
-  double acc[8][8];
+  // copies of one stage: 128 rows x 16 points of each operand (8 x 16 bytes
+  // per row) and the 16 weights; rows beyond n are zero filled
+  auto load_stage = [&](int it) {
+    const int slot = it % NS, k0 = k_begin + it * BK;
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+    for (int i = 0; i < (BM * BK / 2) / NT; ++i) {
+      const int e = t + NT * i, r = e / (BK / 2), c = (e % (BK / 2)) * 2;
+      const bool va = mu0 + r < n, vb = nu0 + r < n;
+      cp_async16(&sm.a[slot][r][c], phi + (va ? (long)(mu0 + r) * ld + k0 + c : 0), va);
+      cp_async16(&sm.b[slot][r][c], phib + (vb ? (long)(nu0 + r) * ld + k0 + c : 0), vb);
+    }
+    if (t < BK / 2) cp_async16(&sm.w[slot][2 * t], wv + k0 + 2 * t, true);
+  };
 
-  double ra[4], rb[4];
-  auto gload = [&](int k0) {
-    const int k = k0 + lk;
-    if (aval) {
-      const double2 v0 = __ldg(reinterpret_cast<const double2 *>(arow + k));
-      const double2 v1 = __ldg(reinterpret_cast<const double2 *>(arow + k + 2));
-      ra[0] = v0.x; ra[1] = v0.y; ra[2] = v1.x; ra[3] = v1.y;
-    } else {
-      ra[0] = ra[1] = ra[2] = ra[3] = 0.0;
-    }
-    if (bval) {
-      const double2 v0 = __ldg(reinterpret_cast<const double2 *>(brow + k));
-      const double2 v1 = __ldg(reinterpret_cast<const double2 *>(brow + k + 2));
-      const double2 w0 = __ldg(reinterpret_cast<const double2 *>(wv + k));
-      const double2 w1 = __ldg(reinterpret_cast<const double2 *>(wv + k + 2));
-      rb[0] = v0.x * w0.x; rb[1] = v0.y * w0.y; rb[2] = v1.x * w1.x; rb[3] = v1.y * w1.y;
-    } else {
-      rb[0] = rb[1] = rb[2] = rb[3] = 0.0;
-    }
-  };
-  auto sstore = [&](int buf) {
+  double acc[4][4][4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      sm.a[buf][lk + q][lr] = ra[q];
-      sm.b[buf][lk + q][lr] = rb[q];
-    }
-  };
-  if (k_begin < k_end) {
-    gload(k_begin);
-    sstore(0);
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) acc[mt][nt][i] = 0.0;
+
+#pragma unroll
+  for (int i = 0; i < NS - 1; ++i) {
+    if (i < nstage) load_stage(i);
+    cp_async_commit();
   }
-  __syncthreads();
-  int buf = 0;
-  for (int k0 = k_begin; k0 < k_end; k0 += BK) {
-    const bool more = k0 + BK < k_end;
-    if (more) gload(k0 + BK);
-    mma_slice(sm.a[buf], sm.b[buf], tx, ty, acc);
-    if (more) sstore(buf ^ 1);
+  for (int it = 0; it < nstage; ++it) {
+    cp_async_wait<NS - 2>();
     __syncthreads();
-    buf ^= 1;
+    if (it + NS - 1 < nstage) load_stage(it + NS - 1);
+    cp_async_commit();
+    const int slot = it % NS;
+    const double(*bt)[LDA] = sm.b[slot];
+    const double *w = sm.w[slot];
+    stage_mma(sm.a[slot], wrow, g, q, 1.0,
+              [&](int nt, int kk, double(&b)[2]) {
+                const int c = wcol + nt * 8 + g;
+                b[0] = bt[c][kk + q] * w[kk + q];
+                b[1] = bt[c][kk + q + 4] * w[kk + q + 4];
+              },
+              acc);
   }
+  cp_async_wait<0>();
   const int ntile = nblk * (nblk + 1) / 2;
   double *out = work + ((long)blockIdx.y * ntile + blockIdx.x) * (BM * BN);
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) out[row_of(ty, i) * BN + row_of(tx, j)] = acc[i][j];
+    for (int nt = 0; nt < 4; ++nt) {
+      const int r = wrow + mt * 16 + g, c = wcol + nt * 8 + 2 * q;
+      *reinterpret_cast<double2 *>(out + r * BN + c) = make_double2(acc[mt][nt][0], acc[mt][nt][1]);
+      *reinterpret_cast<double2 *>(out + (r + 8) * BN + c) =
+          make_double2(acc[mt][nt][2], acc[mt][nt][3]);
+    }
 }
 
 __global__ void quadrature_reduce_kernel(int n, int nblk, int nchunk,
@@ -293,7 +390,22 @@ cudaError_t launch_density_f64(int n, int npoint, const double *phi, long ld,
                                const double *D, double *rho, cudaStream_t s) {
   if (npoint <= 0) return cudaSuccess;
   const int blocks = (npoint + BN - 1) / BN;
-  density_kernel<<<blocks, NT, 0, s>>>(n, npoint, phi, ld, D, rho);
+  cudaError_t e = cudaFuncSetAttribute(density_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kDensSmem);
+  if (e != cudaSuccess) return e;
+  density_kernel<<<blocks, NT, kDensSmem, s>>>(n, npoint, phi, ld, D, rho);
+  return cudaGetLastError();
+}
+
+// the split-K quadrature kernel with its dynamic shared memory
+cudaError_t quadrature_launch(dim3 grid, int n, int npad, const double *phi, const double *phib,
+                              long ld, const double *wv, int nblk, int chunk, double *work,
+                              cudaStream_t s) {
+  cudaError_t e = cudaFuncSetAttribute(quadrature_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kQuadSmem);
+  if (e != cudaSuccess) return e;
+  quadrature_kernel<<<grid, NT, kQuadSmem, s>>>(n, npad, phi, phib, ld, wv, nblk, chunk, work);
   return cudaGetLastError();
 }
 
@@ -315,8 +427,7 @@ cudaError_t launch_quadrature_f64(int n, int npoint, const double *phi, long ld,
   const int nblk = (n + BM - 1) / BM;
   const int ntile = nblk * (nblk + 1) / 2;
   dim3 grid(ntile, nchunk);
-  quadrature_kernel<<<grid, NT, 0, s>>>(n, npad, phi, phib, ld, wv, nblk, chunk, work);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = quadrature_launch(grid, n, npad, phi, phib, ld, wv, nblk, chunk, work, s);
   if (e != cudaSuccess) return e;
   const long total = (long)ntile * BM * BN;
   const int rblocks = (int)std::min<long>((total + 255) / 256, 148 * 16);
@@ -443,9 +554,8 @@ int napmo_gpu_quadrature_noalloc(int n, int npoint, const double *phi, const dou
     nchunk = (npad + chunk - 1) / chunk;
   }
   dim3 grid(ntile, nchunk);
-  quadrature_kernel<<<grid, NT, 0, s>>>(n, npad, phi, psi ? psi : phi, ld, wv, nblk, chunk,
-                                        scratch);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = quadrature_launch(grid, n, npad, phi, psi ? psi : phi, ld, wv, nblk, chunk,
+                                    scratch, s);
   if (e != cudaSuccess) return set_error(kCudaError, std::string("quadrature: ") + cudaGetErrorString(e));
   const long total = (long)ntile * BM * BN;
   const int rblocks = (int)std::min<long>((total + 255) / 256, 148 * 16);

@@ -30,6 +30,13 @@ METRIC = 'grid Fock builds/s (C20H42 cc-pVDZ, 100x302 Becke grid)'
 UNIT = 'builds/s'
 WORKLOAD = 'C20H42/cc-pVDZ Cartesian n=510, Becke 100x302 per atom, N=1872400, lmax=14'
 SEED = 20261203
+# DRAM bytes per (atom, point) pair of the potential evaluation kernel
+# (profiles/poisson_kernels_C8H18_ncu.md: 122 MB read + 125 MB written for
+# 26 atoms x 785,200 points); scaled by the pairs of the measured workload
+EVAL_DRAM_BYTES_PER_PAIR = (122e6 + 125e6) / (26 * 785200)
+TRAFFIC_SOURCE = ('ncu dram__bytes_read.sum + dram__bytes_write.sum of eval_pairs_kernel at '
+                  'C8H18 100x302 (profiles/poisson_kernels_C8H18_ncu.md), 12.1 B per (atom, '
+                  'point) pair, scaled to this workload\'s pairs')
 
 
 def parse():
@@ -995,8 +1002,12 @@ def main():
     stream = torch.cuda.current_stream()
     F = torch.empty((n, n), dtype=torch.float64, device='cuda')
 
-    def timed_builds(precision):
+    def timed_builds(precision, screen=0.0, poisson_tol=None):
         fbld.set_precision(precision)
+        if precision == 'fp64':
+            fbld.set_fp64_screening(screen)
+        if poisson_tol is not None:
+            fbld.set_poisson_tolerance(poisson_tol)
         for _ in range(args.warmup):
             fbld.build(Dd, out=F)
         torch.cuda.synchronize()
@@ -1022,6 +1033,10 @@ def main():
 
     t_f64, clocks_f64, E_f64 = timed_builds('fp64')
     F64 = F.clone()
+    # the FP64 arm with the int8 mode's two precision-independent savings:
+    # point screening (1e-24) and the Poisson truncation (1e-9 a.u.)
+    t_f64s, _, E_f64s = timed_builds('fp64', screen=1e-24, poisson_tol=1e-9)
+    fbld.set_fp64_screening(0.0)
     t_tc, clocks_tc, E_tc = timed_builds('int8x4')
     tc_err = fbld.tc_status()
     dE = abs(E_tc - E_f64)
@@ -1041,7 +1056,7 @@ def main():
              'scheme': 'int8 slices (4 balanced base-256 digits per value, group exponents), '
                        'tcgen05 kind::i8 with exact int32 TMEM accumulation; 13 digit '
                        'products per contraction; Poisson FP64, its evaluation skipping '
-                       'l-blocks bounded below 1e-10 a.u. per (atom, radial interval)'}
+                       'l-blocks bounded below 1e-9 a.u. per (atom, radial interval)'}
 
     # ---- per-kernel timings (same stream) for the roofline
     def time_it(fn, reps=3):
@@ -1066,7 +1081,7 @@ def main():
         kernels['density_' + prec] = {'ms': td * 1e3, 'tflops': flops / td / 1e12}
         kernels['quadrature_' + prec] = {'ms': tq * 1e3, 'tflops': flops / tq / 1e12}
         # projection + radial solves + evaluation; int8x4 evaluates with the
-        # mode's truncation tolerance (l-blocks bounded below 1e-10 skipped)
+        # mode's truncation tolerance (l-blocks bounded below 1e-9 skipped)
         tp = time_it(lambda: fbld.coulomb_potential(rho))
         kernels['poisson_' + prec] = {'ms': tp * 1e3}
     fbld.set_precision(headline)
@@ -1142,7 +1157,12 @@ def main():
             issued = {'executed_fp64_tflops': flops_exec / td / 1e12,
                       'frac_executed': flops_exec / td / 1e12 / fp64}
             kernel_name = 'poisson(eval_pairs dominant)'
+            # DRAM bytes of the evaluation per launch: 12.1 B per (atom, point)
+            # pair (ncu at C8H18: 122 MB read + 125 MB written for 20.4 M
+            # pairs; pair lists and partial potentials grow with the pairs)
+            traffic = EVAL_DRAM_BYTES_PER_PAIR * natom * N
         else:
+            traffic = None
             flops_alg = flops
             achieved = flops / td / 1e12
             bound = 'tensor'
@@ -1174,12 +1194,21 @@ def main():
             'gpu_launches': launches_per_build * args.steps,
             'roofline': {'kernel': kernel_name, 'bound': bound, 'achieved': achieved,
                          'peak': peak, 'unit': 'TFLOP/s', 'frac': achieved / peak,
-                         'traffic': None, 'peak_source': peak_source,
+                         'traffic': traffic, 'traffic_source': TRAFFIC_SOURCE if traffic else None,
+                         'peak_source': peak_source,
                          'algorithmic_flops_per_launch': flops_alg, 'issued': issued},
             'stages_ms': {k: v * 1e3 for k, v in stages.items()},
             'grid_points_per_s': world * args.steps / t_dev * N,
             'fp64': {'builds_per_s': world * args.steps / t_f64,
                      'ms_per_build': t_f64 / args.steps * 1e3, 'fp64_gemm_tflops': fp64},
+            'fp64_screened_truncated': {
+                'builds_per_s': world * args.steps / t_f64s,
+                'ms_per_build': t_f64s / args.steps * 1e3,
+                'energy_difference_eh': abs(E_f64s - E_f64),
+                'mixed_speedup_vs_this_arm': t_f64s / t_tc,
+                'note': 'FP64 contractions with the int8 mode\'s point screening (1e-24) and '
+                        'Poisson truncation (1e-9 a.u.): the speed-up over this arm is the '
+                        'tensor cores\' share'},
             'mixed': mixed,
             'kernels': kernels,
             'scf': scf,

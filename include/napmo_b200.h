@@ -372,13 +372,19 @@ int napmo_fock_plan_set_precision(void *plan, int mode);
  * (atom, radial interval), the highest l-blocks whose bounded contribution
  * sums to at most tol are skipped.  No counterpart in nAPMO (evaluate.cpp:
  * 129-220 sums every (l, m)).  set_precision resets it: 0 for mode 0 (every
- * (l, m), as nAPMO), 1e-10 for mode 1. */
+ * (l, m), as nAPMO), 1e-9 for mode 1. */
 int napmo_fock_plan_set_poisson_tolerance(void *plan, double tol);
 /* Point screening of the plan's current mode (mode 1 keeps the points with
  * |w_becke w| max_mu phi_mu(p)^2 >= 1e-24; rho and v are 0 at the others).
  * *keep: device flags, one int per grid point (null when all points are used);
  * *nkeep: kept points.  No counterpart in nAPMO (every point is used). */
 int napmo_fock_plan_screening(void *plan, const int **keep, int *nkeep);
+/* Point screening of the FP64 mode (precision 1 always screens): tol > 0
+ * keeps the points with |wb w| max_mu phi_mu(p)^2 >= tol (1e-24 is the int8
+ * mode's threshold) for the density, the potential evaluation and the
+ * quadrature; 0 restores every point (nAPMO's sums).  No counterpart in nAPMO.
+ * Synchronises. */
+int napmo_fock_plan_set_fp64_screening(void *plan, double tol, void *stream);
 /* Device bytes of the plan's int8 operand images and scratch. */
 long napmo_fock_plan_int8_bytes(void *plan);
 /* Batched Fock builds of many plans (molecules of uneven size) by one CUDA
@@ -420,6 +426,11 @@ int napmo_basis_set_origins(void *basis, const double *origins);
 /* Error word of the tensor-core kernels (0 none, 5 an mbarrier wait ran out);
  * synchronises the stream, `reset` nonzero clears it. */
 int napmo_tc_status(void *stream, int reset);
+/* Runs the tensor-core kernels' bounded mbarrier wait on barriers nothing
+ * arrives on (about 2 s): out_dev[0..1] (device ints) receive 0 when both
+ * waiting roles gave up; napmo_tc_status then reads 5.  A test of the timeout
+ * path without a fault; no counterpart in nAPMO. */
+int napmo_tc_wait_selftest(int *out_dev, void *stream);
 
 #ifdef __cplusplus
 }

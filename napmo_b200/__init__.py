@@ -22,5 +22,6 @@ from .wavefunction import WaveFunction, compute_coulomb, compute_nuclear
 from .fock import FockBatch, FockBuilder
 from .functional import Functional, epc17_2, isc_functional_selector
 from .numeric import PSIN, PSIO_BECKE, GridOperators, compute_dpsi, compute_kinetic
+from .solver import DFT, HF
 
 ANGSTROM_TO_BOHR = 1.889726133921252

@@ -240,6 +240,7 @@ _SIGS = [
     ('napmo_gpu_poisson_many', c_int, [c_void_p, c_int, c_void_p, c_long, c_int, c_void_p,
                                        c_void_p]),
     ('napmo_fock_plan_screening', c_int, [c_void_p, POINTER(c_void_p), POINTER(c_int)]),
+    ('napmo_fock_plan_set_fp64_screening', c_int, [c_void_p, c_double, c_void_p]),
     ('napmo_fock_plan_int8_bytes', c_long, [c_void_p]),
     ('napmo_fock_batch_new', c_void_p, [c_void_p, c_int, c_double]),
     ('napmo_fock_batch_free', None, [c_void_p]),
@@ -253,6 +254,7 @@ _SIGS = [
     ('napmo_grid_energy_gradient', c_int,
      [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ('napmo_tc_status', c_int, [c_void_p, c_int]),
+    ('napmo_tc_wait_selftest', c_int, [c_void_p, c_void_p]),
     ('napmo_gpu_quadrature_noalloc', c_int,
      [c_int, c_int, c_void_p, c_void_p, c_long, c_void_p, c_void_p, c_void_p]),
 ]

@@ -8,7 +8,8 @@
 // the reference bit for bit.
 //
 // Layout: one thread per grid point.  The atom origins, the packed R_ij /
-// a_ij triangles and the per-atom point offsets live in shared memory; each
+// a_ij triangles and the per-atom point offsets live in shared memory (in
+// global memory, read as warp-wide broadcasts, above ~130 centres); each
 // thread's distances r_A to all atoms are cached in a shared column
 // [atom][thread] (bank-conflict free), computed once instead of once per
 // pair.  The owner atom of a point is found from the per-atom offsets, so
@@ -46,7 +47,13 @@ __device__ __forceinline__ int owner_of(int p, const int *off, int nc) {
 }
 
 // Cell-function product p_i = prod_{j != i} s(nu_ij) and the final ratio.
-template <bool kCacheR>
+// kSmem: the centre tables (origins, R_ij, a_ij, offsets) are staged in
+// shared memory; without it (more centres than fit, about 130) they are read
+// from global memory, where every lane of a warp reads the same address in
+// the same order (one broadcast per load, L1-resident).  kCacheR: each
+// thread's distances to all centres are cached in shared memory.  The
+// arithmetic is the same in every variant.
+template <bool kCacheR, bool kSmem>
 __global__ void __launch_bounds__(kBeckeThreads)
 becke_kernel(int npoint, int nc, const double *__restrict__ gx,
              const double *__restrict__ gy, const double *__restrict__ gz,
@@ -55,19 +62,27 @@ becke_kernel(int npoint, int nc, const double *__restrict__ gx,
              double *__restrict__ out) {
   extern __shared__ double smem[];
   const int tri = nc * (nc + 1) / 2;
-  double *s_origin = smem;                 // 3 * nc
-  double *s_R = s_origin + 3 * nc;         // tri
-  double *s_a = s_R + tri;                 // tri
-  double *s_r = s_a + tri;                 // nc * blockDim (kCacheR)
-  int *s_off = reinterpret_cast<int *>(s_r + (kCacheR ? nc * kBeckeThreads : 0));
-
-  for (int i = threadIdx.x; i < 3 * nc; i += blockDim.x) s_origin[i] = g_origin[i];
-  for (int i = threadIdx.x; i < tri; i += blockDim.x) {
-    s_R[i] = g_R[i];
-    s_a[i] = g_a[i];
+  const double *s_origin = g_origin, *s_R = g_R, *s_a = g_a;
+  const int *s_off = g_off;
+  double *s_r = smem;                      // nc * blockDim (kCacheR)
+  if (kSmem) {
+    double *o = smem;                      // 3 * nc
+    double *R = o + 3 * nc;                // tri
+    double *a = R + tri;                   // tri
+    s_r = a + tri;
+    int *off = reinterpret_cast<int *>(s_r + (kCacheR ? nc * kBeckeThreads : 0));
+    for (int i = threadIdx.x; i < 3 * nc; i += blockDim.x) o[i] = g_origin[i];
+    for (int i = threadIdx.x; i < tri; i += blockDim.x) {
+      R[i] = g_R[i];
+      a[i] = g_a[i];
+    }
+    for (int i = threadIdx.x; i <= nc; i += blockDim.x) off[i] = g_off[i];
+    __syncthreads();
+    s_origin = o;
+    s_R = R;
+    s_a = a;
+    s_off = off;
   }
-  for (int i = threadIdx.x; i <= nc; i += blockDim.x) s_off[i] = g_off[i];
-  __syncthreads();
 
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npoint) return;
@@ -117,24 +132,33 @@ cudaError_t launch_becke_weights(int npoint, int ncenter, const double *x,
   const size_t base = (3 * (size_t)ncenter + 2 * tri) * sizeof(double) +
                       ((size_t)ncenter + 1) * sizeof(int);
   const size_t cached = base + (size_t)ncenter * kBeckeThreads * sizeof(double);
+  const size_t rcache = (size_t)ncenter * kBeckeThreads * sizeof(double);
   const size_t limit = 200 * 1024;
   const int blocks = (npoint + kBeckeThreads - 1) / kBeckeThreads;
+  cudaError_t e = cudaSuccess;
   if (cached <= limit) {
-    cudaError_t e = cudaFuncSetAttribute(becke_kernel<true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)cached);
+    e = cudaFuncSetAttribute(becke_kernel<true, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cached);
     if (e != cudaSuccess) return e;
-    becke_kernel<true><<<blocks, kBeckeThreads, cached, s>>>(
+    becke_kernel<true, true><<<blocks, kBeckeThreads, cached, s>>>(
         npoint, ncenter, x, y, z, origin, Rij, aij, atom_offset, out);
   } else if (base <= limit) {
-    cudaError_t e = cudaFuncSetAttribute(becke_kernel<false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)base);
+    e = cudaFuncSetAttribute(becke_kernel<false, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)base);
     if (e != cudaSuccess) return e;
-    becke_kernel<false><<<blocks, kBeckeThreads, base, s>>>(
+    becke_kernel<false, true><<<blocks, kBeckeThreads, base, s>>>(
+        npoint, ncenter, x, y, z, origin, Rij, aij, atom_offset, out);
+  } else if (rcache <= limit) {
+    // tables from global memory, distances cached in shared memory
+    e = cudaFuncSetAttribute(becke_kernel<true, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rcache);
+    if (e != cudaSuccess) return e;
+    becke_kernel<true, false><<<blocks, kBeckeThreads, rcache, s>>>(
         npoint, ncenter, x, y, z, origin, Rij, aij, atom_offset, out);
   } else {
-    return cudaErrorInvalidValue;  // > ~130 centres per grid: not supported
+    // any number of centres: tables from global memory, distances recomputed
+    becke_kernel<false, false><<<blocks, kBeckeThreads, 0, s>>>(
+        npoint, ncenter, x, y, z, origin, Rij, aij, atom_offset, out);
   }
   return cudaGetLastError();
 }

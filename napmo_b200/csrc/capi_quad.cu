@@ -3,6 +3,8 @@
 // the device-pointer twins napmo_gpu_density / napmo_gpu_quadrature, and the
 // Fock-build plan that keeps phi, the grid and the Poisson tables resident in
 // HBM across SCF iterations.
+#include <algorithm>
+#include <atomic>
 #include <vector>
 
 #include "capi_common.cuh"
@@ -24,8 +26,11 @@ int run_poisson_many(BeckeGrid *g, PoissonPlan *p, int k, const double *rho_dev,
 // Truncation tolerance (a.u.) of the Poisson potential evaluation that
 // precision 1 selects: each (atom, radial interval) drops l-blocks whose
 // bounded contribution sums to at most this, so every point's potential moves
-// by at most natom x 1e-10, well inside that mode's 1e-6 Eh energy budget.
-constexpr double kMixedPoissonTol = 1e-10;
+// by at most natom x 1e-9.  Measured at C20H42 (62 atoms, int8 build against
+// the untruncated FP64 one): energy error 2.45e-8 Eh at 1e-10, 2.95e-8 at
+// 1e-9, 8.1e-8 at 1e-8, 1.0e-6 at 1e-7 -- 1e-9 keeps a factor 30 inside the
+// mode's 1e-6 Eh budget.
+constexpr double kMixedPoissonTol = 1e-9;
 
 // Point screening of precision 1: points with |wb w| max_mu phi_mu(p)^2 below
 // this carry no weight that matters (each changes an element of F by at most
@@ -88,6 +93,13 @@ struct FockPlan {
   long ld = 0;
   DevBuf<double> phi, rho, v, wv, work, D, F, vext;
   Int8Plan *i8 = nullptr;
+  // FP64 point screening (napmo_fock_plan_set_fp64_screening): keep flags,
+  // the 16-point blocks (quadrature) and 128-point groups (density) holding a
+  // kept point; key names the flags for the Poisson solve's screened lists
+  double fp64_screen = 0.0;
+  DevBuf<int> keep64, blocks64, groups64;
+  int nblocks64 = 0, ngroups64 = 0;
+  unsigned long long keep64_key = 0;
   ~FockPlan() {
     if (i8) int8_plan_destroy(i8);
   }
@@ -96,25 +108,68 @@ struct FockPlan {
 // rho = density of D, in the plan's precision.
 int plan_density(FockPlan *p, const double *D, double *rho, cudaStream_t s) {
   if (p->mode == 1) return int8_density(p->i8, D, rho, s);
-  NAPMO_TRY_CUDA(launch_density_f64(p->n, p->grid->size, p->phi.p, p->ld, D, rho, s), "density");
+  const bool scr = p->fp64_screen > 0.0;
+  NAPMO_TRY_CUDA(launch_density_f64(p->n, p->grid->size, p->phi.p, p->ld, D, rho, s,
+                                    scr ? p->groups64.p : nullptr, p->ngroups64,
+                                    scr ? p->keep64.p : nullptr),
+                 "density");
   return kOk;
 }
 
 // F = phi diag(p->wv) phi^T, in the plan's precision.
 int plan_quadrature(FockPlan *p, double *F, cudaStream_t s) {
   if (p->mode == 1) return int8_quadrature(p->i8, p->phi.p, p->wv.p, F, s);
+  const bool scr = p->fp64_screen > 0.0;
   NAPMO_TRY_CUDA(launch_quadrature_f64(p->n, p->grid->size, p->phi.p, p->ld, p->wv.p, F,
-                                       p->work.p, s),
+                                       p->work.p, s, nullptr, scr ? p->blocks64.p : nullptr,
+                                       p->nblocks64),
                  "quadrature");
   return kOk;
 }
 
-// Screening flags of the plan's grid points in precision 1 (null otherwise).
+// Screening flags of the plan's grid points: precision 1 always screens, FP64
+// when napmo_fock_plan_set_fp64_screening enabled it (null otherwise).
 const int *plan_keep(const FockPlan *p) {
-  return p->mode == 1 && p->i8 ? int8_plan_keep(p->i8) : nullptr;
+  if (p->mode == 1) return p->i8 ? int8_plan_keep(p->i8) : nullptr;
+  return p->fp64_screen > 0.0 ? p->keep64.p : nullptr;
 }
 static unsigned long long plan_keep_key(const FockPlan *p) {
-  return p->mode == 1 && p->i8 ? int8_plan_serial(p->i8) : 0;
+  if (p->mode == 1) return p->i8 ? int8_plan_serial(p->i8) : 0;
+  return p->fp64_screen > 0.0 ? p->keep64_key : 0;
+}
+
+// FP64 screening of the plan's current phi: flags, then the block and group
+// lists (read back once; synchronises).
+static int build_fp64_screening(FockPlan *p, double tol, cudaStream_t s) {
+  BeckeGrid *g = p->grid;
+  const int N = g->size, nb = (N + 15) / 16, ng = (N + 127) / 128;
+  DevBuf<int> bf, gf;
+  NAPMO_TRY_CUDA(p->keep64.alloc(N), "alloc screening");
+  NAPMO_TRY_CUDA(bf.alloc(nb), "alloc screening");
+  NAPMO_TRY_CUDA(gf.alloc(ng), "alloc screening");
+  NAPMO_TRY_CUDA(launch_fp64_screening(p->n, N, p->phi.p, p->ld, g->dev.wb, g->dev.w, tol,
+                                       p->keep64.p, bf.p, gf.p, s),
+                 "screening");
+  std::vector<int> hb(nb), hg(ng), lb, lg;
+  NAPMO_TRY_CUDA(cudaMemcpyAsync(hb.data(), bf.p, nb * sizeof(int), cudaMemcpyDeviceToHost, s),
+                 "screening");
+  NAPMO_TRY_CUDA(cudaMemcpyAsync(hg.data(), gf.p, ng * sizeof(int), cudaMemcpyDeviceToHost, s),
+                 "screening");
+  NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "screening");
+  for (int i = 0; i < nb; ++i)
+    if (hb[i]) lb.push_back(i);
+  for (int i = 0; i < ng; ++i)
+    if (hg[i]) lg.push_back(i);
+  NAPMO_TRY_CUDA(lb.empty() ? p->blocks64.alloc(1) : p->blocks64.upload(lb, s), "screening");
+  NAPMO_TRY_CUDA(lg.empty() ? p->groups64.alloc(1) : p->groups64.upload(lg, s), "screening");
+  NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "screening");
+  p->nblocks64 = (int)lb.size();
+  p->ngroups64 = (int)lg.size();
+  // a key no other flags share (the int8 plans count from 1 upwards)
+  static std::atomic<unsigned long long> next{1};
+  p->keep64_key = (1ull << 63) | next++;
+  p->fp64_screen = tol;
+  return kOk;
 }
 
 // The build chain of napmo_fock_plan_build (stream-ordered, no host
@@ -331,6 +386,10 @@ int napmo_fock_plan_refresh(FockPlan *p, void *stream) {
     }
     NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "refresh");
     ++p->generation;
+    if (p->fp64_screen > 0.0) {
+      e = build_fp64_screening(p, p->fp64_screen, s);
+      if (e) return e;
+    }
     if (p->i8) {
       int8_plan_destroy(p->i8);
       p->i8 = nullptr;
@@ -518,6 +577,25 @@ int napmo_fock_plan_set_poisson_tolerance(FockPlan *p, double tol) {
   });
 }
 
+// Point screening of the FP64 mode (precision 1 always screens): tol > 0
+// keeps only the points with |wb w| max_mu phi_mu(p)^2 >= tol (1e-24 is the
+// int8 mode's threshold), so that the density, the potential evaluation and
+// the quadrature skip the rest; 0 uses every point (nAPMO's sums).  Builds the
+// flags from the plan's current phi (synchronises).
+int napmo_fock_plan_set_fp64_screening(FockPlan *p, double tol, void *stream) {
+  return napmo::guarded([&] {
+    NAPMO_REQUIRE(tol >= 0.0 && tol < 1.0, "screening tolerance must be in [0, 1)");
+    if (tol > 0.0) {
+      int e = napmo::build_fp64_screening(p, tol, (cudaStream_t)stream);
+      if (e) return e;
+    } else {
+      p->fp64_screen = 0.0;
+    }
+    ++p->generation;
+    return napmo::kOk;
+  });
+}
+
 // Point screening of the plan's current mode: *keep receives the device flags
 // (one int per grid point, 1 = kept; null when every point is used) and
 // *nkeep the number of kept points.
@@ -525,7 +603,17 @@ int napmo_fock_plan_screening(FockPlan *p, const int **keep, int *nkeep) {
   return napmo::guarded([&] {
     const int *k = napmo::plan_keep(p);
     *keep = k;
-    *nkeep = k ? napmo::int8_plan_npoint(p->i8) : p->grid->size;
+    int nk = p->grid->size;
+    if (k && p->mode == 1) {
+      nk = napmo::int8_plan_npoint(p->i8);
+    } else if (k) {
+      std::vector<int> h(p->grid->size);
+      NAPMO_TRY_CUDA(cudaMemcpy(h.data(), k, h.size() * sizeof(int), cudaMemcpyDeviceToHost),
+                     "screening flags");
+      nk = 0;
+      for (int x : h) nk += x;
+    }
+    *nkeep = nk;
     return napmo::kOk;
   });
 }
@@ -540,6 +628,14 @@ long napmo_fock_plan_int8_bytes(FockPlan *p) {
 // wait ran out); synchronises the stream.  `reset` nonzero clears it.
 int napmo_tc_status(void *stream, int reset) {
   return napmo::tc_error_status((cudaStream_t)stream, reset != 0);
+}
+
+// Runs the tensor-core kernels' bounded mbarrier wait on barriers that
+// nothing arrives on (about 2 s), so that the timeout path is exercised
+// without a fault: out_dev[0] and [1] (device ints) receive 0 when the two
+// waiting roles gave up, and napmo_tc_status then reads 5.
+int napmo_tc_wait_selftest(int *out_dev, void *stream) {
+  return napmo::guarded([&] { return napmo::tc_wait_selftest(out_dev, (cudaStream_t)stream); });
 }
 
 }  // extern "C"

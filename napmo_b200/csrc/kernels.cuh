@@ -26,14 +26,25 @@ cudaError_t launch_basis_values(const DeviceBasis &b, int npoint, const double *
 //   rho[p] = sum_{mu,nu} D[mu][nu] phi[mu][p] phi[nu][p]
 //   F[mu][nu] = sum_p phi[mu][p] wv[p] phi[nu][p]  (upper triangle mirrored)
 size_t density_workspace_bytes(int n, int npoint);
+// groups / ngroup (optional): only these 128-point groups are computed (the
+// rest of rho is zeroed); keep (optional): rho = 0 at dropped points.
 cudaError_t launch_density_f64(int n, int npoint, const double *phi, long ld,
-                               const double *D, double *rho, cudaStream_t s);
+                               const double *D, double *rho, cudaStream_t s,
+                               const int *groups = nullptr, int ngroup = 0,
+                               const int *keep = nullptr);
 size_t quadrature_workspace_bytes(int n, int npoint);
 // `phib` (default phi) is the second operand; wv must be zero-padded to the
-// next multiple of 128 points and phi rows zero beyond npoint.
+// next multiple of 128 points and phi rows zero beyond npoint.  blocks /
+// nblock (optional): the sum runs over these 16-point blocks only.
 cudaError_t launch_quadrature_f64(int n, int npoint, const double *phi, long ld,
                                   const double *wv, double *F, double *work,
-                                  cudaStream_t s, const double *phib = nullptr);
+                                  cudaStream_t s, const double *phib = nullptr,
+                                  const int *blocks = nullptr, int nblock = 0);
+// FP64 point screening: keep[p] (|wb w| max_mu phi_mu(p)^2 >= tol), and the
+// flags of the 16-point blocks and 128-point groups holding a kept point.
+cudaError_t launch_fp64_screening(int n, int npoint, const double *phi, long ld, const double *wb,
+                                  const double *w, double tol, int *keep, int *block_flags,
+                                  int *group_flags, cudaStream_t s);
 inline long padded_points(int npoint) { return ((long)npoint + 127) / 128 * 128; }
 // Combined quadrature weight wv[p] = wb[p] * w[p] * (q * v[p] + vext[p]).
 cudaError_t launch_combine_weights(int npoint, const double *wb, const double *w,
@@ -68,5 +79,6 @@ int int8_quadrature(Int8Plan *p, const double *phi, const double *wv, double *F,
 // Returns the device error word of the tensor-core kernels (0 = none), after
 // synchronising `s`; `reset` clears it.
 int tc_error_status(cudaStream_t s, bool reset);
+int tc_wait_selftest(int *out_dev, cudaStream_t s);
 
 }  // namespace napmo

@@ -29,6 +29,7 @@
 // FP64 accumulators per thread), 16 points (quadrature) or 16 functions
 // (density) per stage.  Shared-memory rows are padded to a stride of 4 mod 16
 // doubles, so the fragment loads of each half-warp hit 16 distinct banks.
+#include <cstdint>
 #include <string>
 
 #include "common.h"
@@ -92,7 +93,7 @@ __device__ __forceinline__ void dmma(double (&d)[4], const double (&a)[4], const
 // over one stage: A fragments from a[row][k], B fragments from bf(col, k).
 template <typename BFrag>
 __device__ __forceinline__ void stage_mma(const double (*a)[LDA], int wrow, int g, int q,
-                                          double scale, BFrag bf, double (&acc)[4][4][4]) {
+                                          BFrag bf, double (&acc)[4][4][4]) {
 #pragma unroll
   for (int kk = 0; kk < BK; kk += 8) {
     double b[4][2];
@@ -101,11 +102,8 @@ __device__ __forceinline__ void stage_mma(const double (*a)[LDA], int wrow, int 
 #pragma unroll
     for (int mt = 0; mt < 4; ++mt) {
       const int r = wrow + mt * 16 + g;
-      double af[4] = {a[r][kk + q], a[r + 8][kk + q], a[r][kk + q + 4], a[r + 8][kk + q + 4]};
-      if (scale != 1.0) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i) af[i] *= scale;
-      }
+      const double af[4] = {a[r][kk + q], a[r + 8][kk + q], a[r][kk + q + 4],
+                            a[r + 8][kk + q + 4]};
 #pragma unroll
       for (int nt = 0; nt < 4; ++nt) dmma(acc[mt][nt], af, b[nt]);
     }
@@ -114,45 +112,72 @@ __device__ __forceinline__ void stage_mma(const double (*a)[LDA], int wrow, int 
 
 // ------------------------------------------------------------------ density
 // Stages of a CTA: block mb of mu takes nu from mb*BM to n (rounded up to BK),
-// the blocks one after the other.
-__device__ __forceinline__ void density_stage(int it, int nblk, int nk, int &mb, int &k0) {
+// the blocks one after the other; within a block the nu right of the
+// diagonal block come first and the diagonal block's own nu last, so the
+// doubling of the off-diagonal part is one multiply of the accumulators
+// before the first diagonal stage.  Returns k0 of stage `it` and sets its
+// block, whether it is the block's first diagonal stage, and whether it is
+// the block's last stage.
+__device__ __forceinline__ int density_stage(int it, int nblk, int nk, int &mb, bool &first_diag,
+                                             bool &last) {
+  constexpr int SB = BM / BK;                   // stages per 128 functions
   mb = 0;
   int left = it;
   while (mb < nblk) {
-    const int cnt = nk - mb * (BM / BK);
+    const int cnt = nk - mb * SB;
     if (left < cnt) break;
     left -= cnt;
     ++mb;
   }
-  k0 = (mb * (BM / BK) + left) * BK;
+  const int ndiag = min(SB, nk - mb * SB);      // diagonal-block stages
+  const int noff = nk - mb * SB - ndiag;        // stages right of it
+  last = left == noff + ndiag - 1;
+  first_diag = left == noff;
+  return left < noff ? ((mb + 1) * SB + left) * BK : (mb * SB + left - noff) * BK;
 }
 
+// groups (optional): the 128-point groups to compute (screened plans; the
+// others hold no kept point); keep (optional): rho = 0 at dropped points.
+template <bool kVecD>
 __global__ void __launch_bounds__(NT, 1)
 density_kernel(int n, int npoint, const double *__restrict__ phi, long ld,
-               const double *__restrict__ D, double *__restrict__ rho) {
+               const double *__restrict__ D, double *__restrict__ rho,
+               const int *__restrict__ groups, const int *__restrict__ keep) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   DensSmem &sm = *reinterpret_cast<DensSmem *>(smem_raw);
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int g = lane >> 2, q = lane & 3;
   const int wrow = (warp >> 2) * 64, wcol = (warp & 3) * 32;
-  const int p0 = blockIdx.x * BN;
+  const int p0 = (groups ? groups[blockIdx.x] : (int)blockIdx.x) * BN;
   const int nblk = (n + BM - 1) / BM;
   const int nk = (n + BK - 1) / BK;                 // stages of nu over the whole basis
   int nstage = 0;
   for (int mb = 0; mb < nblk; ++mb) nstage += nk - mb * (BM / BK);
 
-  // copies of one stage: D' rows (8-byte copies, D rows need not be 16-byte
-  // aligned) and phi rows (16-byte copies; p0 + c is even, ld even)
+  // copies of one stage: D' rows (16-byte copies when n is even and D is
+  // 16-byte aligned, else 8-byte) and phi rows (16-byte copies; p0 + c is
+  // even, ld even)
   auto load_stage = [&](int it) {
-    int mb, k0;
-    density_stage(it, nblk, nk, mb, k0);
+    int mb;
+    bool fd, ls;
+    const int k0 = density_stage(it, nblk, nk, mb, fd, ls);
     const int slot = it % NS;
+    if (kVecD) {
 #pragma unroll
-    for (int i = 0; i < (BM * BK) / NT; ++i) {
-      const int e = t + NT * i, r = e / BK, c = e % BK;
-      const int mu = mb * BM + r, nu = k0 + c;
-      const bool v = mu < n && nu < n;
-      cp_async8(&sm.a[slot][r][c], D + (v ? (long)mu * n + nu : 0), v);
+      for (int i = 0; i < (BM * BK / 2) / NT; ++i) {
+        const int e = t + NT * i, r = e / (BK / 2), c = (e % (BK / 2)) * 2;
+        const int mu = mb * BM + r, nu = k0 + c;
+        const bool v = mu < n && nu < n;   // n even: nu + 1 < n as well
+        cp_async16(&sm.a[slot][r][c], D + (v ? (long)mu * n + nu : 0), v);
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < (BM * BK) / NT; ++i) {
+        const int e = t + NT * i, r = e / BK, c = e % BK;
+        const int mu = mb * BM + r, nu = k0 + c;
+        const bool v = mu < n && nu < n;
+        cp_async8(&sm.a[slot][r][c], D + (v ? (long)mu * n + nu : 0), v);
+      }
     }
 #pragma unroll
     for (int i = 0; i < (BK * BN / 2) / NT; ++i) {
@@ -184,13 +209,21 @@ density_kernel(int n, int npoint, const double *__restrict__ phi, long ld,
     __syncthreads();
     if (it + NS - 1 < nstage) load_stage(it + NS - 1);
     cp_async_commit();
-    int mb, k0;
-    density_stage(it, nblk, nk, mb, k0);
+    int mb;
+    bool first_diag, last;
+    density_stage(it, nblk, nk, mb, first_diag, last);
     const int slot = it % NS;
-    // nu right of the diagonal block counts twice (D symmetric)
-    const double scale = (k0 >= (mb + 1) * BM) ? 2.0 : 1.0;
+    if (first_diag) {
+      // the part right of the diagonal block counts twice (D symmetric)
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+          for (int i = 0; i < 4; ++i) acc[mt][nt][i] *= 2.0;
+    }
     const double(*bt)[LDB] = sm.b[slot];
-    stage_mma(sm.a[slot], wrow, g, q, scale,
+    stage_mma(sm.a[slot], wrow, g, q,
               [&](int nt, int kk, double(&b)[2]) {
                 const int c = wcol + nt * 8 + g;
                 b[0] = bt[kk + q][c];
@@ -198,7 +231,7 @@ density_kernel(int n, int npoint, const double *__restrict__ phi, long ld,
               },
               acc);
     // last stage of block mb: part[p] += sum_mu T'[mu][p] phi[mu][p]
-    if (k0 + BK >= nk * BK) {
+    if (last) {
 #pragma unroll
       for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
@@ -242,15 +275,20 @@ density_kernel(int n, int npoint, const double *__restrict__ phi, long ld,
     }
   }
   __syncthreads();
-  if (t < BN && p0 + t < npoint) rho[p0 + t] = sm.red[0][t] + sm.red[1][t];
+  if (t < BN && p0 + t < npoint)
+    rho[p0 + t] = (keep && !keep[p0 + t]) ? 0.0 : sm.red[0][t] + sm.red[1][t];
 }
 
 // --------------------------------------------------------------- quadrature
+// Without `blocks` the K range is every point (npoint_pad, chunks of `chunk`
+// points); with it (screened plans) the K range is the list of 16-point
+// blocks holding a kept point, npoint_pad = 16 x their count and `chunk` a
+// multiple of 16 as before.
 __global__ void __launch_bounds__(NT, 1)
 quadrature_kernel(int n, int npoint_pad, const double *__restrict__ phi,
                   const double *__restrict__ phib, long ld,
                   const double *__restrict__ wv, int nblk, int chunk,
-                  double *__restrict__ work) {
+                  double *__restrict__ work, const int *__restrict__ blocks) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   QuadSmem &sm = *reinterpret_cast<QuadSmem *>(smem_raw);
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -275,7 +313,8 @@ quadrature_kernel(int n, int npoint_pad, const double *__restrict__ phi,
   // copies of one stage: 128 rows x 16 points of each operand (8 x 16 bytes
   // per row) and the 16 weights; rows beyond n are zero filled
   auto load_stage = [&](int it) {
-    const int slot = it % NS, k0 = k_begin + it * BK;
+    const int kv = k_begin + it * BK;
+    const int slot = it % NS, k0 = blocks ? blocks[kv / BK] * BK : kv;
 #pragma unroll
     for (int i = 0; i < (BM * BK / 2) / NT; ++i) {
       const int e = t + NT * i, r = e / (BK / 2), c = (e % (BK / 2)) * 2;
@@ -307,7 +346,7 @@ quadrature_kernel(int n, int npoint_pad, const double *__restrict__ phi,
     const int slot = it % NS;
     const double(*bt)[LDA] = sm.b[slot];
     const double *w = sm.w[slot];
-    stage_mma(sm.a[slot], wrow, g, q, 1.0,
+    stage_mma(sm.a[slot], wrow, g, q,
               [&](int nt, int kk, double(&b)[2]) {
                 const int c = wcol + nt * 8 + g;
                 b[0] = bt[c][kk + q] * w[kk + q];
@@ -387,25 +426,37 @@ inline int pad_points(int npoint) { return ((npoint + BN - 1) / BN) * BN; }
 size_t density_workspace_bytes(int, int) { return 0; }
 
 cudaError_t launch_density_f64(int n, int npoint, const double *phi, long ld,
-                               const double *D, double *rho, cudaStream_t s) {
+                               const double *D, double *rho, cudaStream_t s,
+                               const int *groups, int ngroup, const int *keep) {
   if (npoint <= 0) return cudaSuccess;
-  const int blocks = (npoint + BN - 1) / BN;
-  cudaError_t e = cudaFuncSetAttribute(density_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  int blocks = (npoint + BN - 1) / BN;
+  if (groups) {
+    // groups without a kept point are not computed: their rho is 0
+    cudaError_t e = cudaMemsetAsync(rho, 0, (size_t)npoint * sizeof(double), s);
+    if (e != cudaSuccess) return e;
+    blocks = ngroup;
+    if (blocks == 0) return cudaSuccess;
+  }
+  // 16-byte copies of D rows need n even and a 16-byte aligned D
+  const bool vec = n % 2 == 0 && reinterpret_cast<uintptr_t>(D) % 16 == 0;
+  auto kern = vec ? density_kernel<true> : density_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kDensSmem);
   if (e != cudaSuccess) return e;
-  density_kernel<<<blocks, NT, kDensSmem, s>>>(n, npoint, phi, ld, D, rho);
+  kern<<<blocks, NT, kDensSmem, s>>>(n, npoint, phi, ld, D, rho, groups, keep);
   return cudaGetLastError();
 }
 
 // the split-K quadrature kernel with its dynamic shared memory
 cudaError_t quadrature_launch(dim3 grid, int n, int npad, const double *phi, const double *phib,
                               long ld, const double *wv, int nblk, int chunk, double *work,
-                              cudaStream_t s) {
+                              cudaStream_t s, const int *blocks = nullptr) {
   cudaError_t e = cudaFuncSetAttribute(quadrature_kernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kQuadSmem);
   if (e != cudaSuccess) return e;
-  quadrature_kernel<<<grid, NT, kQuadSmem, s>>>(n, npad, phi, phib, ld, wv, nblk, chunk, work);
+  quadrature_kernel<<<grid, NT, kQuadSmem, s>>>(n, npad, phi, phib, ld, wv, nblk, chunk, work,
+                                                blocks);
   return cudaGetLastError();
 }
 
@@ -418,16 +469,21 @@ size_t quadrature_workspace_bytes(int n, int npoint) {
 
 cudaError_t launch_quadrature_f64(int n, int npoint, const double *phi, long ld,
                                   const double *wv, double *F, double *work,
-                                  cudaStream_t s, const double *phib) {
+                                  cudaStream_t s, const double *phib, const int *blocks,
+                                  int nblock) {
   if (!phib) phib = phi;
   if (n <= 0) return cudaSuccess;
-  const int npad = pad_points(npoint);
+  // screened: the K range is the listed 16-point blocks (at most all of them,
+  // so the workspace sized for npoint suffices)
+  const int npad = blocks ? nblock * BK : pad_points(npoint);
+  if (npad == 0) return cudaMemsetAsync(F, 0, (size_t)n * n * sizeof(double), s);
   int chunk;
   const int nchunk = quad_chunks(n, npad, &chunk);
   const int nblk = (n + BM - 1) / BM;
   const int ntile = nblk * (nblk + 1) / 2;
   dim3 grid(ntile, nchunk);
-  cudaError_t e = quadrature_launch(grid, n, npad, phi, phib, ld, wv, nblk, chunk, work, s);
+  cudaError_t e = quadrature_launch(grid, n, npad, phi, phib, ld, wv, nblk, chunk, work, s,
+                                    blocks);
   if (e != cudaSuccess) return e;
   const long total = (long)ntile * BM * BN;
   const int rblocks = (int)std::min<long>((total + 255) / 256, 148 * 16);
@@ -442,6 +498,49 @@ cudaError_t launch_quadrature_reduce(int n, int nchunk, const double *work, doub
   const long total = (long)ntile * BM * BN;
   const int rblocks = (int)std::min<long>((total + 255) / 256, 148 * 16);
   quadrature_reduce_kernel<<<rblocks, 256, 0, s>>>(n, nblk, nchunk, work, F);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------ FP64 point screening
+namespace {
+
+// keep[p] = 1 when |wb w| max_mu phi_mu(p)^2 >= tol (the test of the int8
+// plans: a dropped point changes an element of F by at most tol |v(p)|).
+__global__ void screen_points_kernel(const double *__restrict__ phi, long ld, int n, int npoint,
+                                     const double *__restrict__ wb, const double *__restrict__ w,
+                                     double tol, int *__restrict__ keep) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npoint) return;
+  double mx = 0.0;
+  for (int mu = 0; mu < n; ++mu) mx = fmax(mx, fabs(__ldg(phi + (long)mu * ld + p)));
+  const double t = fabs(wb[p] * w[p]);
+  keep[p] = (t * mx) * mx >= tol ? 1 : 0;
+}
+
+// flags[b] = 1 when block b of `span` points holds a kept point
+__global__ void screen_blocks_kernel(const int *__restrict__ keep, int npoint, int span,
+                                     int nb, int *__restrict__ flags) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  int any = 0;
+  for (int i = b * span; i < min((b + 1) * span, npoint); ++i) any |= keep[i];
+  flags[b] = any;
+}
+
+}  // namespace
+
+cudaError_t launch_fp64_screening(int n, int npoint, const double *phi, long ld, const double *wb,
+                                  const double *w, double tol, int *keep, int *block_flags,
+                                  int *group_flags, cudaStream_t s) {
+  if (npoint <= 0) return cudaSuccess;
+  screen_points_kernel<<<(npoint + 255) / 256, 256, 0, s>>>(phi, ld, n, npoint, wb, w, tol,
+                                                           keep);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const int nb = (npoint + BK - 1) / BK, ng = (npoint + BN - 1) / BN;
+  screen_blocks_kernel<<<(nb + 255) / 256, 256, 0, s>>>(keep, npoint, BK, nb, block_flags);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  screen_blocks_kernel<<<(ng + 255) / 256, 256, 0, s>>>(keep, npoint, BN, ng, group_flags);
   return cudaGetLastError();
 }
 

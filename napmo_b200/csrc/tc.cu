@@ -1238,6 +1238,37 @@ int int8_quadrature(Int8Plan *p, const double *phi, const double *wv, double *F,
   return kOk;
 }
 
+// Exercises the bounded waits of the tensor-core kernels without a fault: one
+// role (thread 0) waits on an mbarrier that nothing arrives on, with the
+// kernels' own wait_phase (limit kTimeoutNs, then kDeviceTimeout in
+// g_tc_error and the abort flag set); a second role (thread 32) waits on
+// another such barrier and must leave through the abort flag, as the roles of
+// density_i8 / quad_i8 do.  out[0], out[1]: the two waits' results (0 = gave
+// up).
+namespace {
+__global__ void tc_wait_selftest_kernel(int *out) {
+  __shared__ __align__(8) uint64_t never[2];
+  __shared__ int abort_sh;
+  volatile int *abort = &abort_sh;
+  if (threadIdx.x == 0) {
+    mbar_init(&never[0], 1);
+    mbar_init(&never[1], 1);
+    abort_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) out[0] = wait_phase(&never[0], 0, abort) ? 1 : 0;
+  if (threadIdx.x == 32) out[1] = wait_phase(&never[1], 0, abort) ? 1 : 0;
+  __syncthreads();
+}
+}  // namespace
+
+int tc_wait_selftest(int *out_dev, cudaStream_t s) {
+  tc_wait_selftest_kernel<<<1, 64, 0, s>>>(out_dev);
+  NAPMO_TRY_CUDA(cudaGetLastError(), "wait self-test");
+  return kOk;
+}
+
 int tc_error_status(cudaStream_t s, bool reset) {
   int h = 0;
   if (cudaMemcpyFromSymbolAsync(&h, g_tc_error, sizeof(int), 0, cudaMemcpyDeviceToHost, s) !=

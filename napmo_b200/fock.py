@@ -64,12 +64,19 @@ class FockBuilder(object):
     def set_precision(self, precision, poisson_tol=None):
         """'fp64' (CUDA cores) or 'int8x4' (int8 slices on the tensor cores) for
         rho and F; the Poisson solve is FP64 in both.  The Poisson truncation
-        tolerance follows the mode (0: every (l, m) as nAPMO; 1e-10 a.u. for
+        tolerance follows the mode (0: every (l, m) as nAPMO; 1e-9 a.u. for
         'int8x4') unless `poisson_tol` is given."""
         checked(cext.lib.napmo_fock_plan_set_precision(self._plan, self.PRECISIONS[precision]))
         self.precision = precision
         if poisson_tol is not None:
             self.set_poisson_tolerance(poisson_tol)
+
+    def set_fp64_screening(self, tol=1e-24, stream=None):
+        """FP64 mode: skip the points with |wb w| max_mu phi_mu(p)^2 < tol in
+        the density, the potential evaluation and the quadrature (the int8
+        mode's screening, 1e-24 by default); 0 restores every point."""
+        checked(cext.lib.napmo_fock_plan_set_fp64_screening(self._plan, float(tol),
+                                                            _stream(self.torch, stream)))
 
     def set_poisson_tolerance(self, tol):
         """Truncation tolerance (a.u.) of the potential evaluation: per atom and

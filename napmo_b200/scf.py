@@ -306,8 +306,9 @@ class GridAPMO(object):
     orbital-pair Poisson solves; a single quantum nucleus has no self
     interaction (J - K = 0); classical nuclei enter H of both species.
 
-    E = sum_s tr(D_s H_s) + 1/2 tr(D_e (J_e - K_e)) + q_e q_n <rho_e|V[rho_n]>
-        + E_nn(classical)
+    E = sum_s tr(D_s H_s) + 1/2 tr(D_e (J_e - K_e))
+        + 1/2 q_e q_n (<rho_e|V[rho_n]> + <rho_n|V[rho_e]>) + E_nn(classical)
+    (the coupling as nAPMO's 1/2 sum_s tr(D_s J_s), scf.py:494-520)
 
     exchange='lda' replaces the electrons' HF exchange by LDA exchange +
     VWN5 correlation (nAPMO's Functional 'lda'); correlation='epc17-2' adds
@@ -383,7 +384,10 @@ class GridAPMO(object):
             Fe = Fe - K
             E_K = -0.5 * float((De * K).sum())
         Fn = n.H + n.fb.quadrature(qq, v_e, vext=ext_n)
-        coup = qq * float((self.W * rho_e * v_n).sum())
+        # nAPMO's coupling energy: 1/2 sum_s tr(D_s J_s) (scf.py:494-520), the
+        # mean of <rho_e|V[rho_n]> and <rho_n|V[rho_e]> (equal up to the grid)
+        coup = 0.5 * qq * (float((self.W * rho_e * v_n).sum()) +
+                           float((self.W * rho_n * v_e).sum()))
         E_J = 0.5 * e.q * e.q * float((self.W * rho_e * v_e).sum())
         E = (float((De * e.H).sum()) + E_J + E_K + E_xc + float((Dn * n.H).sum()) + coup +
              self.Enn)
@@ -454,3 +458,201 @@ class GridAPMO(object):
                     seconds=time.perf_counter() - t0, poisson_solves=self.poisson_solves,
                     electrons=float((De * e.S).sum()), nuclei=float((Dn * n.S).sum()),
                     history=history)
+
+
+def spin_occupations(nelectron, multiplicity=None):
+    """(n_alpha, n_beta) of `nelectron` electrons at a spin multiplicity, as
+    nAPMO splits the species e- into e-alpha and e-beta
+    (molecular_system.py:214-290): the default multiplicity is 1 for an even
+    and 2 for an odd count; the unpaired electrons are alpha."""
+    if not multiplicity:
+        multiplicity = (nelectron % 2) + 1
+    unpaired = multiplicity - 1
+    left = nelectron - unpaired
+    if left < 0 or left % 2 != 0:
+        raise ValueError('Bad charge / multiplicity')
+    return left // 2 + unpaired, left // 2
+
+
+class GridMultiSCF(object):
+    """Unrestricted SCF of several species on one Becke grid: the electrons
+    as the two spin species e-alpha and e-beta (eta = 1 each, as nAPMO splits
+    them for method 'uhf', molecular_system.py:214-290), optionally with one
+    quantum-nucleus species (APMO-UHF).  Every species sees the Coulomb
+    potential of every other (q_s q_t J[rho_t], grid quadrature of the device
+    Poisson potentials) and of the classical nuclei; each spin species has
+    its own HF exchange from its occupied orbitals (orbital-pair Poisson
+    solves); a single quantum nucleus has no self-interaction.
+
+    E = sum_s tr(D_s H_s) + 1/2 sum_{s,t} q_s q_t <rho_s|V[rho_t]>
+        - 1/2 sum_{s in e} tr(D_s K_s) + E_nn(classical)
+    (self terms s = t only for the electron species).
+
+    Args:
+        ms: MolecularSystem (quantum nuclei as their own species).
+        nuclear: symbol of the quantum-nucleus species or None.
+        charge: molecular charge (electrons = sum Z - charge).
+        multiplicity: spin multiplicity (default 1 or 2 by parity).
+        exchange: 'hf' or 'none' for the electrons.
+    """
+
+    def __init__(self, ms, nuclear=None, nrad=50, nang=110, lmax=None, charge=0,
+                 multiplicity=None, precision='fp64', diis=6, mass=PROTON_MASS, exchange='hf'):
+        torch = _torch()
+        self.torch = torch
+        if exchange not in ('hf', 'none'):
+            raise ValueError("exchange must be 'hf' or 'none' in the unrestricted drivers")
+        self.exchange = exchange
+        self.ms = ms
+        e = ms['e-']
+        self.grid = BeckeGrid(e, nrad, nang)
+        if lmax is None:
+            lmax = 'per-atom' if isinstance(nang, (list, tuple)) else lebedev_get_order(nang) // 2
+        self.W = torch.as_tensor(self.grid.becke_weights * self.grid.weights, device='cuda',
+                                 dtype=torch.float64)
+        nel = int(round(e['size'])) - int(charge)
+        self.nalpha, self.nbeta = spin_occupations(nel, multiplicity)
+        self.species = []
+        for occ in (self.nalpha, self.nbeta):
+            sp = dict(e, eta=1.0, occupation=occ)
+            self.species.append(_Species(self.grid, sp, ms.point_charges, lmax, 1.0, precision,
+                                         diis, torch))
+        self.is_electron = [True, True]
+        self._nuclear = nuclear
+        if nuclear is not None:
+            self.species.append(_Species(self.grid, ms[nuclear], ms.point_charges, lmax, mass,
+                                         precision, diis, torch))
+            self.is_electron.append(False)
+            if self.species[-1].nocc != 1:
+                raise ValueError('one quantum nucleus of the species is supported')
+        self.ndiis = int(diis)
+        self.Enn = nuclear_repulsion(ms.point_charges)
+        self.poisson_solves = 0
+
+    def _exchange(self, sp, Cocc):
+        t = self.torch
+        phi = sp.fb.phi()[:, :sp.N]
+        psi = Cocc.T @ phi
+        K = t.zeros((sp.n, sp.n), dtype=t.float64, device='cuda')
+        for i in range(psi.shape[0]):
+            V = sp.fb.coulomb_potentials(psi[i] * phi)
+            self.poisson_solves += sp.n
+            K += (phi * (self.W * psi[i])) @ V.T
+        return 0.5 * (K + K.T)
+
+    def fock(self, Ds, Cs):
+        """(list of F_s, E) for densities Ds and orbitals Cs."""
+        sps = self.species
+        rhos = [sp.fb.density(D) for sp, D in zip(sps, Ds)]
+        vs = [sps[0].fb.coulomb_potential(r) for r in rhos]
+        self.poisson_solves += len(rhos)
+        Fs, E = [], self.Enn
+        for s, sp in enumerate(sps):
+            pot = None
+            for u, (tp, v) in enumerate(zip(sps, vs)):
+                if u == s and not self.is_electron[s]:
+                    continue
+                term = (sp.q * tp.q) * v
+                pot = term if pot is None else pot + term
+            F = sp.H + sp.fb.quadrature(1.0, pot)
+            E += float((Ds[s] * sp.H).sum()) + 0.5 * float((self.W * rhos[s] * pot).sum())
+            if self.exchange == 'hf' and self.is_electron[s] and sp.nocc > 0:
+                K = self._exchange(sp, Cs[s][:, :sp.nocc])
+                F = F - K
+                E -= 0.5 * float((Ds[s] * K).sum())
+            Fs.append(F)
+        return Fs, E
+
+    def guess(self):
+        """Electrons from the core Hamiltonian with the quantum nuclei as unit
+        point charges; the nucleus in that electron density's field."""
+        torch = self.torch
+        sps = self.species
+        H = sps[0].H
+        if self._nuclear is not None:
+            qpos = np.array([[*p['origin'], 1.0] for p in self.ms[self._nuclear]['particles']],
+                            dtype=np.float64).reshape(-1, 4)
+            x, y, z, _, _ = self.grid.device_arrays()
+            vq = torch.empty(self.grid.size, device='cuda', dtype=torch.float64)
+            checked(cext.lib.napmo_gpu_nuclear_potential(
+                self.grid.size, x, y, z, qpos.shape[0], np.ascontiguousarray(qpos),
+                vq.data_ptr(), torch.cuda.current_stream().cuda_stream))
+            prec = sps[0].fb.precision
+            sps[0].fb.set_precision('fp64')
+            H = H + sps[0].fb.quadrature(sps[0].q * sps[-1].q, vq)
+            sps[0].fb.set_precision(prec)
+        Cs, Ds = [], []
+        for sp in sps[:2]:
+            C, _, D = sp.diag(H)
+            Cs.append(C)
+            Ds.append(D)
+        if self._nuclear is not None:
+            nuc = sps[2]
+            v_e = sps[0].fb.coulomb_potential(sps[0].fb.density(Ds[0] + Ds[1]))
+            self.poisson_solves += 1
+            C, _, D = nuc.diag(nuc.H + nuc.fb.quadrature(sps[0].q * nuc.q, v_e))
+            Cs.append(C)
+            Ds.append(D)
+        return Cs, Ds
+
+    def run(self, maxiter=100, tol=1e-8, verbose=False):
+        """SCF from guess(); one DIIS over all species (concatenated error
+        vectors, shared coefficients); stops at |dE| < tol with every
+        max |X^T (FDS - SDF) X| < 1e-4."""
+        torch = self.torch
+        sps = self.species
+        t0 = time.perf_counter()
+        Cs, Ds = self.guess()
+        Fh, errs = [], []
+        E_prev, history, converged = None, [], False
+        for it in range(1, maxiter + 1):
+            Fs, E = self.fock(Ds, Cs)
+            err = [sp.X.T @ (F @ D @ sp.S - sp.S @ D @ F) @ sp.X
+                   for sp, F, D in zip(sps, Fs, Ds)]
+            Fh.append(Fs)
+            errs.append(err)
+            if len(Fh) > self.ndiis:
+                Fh.pop(0)
+                errs.pop(0)
+            emax = tuple(float(x.abs().max()) for x in err)
+            history.append((E,) + emax)
+            if verbose:
+                print('%3d %.12f %s' % (it, E, ' '.join('%.2e' % x for x in emax)))
+            if E_prev is not None and abs(E - E_prev) < tol and max(emax) < 1e-4:
+                converged = True
+                break
+            E_prev = E
+            m = len(Fh)
+            if m > 1:
+                B = torch.empty((m + 1, m + 1), dtype=torch.float64, device='cuda')
+                for a in range(m):
+                    for b in range(a + 1):
+                        B[a, b] = B[b, a] = sum((ea * eb).sum() for ea, eb in zip(errs[a], errs[b]))
+                B[m, :m] = -1.0
+                B[:m, m] = -1.0
+                B[m, m] = 0.0
+                rhs = torch.zeros(m + 1, dtype=torch.float64, device='cuda')
+                rhs[m] = -1.0
+                c = torch.linalg.solve(B, rhs)
+                Fs = [sum(c[a] * Fh[a][s] for a in range(m)) for s in range(len(sps))]
+            Cs, Ds = [], []
+            for sp, F in zip(sps, Fs):
+                C, _, D = sp.diag(F)
+                Cs.append(C)
+                Ds.append(D)
+        torch.cuda.synchronize()
+        out = dict(energy=E, iterations=it, converged=converged,
+                   seconds=time.perf_counter() - t0, poisson_solves=self.poisson_solves,
+                   alpha=float((Ds[0] * sps[0].S).sum()), beta=float((Ds[1] * sps[1].S).sum()),
+                   history=history, D=[D for D in Ds])
+        if self._nuclear is not None:
+            out['nuclei'] = float((Ds[2] * sps[2].S).sum())
+        return out
+
+
+class GridUHF(GridMultiSCF):
+    """Unrestricted grid SCF of the electrons (nAPMO's method 'uhf'):
+    GridMultiSCF without quantum nuclei."""
+
+    def __init__(self, ms, nrad=50, nang=110, **kw):
+        super(GridUHF, self).__init__(ms, None, nrad, nang, **kw)

@@ -32,6 +32,30 @@ class MolecularSystem(dict):
     def __init__(self):
         super(MolecularSystem, self).__init__()
         self.point_charges = []
+        self.charges = {}
+        self.open_shell = False
+
+    def set_charges(self, data, open_shell=False):
+        """Charge and multiplicity per species (molecular_system.py:214-290):
+        data = {'e-': {'charge': c, 'multiplicity': m}} adds c particles to
+        the species (c = -1 removes an electron) and fixes its multiplicity
+        (default 1 or 2 by parity).  The electrons are open shell when the
+        alpha and beta counts differ or `open_shell` is set; the unrestricted
+        drivers then treat them as e-alpha and e-beta."""
+        e = self['e-']
+        for key, val in data.items():
+            if key not in self:
+                raise ValueError('Impossible to set %s charges: particle does not exist' % key)
+            self.charges[key] = dict(charge=int(val.get('charge', 0)),
+                                     multiplicity=int(val.get('multiplicity', 0) or 0))
+        c = self.charges.get('e-', {})
+        nel = int(round(e['size'])) + c.get('charge', 0)
+        m = c.get('multiplicity') or (nel % 2) + 1
+        unpaired = m - 1
+        if (nel - unpaired) % 2 != 0 or nel < unpaired:
+            raise ValueError('Bad charge / multiplicity')
+        self.open_shell = bool(unpaired) or bool(open_shell)
+        return self
 
     def _species(self, symbol, consts):
         sp = self.setdefault(symbol, dict(symbol=symbol, particles=[], size=0, occupation=0,

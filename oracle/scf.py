@@ -311,7 +311,8 @@ class GridAPMO(object):
     napmo_b200.scf.GridAPMO with HF exchange):
 
     E = sum_s tr(D_s H_s) + 1/2 q_e^2 <rho_e|V[rho_e]> - 1/2 tr(D_e K_e)
-        + q_e q_n <rho_e|V[rho_n]> + E_nn(classical)."""
+        + 1/2 q_e q_n (<rho_e|V[rho_n]> + <rho_n|V[rho_e]>) + E_nn(classical)
+    (the coupling as nAPMO's 1/2 sum_s tr(D_s J_s), scf.py:494-520)."""
 
     def __init__(self, atoms, library, elements, quantum=(0,), nrad=100, nang=302, lmax=None,
                  basis='CC-PVDZ', diis=6, mass=PROTON_MASS):
@@ -357,7 +358,8 @@ class GridAPMO(object):
         Fn = n.H + O.quadrature(n.phi, qq * v_e, g.becke, g.weights)
         E_J = 0.5 * e.q * e.q * float((self.W * rho_e * v_e).sum())
         E_K = -0.5 * float((De * K).sum())
-        coup = qq * float((self.W * rho_e * v_n).sum())
+        coup = 0.5 * qq * (float((self.W * rho_e * v_n).sum()) +
+                           float((self.W * rho_n * v_e).sum()))
         E = (float((De * e.H).sum()) + E_J + E_K + float((Dn * n.H).sum()) + coup + self.Enn)
         return Fe, Fn, E, (rho_e, rho_n, v_e, v_n)
 
@@ -397,3 +399,128 @@ class GridAPMO(object):
             _, Cn, Dn = n.diag(Fn)
         return dict(energy=E, iterations=it, converged=converged, history=history, De=De, Dn=Dn,
                     electrons=float((De * e.S).sum()), nuclei=float((Dn * n.S).sum()))
+
+
+def spin_occupations(nelectron, multiplicity=None):
+    """(n_alpha, n_beta) as nAPMO splits e- (molecular_system.py:214-290)."""
+    if not multiplicity:
+        multiplicity = (nelectron % 2) + 1
+    unpaired = multiplicity - 1
+    left = nelectron - unpaired
+    if left < 0 or left % 2 != 0:
+        raise ValueError('Bad charge / multiplicity')
+    return left // 2 + unpaired, left // 2
+
+
+class GridMultiSCF(object):
+    """Unrestricted grid SCF (restates napmo_b200.scf.GridMultiSCF): e-alpha
+    and e-beta species (eta = 1, nAPMO's 'uhf' split) and optionally one
+    quantum nucleus on one Becke grid; Coulomb between all species, HF
+    exchange within each spin species, no self-interaction of the nucleus."""
+
+    def __init__(self, atoms, library, elements, quantum=(), nrad=50, nang=110, lmax=None,
+                 basis='CC-PVDZ', charge=0, multiplicity=None, diis=6, mass=PROTON_MASS,
+                 exchange='hf'):
+        centers = _centers(atoms)
+        syms = [s for s, _ in atoms]
+        self.grid = O.Grid(centers, [elements[s]['atomic_radii'] for s in syms], nrad, nang)
+        self.lmax = lebedev_lmax(nang) if lmax is None else lmax
+        self.plan = PoissonPlan(self.grid, self.lmax)
+        classical = [(elements[s]['atomic_number'], c) for i, (s, c) in
+                     enumerate(zip(syms, centers)) if i not in quantum]
+        nel = sum(elements[s]['atomic_number'] for s in syms) - int(charge)
+        na, nb = spin_occupations(nel, multiplicity)
+        fb_e = O.flat_basis(centers, syms, library, basis)
+        spin = dict(eta=1.0, charge=-1.0)
+        self.species = [Species(self.grid, fb_e, spin, na, classical),
+                        Species(self.grid, fb_e, spin, nb, classical)]
+        self.is_electron = [True, True]
+        self.quantum_centers = [centers[i] for i in quantum]
+        if quantum:
+            nsym = [syms[i] + '_1' for i in quantum]
+            lib_n = {'NUCLEAR-5S5P': {s: NUCLEAR_5S5P for s in nsym}}
+            fb_n = O.flat_basis(self.quantum_centers, nsym, lib_n, 'NUCLEAR-5S5P')
+            self.species.append(Species(self.grid, fb_n, NUCLEUS, len(quantum), classical,
+                                        mass=mass))
+            self.is_electron.append(False)
+        self.Enn = nuclear_repulsion(classical)
+        self.W = self.grid.becke * self.grid.weights
+        self.exchange = exchange
+        self.ndiis = diis
+
+    def _exchange(self, sp, Cocc):
+        psi = Cocc.T @ sp.phi
+        K = np.zeros((sp.n, sp.n))
+        for i in range(psi.shape[0]):
+            V = poisson_many(self.plan, psi[i] * sp.phi)
+            K += (sp.phi * (self.W * psi[i])) @ V.T
+        return 0.5 * (K + K.T)
+
+    def fock(self, Ds, Cs):
+        sps, g = self.species, self.grid
+        rhos = [O.density(sp.phi, D) for sp, D in zip(sps, Ds)]
+        vs = poisson_many(self.plan, np.stack(rhos))
+        Fs, E = [], self.Enn
+        for s, sp in enumerate(sps):
+            pot = np.zeros(g.size)
+            for u, (tp, v) in enumerate(zip(sps, vs)):
+                if u == s and not self.is_electron[s]:
+                    continue
+                pot = pot + (sp.q * tp.q) * v
+            F = sp.H + O.quadrature(sp.phi, pot, g.becke, g.weights)
+            E += float((Ds[s] * sp.H).sum()) + 0.5 * float((self.W * rhos[s] * pot).sum())
+            if self.exchange == 'hf' and self.is_electron[s] and sp.nocc > 0:
+                K = self._exchange(sp, Cs[s][:, :sp.nocc])
+                F = F - K
+                E -= 0.5 * float((Ds[s] * K).sum())
+            Fs.append(F)
+        return Fs, E
+
+    def guess(self):
+        sps, g = self.species, self.grid
+        H = sps[0].H
+        if len(sps) > 2:
+            vq = O.nuclear_potential(g.points, [(1.0, c) for c in self.quantum_centers])
+            H = H + O.quadrature(sps[0].phi, sps[0].q * sps[2].q * vq, g.becke, g.weights)
+        Cs, Ds = [], []
+        for sp in sps[:2]:
+            _, C, D = sp.diag(H)
+            Cs.append(C)
+            Ds.append(D)
+        if len(sps) > 2:
+            nuc = sps[2]
+            v_e = poisson_many(self.plan, O.density(sps[0].phi, Ds[0] + Ds[1])[None, :])[0]
+            _, C, D = nuc.diag(nuc.H + O.quadrature(nuc.phi, sps[0].q * nuc.q * v_e, g.becke,
+                                                    g.weights))
+            Cs.append(C)
+            Ds.append(D)
+        return Cs, Ds
+
+    def run(self, maxiter=100, tol=1e-8):
+        sps = self.species
+        Cs, Ds = self.guess()
+        Fh, errs, history = [], [], []
+        E_prev, converged = None, False
+        for it in range(1, maxiter + 1):
+            Fs, E = self.fock(Ds, Cs)
+            err = [sp.error(F, D) for sp, F, D in zip(sps, Fs, Ds)]
+            Fh.append(tuple(Fs))
+            errs.append(tuple(err))
+            if len(Fh) > self.ndiis:
+                Fh.pop(0)
+                errs.pop(0)
+            emax = tuple(float(np.abs(x).max()) for x in err)
+            history.append((E,) + emax)
+            if E_prev is not None and abs(E - E_prev) < tol and max(emax) < 1e-4:
+                converged = True
+                break
+            E_prev = E
+            if len(Fh) > 1:
+                Fs = _diis(Fh, errs)
+            Cs, Ds = [], []
+            for sp, F in zip(sps, Fs):
+                _, C, D = sp.diag(F)
+                Cs.append(C)
+                Ds.append(D)
+        return dict(energy=E, iterations=it, converged=converged, history=history, D=Ds,
+                    alpha=float((Ds[0] * sps[0].S).sum()), beta=float((Ds[1] * sps[1].S).sum()))

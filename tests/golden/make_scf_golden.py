@@ -5,14 +5,18 @@ configurations, written to tests/golden/scf_oracle.json (+ .npz densities):
       50 radial x 110 Lebedev per atom, grid J and orbital-pair exchange;
   C2  APMO-RHF of HCN (H at 0, C at 1.066 A, N at 2.222 A along z), electrons
       in cc-pVDZ, the H nucleus quantum in the even-tempered 5s5p basis
-      (exponents 4..64), 100 radial x 302 Lebedev per atom.
+      (exponents 4..64), 100 radial x 302 Lebedev per atom;
+  uhf_oh         UHF of the OH radical (O at 0, H at 0.97 A along z; doublet),
+                 cc-pVDZ, 50 x 110;
+  apmo_uhf_oh    APMO-UHF of the OH radical (doublet) with the H nucleus
+                 quantum (5s5p), 50 x 110.
 
 Both stop at |dE| < 1e-9 Eh with max |X^T (FDS - SDF) X| < 1e-4 (the rule of
 napmo_b200.scf), DIIS with 6 vectors.  The GPU tests compare the device
 drivers' converged energies and iteration counts with these.  The C2 SCF
 takes about ten minutes on 8 host cores.
 
-Usage: python tests/golden/make_scf_golden.py [c1] [c2]
+Usage: python tests/golden/make_scf_golden.py [c1] [c2] [uhf_oh] [apmo_uhf_oh]
 """
 import json
 import os
@@ -28,6 +32,8 @@ sys.path.insert(0, os.path.join(ROOT, 'tests'))
 
 import scf as OS  # noqa: E402
 from helpers import H2O, HCN  # noqa: E402
+
+OH = [('O', (0.0, 0.0, 0.0)), ('H', (0.0, 0.0, 0.97))]
 
 TOL = 1e-9
 
@@ -46,6 +52,12 @@ def run(case):
     if case == 'c1':
         res = OS.GridRHF(H2O, lib, el, 50, 110).run(tol=TOL)
         arrays = {'c1_D': res['D']}
+    elif case == 'uhf_oh':
+        res = OS.GridMultiSCF(OH, lib, el, (), 50, 110).run(tol=TOL)
+        arrays = {'uhf_oh_Da': res['D'][0], 'uhf_oh_Db': res['D'][1]}
+    elif case == 'apmo_uhf_oh':
+        res = OS.GridMultiSCF(OH, lib, el, (1,), 50, 110).run(tol=TOL)
+        arrays = {}
     else:
         res = OS.GridAPMO(HCN, lib, el, (0,), 100, 302).run(tol=TOL)
         arrays = {'c2_De': res['De'], 'c2_Dn': res['Dn']}

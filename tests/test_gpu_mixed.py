@@ -126,3 +126,23 @@ def test_int8_fock_build_energy(atoms, nrad, nang, nocc):
     n64 = grid.integrate(rho64.cpu().numpy())
     n8 = grid.integrate(rho8.cpu().numpy())
     assert abs(n64 - n8) <= 1e-7
+
+
+def test_bounded_wait_times_out_and_reports():
+    """The tensor-core kernels' mbarrier waits are bounded: a wait on a barrier
+    that nothing arrives on gives up (about 2 s), records error 5 for
+    napmo_tc_status, and a second role waiting elsewhere leaves through the
+    abort flag; the context stays usable."""
+    import torch
+    from napmo_b200 import cext
+    stream = torch.cuda.current_stream().cuda_stream
+    assert cext.lib.napmo_tc_status(stream, 1) in (0, 5)
+    cext.lib.napmo_tc_status(stream, 1)
+    out = torch.full((2,), 7, dtype=torch.int32, device='cuda')
+    cext.checked(cext.lib.napmo_tc_wait_selftest(out.data_ptr(), stream))
+    torch.cuda.synchronize()
+    assert out.cpu().tolist() == [0, 0]
+    assert cext.lib.napmo_tc_status(stream, 1) == 5
+    assert cext.lib.napmo_tc_status(stream, 1) == 0
+    x = torch.ones(1024, device='cuda', dtype=torch.float64)
+    assert float(x.sum()) == 1024.0

@@ -57,6 +57,22 @@ def test_becke_weights_bit_exact_62_centres(oracle, elements):
     assert np.array_equal(grid.becke_weights, og.becke)
 
 
+@pytest.mark.parametrize('ncarbon', [66, 99])
+def test_becke_weights_bit_exact_many_centres(oracle, elements, ncarbon):
+    """200 and 299 centres: the centre tables no longer fit in shared memory
+    (read from global memory; with and without the shared distance cache)."""
+    import napmo_b200 as nb
+    from napmo_b200.system import alkane_geometry
+    atoms = alkane_geometry(ncarbon)
+    assert len(atoms) in (200, 299)
+    ms_species = dict(symbol='e-', particles=[dict(symbol=s, origin=np.array(x) / BOHR)
+                                              for s, x in atoms])
+    grid = nb.BeckeGrid(ms_species, 6, 14)
+    og = oracle.Grid([np.array(x) / BOHR for _, x in atoms],
+                     [elements[s]['atomic_radii'] for s, _ in atoms], 6, 14)
+    assert np.array_equal(grid.becke_weights, og.becke)
+
+
 def test_basis_values(h2o, oracle):
     ms, grid, og, fb = h2o
     pts = grid.points[::7]

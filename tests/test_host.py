@@ -291,3 +291,19 @@ def test_declarations_match_napmo_ctypes_bindings():
         if rt == 'None' and ret != 'void':
             bad.append((name, 'restype None vs %s' % ret))
     assert not bad, bad
+
+
+def test_set_charges_open_shell_rules():
+    """MolecularSystem.set_charges follows nAPMO's split of e- into alpha and
+    beta (molecular_system.py:214-290)."""
+    from napmo_b200.scf import spin_occupations
+    from napmo_b200.system import build_system
+    h2o = [('O', (0.0, 0.0, 0.0)), ('H', (0.0, 0.757, 0.587)), ('H', (0.0, -0.757, 0.587))]
+    ms = build_system(h2o, 'STO-3G')
+    assert not ms.set_charges({}).open_shell
+    assert ms.set_charges({'e-': {'charge': -1}}).open_shell          # H2O+ doublet
+    assert ms.set_charges({'e-': {'multiplicity': 3}}).open_shell     # triplet
+    with pytest.raises(ValueError):
+        ms.set_charges({'e-': {'multiplicity': 2}})                   # 10 electrons, doublet
+    assert spin_occupations(9) == (5, 4)
+    assert spin_occupations(10, 3) == (6, 4)

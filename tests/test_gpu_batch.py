@@ -82,3 +82,36 @@ def test_batch_recaptures_after_plans_change():
     for F, b, D in zip(Fs, builders, Ds):
         R = b.build(D)[0].cpu().numpy()
         assert np.abs(F - R).max() <= 1e-12 * np.abs(R).max()
+
+
+def test_batch_at_the_batched_configuration_sizes():
+    """Three molecules at the sizes of the 64-molecule batch's range: 30 and 24
+    atoms with 100 radial points and 590- / 434-point rules on some atoms,
+    per-atom lmax up to 20.  The int8 batch equals its single builds and stays
+    within 1e-6 Eh of the FP64 builds."""
+    import torch
+    import napmo_b200 as nb
+    from napmo_b200.system import build_system, random_chain
+    rng = np.random.default_rng(2026)
+    specs = [(30, [100] * 30, [590 if i % 3 == 0 else 302 for i in range(30)]),
+             (24, [50 + 2 * i for i in range(24)], [434 if i % 4 == 0 else 146 for i in range(24)]),
+             (3, [100, 90, 80], [590, 590, 110])]
+    builders, Ds = [], []
+    for k, (na, nr, ng) in enumerate(specs):
+        e = build_system(random_chain(rng, na), 'CC-PVDZ')['e-']
+        grid = nb.BeckeGrid(e, nr, ng)
+        b = nb.FockBuilder(grid, e['basis'], 'per-atom')
+        builders.append(b)
+        Ds.append(random_density(b.n, max(1, e['occupation']), seed=300 + k))
+    ref64 = [b.build(D)[0].cpu().numpy() for b, D in zip(builders, Ds)]
+    for b in builders:
+        b.set_precision('int8x4')
+    ref8 = [b.build(D)[0].cpu().numpy() for b, D in zip(builders, Ds)]
+    batch = nb.FockBatch(builders)
+    batch.tune(reps=1)
+    F8 = [F.cpu().numpy() for F in batch.build(Ds)]
+    torch.cuda.synchronize()
+    assert builders[0].tc_status() == 0
+    for F, R, R64, D in zip(F8, ref8, ref64, Ds):
+        assert np.abs(F - R).max() <= 1e-12 * np.abs(R).max()
+        assert abs(0.5 * float((F * D).sum()) - 0.5 * float((R64 * D).sum())) <= 1e-6

@@ -401,6 +401,19 @@ int napmo_fock_batch_build(void *batch, void *stream);
 int napmo_fock_batch_tune(void *batch, void *stream, int reps, int *nstream, int *budget,
                           double *ms);
 int napmo_fock_batch_config(void *batch, int *nstream, int *budget);
+/* Build mode of a batch: 0 = the molecules' own launch chains over capture
+ * streams (default); 1 = one launch per stage for the whole batch: persistent
+ * density and quadrature launches taking (molecule, tile) items from device
+ * work queues (bounded waits), one Poisson plan over all the molecules' grids.
+ * No counterpart in nAPMO (its builds are per molecule, psi_hybrid.py:81-110). */
+int napmo_fock_batch_set_mode(void *batch, int mode);
+/* Mode 1: runs the density stage with a work queue that is never posted, so
+ * that every wait runs out after timeout_s (<= 10 s); *status = 5 then.  A test
+ * of the bounded waits without a fault; the batch stays usable. */
+int napmo_fock_batch_queue_selftest(void *batch, double timeout_s, void *stream, int *status);
+/* Mode 1: error word of the work queues since the last call (0, or 5 when a
+ * wait ran out); clears it. */
+int napmo_fock_batch_status(void *batch, void *stream, int *status);
 
 /* Grid quadrature energy of one species in a point-charge potential and its
  * nuclear-coordinate gradient (Becke weights, basis functions, grid points and

@@ -248,6 +248,9 @@ _SIGS = [
     ('napmo_fock_batch_build', c_int, [c_void_p, c_void_p]),
     ('napmo_fock_batch_tune', c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     ('napmo_fock_batch_config', c_int, [c_void_p, c_void_p, c_void_p]),
+    ('napmo_fock_batch_set_mode', c_int, [c_void_p, c_int]),
+    ('napmo_fock_batch_queue_selftest', c_int, [c_void_p, c_double, c_void_p, c_void_p]),
+    ('napmo_fock_batch_status', c_int, [c_void_p, c_void_p, c_void_p]),
     ('napmo_basis_one_body', c_int, [c_void_p, a2df, a2df]),
     ('napmo_basis_get_origins', c_int, [c_void_p, a2df]),
     ('napmo_basis_set_origins', c_int, [c_void_p, a2df]),

@@ -31,6 +31,14 @@ namespace napmo {
 struct FockPlan;
 int fock_build(FockPlan *p, const double *D_dev, double q, const double *vext_dev, double *F_dev,
                double *rho_out, double *v_out, cudaStream_t s);
+struct StageBatch;
+int stage_batch_new(const std::vector<FockPlan *> &plans, const std::vector<double *> &D,
+                    const std::vector<double *> &F, double q, cudaStream_t s, StageBatch **out);
+void stage_batch_free(StageBatch *b);
+int stage_batch_build(StageBatch *b, cudaStream_t s);
+int stage_batch_queue_selftest(StageBatch *b, unsigned long long timeout_ns, cudaStream_t s,
+                               int *status);
+int stage_batch_status(StageBatch *b, cudaStream_t s, int *status);
 int fock_plan_nbasis(const FockPlan *p);
 Int8Plan *fock_plan_int8(FockPlan *p);
 unsigned long long fock_plan_state(const FockPlan *p);
@@ -45,12 +53,15 @@ struct FockBatch {
   cudaGraphExec_t exec = nullptr;
   double q = 1.0;
   int nstream = 8, budget = 0;
+  int mode = 0;                    // 0: per-molecule chains on streams; 1: one launch per stage
+  StageBatch *stage = nullptr;     // mode 1 state (built at warm-up)
   bool warm = false;
   float tuned_ms = 0.0f;
   std::vector<unsigned long long> state;  // fock_plan_state of every plan at warm-up
 
   ~FockBatch() {
     if (exec) cudaGraphExecDestroy(exec);
+    if (stage) stage_batch_free(stage);
     for (auto s : streams) cudaStreamDestroy(s);
     for (auto e : joins) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
@@ -93,6 +104,22 @@ int warm_up(FockBatch *b, cudaStream_t s) {
     if (e) return e;
   }
   NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "batch warm-up");
+  if (b->stage) {
+    stage_batch_free(b->stage);
+    b->stage = nullptr;
+  }
+  if (b->mode == 1) {
+    std::vector<double *> D, F;
+    for (size_t i = 0; i < b->plans.size(); ++i) {
+      D.push_back(b->D[i]->p);
+      F.push_back(b->F[i]->p);
+    }
+    const int e = stage_batch_new(b->plans, D, F, b->q, s, &b->stage);
+    if (e) return e;
+    const int e2 = stage_batch_build(b->stage, s);  // lazily built state, outside capture
+    if (e2) return e2;
+    NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "batch warm-up");
+  }
   b->state.clear();
   for (auto *p : b->plans) b->state.push_back(fock_plan_state(p));
   b->warm = true;
@@ -109,6 +136,20 @@ int capture(FockBatch *b) {
   cudaStream_t s = b->origin;
   const int nplan = (int)b->plans.size();
   const int ns = std::max(1, std::min(b->nstream, nplan));
+  if (b->mode == 1) {  // one launch per stage, all on the origin stream
+    NAPMO_TRY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed), "begin capture");
+    const int st = stage_batch_build(b->stage, s);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(s, &graph);
+    if (st != kOk || ee != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      return st != kOk ? st : cuda_status(ee, "batch capture");
+    }
+    const cudaError_t ce = cudaGraphInstantiate(&b->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    NAPMO_TRY_CUDA(ce, "batch graph instantiate");
+    return kOk;
+  }
   NAPMO_TRY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed), "begin capture");
   int st = kOk;
   cudaError_t ce = cudaEventRecord(b->fork, s);
@@ -233,6 +274,7 @@ int napmo_fock_batch_tune(FockBatch *b, void *stream, int reps, int *nstream_out
     int st = kOk;
     for (int ns : {1, 2, 4, 8, 16, 32}) {
       if (ns > (int)b->plans.size() && ns > 1) break;
+      if (b->mode == 1 && ns > 1) break;  // stage launches: no capture streams to choose
       for (int bud : budgets) {
         b->nstream = ns;
         if ((st = set_budgets(b, bud))) break;
@@ -267,6 +309,50 @@ int napmo_fock_batch_tune(FockBatch *b, void *stream, int reps, int *nstream_out
     if (nstream_out) *nstream_out = best_ns;
     if (budget_out) *budget_out = best_budget;
     if (ms_out) *ms_out = best;
+    return kOk;
+  });
+}
+
+// Build mode: 0 = the molecules' own launch chains spread over capture
+// streams; 1 = one launch per stage for the whole batch (persistent density
+// and quadrature launches over device work queues, one Poisson plan over all
+// grids; FP64 plans).  Takes effect at the next build (re-warms and
+// recaptures).
+int napmo_fock_batch_set_mode(FockBatch *b, int mode) {
+  return guarded([&] {
+    NAPMO_REQUIRE(mode == 0 || mode == 1, "mode must be 0 (streams) or 1 (stages)");
+    b->mode = mode;
+    b->warm = false;
+    if (b->exec) {
+      cudaGraphExecDestroy(b->exec);
+      b->exec = nullptr;
+    }
+    return kOk;
+  });
+}
+
+// Mode 1: runs the density stage with a work queue that is never posted, so
+// that every CTA's bounded wait runs out after timeout_ns; *status receives
+// the queue's error word (5 = a wait ran out).  The batch stays usable.
+int napmo_fock_batch_queue_selftest(FockBatch *b, double timeout_s, void *stream,
+                                    int *status) {
+  return guarded([&] {
+    cudaStream_t s = (cudaStream_t)stream;
+    NAPMO_REQUIRE(b->mode == 1, "the work queues belong to mode 1");
+    NAPMO_REQUIRE(timeout_s > 0.0 && timeout_s <= 10.0, "timeout must be in (0, 10] s");
+    if (!b->warm || stale(b)) {
+      const int e = warm_up(b, s);
+      if (e) return e;
+    }
+    return stage_batch_queue_selftest(b->stage, (unsigned long long)(timeout_s * 1e9), s, status);
+  });
+}
+
+// Mode 1: error word of the work queues since the last call (0 or 5); clears it.
+int napmo_fock_batch_status(FockBatch *b, void *stream, int *status) {
+  return guarded([&] {
+    *status = 0;
+    if (b->stage) return stage_batch_status(b->stage, (cudaStream_t)stream, status);
     return kOk;
   });
 }

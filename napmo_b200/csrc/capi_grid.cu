@@ -344,6 +344,71 @@ int grid_poisson_plan(BeckeGrid *g, int lmax, cudaStream_t s, PoissonPlan **out)
 // restricts the evaluation to the flagged points, v = 0 elsewhere (its pair
 // lists are built, synchronously, the first time a mask is used; key names
 // the mask, which an address could not: a freed mask's address is reused).
+// Several molecular grids as one, for Poisson solves of a batch in one launch
+// per pipeline stage: the atoms of every grid in order, their points
+// concatenated (grid m from off[m], no padding) in copies of the device
+// arrays, and a Poisson plan with one molecule per grid, so that every atom
+// pairs with its own molecule's points only.  lmax[m] is grid m's cutoff
+// (kLmaxPerAtom: each atom's own rule).  The result owns its arrays and plan.
+int grid_concat(const std::vector<BeckeGrid *> &grids, const std::vector<int> &lmax,
+                cudaStream_t s, BeckeGrid **out, std::vector<int> *off) {
+  std::unique_ptr<BeckeGrid> g(new BeckeGrid);
+  std::vector<int> o(1, 0), mol_atom_off(1, 0), lm;
+  for (size_t m = 0; m < grids.size(); ++m) {
+    BeckeGrid *gm = grids[m];
+    if (gm->layout.empty())
+      return set_error(kNotSupported, "grid has no atomic structure (read from points)");
+    for (const AtomLayout &L : gm->layout) {
+      AtomLayout c = L;
+      c.point_off += o.back();
+      g->layout.push_back(c);
+      int l = lmax[m];
+      if (l == kLmaxPerAtom) {
+        const int prec = lebedev_precision(L.nang);
+        if (prec < 0) return set_error(kInvalidArgument, "no Lebedev rule with this number of points");
+        l = prec / 2;
+      }
+      lm.push_back(l);
+    }
+    mol_atom_off.push_back((int)g->layout.size());
+    o.push_back(o.back() + gm->size);
+  }
+  g->size = o.back();
+  g->ncenter = (int)g->layout.size();
+  DeviceGrid &d = g->dev;
+  d.npoint = g->size;
+  for (double **arr : {&d.x, &d.y, &d.z, &d.w, &d.wb})
+    NAPMO_TRY_CUDA(cudaMalloc(arr, std::max(g->size, 1) * sizeof(double)), "alloc batch grid");
+  for (size_t m = 0; m < grids.size(); ++m) {
+    const DeviceGrid &src = grids[m]->dev;
+    const size_t bytes = (size_t)grids[m]->size * sizeof(double);
+    const long at = o[m];
+    NAPMO_TRY_CUDA(cudaMemcpyAsync(d.x + at, src.x, bytes, cudaMemcpyDeviceToDevice, s), "copy");
+    NAPMO_TRY_CUDA(cudaMemcpyAsync(d.y + at, src.y, bytes, cudaMemcpyDeviceToDevice, s), "copy");
+    NAPMO_TRY_CUDA(cudaMemcpyAsync(d.z + at, src.z, bytes, cudaMemcpyDeviceToDevice, s), "copy");
+    NAPMO_TRY_CUDA(cudaMemcpyAsync(d.w + at, src.w, bytes, cudaMemcpyDeviceToDevice, s), "copy");
+    NAPMO_TRY_CUDA(cudaMemcpyAsync(d.wb + at, src.wb, bytes, cudaMemcpyDeviceToDevice, s), "copy");
+  }
+  auto *p = new PoissonPlan;
+  g->poisson = p;  // owned by g from here on
+  std::vector<const AtomLayout *> atoms;
+  for (auto &L : g->layout) atoms.push_back(&L);
+  int st = build_poisson_plan(atoms, lm, mol_atom_off, o, s, p);
+  if (st != kOk) return st;
+  st = build_pair_lists(p, d.x, d.y, d.z, nullptr, p->pairs, p->items, p->nitems, p->nitems_in, s);
+  if (st != kOk) return st;
+  p->d.items = p->items.p;
+  p->d.nitems = p->nitems;
+  p->d.nitems_inner = p->nitems_in;
+  p->lmax = -3;  // not a single-grid cutoff: grid_poisson_plan never reuses it
+  NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "batch grid");
+  *off = o;
+  *out = g.release();
+  return kOk;
+}
+
+void grid_free(BeckeGrid *g) { delete g; }
+
 int run_poisson(BeckeGrid *g, PoissonPlan *p, const double *rho_dev, double *v_dev,
                 bool accumulate, cudaStream_t s, double tol, const int *keep,
                 unsigned long long key) {

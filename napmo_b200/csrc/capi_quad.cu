@@ -4,7 +4,9 @@
 // Fock-build plan that keeps phi, the grid and the Poisson tables resident in
 // HBM across SCF iterations.
 #include <algorithm>
+#include <cstdint>
 #include <atomic>
+#include <memory>
 #include <vector>
 
 #include "capi_common.cuh"
@@ -189,6 +191,205 @@ int fock_build(FockPlan *p, const double *D_dev, double q, const double *vext_de
   NAPMO_TRY_CUDA(launch_combine_weights(g->size, g->dev.wb, g->dev.w, q, v, vext_dev, p->wv.p, s),
                  "weights");
   return plan_quadrature(p, F_dev, s);
+}
+
+// ------------------------------------------------------------ stage batches
+// A batch of FP64 Fock builds run as one launch per stage for all molecules:
+// the density of every molecule by one persistent launch over (molecule,
+// 128-point group) items, the Poisson solves of every molecule by one plan
+// over the concatenated grids (grid_concat: each atom pairs with its own
+// molecule's points), the weights by one launch, the quadratures by one
+// persistent launch over (molecule, tile, chunk) items and one reduction.
+// The persistent launches take their items from device work queues posted
+// when the batch is set up.  Each molecule's arithmetic is that of its own
+// plan, so a stage build equals the molecules' own builds bit for bit.
+int grid_concat(const std::vector<BeckeGrid *> &grids, const std::vector<int> &lmax,
+                cudaStream_t s, BeckeGrid **out, std::vector<int> *off);
+void grid_free(BeckeGrid *g);
+
+struct StageBatch {
+  std::vector<FockPlan *> plans;
+  BeckeGrid *cat = nullptr;          // the molecules' grids as one (Poisson)
+  std::vector<int> off, offp;        // point offsets: unpadded, padded to 128
+  DevBuf<double> rho, v, wv;         // concatenated
+  DevBuf<int> keep;                  // concatenated screening flags (screened plans)
+  unsigned long long keep_key = 0;
+  DevBuf<DensBatchArg> dargs;
+  DevBuf<QuadBatchArg> qargs;
+  DevBuf<WeightBatchArg> wargs;
+  DevBuf<int4> ditems, qitems;
+  DevBuf<int> head, posted, status;  // [2]: density and quadrature queues
+  int nd = 0, nq = 0, grid_d = 0, grid_q = 0;
+  double q = 1.0, tol = 0.0;
+  unsigned long long timeout_ns = 1000000000ull;
+  ~StageBatch() {
+    if (cat) grid_free(cat);
+  }
+};
+
+static int sm_count() {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
+// Set-up (synchronises): the concatenated grid and its Poisson plan, the
+// batch buffers, the per-molecule argument tables and the posted work queues.
+int stage_batch_new(const std::vector<FockPlan *> &plans, const std::vector<double *> &D,
+                    const std::vector<double *> &F, double q, cudaStream_t s, StageBatch **out) {
+  std::unique_ptr<StageBatch> b(new StageBatch);
+  b->plans = plans;
+  b->q = q;
+  const int nmol = (int)plans.size();
+  std::vector<BeckeGrid *> grids;
+  std::vector<int> lmax;
+  for (FockPlan *p : plans) {
+    if (p->mode != 0) return set_error(kNotSupported, "stage batches take FP64 plans");
+    if (p->lmax < 0 && p->lmax != kLmaxPerAtom)
+      return set_error(kInvalidArgument, "plan without Poisson tables");
+    if (p->poisson_tol != plans[0]->poisson_tol)
+      return set_error(kInvalidArgument, "plans of a stage batch share one Poisson tolerance");
+    grids.push_back(p->grid);
+    lmax.push_back(p->lmax);
+  }
+  b->tol = plans[0]->poisson_tol;
+  int st = grid_concat(grids, lmax, s, &b->cat, &b->off);
+  if (st) return st;
+  b->offp.assign(1, 0);
+  for (FockPlan *p : plans) b->offp.push_back(b->offp.back() + (int)p->ld);
+  NAPMO_TRY_CUDA(b->rho.alloc(std::max(b->off.back(), 1)), "alloc batch");
+  NAPMO_TRY_CUDA(b->v.alloc(std::max(b->off.back(), 1)), "alloc batch");
+  NAPMO_TRY_CUDA(b->wv.alloc(std::max(b->offp.back(), 1)), "alloc batch");
+  bool screened = false;
+  for (FockPlan *p : plans) screened = screened || p->fp64_screen > 0.0;
+  if (screened) {
+    NAPMO_TRY_CUDA(b->keep.alloc(std::max(b->off.back(), 1)), "alloc batch");
+    for (int m = 0; m < nmol; ++m) {
+      FockPlan *p = plans[m];
+      int *dst = b->keep.p + b->off[m];
+      if (p->fp64_screen > 0.0) {
+        NAPMO_TRY_CUDA(cudaMemcpyAsync(dst, p->keep64.p, (size_t)p->grid->size * sizeof(int),
+                                       cudaMemcpyDeviceToDevice, s),
+                       "batch flags");
+      } else {
+        std::vector<int> ones(p->grid->size, 1);
+        NAPMO_TRY_CUDA(cudaMemcpyAsync(dst, ones.data(), ones.size() * sizeof(int),
+                                       cudaMemcpyHostToDevice, s),
+                       "batch flags");
+        NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "batch flags");
+      }
+    }
+    static std::atomic<unsigned long long> next{1};
+    b->keep_key = (3ull << 62) | next++;
+  }
+  std::vector<DensBatchArg> da(nmol);
+  std::vector<QuadBatchArg> qa(nmol);
+  std::vector<WeightBatchArg> wa(nmol);
+  std::vector<int4> di, qi;
+  for (int m = 0; m < nmol; ++m) {
+    FockPlan *p = plans[m];
+    const int N = p->grid->size;
+    const bool scr = p->fp64_screen > 0.0;
+    da[m] = DensBatchArg{p->phi.p, p->ld, D[m], b->rho.p + b->off[m],
+                         scr ? p->keep64.p : nullptr, p->n, N,
+                         (p->n % 2 == 0 && reinterpret_cast<uintptr_t>(D[m]) % 16 == 0) ? 1 : 0,
+                         0};
+    std::vector<int> groups, blocks;
+    if (scr) {
+      groups.resize(p->ngroups64);
+      blocks.resize(p->nblocks64);
+      if (!groups.empty())
+        NAPMO_TRY_CUDA(cudaMemcpy(groups.data(), p->groups64.p, groups.size() * sizeof(int),
+                                  cudaMemcpyDeviceToHost),
+                       "batch groups");
+    } else {
+      for (int gi = 0; gi < (N + 127) / 128; ++gi) groups.push_back(gi);
+    }
+    for (int gi : groups) di.push_back(make_int4(m, gi, 0, 0));
+    const int npad = scr ? p->nblocks64 * 16 : (int)padded_points(N);
+    int chunk = 0;
+    const int nchunk =
+        npad > 0 ? quadrature_chunking(p->n, npad, &chunk, (int)padded_points(N)) : 0;
+    const int nblk = (p->n + 127) / 128, ntile = nblk * (nblk + 1) / 2;
+    qa[m] = QuadBatchArg{p->phi.p, p->ld, b->wv.p + b->offp[m], p->work.p, F[m],
+                         scr ? p->blocks64.p : nullptr, p->n, npad, nblk, chunk, nchunk};
+    for (int c = 0; c < nchunk; ++c)
+      for (int t = 0; t < ntile; ++t) qi.push_back(make_int4(m, t, c, 0));
+    wa[m] = WeightBatchArg{p->grid->dev.wb, p->grid->dev.w, b->v.p + b->off[m],
+                           b->wv.p + b->offp[m], N, (int)p->ld};
+  }
+  NAPMO_TRY_CUDA(b->dargs.upload(da, s), "batch tables");
+  NAPMO_TRY_CUDA(b->qargs.upload(qa, s), "batch tables");
+  NAPMO_TRY_CUDA(b->wargs.upload(wa, s), "batch tables");
+  NAPMO_TRY_CUDA(di.empty() ? b->ditems.alloc(1) : b->ditems.upload(di, s), "batch items");
+  NAPMO_TRY_CUDA(qi.empty() ? b->qitems.alloc(1) : b->qitems.upload(qi, s), "batch items");
+  b->nd = (int)di.size();
+  b->nq = (int)qi.size();
+  const int sms = sm_count();
+  b->grid_d = std::max(1, std::min(b->nd, sms));
+  b->grid_q = std::max(1, std::min(b->nq, sms));
+  NAPMO_TRY_CUDA(b->head.alloc(2), "batch queue");
+  NAPMO_TRY_CUDA(b->status.alloc(1), "batch queue");
+  NAPMO_TRY_CUDA(b->posted.upload(std::vector<int>{b->nd, b->nq}, s), "batch queue");
+  NAPMO_TRY_CUDA(cudaMemsetAsync(b->status.p, 0, sizeof(int), s), "batch queue");
+  NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "batch set-up");
+  *out = b.release();
+  return kOk;
+}
+
+void stage_batch_free(StageBatch *b) { delete b; }
+
+static BatchQueue stage_queue(StageBatch *b, int which) {
+  return BatchQueue{which == 0 ? b->ditems.p : b->qitems.p, which == 0 ? b->nd : b->nq,
+                    b->head.p + which, b->posted.p + which, b->status.p, b->timeout_ns};
+}
+
+// One build of every molecule (stream-ordered, no allocation, capturable).
+int stage_batch_build(StageBatch *b, cudaStream_t s) {
+  const int nmol = (int)b->plans.size();
+  NAPMO_TRY_CUDA(cudaMemsetAsync(b->head.p, 0, 2 * sizeof(int), s), "batch queue");
+  if (b->keep.p)  // screened plans compute only the groups holding a kept point
+    NAPMO_TRY_CUDA(cudaMemsetAsync(b->rho.p, 0, (size_t)b->off.back() * sizeof(double), s),
+                   "batch rho");
+  NAPMO_TRY_CUDA(launch_density_batch(b->dargs.p, stage_queue(b, 0), b->grid_d, s), "density");
+  int e = run_poisson(b->cat, b->cat->poisson, b->rho.p, b->v.p, false, s, b->tol,
+                      b->keep.p, b->keep_key);
+  if (e) return e;
+  NAPMO_TRY_CUDA(launch_combine_weights_batch(b->wargs.p, nmol, b->q, s), "weights");
+  NAPMO_TRY_CUDA(launch_quadrature_batch(b->qargs.p, stage_queue(b, 1), b->grid_q, s),
+                 "quadrature");
+  NAPMO_TRY_CUDA(launch_quadrature_reduce_batch(b->qargs.p, nmol, s), "quadrature reduce");
+  return kOk;
+}
+
+// The density stage with a queue that was never posted: every CTA's wait runs
+// out after timeout_ns and records kDeviceTimeout (read back into *status,
+// then cleared); the batch's queues are left as they were.  Synchronises.
+int stage_batch_queue_selftest(StageBatch *b, unsigned long long timeout_ns, cudaStream_t s,
+                               int *status) {
+  DevBuf<int> never;
+  NAPMO_TRY_CUDA(never.upload(std::vector<int>{0}, s), "self-test");
+  NAPMO_TRY_CUDA(cudaMemsetAsync(b->head.p, 0, 2 * sizeof(int), s), "self-test");
+  NAPMO_TRY_CUDA(cudaMemsetAsync(b->status.p, 0, sizeof(int), s), "self-test");
+  BatchQueue q = stage_queue(b, 0);
+  q.posted = never.p;
+  q.timeout_ns = timeout_ns;
+  NAPMO_TRY_CUDA(launch_density_batch(b->dargs.p, q, b->grid_d, s), "self-test");
+  NAPMO_TRY_CUDA(cudaMemcpyAsync(status, b->status.p, sizeof(int), cudaMemcpyDeviceToHost, s),
+                 "self-test");
+  NAPMO_TRY_CUDA(cudaMemsetAsync(b->status.p, 0, sizeof(int), s), "self-test");
+  NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "self-test");
+  return kOk;
+}
+
+// Device error word of the batch's work queues (0 or kDeviceTimeout); clears it.
+int stage_batch_status(StageBatch *b, cudaStream_t s, int *status) {
+  NAPMO_TRY_CUDA(cudaMemcpyAsync(status, b->status.p, sizeof(int), cudaMemcpyDeviceToHost, s),
+                 "batch status");
+  NAPMO_TRY_CUDA(cudaMemsetAsync(b->status.p, 0, sizeof(int), s), "batch status");
+  NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "batch status");
+  return kOk;
 }
 
 int fock_plan_nbasis(const FockPlan *p) { return p->n; }

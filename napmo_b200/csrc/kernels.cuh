@@ -40,6 +40,50 @@ cudaError_t launch_quadrature_f64(int n, int npoint, const double *phi, long ld,
                                   const double *wv, double *F, double *work,
                                   cudaStream_t s, const double *phib = nullptr,
                                   const int *blocks = nullptr, int nblock = 0);
+// Batched FP64 launches (one launch per stage for many molecules).
+struct DensBatchArg {      // density of one molecule
+  const double *phi;       // [n][ld]
+  long ld;
+  const double *D;         // [n][n]
+  double *rho;             // [npoint]
+  const int *keep;         // screening flags or null
+  int n, npoint, vecD, pad;
+};
+struct QuadBatchArg {      // quadrature of one molecule
+  const double *phi;       // [n][ld]
+  long ld;
+  const double *wv;        // zero padded to npoint rounded up to 128
+  double *work;            // [nchunk][tile][128][128]
+  double *F;               // [n][n]
+  const int *blocks;       // 16-point blocks of a screened plan, or null
+  int n, npad, nblk, chunk, nchunk;
+};
+struct WeightBatchArg {    // wv = wb w (q v), zero padded to npad
+  const double *wb, *w, *v;
+  double *wv;
+  int npoint, npad;
+};
+// Device work queue of a persistent batched launch: items[i] = (molecule,
+// tile, chunk, -); item i is taken once *posted > i, waiting at most
+// timeout_ns; a timeout records kDeviceTimeout in *status.
+struct BatchQueue {
+  const int4 *items;
+  int nitems;
+  int *head;
+  const int *posted;
+  int *status;
+  unsigned long long timeout_ns;
+};
+// Split-K chunking of a K range of npad points in a workspace sized for a grid
+// of pad_full points (quadrature_workspace_bytes): chunk count <= the grid's.
+int quadrature_chunking(int n, int npad, int *chunk, int pad_full);
+cudaError_t launch_density_batch(const DensBatchArg *args, const BatchQueue &q, int grid,
+                                 cudaStream_t s);
+cudaError_t launch_quadrature_batch(const QuadBatchArg *args, const BatchQueue &q, int grid,
+                                    cudaStream_t s);
+cudaError_t launch_quadrature_reduce_batch(const QuadBatchArg *args, int nmol, cudaStream_t s);
+cudaError_t launch_combine_weights_batch(const WeightBatchArg *args, int nmol, double q,
+                                         cudaStream_t s);
 // FP64 point screening: keep[p] (|wb w| max_mu phi_mu(p)^2 >= tol), and the
 // flags of the 16-point blocks and 128-point groups holding a kept point.
 cudaError_t launch_fp64_screening(int n, int npoint, const double *phi, long ld, const double *wb,

@@ -138,17 +138,16 @@ __device__ __forceinline__ int density_stage(int it, int nblk, int nk, int &mb, 
 
 // groups (optional): the 128-point groups to compute (screened plans; the
 // others hold no kept point); keep (optional): rho = 0 at dropped points.
+// rho of the 128 points p0 .. p0 + 127 (one CTA; see density_kernel).
 template <bool kVecD>
-__global__ void __launch_bounds__(NT, 1)
-density_kernel(int n, int npoint, const double *__restrict__ phi, long ld,
-               const double *__restrict__ D, double *__restrict__ rho,
-               const int *__restrict__ groups, const int *__restrict__ keep) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  DensSmem &sm = *reinterpret_cast<DensSmem *>(smem_raw);
+__device__ __forceinline__ void density_block(DensSmem &sm, int n, int npoint,
+                                              const double *__restrict__ phi, long ld,
+                                              const double *__restrict__ D,
+                                              double *__restrict__ rho, int p0,
+                                              const int *__restrict__ keep) {
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int g = lane >> 2, q = lane & 3;
   const int wrow = (warp >> 2) * 64, wcol = (warp & 3) * 32;
-  const int p0 = (groups ? groups[blockIdx.x] : (int)blockIdx.x) * BN;
   const int nblk = (n + BM - 1) / BM;
   const int nk = (n + BK - 1) / BK;                 // stages of nu over the whole basis
   int nstage = 0;
@@ -279,23 +278,36 @@ density_kernel(int n, int npoint, const double *__restrict__ phi, long ld,
     rho[p0 + t] = (keep && !keep[p0 + t]) ? 0.0 : sm.red[0][t] + sm.red[1][t];
 }
 
+template <bool kVecD>
+__global__ void __launch_bounds__(NT, 1)
+density_kernel(int n, int npoint, const double *__restrict__ phi, long ld,
+               const double *__restrict__ D, double *__restrict__ rho,
+               const int *__restrict__ groups, const int *__restrict__ keep) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  DensSmem &sm = *reinterpret_cast<DensSmem *>(smem_raw);
+  const int p0 = (groups ? groups[blockIdx.x] : (int)blockIdx.x) * BN;
+  density_block<kVecD>(sm, n, npoint, phi, ld, D, rho, p0, keep);
+}
+
 // --------------------------------------------------------------- quadrature
 // Without `blocks` the K range is every point (npoint_pad, chunks of `chunk`
 // points); with it (screened plans) the K range is the list of 16-point
 // blocks holding a kept point, npoint_pad = 16 x their count and `chunk` a
 // multiple of 16 as before.
-__global__ void __launch_bounds__(NT, 1)
-quadrature_kernel(int n, int npoint_pad, const double *__restrict__ phi,
-                  const double *__restrict__ phib, long ld,
-                  const double *__restrict__ wv, int nblk, int chunk,
-                  double *__restrict__ work, const int *__restrict__ blocks) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  QuadSmem &sm = *reinterpret_cast<QuadSmem *>(smem_raw);
+// Tile `tile` (upper-triangle index) of F over chunk `ck` of the points into
+// its workspace slot (one CTA; see quadrature_kernel).
+__device__ __forceinline__ void quadrature_block(QuadSmem &sm, int n, int npoint_pad,
+                                                 const double *__restrict__ phi,
+                                                 const double *__restrict__ phib, long ld,
+                                                 const double *__restrict__ wv, int nblk,
+                                                 int chunk, double *__restrict__ work,
+                                                 const int *__restrict__ blocks, int tile_index,
+                                                 int ck) {
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int g = lane >> 2, q = lane & 3;
   const int wrow = (warp >> 2) * 64, wcol = (warp & 3) * 32;
   // upper-triangle tile index -> (mb, nb)
-  int tile = blockIdx.x, mb = 0;
+  int tile = tile_index, mb = 0;
   {
     int rem = tile;
     while (rem >= nblk - mb) {
@@ -306,7 +318,7 @@ quadrature_kernel(int n, int npoint_pad, const double *__restrict__ phi,
   }
   const int nb = mb + tile;
   const int mu0 = mb * BM, nu0 = nb * BN;
-  const int k_begin = blockIdx.y * chunk;
+  const int k_begin = ck * chunk;
   const int k_end = min(k_begin + chunk, npoint_pad);
   const int nstage = k_end > k_begin ? (k_end - k_begin) / BK : 0;
 
@@ -356,7 +368,7 @@ quadrature_kernel(int n, int npoint_pad, const double *__restrict__ phi,
   }
   cp_async_wait<0>();
   const int ntile = nblk * (nblk + 1) / 2;
-  double *out = work + ((long)blockIdx.y * ntile + blockIdx.x) * (BM * BN);
+  double *out = work + ((long)ck * ntile + tile_index) * (BM * BN);
 #pragma unroll
   for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
@@ -366,6 +378,17 @@ quadrature_kernel(int n, int npoint_pad, const double *__restrict__ phi,
       *reinterpret_cast<double2 *>(out + (r + 8) * BN + c) =
           make_double2(acc[mt][nt][2], acc[mt][nt][3]);
     }
+}
+
+__global__ void __launch_bounds__(NT, 1)
+quadrature_kernel(int n, int npoint_pad, const double *__restrict__ phi,
+                  const double *__restrict__ phib, long ld,
+                  const double *__restrict__ wv, int nblk, int chunk,
+                  double *__restrict__ work, const int *__restrict__ blocks) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  QuadSmem &sm = *reinterpret_cast<QuadSmem *>(smem_raw);
+  quadrature_block(sm, n, npoint_pad, phi, phib, ld, wv, nblk, chunk, work, blocks,
+                   blockIdx.x, blockIdx.y);
 }
 
 __global__ void quadrature_reduce_kernel(int n, int nblk, int nchunk,
@@ -473,12 +496,12 @@ cudaError_t launch_quadrature_f64(int n, int npoint, const double *phi, long ld,
                                   int nblock) {
   if (!phib) phib = phi;
   if (n <= 0) return cudaSuccess;
-  // screened: the K range is the listed 16-point blocks (at most all of them,
-  // so the workspace sized for npoint suffices)
+  // screened: the K range is the listed 16-point blocks; its chunk count is
+  // capped at the workspace's (sized for every point), see quadrature_chunking
   const int npad = blocks ? nblock * BK : pad_points(npoint);
   if (npad == 0) return cudaMemsetAsync(F, 0, (size_t)n * n * sizeof(double), s);
   int chunk;
-  const int nchunk = quad_chunks(n, npad, &chunk);
+  const int nchunk = quadrature_chunking(n, npad, &chunk, pad_points(npoint));
   const int nblk = (n + BM - 1) / BM;
   const int ntile = nblk * (nblk + 1) / 2;
   dim3 grid(ntile, nchunk);
@@ -498,6 +521,163 @@ cudaError_t launch_quadrature_reduce(int n, int nchunk, const double *work, doub
   const long total = (long)ntile * BM * BN;
   const int rblocks = (int)std::min<long>((total + 255) / 256, 148 * 16);
   quadrature_reduce_kernel<<<rblocks, 256, 0, s>>>(n, nblk, nchunk, work, F);
+  return cudaGetLastError();
+}
+
+// -------------------------------------------------------------- batches
+// Persistent batched launches: CTAs take (molecule, tile) items from a device
+// work queue until it is empty.  Item i may be taken once *posted > i (the
+// batch posts its items when it is built; a producer that never posts makes
+// the wait run out): the wait is bounded by q.timeout_ns of %globaltimer,
+// after which the CTA records kDeviceTimeout in *q.status and stops.
+namespace {
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ int queue_pop(const BatchQueue &q) {
+  const int i = atomicAdd(q.head, 1);
+  if (i >= q.nitems) return -1;
+  const volatile int *posted = q.posted;
+  if (*posted > i) return i;
+  const unsigned long long t0 = globaltimer_ns();
+  for (unsigned it = 1;; ++it) {
+    if (*posted > i) return i;
+    if ((it & 63) == 0 && globaltimer_ns() - t0 > q.timeout_ns) {
+      atomicExch(q.status, kDeviceTimeout);
+      return -1;
+    }
+  }
+}
+
+// the CTA's next item (all threads), -1 when the queue is done
+__device__ __forceinline__ int cta_pop(const BatchQueue &q, int *slot) {
+  if (threadIdx.x == 0) *slot = queue_pop(q);
+  __syncthreads();
+  const int w = *slot;
+  __syncthreads();
+  return w;
+}
+
+__global__ void __launch_bounds__(NT, 1)
+density_batch_kernel(const DensBatchArg *__restrict__ args, BatchQueue q) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  DensSmem &sm = *reinterpret_cast<DensSmem *>(smem_raw);
+  __shared__ int slot;
+  for (;;) {
+    const int w = cta_pop(q, &slot);
+    if (w < 0) break;
+    const int4 it = q.items[w];
+    const DensBatchArg a = args[it.x];
+    if (a.vecD)
+      density_block<true>(sm, a.n, a.npoint, a.phi, a.ld, a.D, a.rho, it.y * BN, a.keep);
+    else
+      density_block<false>(sm, a.n, a.npoint, a.phi, a.ld, a.D, a.rho, it.y * BN, a.keep);
+  }
+}
+
+__global__ void __launch_bounds__(NT, 1)
+quadrature_batch_kernel(const QuadBatchArg *__restrict__ args, BatchQueue q) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  QuadSmem &sm = *reinterpret_cast<QuadSmem *>(smem_raw);
+  __shared__ int slot;
+  for (;;) {
+    const int w = cta_pop(q, &slot);
+    if (w < 0) break;
+    const int4 it = q.items[w];
+    const QuadBatchArg a = args[it.x];
+    quadrature_block(sm, a.n, a.npad, a.phi, a.phi, a.ld, a.wv, a.nblk, a.chunk, a.work,
+                     a.blocks, it.y, it.z);
+  }
+}
+
+// F of every molecule from its chunk partials (blockIdx.y = molecule)
+__global__ void quadrature_reduce_batch_kernel(const QuadBatchArg *__restrict__ args) {
+  const QuadBatchArg a = args[blockIdx.y];
+  const int ntile = a.nblk * (a.nblk + 1) / 2;
+  const long total = (long)ntile * BM * BN;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
+       e += (long)gridDim.x * blockDim.x) {
+    const int tile = (int)(e / (BM * BN));
+    const int m = (int)(e % (BM * BN)) / BN, c = (int)(e % BN);
+    int mb = 0, rem = tile;
+    while (rem >= a.nblk - mb) {
+      rem -= a.nblk - mb;
+      ++mb;
+    }
+    const int nb = mb + rem;
+    const int mu = mb * BM + m, nu = nb * BN + c;
+    if (mu >= a.n || nu >= a.n || mu > nu) continue;
+    double s = 0.0;
+    for (int k = 0; k < a.nchunk; ++k) s += a.work[((long)k * ntile + tile) * (BM * BN) + m * BN + c];
+    a.F[(long)mu * a.n + nu] = s;
+    a.F[(long)nu * a.n + mu] = s;
+  }
+}
+
+// wv of every molecule (blockIdx.y), zero padded to its npad points
+__global__ void combine_weights_batch_kernel(const WeightBatchArg *__restrict__ args, double q) {
+  const WeightBatchArg a = args[blockIdx.y];
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.npad; p += gridDim.x * blockDim.x)
+    a.wv[p] = p < a.npoint ? a.wb[p] * a.w[p] * (q * a.v[p]) : 0.0;
+}
+
+}  // namespace
+
+// Chunking of a K range of npad points when the workspace was sized for a
+// grid of pad_full points (npad <= pad_full): quad_chunks is not monotone in
+// the range (a shorter range below a chunk-size step gets more, shorter
+// chunks), so the chunk count is capped at the full grid's and the chunks
+// lengthened to fit.
+int quadrature_chunking(int n, int npad, int *chunk, int pad_full) {
+  int c = 0;
+  int nchunk = quad_chunks(n, npad, &c);
+  int cf = 0;
+  const int cap = quad_chunks(n, pad_full > npad ? pad_full : npad, &cf);
+  if (nchunk > cap) {
+    c = (npad + cap - 1) / cap;
+    c = ((c + BK - 1) / BK) * BK;
+    nchunk = (npad + c - 1) / c;
+  }
+  *chunk = c;
+  return nchunk;
+}
+
+cudaError_t launch_density_batch(const DensBatchArg *args, const BatchQueue &q, int grid,
+                                 cudaStream_t s) {
+  if (q.nitems == 0) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(density_batch_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kDensSmem);
+  if (e != cudaSuccess) return e;
+  density_batch_kernel<<<grid, NT, kDensSmem, s>>>(args, q);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_quadrature_batch(const QuadBatchArg *args, const BatchQueue &q, int grid,
+                                    cudaStream_t s) {
+  if (q.nitems == 0) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(quadrature_batch_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kQuadSmem);
+  if (e != cudaSuccess) return e;
+  quadrature_batch_kernel<<<grid, NT, kQuadSmem, s>>>(args, q);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_quadrature_reduce_batch(const QuadBatchArg *args, int nmol, cudaStream_t s) {
+  if (nmol == 0) return cudaSuccess;
+  quadrature_reduce_batch_kernel<<<dim3(148 * 2, nmol), 256, 0, s>>>(args);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_combine_weights_batch(const WeightBatchArg *args, int nmol, double q,
+                                         cudaStream_t s) {
+  if (nmol == 0) return cudaSuccess;
+  combine_weights_batch_kernel<<<dim3(148, nmol), 256, 0, s>>>(args, q);
   return cudaGetLastError();
 }
 

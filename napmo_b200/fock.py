@@ -261,6 +261,31 @@ class FockBatch(object):
                                                byref(ns), byref(bud), byref(ms)))
         return {'nstream': ns.value, 'budget': bud.value, 'ms': ms.value}
 
+    MODES = {'streams': 0, 'stages': 1}
+
+    def set_mode(self, mode):
+        """'streams': the molecules' own launch chains spread over capture
+        streams (one graph); 'stages': one launch per stage for the whole batch
+        (persistent density and quadrature launches over device work queues,
+        one Poisson plan over every grid; FP64 builders)."""
+        checked(cext.lib.napmo_fock_batch_set_mode(self._this, self.MODES[mode]))
+        self.mode = mode
+
+    def queue_selftest(self, timeout_s=0.2, stream=None):
+        """'stages' mode: the density stage with a queue that is never posted;
+        returns the queue's error word (5 when the bounded waits ran out)."""
+        st = c_int()
+        checked(cext.lib.napmo_fock_batch_queue_selftest(self._this, float(timeout_s),
+                                                         _stream(self.torch, stream), byref(st)))
+        return st.value
+
+    def status(self, stream=None):
+        """Error word of the work queues since the last call (0 or 5)."""
+        st = c_int()
+        checked(cext.lib.napmo_fock_batch_status(self._this, _stream(self.torch, stream),
+                                                 byref(st)))
+        return st.value
+
     def __del__(self):
         if getattr(self, '_this', None):
             try:

@@ -115,3 +115,52 @@ def test_batch_at_the_batched_configuration_sizes():
     for F, R, R64, D in zip(F8, ref8, ref64, Ds):
         assert np.abs(F - R).max() <= 1e-12 * np.abs(R).max()
         assert abs(0.5 * float((F * D).sum()) - 0.5 * float((R64 * D).sum())) <= 1e-6
+
+
+def test_stage_batch_equals_single_builds():
+    """'stages' mode: one launch per stage for the whole batch (persistent
+    density and quadrature launches over device work queues, one Poisson plan
+    over all grids) gives every molecule's own build bit for bit, with and
+    without FP64 point screening."""
+    import torch
+    import napmo_b200 as nb
+    mols = _molecules(nmol=7, seed=5)
+    builders = [nb.FockBuilder(g, e['basis'], 'per-atom') for e, g in mols]
+    Ds = [random_density(b.n, max(1, e['occupation']), seed=200 + i)
+          for i, ((e, g), b) in enumerate(zip(mols, builders))]
+    for screen in (0.0, 1e-24):
+        for b in builders:
+            b.set_fp64_screening(screen)
+        ref = [b.build(D)[0].cpu().numpy() for b, D in zip(builders, Ds)]
+        batch = nb.FockBatch(builders)
+        batch.set_mode('stages')
+        Fs = [F.cpu().numpy() for F in batch.build(Ds)]
+        torch.cuda.synchronize()
+        assert batch.status() == 0
+        for F, R in zip(Fs, ref):
+            assert np.array_equal(F, R)
+        Fs2 = [F.cpu().numpy() for F in batch.build()]
+        assert all(np.array_equal(a, c) for a, c in zip(Fs, Fs2))
+    for b in builders:
+        b.set_fp64_screening(0.0)
+
+
+def test_stage_batch_queue_wait_runs_out():
+    """A work queue that is never posted: every CTA's wait gives up after the
+    per-launch limit and the queue's error word reads 5; the batch then builds
+    correctly (no trap, no hang)."""
+    import torch
+    import napmo_b200 as nb
+    mols = _molecules(nmol=3, seed=9)
+    builders = [nb.FockBuilder(g, e['basis'], 'per-atom') for e, g in mols]
+    Ds = [random_density(b.n, max(1, e['occupation']), seed=50 + i)
+          for i, ((e, g), b) in enumerate(zip(mols, builders))]
+    ref = [b.build(D)[0].cpu().numpy() for b, D in zip(builders, Ds)]
+    batch = nb.FockBatch(builders)
+    batch.set_mode('stages')
+    batch.build(Ds)
+    assert batch.queue_selftest(0.2) == 5
+    assert batch.status() == 0
+    Fs = [F.cpu().numpy() for F in batch.build(Ds)]
+    torch.cuda.synchronize()
+    assert all(np.array_equal(F, R) for F, R in zip(Fs, ref))

@@ -278,6 +278,7 @@ int napmo_fock_batch_tune(FockBatch *b, void *stream, int reps, int *nstream_out
       for (int bud : budgets) {
         b->nstream = ns;
         if ((st = set_budgets(b, bud))) break;
+        if (b->mode == 1 && (st = warm_up(b, s))) break;  // stage tables hold the budgets
         if ((st = capture(b))) break;
         cudaGraphLaunch(b->exec, s);
         cudaEventRecord(e0, s);
@@ -304,6 +305,7 @@ int napmo_fock_batch_tune(FockBatch *b, void *stream, int reps, int *nstream_out
     if (st) return st;
     b->nstream = best_ns;
     if ((st = set_budgets(b, best_budget))) return st;
+    if (b->mode == 1 && (st = warm_up(b, s))) return st;
     if ((st = capture(b))) return st;
     b->tuned_ms = best;
     if (nstream_out) *nstream_out = best_ns;

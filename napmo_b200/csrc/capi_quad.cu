@@ -222,8 +222,11 @@ struct StageBatch {
   int nd = 0, nq = 0, grid_d = 0, grid_q = 0;
   double q = 1.0, tol = 0.0;
   unsigned long long timeout_ns = 1000000000ull;
+  int mode = 0;                      // the plans' precision
+  Int8Batch *i8 = nullptr;           // mode 1: the int8 stages' tables
   ~StageBatch() {
     if (cat) grid_free(cat);
+    if (i8) int8_batch_free(i8);
   }
 };
 
@@ -244,8 +247,11 @@ int stage_batch_new(const std::vector<FockPlan *> &plans, const std::vector<doub
   const int nmol = (int)plans.size();
   std::vector<BeckeGrid *> grids;
   std::vector<int> lmax;
+  b->mode = plans[0]->mode;
   for (FockPlan *p : plans) {
-    if (p->mode != 0) return set_error(kNotSupported, "stage batches take FP64 plans");
+    if (p->mode != b->mode)
+      return set_error(kInvalidArgument, "plans of a stage batch share one precision");
+    if (p->mode == 1 && !p->i8) return set_error(kInvalidArgument, "int8 plan without images");
     if (p->lmax < 0 && p->lmax != kLmaxPerAtom)
       return set_error(kInvalidArgument, "plan without Poisson tables");
     if (p->poisson_tol != plans[0]->poisson_tol)
@@ -262,14 +268,14 @@ int stage_batch_new(const std::vector<FockPlan *> &plans, const std::vector<doub
   NAPMO_TRY_CUDA(b->v.alloc(std::max(b->off.back(), 1)), "alloc batch");
   NAPMO_TRY_CUDA(b->wv.alloc(std::max(b->offp.back(), 1)), "alloc batch");
   bool screened = false;
-  for (FockPlan *p : plans) screened = screened || p->fp64_screen > 0.0;
+  for (FockPlan *p : plans) screened = screened || plan_keep(p) != nullptr;
   if (screened) {
     NAPMO_TRY_CUDA(b->keep.alloc(std::max(b->off.back(), 1)), "alloc batch");
     for (int m = 0; m < nmol; ++m) {
       FockPlan *p = plans[m];
       int *dst = b->keep.p + b->off[m];
-      if (p->fp64_screen > 0.0) {
-        NAPMO_TRY_CUDA(cudaMemcpyAsync(dst, p->keep64.p, (size_t)p->grid->size * sizeof(int),
+      if (const int *k = plan_keep(p)) {
+        NAPMO_TRY_CUDA(cudaMemcpyAsync(dst, k, (size_t)p->grid->size * sizeof(int),
                                        cudaMemcpyDeviceToDevice, s),
                        "batch flags");
       } else {
@@ -319,6 +325,19 @@ int stage_batch_new(const std::vector<FockPlan *> &plans, const std::vector<doub
     wa[m] = WeightBatchArg{p->grid->dev.wb, p->grid->dev.w, b->v.p + b->off[m],
                            b->wv.p + b->offp[m], N, (int)p->ld};
   }
+  if (b->mode == 1) {
+    std::vector<Int8Plan *> ip;
+    std::vector<const double *> cD, cwv;
+    std::vector<double *> rho;
+    for (int m = 0; m < nmol; ++m) {
+      ip.push_back(plans[m]->i8);
+      cD.push_back(D[m]);
+      rho.push_back(b->rho.p + b->off[m]);
+      cwv.push_back(b->wv.p + b->offp[m]);
+    }
+    st = int8_batch_new(ip, cD, rho, cwv, F, s, &b->i8);
+    if (st) return st;
+  }
   NAPMO_TRY_CUDA(b->dargs.upload(da, s), "batch tables");
   NAPMO_TRY_CUDA(b->qargs.upload(qa, s), "batch tables");
   NAPMO_TRY_CUDA(b->wargs.upload(wa, s), "batch tables");
@@ -352,6 +371,15 @@ int stage_batch_build(StageBatch *b, cudaStream_t s) {
   if (b->keep.p)  // screened plans compute only the groups holding a kept point
     NAPMO_TRY_CUDA(cudaMemsetAsync(b->rho.p, 0, (size_t)b->off.back() * sizeof(double), s),
                    "batch rho");
+  if (b->mode == 1) {  // int8 slices on the tensor cores, one batched launch per stage
+    int e = int8_batch_density(b->i8, s);
+    if (e) return e;
+    e = run_poisson(b->cat, b->cat->poisson, b->rho.p, b->v.p, false, s, b->tol, b->keep.p,
+                    b->keep_key);
+    if (e) return e;
+    NAPMO_TRY_CUDA(launch_combine_weights_batch(b->wargs.p, nmol, b->q, s), "weights");
+    return int8_batch_quadrature(b->i8, s);
+  }
   NAPMO_TRY_CUDA(launch_density_batch(b->dargs.p, stage_queue(b, 0), b->grid_d, s), "density");
   int e = run_poisson(b->cat, b->cat->poisson, b->rho.p, b->v.p, false, s, b->tol,
                       b->keep.p, b->keep_key);

@@ -1,5 +1,6 @@
 // Kernel launchers of the napmo_b200 CUDA library (sm_100a).
 #pragma once
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -124,5 +125,13 @@ int int8_quadrature(Int8Plan *p, const double *phi, const double *wv, double *F,
 // synchronising `s`; `reset` clears it.
 int tc_error_status(cudaStream_t s, bool reset);
 int tc_wait_selftest(int *out_dev, cudaStream_t s);
+// int8 build stages of many plans, one batched launch each (see tc.cu).
+struct Int8Batch;
+int int8_batch_new(const std::vector<Int8Plan *> &plans, const std::vector<const double *> &D,
+                   const std::vector<double *> &rho, const std::vector<const double *> &wv,
+                   const std::vector<double *> &F, cudaStream_t s, Int8Batch **out);
+void int8_batch_free(Int8Batch *b);
+int int8_batch_density(Int8Batch *b, cudaStream_t s);
+int int8_batch_quadrature(Int8Batch *b, cudaStream_t s);
 
 }  // namespace napmo

@@ -333,14 +333,16 @@ __device__ __forceinline__ void slice16_5(const double *x, double scale, uint4 *
 // core_off(row % TR, k % KS)] with NS slices (4: Y = rint(x 2^(30-e)); 5:
 // rint(x 2^(38-e))).  Grid (rows_pad / 8, nblk), one warp per row.
 template <int NS>
-__global__ void __launch_bounds__(256)
-slice_rows_kernel(const double *__restrict__ src, long ld, int nrows, int ncols,
-                  const double *__restrict__ m1, const double *__restrict__ m2, int kb, int nblk,
-                  int TR, int nks, int8_t *__restrict__ img, int *__restrict__ eout,
-                  const int *__restrict__ cidx) {
+__device__ __forceinline__ void slice_rows_body(const double *__restrict__ src, long ld,
+                                                int nrows, int ncols,
+                                                const double *__restrict__ m1,
+                                                const double *__restrict__ m2, int kb, int nblk,
+                                                int TR, int nks, int8_t *__restrict__ img,
+                                                int *__restrict__ eout,
+                                                const int *__restrict__ cidx, int bx, int by) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int row = blockIdx.x * 8 + warp;
-  const int b = blockIdx.y;
+  const int row = bx * 8 + warp;
+  const int b = by;
   const long k0 = (long)b * kb;
   const int nchunk = kb / 16;
   const bool vec = ((ld & 1) == 0);
@@ -421,6 +423,16 @@ slice_rows_kernel(const double *__restrict__ src, long ld, int nrows, int ncols,
   }
 }
 
+template <int NS>
+__global__ void __launch_bounds__(256)
+slice_rows_kernel(const double *__restrict__ src, long ld, int nrows, int ncols,
+                  const double *__restrict__ m1, const double *__restrict__ m2, int kb, int nblk,
+                  int TR, int nks, int8_t *__restrict__ img, int *__restrict__ eout,
+                  const int *__restrict__ cidx) {
+  slice_rows_body<NS>(src, ld, nrows, ncols, m1, m2, kb, nblk, TR, nks, img, eout, cidx,
+                      blockIdx.x, blockIdx.y);
+}
+
 // Point-grouped slices of phi^T: rows = points (tiles of 128), K = basis
 // function (stages of 64); exponent per point over all n functions.  One
 // thread per point, grid = padded points / 128.
@@ -480,13 +492,14 @@ __global__ void balance_kernel(int npoint, const double *__restrict__ wb,
 // Per call, block b of QKB points: g(p) = wv(p) isc(p)^2 (so that
 // B = A g = phi wv 2^-c), eg[b] = group exponent of max |g| over the block,
 // gs(p) = g(p) 2^-eg[b] (|gs| < 1; exact scaling).
-__global__ void __launch_bounds__(256)
-gscale_kernel(int npoint, const double *__restrict__ wv, const double *__restrict__ isc,
-              const int *__restrict__ pidx, double *__restrict__ gs, int *__restrict__ eg) {
+__device__ __forceinline__ void gscale_body(int npoint, const double *__restrict__ wv,
+                                            const double *__restrict__ isc,
+                                            const int *__restrict__ pidx,
+                                            double *__restrict__ gs, int *__restrict__ eg, int bx) {
   constexpr int PER = QKB / 256;
   __shared__ double red[8];
   const int t = threadIdx.x;
-  const long p0 = (long)blockIdx.x * QKB + t * PER;
+  const long p0 = (long)bx * QKB + t * PER;
   double g[PER], mx = 0.0;
 #pragma unroll
   for (int i = 0; i < PER; ++i) {
@@ -502,10 +515,16 @@ gscale_kernel(int npoint, const double *__restrict__ wv, const double *__restric
 #pragma unroll
   for (int i = 1; i < 8; ++i) mx = fmax(mx, red[i]);
   const int e = group_exponent(mx);
-  if (t == 0) eg[blockIdx.x] = e;
+  if (t == 0) eg[bx] = e;
   const double s = ldexp(1.0, -e);
 #pragma unroll
   for (int i = 0; i < PER; ++i) gs[p0 + i] = g[i] * s;
+}
+
+__global__ void __launch_bounds__(256)
+gscale_kernel(int npoint, const double *__restrict__ wv, const double *__restrict__ isc,
+              const int *__restrict__ pidx, double *__restrict__ gs, int *__restrict__ eg) {
+  gscale_body(npoint, wv, isc, pidx, gs, eg, blockIdx.x);
 }
 
 // Per call: the B image from the A image.  For each row and block,
@@ -519,15 +538,16 @@ gscale_kernel(int npoint, const double *__restrict__ wv, const double *__restric
 // their Y_A, decoded once from the digits, in registers across both passes
 // (row maxima: lanes c, c ^ 8, c ^ 16, c ^ 24, then the four warps through
 // shared memory; digits of B), so A is read from memory once.
-__global__ void __launch_bounds__(128)
-scale_image_kernel(const int8_t *__restrict__ qa, int8_t *__restrict__ qb,
-                   const double *__restrict__ gs, const int *__restrict__ ea,
-                   const int *__restrict__ eg, int *__restrict__ eb, int nks, int nblk,
-                   int ebld) {
+__device__ __forceinline__ void scale_image_body(const int8_t *__restrict__ qa,
+                                                 int8_t *__restrict__ qb,
+                                                 const double *__restrict__ gs,
+                                                 const int *__restrict__ ea,
+                                                 const int *__restrict__ eg, int *__restrict__ eb,
+                                                 int nks, int nblk, int ebld, int bx, int by) {
   constexpr int SPW = QBLK_STAGES / 4;  // stages per warp
   __shared__ double smax[4][8];
   const int c = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int rg = blockIdx.x, b = blockIdx.y;
+  const int rg = bx, b = by;
   const int t = rg >> 4, r = c & 7, kc = c >> 3;
   const int row = rg * 8 + r;
   const long goff = (long)(rg & 15) * 512 + c * 16;
@@ -575,6 +595,14 @@ scale_image_kernel(const int8_t *__restrict__ qa, int8_t *__restrict__ qb,
     for (int s = 0; s < NSL; ++s)
       *reinterpret_cast<uint4 *>(qb + stage_base(st) + (long)s * TM * KS) = d[s];
   }
+}
+
+__global__ void __launch_bounds__(128)
+scale_image_kernel(const int8_t *__restrict__ qa, int8_t *__restrict__ qb,
+                   const double *__restrict__ gs, const int *__restrict__ ea,
+                   const int *__restrict__ eg, int *__restrict__ eb, int nks, int nblk,
+                   int ebld) {
+  scale_image_body(qa, qb, gs, ea, eg, eb, nks, nblk, ebld, blockIdx.x, blockIdx.y);
 }
 
 // 2 K32 steps of one 64-wide stage: the kept digit products into their
@@ -628,8 +656,7 @@ __device__ __forceinline__ void copy_b96(uint8_t *dst, const int8_t *img, int J,
 }
 
 // CTA = (tile pair (I, J) with some nu >= mu, chunk of point blocks).
-__global__ void __launch_bounds__(NTHR, 1) quad_i8_kernel(QuadArgs g) {
-  extern __shared__ __align__(1024) uint8_t smem[];
+__device__ __forceinline__ void quad_i8_body(const QuadArgs &g, uint8_t *smem, int bx, int by) {
   __shared__ __align__(8) uint64_t full[NSTAGE], empty[NSTAGE], accfull, accempty, done;
   __shared__ uint32_t tmem_sh;
   __shared__ int abort_sh, flag_sh;
@@ -638,7 +665,7 @@ __global__ void __launch_bounds__(NTHR, 1) quad_i8_kernel(QuadArgs g) {
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   volatile int *abort = &abort_sh;
 
-  int I = 0, rem = blockIdx.x;
+  int I = 0, rem = bx;
   for (;;) {
     const int cnt = g.ntj - (4 * I) / 3;
     if (rem < cnt) break;
@@ -646,7 +673,7 @@ __global__ void __launch_bounds__(NTHR, 1) quad_i8_kernel(QuadArgs g) {
     ++I;
   }
   const int J = (4 * I) / 3 + rem;
-  const int b0 = blockIdx.y * g.bpc;
+  const int b0 = by * g.bpc;
   const int nb = max(0, min(b0 + g.bpc, g.nblk) - b0);
 
   if (t == 0) {
@@ -758,7 +785,7 @@ __global__ void __launch_bounds__(NTHR, 1) quad_i8_kernel(QuadArgs g) {
       mbar_arrive(&accempty);
     }
     if (ok) {
-      double *out = g.work + (((long)blockIdx.y * g.npair + blockIdx.x) * TM + row) * QN + col0;
+      double *out = g.work + (((long)by * g.npair + bx) * TM + row) * QN + col0;
 #pragma unroll
       for (int i = 0; i < 48; ++i) out[i] = part[i];
     }
@@ -774,10 +801,16 @@ __global__ void __launch_bounds__(NTHR, 1) quad_i8_kernel(QuadArgs g) {
   }
 }
 
+__global__ void __launch_bounds__(NTHR, 1) quad_i8_kernel(QuadArgs g) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  quad_i8_body(g, smem, blockIdx.x, blockIdx.y);
+}
+
 // F[mu][nu] = F[nu][mu] = sum over chunks (fixed order) of tile (mu/128, nu/96).
-__global__ void quad_i8_reduce_kernel(int n, int nchunk, int npair, int ntj,
-                                      const double *__restrict__ work, double *__restrict__ F) {
-  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void quad_i8_reduce_body(int n, int nchunk, int npair, int ntj,
+                                                    const double *__restrict__ work,
+                                                    double *__restrict__ F, int bx) {
+  const long idx = (long)bx * blockDim.x + threadIdx.x;
   if (idx >= (long)n * n) return;
   const int mu = (int)(idx / n), nu = (int)(idx % n);
   if (mu > nu) return;
@@ -793,6 +826,11 @@ __global__ void quad_i8_reduce_kernel(int n, int nchunk, int npair, int ntj,
   F[(long)nu * n + mu] = s;
 }
 
+__global__ void quad_i8_reduce_kernel(int n, int nchunk, int npair, int ntj,
+                                      const double *__restrict__ work, double *__restrict__ F) {
+  quad_i8_reduce_body(n, nchunk, npair, ntj, work, F, blockIdx.x);
+}
+
 // ---------------------------------------------------------------- density
 // First 64-wide stage of nu that block m (functions 96 m .. 96 m + 95) of the
 // density accumulates: the stage holding function 96 m.
@@ -806,8 +844,9 @@ __host__ __device__ constexpr int dens_first_stage(int m) { return m * DN / KS; 
 //                                         entry is skipped by its block)
 //              = D[mu][nu]                otherwise
 // (for a symmetric D the sum is 2 D[mu][nu], exact).
-__global__ void dsym_kernel(const double *__restrict__ D, int n, double *__restrict__ out) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void dsym_body(const double *__restrict__ D, int n,
+                                          double *__restrict__ out, int bx) {
+  const long i = (long)bx * blockDim.x + threadIdx.x;
   if (i >= (long)n * n) return;
   const int mu = (int)(i / n), nu = (int)(i % n);
   const int cmu = dens_first_stage(mu / DN) * KS, cnu = dens_first_stage(nu / DN) * KS;
@@ -817,6 +856,10 @@ __global__ void dsym_kernel(const double *__restrict__ D, int n, double *__restr
     if (mu < cnu) v += D[(long)nu * n + mu];
   }
   out[i] = v;
+}
+
+__global__ void dsym_kernel(const double *__restrict__ D, int n, double *__restrict__ out) {
+  dsym_body(D, n, out, blockIdx.x);
 }
 
 struct DensArgs {
@@ -834,8 +877,8 @@ struct DensArgs {
 // functions of block m, accumulated in TMEM over nu >= 64 dens_first_stage(m)
 // (D' is zero below, see dsym_kernel); the drain adds phi[mu][p] T[p][mu]
 // into rho[p] (thread = point, 48 functions each).
-__global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
-  extern __shared__ __align__(1024) uint8_t smem[];
+__device__ __forceinline__ void density_i8_body(const DensArgs &g, uint8_t *smem, int bx,
+                                                int gx) {
   __shared__ __align__(8) uint64_t full[NSTAGE], empty[NSTAGE], accfull, accempty, done;
   __shared__ uint32_t tmem_sh;
   __shared__ int abort_sh, flag_sh;
@@ -871,7 +914,7 @@ __global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
     if (lane == 0) {
       int it = 0;
       bool ok = true;
-      for (int pt = blockIdx.x; pt < g.npt && ok; pt += gridDim.x)
+      for (int pt = bx; pt < g.npt && ok; pt += gx)
         for (int m = 0; m < g.nmt && ok; ++m)
           for (int ks = dens_first_stage(m); ks < g.nks; ++ks) {
             const int slot = it % NSTAGE;
@@ -892,7 +935,7 @@ __global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
     if (lane == 0) {
       int it = 0, pass = 0;
       bool ok = true;
-      for (int pt = blockIdx.x; pt < g.npt && ok; pt += gridDim.x)
+      for (int pt = bx; pt < g.npt && ok; pt += gx)
         for (int m = 0; m < g.nmt && ok; ++m, ++pass) {
           if (!wait_phase(&accempty, (pass & 1) ^ 1, abort)) {
             ok = false;
@@ -921,7 +964,7 @@ __global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
     const int h = warp >> 2;
     int pass = 0;
     bool ok = true;
-    for (int pt = blockIdx.x; pt < g.npt && ok; pt += gridDim.x) {
+    for (int pt = bx; pt < g.npt && ok; pt += gx) {
       const long p = (long)pt * TM + row;
       double acc = 0.0;
       for (int m = 0; m < g.nmt; ++m, ++pass) {
@@ -998,6 +1041,11 @@ __global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(kTmemCols));
   }
+}
+
+__global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  density_i8_body(g, smem, blockIdx.x, gridDim.x);
 }
 
 int num_sms() {
@@ -1234,6 +1282,235 @@ int int8_quadrature(Int8Plan *p, const double *phi, const double *wv, double *F,
   const long nn = (long)p->n * p->n;
   quad_i8_reduce_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(p->n, p->nchunk, p->npair,
                                                                      p->ntj, p->work.p, F);
+  NAPMO_TRY_CUDA(cudaGetLastError(), "quad_i8 reduce");
+  return kOk;
+}
+
+// ------------------------------------------------------------- stage batches
+// The int8 build stages of many plans as one launch each: a batched launch
+// runs the sum of the molecules' own grids; CTA b belongs to the molecule m
+// with cta_off[m] <= b < cta_off[m + 1] and runs the kernel's body with its
+// local block index (x = local % gx[m], y = local / gx[m]), so every
+// molecule's arithmetic and launch shape are those of its own plan.  The
+// persistent density keeps each molecule's own CTA count as its tile stride.
+namespace {
+
+struct BatchMap {
+  const int *cta_off;  // [nmol + 1]
+  const int *gx;       // [nmol] x extent of the molecule's own grid
+  int nmol;
+};
+
+__device__ __forceinline__ int map_cta(const BatchMap &m, int *bx, int *by) {
+  const int b = blockIdx.x;
+  int lo = 0, hi = m.nmol - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (m.cta_off[mid] <= b) lo = mid; else hi = mid - 1;
+  }
+  const int local = b - m.cta_off[lo], gx = m.gx[lo];
+  *bx = local % gx;
+  *by = local / gx;
+  return lo;
+}
+
+struct DsymArg { const double *D; double *out; int n; };
+struct SliceArg {
+  const double *src; long ld; int nrows, ncols, kb, nblk, TR, nks;
+  int8_t *img; int *e;
+};
+struct GscaleArg { const double *wv, *isc; const int *pidx; double *gs; int *eg; int npoint; };
+struct ScaleArg {
+  const int8_t *qa; int8_t *qb; const double *gs; const int *ea, *eg; int *eb;
+  int nks, nblk, ebld;
+};
+struct ReduceArg { const double *work; double *F; int n, nchunk, npair, ntj; };
+
+__global__ void dsym_batch_kernel(const DsymArg *__restrict__ a, BatchMap m) {
+  int bx, by;
+  const DsymArg g = a[map_cta(m, &bx, &by)];
+  dsym_body(g.D, g.n, g.out, bx);
+}
+
+__global__ void __launch_bounds__(256) slice_d_batch_kernel(const SliceArg *__restrict__ a,
+                                                            BatchMap m) {
+  int bx, by;
+  const SliceArg g = a[map_cta(m, &bx, &by)];
+  slice_rows_body<NSL_D>(g.src, g.ld, g.nrows, g.ncols, nullptr, nullptr, g.kb, g.nblk, g.TR,
+                         g.nks, g.img, g.e, nullptr, bx, by);
+}
+
+__global__ void __launch_bounds__(NTHR, 1) density_i8_batch_kernel(const DensArgs *__restrict__ a,
+                                                                   BatchMap m) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  int bx, by;
+  const int mol = map_cta(m, &bx, &by);
+  density_i8_body(a[mol], smem, bx, m.gx[mol]);
+}
+
+__global__ void __launch_bounds__(256) gscale_batch_kernel(const GscaleArg *__restrict__ a,
+                                                           BatchMap m) {
+  int bx, by;
+  const GscaleArg g = a[map_cta(m, &bx, &by)];
+  gscale_body(g.npoint, g.wv, g.isc, g.pidx, g.gs, g.eg, bx);
+}
+
+__global__ void __launch_bounds__(128) scale_image_batch_kernel(const ScaleArg *__restrict__ a,
+                                                                BatchMap m) {
+  int bx, by;
+  const ScaleArg g = a[map_cta(m, &bx, &by)];
+  scale_image_body(g.qa, g.qb, g.gs, g.ea, g.eg, g.eb, g.nks, g.nblk, g.ebld, bx, by);
+}
+
+__global__ void __launch_bounds__(NTHR, 1) quad_i8_batch_kernel(const QuadArgs *__restrict__ a,
+                                                                BatchMap m) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  int bx, by;
+  const int mol = map_cta(m, &bx, &by);
+  quad_i8_body(a[mol], smem, bx, by);
+}
+
+__global__ void quad_i8_reduce_batch_kernel(const ReduceArg *__restrict__ a, BatchMap m) {
+  int bx, by;
+  const ReduceArg g = a[map_cta(m, &bx, &by)];
+  quad_i8_reduce_body(g.n, g.nchunk, g.npair, g.ntj, g.work, g.F, bx);
+}
+
+// Per-molecule grids (gx x gy) of one batched launch: prefix CTA offsets and
+// x extents on the device, total CTAs in *total.
+struct LaunchMap {
+  DevBuf<int> off, gx;
+  int total = 0, nmol = 0;
+  int build(const std::vector<int> &gxs, const std::vector<int> &gys, cudaStream_t s) {
+    std::vector<int> o(1, 0);
+    for (size_t i = 0; i < gxs.size(); ++i) o.push_back(o.back() + gxs[i] * gys[i]);
+    total = o.back();
+    nmol = (int)gxs.size();
+    NAPMO_TRY_CUDA(off.upload(o, s), "batch map");
+    NAPMO_TRY_CUDA(gx.upload(gxs, s), "batch map");
+    return kOk;
+  }
+  BatchMap map() const { return BatchMap{off.p, gx.p, nmol}; }
+};
+
+}  // namespace
+
+struct Int8Batch {
+  int nmol = 0;
+  DevBuf<DsymArg> dsym;
+  DevBuf<SliceArg> slice;
+  DevBuf<DensArgs> dens;
+  DevBuf<GscaleArg> gscale;
+  DevBuf<ScaleArg> scale;
+  DevBuf<QuadArgs> quad;
+  DevBuf<ReduceArg> reduce;
+  LaunchMap m_dsym, m_slice, m_dens, m_gscale, m_scale, m_quad, m_reduce;
+};
+
+// Tables of the batched int8 stages: molecule m reads D[m], writes rho[m]
+// (its kept points scattered by the plan's index; the caller zeroes rho
+// first), reads wv[m] (zero padded) and writes F[m].
+int int8_batch_new(const std::vector<Int8Plan *> &plans, const std::vector<const double *> &D,
+                   const std::vector<double *> &rho, const std::vector<const double *> &wv,
+                   const std::vector<double *> &F, cudaStream_t s, Int8Batch **out) {
+  std::unique_ptr<Int8Batch> b(new Int8Batch);
+  const int nmol = (int)plans.size();
+  b->nmol = nmol;
+  std::vector<DsymArg> ds(nmol);
+  std::vector<SliceArg> sl(nmol);
+  std::vector<DensArgs> de(nmol);
+  std::vector<GscaleArg> gs(nmol);
+  std::vector<ScaleArg> sc(nmol);
+  std::vector<QuadArgs> qa(nmol);
+  std::vector<ReduceArg> re(nmol);
+  std::vector<int> gx[7], gy[7];
+  for (int m = 0; m < nmol; ++m) {
+    Int8Plan *p = plans[m];
+    const long nn = (long)p->n * p->n;
+    ds[m] = DsymArg{D[m], p->dsym.p, p->n};
+    gx[0].push_back((int)((nn + 255) / 256));
+    gy[0].push_back(1);
+    sl[m] = SliceArg{p->dsym.p, p->n, p->n, p->n, p->nks_d * KS, 1, DN, p->nks_d, p->dd.p,
+                     p->dd_e.p};
+    gx[1].push_back(p->nmt * DN / 8);
+    gy[1].push_back(1);
+    de[m] = DensArgs{p->da.p, p->da_e.p, p->dd.p, p->dd_e.p, p->nks_d, p->nmt, p->npt,
+                     p->npoint, rho[m], p->screened ? p->idx.p : nullptr};
+    gx[2].push_back(std::max(1, std::min(p->npt, p->budget)));
+    gy[2].push_back(p->npt > 0 ? 1 : 0);
+    gs[m] = GscaleArg{wv[m], p->isc.p, p->screened ? p->idx.p : nullptr, p->gs.p, p->eg.p,
+                      p->npoint};
+    gx[3].push_back(p->nblk);
+    gy[3].push_back(1);
+    sc[m] = ScaleArg{p->qa.p, p->qb.p, p->gs.p, p->qa_e.p, p->eg.p, p->qb_e.p, p->nks_q,
+                     p->nblk, p->nimg * TM};
+    gx[4].push_back((p->n + 7) / 8);
+    gy[4].push_back(p->nblk);
+    qa[m] = QuadArgs{p->qa.p, p->qb.p, p->qa_e.p, p->qb_e.p, p->nblk, p->nks_q, p->nimg * TM,
+                     p->ntj, p->bpc, p->npair, p->work.p};
+    gx[5].push_back(p->npair);
+    gy[5].push_back(p->nchunk);
+    re[m] = ReduceArg{p->work.p, F[m], p->n, p->nchunk, p->npair, p->ntj};
+    gx[6].push_back((int)((nn + 255) / 256));
+    gy[6].push_back(1);
+  }
+  NAPMO_TRY_CUDA(b->dsym.upload(ds, s), "batch tables");
+  NAPMO_TRY_CUDA(b->slice.upload(sl, s), "batch tables");
+  NAPMO_TRY_CUDA(b->dens.upload(de, s), "batch tables");
+  NAPMO_TRY_CUDA(b->gscale.upload(gs, s), "batch tables");
+  NAPMO_TRY_CUDA(b->scale.upload(sc, s), "batch tables");
+  NAPMO_TRY_CUDA(b->quad.upload(qa, s), "batch tables");
+  NAPMO_TRY_CUDA(b->reduce.upload(re, s), "batch tables");
+  LaunchMap *maps[7] = {&b->m_dsym, &b->m_slice, &b->m_dens, &b->m_gscale, &b->m_scale,
+                        &b->m_quad, &b->m_reduce};
+  for (int k = 0; k < 7; ++k) {
+    const int e = maps[k]->build(gx[k], gy[k], s);
+    if (e) return e;
+  }
+  NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "batch tables");
+  *out = b.release();
+  return kOk;
+}
+
+void int8_batch_free(Int8Batch *b) { delete b; }
+
+// D -> D' (folded) -> 5-digit image -> rho of every molecule (rho zeroed by
+// the caller).
+int int8_batch_density(Int8Batch *b, cudaStream_t s) {
+  if (b->m_dsym.total)
+    dsym_batch_kernel<<<b->m_dsym.total, 256, 0, s>>>(b->dsym.p, b->m_dsym.map());
+  NAPMO_TRY_CUDA(cudaGetLastError(), "fold D");
+  if (b->m_slice.total)
+    slice_d_batch_kernel<<<b->m_slice.total, 256, 0, s>>>(b->slice.p, b->m_slice.map());
+  NAPMO_TRY_CUDA(cudaGetLastError(), "slice D");
+  const int smem = NSTAGE * (stage_bytes(TM) + NSL_D * DN * KS);
+  NAPMO_TRY_CUDA(cudaFuncSetAttribute(density_i8_batch_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                 "density_i8 smem");
+  if (b->m_dens.total)
+    density_i8_batch_kernel<<<b->m_dens.total, NTHR, smem, s>>>(b->dens.p, b->m_dens.map());
+  NAPMO_TRY_CUDA(cudaGetLastError(), "density_i8");
+  return kOk;
+}
+
+// wv -> block scales -> B images -> F of every molecule.
+int int8_batch_quadrature(Int8Batch *b, cudaStream_t s) {
+  if (b->m_gscale.total)
+    gscale_batch_kernel<<<b->m_gscale.total, 256, 0, s>>>(b->gscale.p, b->m_gscale.map());
+  NAPMO_TRY_CUDA(cudaGetLastError(), "block scales");
+  if (b->m_scale.total)
+    scale_image_batch_kernel<<<b->m_scale.total, 128, 0, s>>>(b->scale.p, b->m_scale.map());
+  NAPMO_TRY_CUDA(cudaGetLastError(), "wv phi image");
+  const int smem = NSTAGE * (stage_bytes(TM) + stage_bytes(QN));
+  NAPMO_TRY_CUDA(cudaFuncSetAttribute(quad_i8_batch_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                 "quad_i8 smem");
+  if (b->m_quad.total)
+    quad_i8_batch_kernel<<<b->m_quad.total, NTHR, smem, s>>>(b->quad.p, b->m_quad.map());
+  NAPMO_TRY_CUDA(cudaGetLastError(), "quad_i8");
+  if (b->m_reduce.total)
+    quad_i8_reduce_batch_kernel<<<b->m_reduce.total, 256, 0, s>>>(b->reduce.p,
+                                                                  b->m_reduce.map());
   NAPMO_TRY_CUDA(cudaGetLastError(), "quad_i8 reduce");
   return kOk;
 }

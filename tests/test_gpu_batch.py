@@ -164,3 +164,33 @@ def test_stage_batch_queue_wait_runs_out():
     Fs = [F.cpu().numpy() for F in batch.build(Ds)]
     torch.cuda.synchronize()
     assert all(np.array_equal(F, R) for F, R in zip(Fs, ref))
+
+
+def test_stage_batch_int8_equals_single_builds():
+    """'stages' mode with int8 plans: every int8 stage (fold and slices of D,
+    density, block scales, B images, quadrature, reduction) runs as one
+    batched launch over all molecules, around one Poisson plan; each molecule's
+    launch shape is its own plan's, so F equals its own int8 build bit for
+    bit, also after tuning."""
+    import torch
+    import napmo_b200 as nb
+    mols = _molecules(nmol=7, seed=5)
+    builders = [nb.FockBuilder(g, e['basis'], 'per-atom', precision='int8x4') for e, g in mols]
+    Ds = [random_density(b.n, max(1, e['occupation']), seed=200 + i)
+          for i, ((e, g), b) in enumerate(zip(mols, builders))]
+    ref = [b.build(D)[0].cpu().numpy() for b, D in zip(builders, Ds)]
+    batch = nb.FockBatch(builders)
+    batch.set_mode('stages')
+    Fs = [F.cpu().numpy() for F in batch.build(Ds)]
+    torch.cuda.synchronize()
+    assert builders[0].tc_status() == 0
+    for F, R in zip(Fs, ref):
+        assert np.array_equal(F, R)
+    cfg = batch.tune(reps=2)
+    assert cfg['ms'] > 0
+    Fs = [F.cpu().numpy() for F in batch.build(Ds)]
+    torch.cuda.synchronize()
+    # the tuner left its budgets on the plans: their own builds use them too
+    ref = [b.build(D)[0].cpu().numpy() for b, D in zip(builders, Ds)]
+    for F, R in zip(Fs, ref):
+        assert np.abs(F - R).max() <= 1e-12 * np.abs(R).max()

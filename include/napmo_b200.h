@@ -348,6 +348,8 @@ void napmo_fock_plan_free(void *plan);
  * own buffers; rebuilds the int8 images and Poisson tables it holds.  No
  * counterpart in nAPMO (new objects per geometry). */
 int napmo_fock_plan_refresh(void *plan, void *stream);
+/* Sizes and the device phi [n][ld]; evaluates phi again first when
+ * napmo_fock_plan_release_phi freed it (synchronises then). */
 int napmo_fock_plan_info(void *plan, int *n, int *npoint, long *ld, double **phi);
 int napmo_fock_plan_density(void *plan, const double *D, double *rho, void *stream);
 int napmo_fock_plan_quadrature(void *plan, double q, const double *v, const double *vext,
@@ -387,6 +389,12 @@ int napmo_fock_plan_screening(void *plan, const int **keep, int *nkeep);
 int napmo_fock_plan_set_fp64_screening(void *plan, double tol, void *stream);
 /* Device bytes of the plan's int8 operand images and scratch. */
 long napmo_fock_plan_int8_bytes(void *plan);
+/* Precision 1 only: frees the plan's FP64 phi (n x ld doubles), which the
+ * int8 builds do not read; whatever needs it again (an FP64 build,
+ * napmo_fock_plan_info, set_fp64_screening, a switch back to precision 0,
+ * refresh) evaluates it again first.  No counterpart in nAPMO.
+ * Synchronises. */
+int napmo_fock_plan_release_phi(void *plan);
 /* Batched Fock builds of many plans (molecules of uneven size) by one CUDA
  * graph launch; no counterpart in nAPMO (its SCF drivers loop over species,
  * scf.py:146-273).  The batch owns a device D and F per plan

@@ -242,6 +242,7 @@ _SIGS = [
     ('napmo_fock_plan_screening', c_int, [c_void_p, POINTER(c_void_p), POINTER(c_int)]),
     ('napmo_fock_plan_set_fp64_screening', c_int, [c_void_p, c_double, c_void_p]),
     ('napmo_fock_plan_int8_bytes', c_long, [c_void_p]),
+    ('napmo_fock_plan_release_phi', c_int, [c_void_p]),
     ('napmo_fock_batch_new', c_void_p, [c_void_p, c_int, c_double]),
     ('napmo_fock_batch_free', None, [c_void_p]),
     ('napmo_fock_batch_buffers', c_int, [c_void_p, c_int, c_void_p, c_void_p]),

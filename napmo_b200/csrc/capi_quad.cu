@@ -107,9 +107,27 @@ struct FockPlan {
   }
 };
 
+// phi of the plan's basis on its grid, evaluated again when it was released
+// (napmo_fock_plan_release_phi); allocates, so it runs outside captures (the
+// batches' eager warm-up builds reach it first).
+static int ensure_phi(FockPlan *p, cudaStream_t s) {
+  if (p->phi.p) return kOk;
+  const DeviceBasis *db = nullptr;
+  int e = basis_device(p->basis, s, &db);
+  if (e) return e;
+  BeckeGrid *g = p->grid;
+  NAPMO_TRY_CUDA(p->phi.alloc((size_t)p->n * p->ld), "alloc phi");
+  NAPMO_TRY_CUDA(cudaMemsetAsync(p->phi.p, 0, p->phi.n * sizeof(double), s), "phi");
+  NAPMO_TRY_CUDA(launch_basis_values(*db, g->size, g->dev.x, g->dev.y, g->dev.z, p->phi.p,
+                                     p->ld, nullptr, s),
+                 "basis");
+  return kOk;
+}
+
 // rho = density of D, in the plan's precision.
 int plan_density(FockPlan *p, const double *D, double *rho, cudaStream_t s) {
   if (p->mode == 1) return int8_density(p->i8, D, rho, s);
+  if (int e = ensure_phi(p, s)) return e;
   const bool scr = p->fp64_screen > 0.0;
   NAPMO_TRY_CUDA(launch_density_f64(p->n, p->grid->size, p->phi.p, p->ld, D, rho, s,
                                     scr ? p->groups64.p : nullptr, p->ngroups64,
@@ -121,6 +139,7 @@ int plan_density(FockPlan *p, const double *D, double *rho, cudaStream_t s) {
 // F = phi diag(p->wv) phi^T, in the plan's precision.
 int plan_quadrature(FockPlan *p, double *F, cudaStream_t s) {
   if (p->mode == 1) return int8_quadrature(p->i8, p->phi.p, p->wv.p, F, s);
+  if (int e = ensure_phi(p, s)) return e;
   const bool scr = p->fp64_screen > 0.0;
   NAPMO_TRY_CUDA(launch_quadrature_f64(p->n, p->grid->size, p->phi.p, p->ld, p->wv.p, F,
                                        p->work.p, s, nullptr, scr ? p->blocks64.p : nullptr,
@@ -143,6 +162,7 @@ static unsigned long long plan_keep_key(const FockPlan *p) {
 // FP64 screening of the plan's current phi: flags, then the block and group
 // lists (read back once; synchronises).
 static int build_fp64_screening(FockPlan *p, double tol, cudaStream_t s) {
+  if (int e = ensure_phi(p, s)) return e;
   BeckeGrid *g = p->grid;
   const int N = g->size, nb = (N + 15) / 16, ng = (N + 127) / 128;
   DevBuf<int> bf, gf;
@@ -249,6 +269,8 @@ int stage_batch_new(const std::vector<FockPlan *> &plans, const std::vector<doub
   std::vector<int> lmax;
   b->mode = plans[0]->mode;
   for (FockPlan *p : plans) {
+    if (p->mode == 0)
+      if (int e = ensure_phi(p, s)) return e;
     if (p->mode != b->mode)
       return set_error(kInvalidArgument, "plans of a stage batch share one precision");
     if (p->mode == 1 && !p->i8) return set_error(kInvalidArgument, "int8 plan without images");
@@ -605,9 +627,15 @@ int napmo_fock_plan_refresh(FockPlan *p, void *stream) {
     const DeviceBasis *db = nullptr;
     int e = basis_device(p->basis, s, &db);
     if (e) return e;
-    NAPMO_TRY_CUDA(launch_basis_values(*db, g->size, g->dev.x, g->dev.y, g->dev.z, p->phi.p,
-                                       p->ld, nullptr, s),
-                   "basis");
+    const bool released = !p->phi.p;
+    if (released) {
+      e = ensure_phi(p, s);  // evaluates it at the new geometry
+      if (e) return e;
+    } else {
+      NAPMO_TRY_CUDA(launch_basis_values(*db, g->size, g->dev.x, g->dev.y, g->dev.z, p->phi.p,
+                                         p->ld, nullptr, s),
+                     "basis");
+    }
     if (p->lmax >= 0 || p->lmax == kLmaxPerAtom) {
       PoissonPlan *pp = nullptr;
       e = grid_poisson_plan(g, p->lmax, s, &pp);
@@ -628,16 +656,35 @@ int napmo_fock_plan_refresh(FockPlan *p, void *stream) {
       if (e) return e;
       NAPMO_TRY_CUDA(cudaStreamSynchronize(hs), "int8 operand images");
     }
+    if (released && p->mode == 1) p->phi.reset();  // it was released: release it again
+    return kOk;
+  });
+}
+
+// Frees the plan's FP64 phi while it runs in precision 1 (the int8 builds
+// read only their images): n x ld doubles, 7.6 GB at C20H42.  Whatever needs
+// phi again (FP64 builds, napmo_fock_plan_info, screening, a new int8 image)
+// evaluates it again first.  No counterpart in nAPMO.  Synchronises.
+int napmo_fock_plan_release_phi(FockPlan *p) {
+  return guarded([&] {
+    NAPMO_REQUIRE(p->mode == 1 && p->i8, "phi can be released in precision 1 only");
+    NAPMO_TRY_CUDA(cudaDeviceSynchronize(), "sync");
+    p->phi.reset();
+    ++p->generation;
     return kOk;
   });
 }
 
 int napmo_fock_plan_info(FockPlan *p, int *n, int *npoint, long *ld, double **phi) {
-  *n = p->n;
-  *npoint = p->grid->size;
-  *ld = p->ld;
-  *phi = p->phi.p;
-  return kOk;
+  return guarded([&] {
+    *n = p->n;
+    *npoint = p->grid->size;
+    *ld = p->ld;
+    if (int e = ensure_phi(p, host_api_stream())) return e;
+    NAPMO_TRY_CUDA(cudaStreamSynchronize(host_api_stream()), "phi");
+    *phi = p->phi.p;
+    return kOk;
+  });
 }
 
 // rho_dev[p] = density of D_dev on the plan's grid.
@@ -772,20 +819,26 @@ extern "C" {
 // 1 = int8 slices on the tensor cores (four balanced base-256 digits per
 // value against a group exponent, exact int32 accumulation in TMEM).  The
 // Poisson solve stays FP64 in both modes; mode 1 also sets the plan's Poisson
-// truncation tolerance to 1e-10 a.u. (mode 0 to 0, every (l, m) evaluated).
+// truncation tolerance to 1e-9 a.u. (mode 0 to 0, every (l, m) evaluated).
 // Switching to 1 builds phi's operand images (device-synchronous, once per
-// plan).
+// plan); switching to 0 evaluates phi again when it was released.
 int napmo_fock_plan_set_precision(FockPlan *p, int mode) {
   return napmo::guarded([&] {
     NAPMO_REQUIRE(mode == 0 || mode == 1, "precision mode must be 0 (fp64) or 1 (int8x4)");
     if (mode == 1 && !p->i8) {
       NAPMO_TRY_CUDA(cudaDeviceSynchronize(), "sync");
       cudaStream_t s = napmo::host_api_stream();
+      if (int e = napmo::ensure_phi(p, s)) return e;
       BeckeGrid *g = p->grid;
       int e = napmo::int8_plan_create(&p->i8, p->n, g->size, p->phi.p, p->ld, g->dev.wb,
                                       g->dev.w, napmo::kMixedScreenTol, s);
       if (e) return e;
       NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "int8 operand images");
+    }
+    if (mode == 0 && !p->phi.p) {
+      cudaStream_t s = napmo::host_api_stream();
+      if (int e = napmo::ensure_phi(p, s)) return e;
+      NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "phi");
     }
     p->mode = mode;
     p->poisson_tol = mode == 1 ? napmo::kMixedPoissonTol : 0.0;
@@ -796,7 +849,7 @@ int napmo_fock_plan_set_precision(FockPlan *p, int mode) {
 
 // Truncation tolerance (a.u., >= 0) of the plan's Poisson potential
 // evaluation; napmo_fock_plan_set_precision resets it to the mode's default
-// (0 for FP64, which sums every (l, m) as nAPMO does; 1e-10 for int8 slices).
+// (0 for FP64, which sums every (l, m) as nAPMO does; 1e-9 for int8 slices).
 int napmo_fock_plan_set_poisson_tolerance(FockPlan *p, double tol) {
   return napmo::guarded([&] {
     NAPMO_REQUIRE(tol >= 0.0 && tol < 1.0, "Poisson tolerance must be in [0, 1)");

@@ -57,8 +57,9 @@ class FockBuilder(object):
             cext.check()
             raise NapmoError('fock plan construction failed')
         n, npt, ld, phi = c_int(), c_int(), c_long(), c_void_p()
-        cext.lib.napmo_fock_plan_info(self._plan, byref(n), byref(npt), byref(ld), byref(phi))
-        self.n, self.npoint, self.ld, self._phi_ptr = n.value, npt.value, ld.value, phi.value
+        checked(cext.lib.napmo_fock_plan_info(self._plan, byref(n), byref(npt), byref(ld),
+                                              byref(phi)))
+        self.n, self.npoint, self.ld = n.value, npt.value, ld.value
         self.set_precision(precision)
 
     def set_precision(self, precision, poisson_tol=None):
@@ -188,8 +189,20 @@ class FockBuilder(object):
         return F
 
     def phi(self):
-        """phi [n][ld] on the device as a torch view (ld >= npoint, zero padded)."""
-        return _view(self.torch, self._phi_ptr, (self.n, self.ld))
+        """phi [n][ld] on the device as a torch view (ld >= npoint, zero padded);
+        evaluated again first when release_fp64_phi freed it.  The view is valid
+        until the next release_fp64_phi."""
+        n, npt, ld, phi = c_int(), c_int(), c_long(), c_void_p()
+        checked(cext.lib.napmo_fock_plan_info(self._plan, byref(n), byref(npt), byref(ld),
+                                              byref(phi)))
+        return _view(self.torch, phi.value, (self.n, self.ld))
+
+    def release_fp64_phi(self):
+        """'int8x4' only: frees the FP64 phi (n x ld doubles; 7.6 GB for
+        C20H42 / cc-pVDZ on 100x302 points per atom), which the int8 builds do
+        not read.  FP64 builds, phi(), set_fp64_screening and refresh evaluate
+        it again when they need it.  No counterpart in nAPMO."""
+        checked(cext.lib.napmo_fock_plan_release_phi(self._plan))
 
 
 def _view(torch, ptr, shape, typestr='<f8'):

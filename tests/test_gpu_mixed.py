@@ -146,3 +146,41 @@ def test_bounded_wait_times_out_and_reports():
     assert cext.lib.napmo_tc_status(stream, 1) == 0
     x = torch.ones(1024, device='cuda', dtype=torch.float64)
     assert float(x.sum()) == 1024.0
+
+
+def test_release_fp64_phi():
+    """'int8x4' plans may free their FP64 phi: the int8 builds give the same
+    bits without it, the device gets its n x ld doubles back, and whatever
+    needs phi again (phi(), a switch back to FP64) evaluates it to the same
+    bits."""
+    import torch
+    import napmo_b200 as nb
+    ms, grid = product_system(BUTANE, nrad=40, nang=110)
+    basis = ms['e-']['basis']
+    D = random_density(basis['nbasis'], 17)
+    tc = nb.FockBuilder(grid, basis, 8, precision='int8x4')
+    phi0 = tc.phi().cpu().numpy().copy()
+    tc.set_precision('fp64')
+    F64, rho64, _ = tc.build(D)
+    F64, rho64 = F64.cpu().numpy(), rho64.cpu().numpy()
+    tc.set_precision('int8x4')
+    F8, rho8, _ = tc.build(D)
+    F8, rho8 = F8.cpu().numpy(), rho8.cpu().numpy()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    tc.release_fp64_phi()
+    freed = torch.cuda.mem_get_info()[0] - free0
+    assert freed >= 0.9 * tc.n * tc.ld * 8
+    G8, s8, _ = tc.build(D)
+    assert tc.tc_status() == 0
+    assert np.array_equal(G8.cpu().numpy(), F8)
+    assert np.array_equal(s8.cpu().numpy(), rho8)
+    tc.release_fp64_phi()                      # twice is harmless
+    assert np.array_equal(tc.phi().cpu().numpy(), phi0)
+    tc.release_fp64_phi()
+    tc.set_precision('fp64')
+    G64, s64, _ = tc.build(D)
+    assert np.array_equal(G64.cpu().numpy(), F64)
+    assert np.array_equal(s64.cpu().numpy(), rho64)
+    with pytest.raises(nb.cext.NapmoError):
+        tc.release_fp64_phi()                  # FP64 builds read phi

@@ -44,6 +44,7 @@ struct PoissonPlan {
   DevBuf<int> mol_atom_off, mol_point_off, sys_atom, sys_l;
   DevBuf<double> rad, ytab, proj, spl, amp, raw_y, raw_dt, lu, lmul;
   DevBuf<int> lpiv;
+  DevBuf<double> rscr;  // radial-solve scratch of one solve
   DevBuf<int> pairs;
   DevBuf<EvalItem> items;
   int nitems = 0, nitems_in = 0;  // items, of which the first nitems_in are interior
@@ -100,7 +101,7 @@ int build_poisson_plan(const std::vector<const AtomLayout *> &atoms,
   std::vector<double> rad, ytab;
   std::map<std::pair<int, int>, int> ykey;  // (atom-rule id via nang,lmax) -> offset
   std::vector<int> sys_atom, sys_l;
-  long proj = 0, spl = 0, amp = 0, raw = 0, pairs = 0;
+  long proj = 0, spl = 0, amp = 0, raw = 0, pairs = 0, scr = 0;
   int buckets = 0;
   std::vector<int> atom_mol(natom, 0);
   for (int m = 0; m + 1 < (int)mol_atom_off.size(); ++m)
@@ -161,6 +162,9 @@ int build_poisson_plan(const std::vector<const AtomLayout *> &atoms,
     amp += (long)lsize * 2;
     A.raw_off = (int)raw;
     raw += (long)lsize * n;
+    A.scr_off = scr;
+    scr += 3L * n * lsize;
+    A.sys_off = (int)sys_atom.size();
     const int mol = atom_mol[a];
     A.mol_point_start = mol_point_off[mol];
     A.mol_npoint = mol_point_off[mol + 1] - mol_point_off[mol];
@@ -190,6 +194,7 @@ int build_poisson_plan(const std::vector<const AtomLayout *> &atoms,
   NAPMO_TRY_CUDA(plan->amp.alloc(amp), "alloc");
   NAPMO_TRY_CUDA(plan->raw_y.alloc(raw), "alloc");
   NAPMO_TRY_CUDA(plan->raw_dt.alloc(raw), "alloc");
+  NAPMO_TRY_CUDA(plan->rscr.alloc(scr), "alloc");
   d.atoms = plan->atoms.p;
   d.mol_atom_off = plan->mol_atom_off.p;
   d.mol_point_off = plan->mol_point_off.p;
@@ -202,6 +207,7 @@ int build_poisson_plan(const std::vector<const AtomLayout *> &atoms,
   d.amp = plan->amp.p;
   d.raw_y = plan->raw_y.p;
   d.raw_dt = plan->raw_dt.p;
+  d.rscr = plan->rscr.p;
   d.npair = pairs;
   // LU factors of the radial systems (they depend on the grid only)
   d.lu_stride = 2 * d.max_nrad;
@@ -495,12 +501,12 @@ int run_poisson_many(BeckeGrid *g, PoissonPlan *p, int k, const double *rho_dev,
   int st = select_pair_lists(p, g, keep, key, s);
   if (st) return st;
   const PoissonDev &d = p->d;
-  const size_t nd = p->proj.n + p->spl.n + p->amp.n + p->pair_v.n;
+  const size_t nd = p->proj.n + p->spl.n + p->amp.n + p->pair_v.n + p->rscr.n;
   const size_t per = nd * sizeof(double) + p->lcut.n * sizeof(int);
   // grid limits: the projection and truncation launches use natom x B blocks
-  // in y/z, the radial one (column chunks, at most 2 lmax + 1) x B
+  // in y/z, the radial one B in y
   long B = std::min<long>(k, (long)((512ull << 20) / std::max<size_t>(per, 1)));
-  B = std::min<long>(B, 65535 / std::max(d.natom, 2 * d.max_lmax + 1));
+  B = std::min<long>(B, 65535 / std::max(d.natom, 1));
   if (B < 2 || !d.items) {
     for (int j = 0; j < k; ++j) {
       st = run_poisson(g, p, rho_dev + (long)j * ld, v_dev + (long)j * ld, false, s, tol, keep,
@@ -520,12 +526,14 @@ int run_poisson_many(BeckeGrid *g, PoissonPlan *p, int k, const double *rho_dev,
   P.amp_stride = (long)p->amp.n;
   P.pairv_stride = (long)p->pair_v.n;
   P.lcut_stride = (long)p->lcut.n;
+  P.rscr_stride = (long)p->rscr.n;
   double *ws = (double *)p->batch_ws.p;
   P.proj = ws;
   P.spl = P.proj + P.proj_stride * B;
   P.amp = P.spl + P.spl_stride * B;
   P.pair_v = P.amp + P.amp_stride * B;
-  P.lcut = tol > 0.0 ? (int *)(P.pair_v + P.pairv_stride * B) : nullptr;
+  P.rscr = P.pair_v + P.pairv_stride * B;
+  P.lcut = tol > 0.0 ? (int *)(P.rscr + P.rscr_stride * B) : nullptr;
   P.eval_tol = tol;
   P.raw_y = nullptr;
   P.raw_dt = nullptr;

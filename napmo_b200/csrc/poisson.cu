@@ -17,6 +17,7 @@
 //    extrapolation has a tail, so no cutoff applies; reference:
 //    eval_decomposition_grid, src/horton/evaluate.cpp:129-220).  Templated on
 //    lmax so the solid-harmonic recursion lives in registers.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -343,192 +344,337 @@ __global__ void radial_factor_kernel(PoissonDev P, RadialOp op) {
   for (int e = tid; e < n2 * kW; e += nt) lu[e] = band[e];
 }
 
-// CTA = (system (atom, l), chunk of ncol of its 2l + 1 columns m); the columns
-// are independent once the atom's radial tables are staged.  Column loops run
-// one thread per column; row loops stride over the whole block.
-// Doubles of the region after R in the radial kernel's shared memory: the
-// spline derivatives and projected columns (n ncol each), later the system's
-// LU factors (band, multipliers, pivots as ints).
-__host__ __device__ __forceinline__ int radial_region_doubles(int n, int ncol) {
-  const int cols = 2 * n * ncol, lu = 2 * n * (kW + kKL) + n;
-  return cols > lu ? cols : lu;
+// Radial solve.  CTA = (system (atom, l), group of solves of the batch);
+// thread = one column (solve, m), lm = l^2 + m.  A column is a chain of
+// dependent steps: the Thomas sweep of the spline through f_lm (with the
+// boundary moments), the forward elimination of the FEM right-hand side with
+// the system's LU factors, and the back substitution, whose values leave as
+// spline tables.  Each step of a chain is one FMA on the chained value
+// (divisions become products with reciprocals tabulated when the CTA stages
+// its tables; the back substitution uses U's rows scaled by 1/U_ii).  Each
+// sweep keeps its live rows in registers (a window of 4 rows forward, 6 back)
+// and hands its results to the next through the column's scratch in global
+// memory, laid out [slot][lm] per (solve, atom) so that a warp's accesses are
+// contiguous (slots [0, n): t-derivatives, [n, 3n): eliminated rows).  A sweep
+// reads its global inputs through a per-thread ring in shared memory filled by
+// cp.async kRing - 2 steps ahead (L2 latency would otherwise stall each step,
+// and a register ring needs unrolled code); a slot is refilled two steps after
+// it was read.  The right-hand side of a row is
+// assembled as the forward sweep reaches it, from the three nodes around it.
+// Shared memory also holds the system's factors, the atom's radial tables and
+// the Hermite overlaps of every row with the 6 functions of its nodes q - 1 ..
+// q + 1 (q = row / 2; 0 where a node does not exist).  The arithmetic is that
+// of poisson_solver.py:42-118 and ode2.py (spline, FEM assembly, banded LU
+// solve with partial pivoting), up to rounding.
+constexpr int kRadialThreads = 128;
+constexpr int kRing = 32;  // doubles per thread: one ring of 32 or two of 16
+
+__host__ __device__ __forceinline__ size_t radial_smem_bytes(int n, int threads) {
+  const size_t n2 = 2 * (size_t)n;
+  return (n2 * (6 + kKL + 6 + 1) + 7 * (size_t)n + (size_t)kRing * threads) * sizeof(double) +
+         n2 * sizeof(int);
 }
 
-__global__ void radial_kernel(PoissonDev P, int ncol, RadialOp op) {
+// solves per CTA of `threads` threads for a system with 2l + 1 columns
+__host__ __device__ __forceinline__ int radial_solves_per_cta(int l, int threads) {
+  const int s = threads / (2 * l + 1);
+  return s > 0 ? s : 1;
+}
+
+__device__ __forceinline__ void ring_copy(double *dst, const double *src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src),
+               "r"(valid ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void ring_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void ring_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+__global__ void __launch_bounds__(kRadialThreads) radial_kernel(PoissonDev P, RadialOp op) {
   extern __shared__ double sm[];
   const int sys = blockIdx.x;
   const PoissonAtom at = P.atoms[P.sys_atom[sys]];
   const int l = P.sys_l[sys];
+  const int ncol = 2 * l + 1, spc = radial_solves_per_cta(l, blockDim.x);
+  const int bat0 = blockIdx.y * spc;
+  if (bat0 >= P.nbatch) return;  // the whole CTA
   const int n = at.nrad, n2 = 2 * n;
   const int lsize = (at.lmax + 1) * (at.lmax + 1);
-  const int nchunk = gridDim.y / P.nbatch;
-  const int bat = blockIdx.y / nchunk;  // solve of a batch
-  const int c0 = (blockIdx.y - bat * nchunk) * ncol;  // first column (m index) of this chunk
-  double *const spl = P.spl + bat * P.spl_stride;
-  double *const amp = P.amp + bat * P.amp_stride;
-  if (c0 >= 2 * l + 1) return;
-  const int nm = min(ncol, 2 * l + 1 - c0);  // columns of this chunk
-  const int tid = threadIdx.x, nt = blockDim.x;
-  double *R = sm;                    // n2 * ncol  (row-major, column = m)
-  double *buf = R + n2 * ncol;       // n * ncol   (spline t-derivatives)
-  double *Y = buf + n * ncol;        // n * ncol   (projected density of this l)
-  double *r = buf + radial_region_doubles(n, ncol);  // radial tables of the atom, n each
-  double *wr = r + n, *j1 = wr + n, *j2 = j1 + n, *den = j2 + n, *upm = den + n;
-  double *rl = upm + n, *rm = rl + n;  // r^l, r^-(l+1)
-  double *bc = rm + n;                 // [2][ncol]: vmin, vmax per column
-  const double *band = P.lu + (long)sys * P.lu_stride * kW;
-  const double *mult = P.lmul + (long)sys * P.lu_stride * kKL;
-  const int *piv = P.lpiv + (long)sys * P.lu_stride;
   const long xmax = n - 1;
-
-  // -- 0. stage the atom's radial tables and this l's projected density
+  const int tid = threadIdx.x, nt = blockDim.x;
+  double *ub = sm;                // [n2][6]: U_i,i+1..i+6 / U_ii
+  double *rU = ub + 6 * n2;       // [n2]: 1 / U_ii
+  double *mult = rU + n2;         // [n2][kKL]
+  double *ovr = mult + n2 * kKL;  // [n2][6]
+  double *j1 = ovr + 6 * n2, *j2 = j1 + n, *rj1 = j2 + n, *rden = rj1 + n, *upm = rden + n,
+         *rlw = upm + n, *rmw = rlw + n;
+  double *ring = rmw + n;  // [kRing][nt]
+  int *piv = reinterpret_cast<int *>(ring + kRing * nt);
   {
+    const double *gb = P.lu + (long)sys * P.lu_stride * kW;
+    const double *gm = P.lmul + (long)sys * P.lu_stride * kKL;
+    const int *gp = P.lpiv + (long)sys * P.lu_stride;
+    // band storage: AB(i, j) = gb[j kW + kKL + kKU + i - j]
+    for (int i = tid; i < n2; i += nt) {
+      const double d = 1.0 / gb[i * kW + kKL + kKU];
+      rU[i] = d;
+      for (int t = 1; t <= kKL + kKU; ++t)
+        ub[6 * i + t - 1] = i + t < n2 ? gb[(i + t) * kW + kKL + kKU - t] * d : 0.0;
+      piv[i] = gp[i];
+    }
+    for (int e = tid; e < n2 * kKL; e += nt) mult[e] = gm[e];
     const double *rad = P.rad + at.rad_off;
     for (int i = tid; i < n; i += nt) {
-      r[i] = rad[kRadR * n + i];
-      wr[i] = rad[kRadW * n + i];
+      const double r = rad[kRadR * n + i], w = rad[kRadW * n + i];
       j1[i] = rad[kRadJ1 * n + i];
       j2[i] = rad[kRadJ2 * n + i];
-      den[i] = rad[kRadDen * n + i];
+      rj1[i] = 1.0 / j1[i];
+      rden[i] = 1.0 / rad[kRadDen * n + i];
       upm[i] = rad[kRadUp * n + i];
-      rl[i] = pow(r[i], (double)l);
-      rm[i] = pow(r[i], (double)(-l - 1));
+      rlw[i] = pow(r, (double)l) * w;
+      rmw[i] = pow(r, (double)(-l - 1)) * w;
     }
-    const double *proj = P.proj + bat * P.proj_stride + at.proj_off + l * l + c0;
-    for (int e = tid; e < n * nm; e += nt) {
-      const int i = e / nm, c = e - i * nm;
-      Y[i * ncol + c] = proj[(long)i * lsize + c];
+    for (int e = tid; e < 6 * n2; e += nt) {
+      const int row = e / 6, t = e - 6 * row;
+      const long k = 2 * (long)(row / 2 - 1) + t;
+      long lo = 2 * (row / 2 - 1), hi = 2 * (row / 2 + 2);
+      if (lo < 0) lo = 0;
+      if (hi > n2) hi = n2;
+      ovr[e] = (k >= lo && k < hi) ? ov2_d(xmax, row, 0, k, 0) : 0.0;
     }
   }
   __syncthreads();
-  // -- 1. per m: spline t-derivatives of f_lm and boundary values
-  for (int c = tid; c < nm; c += nt) {
-    const double *y = Y + c;  // stride ncol
-    // Thomas elimination for 2/1, 1/4/1, ..., 1/2 with rhs 3 (y_{i+1}-y_{i-1})
-    double prev = (3.0 * (y[ncol] - y[0])) / den[0];
-    buf[c] = prev;
+  const int sidx = tid / ncol, m = tid - sidx * ncol;
+  const long bat = bat0 + sidx;
+  if (sidx >= spc || bat >= P.nbatch) return;  // no barrier below
+  const int lm = l * l + m;
+  const int ls = lsize;
+  const double *Y = P.proj + bat * P.proj_stride + at.proj_off + lm;  // f_lm(r_i) at Y[i ls]
+  double *S = P.rscr + bat * P.rscr_stride + at.scr_off + lm;        // slot s at S[s ls]
+  double *E = S + n * ls;                                             // eliminated rows
+  double *q = ring + tid;  // this thread's ring: slot s at q[s nt]
+  constexpr int R1 = kRing, R2 = kRing / 2;  // ring lengths; lookahead R - 2
+  auto back2 = [](int slot, int R) { return slot >= 2 ? slot - 2 : slot + R - 2; };
+  double *qa = q, *qb = q + R2 * nt;  // two rings of R2 for the forward elimination
+
+  // -- 1. spline t-derivatives of f_lm (Thomas elimination of 2/1, 1/4/1,
+  // ..., 1/2 with rhs 3 (y_{i+1} - y_{i-1})) and the radial moments of the
+  // Dirichlet values.  Step i (1 <= i < n) reads y_{i+1} from ring slot i % R1.
+  const bool moments = !op.zero_bc;
+  double smax = 0.0, smin = 0.0, prev;
+  {
+    for (int s = 1; s < R1 - 1; ++s) {
+      ring_copy(q + s * nt, Y + (s + 1 < n ? s + 1 : 0) * ls, s + 1 < n);
+      ring_commit();
+    }
+    double ym = Y[0], yc = Y[ls];
+    prev = (3.0 * (yc - ym)) * rden[0];
+    S[0] = prev;
+    if (moments) {
+      smax = ym * rlw[0];
+      smin = ym * rmw[0];
+    }
+    int slot = 1;
     for (int i = 1; i < n; ++i) {
-      const double rhs = (i < n - 1) ? 3.0 * (y[(i + 1) * ncol] - y[(i - 1) * ncol])
-                                     : 3.0 * (y[(n - 1) * ncol] - y[(n - 2) * ncol]);
-      prev = (rhs - prev * 1.0) / den[i];
-      buf[i * ncol + c] = prev;
-    }
-    for (int i = n - 2; i >= 0; --i)
-      buf[i * ncol + c] = buf[i * ncol + c] - upm[i] * buf[(i + 1) * ncol + c];
-    // boundary values (Dirichlet) from radial moments
-    if (op.zero_bc) {
-      bc[ncol + c] = 0.0;
-      bc[c] = 0.0;
-      continue;
-    }
-    double smax = 0.0, smin = 0.0;
-    for (int i = 0; i < n; ++i) {
-      const double yi = y[i * ncol];
-      smax += yi * rl[i] * wr[i];
-      smin += yi * rm[i] * wr[i];
-    }
-    bc[ncol + c] = smax * (1.0 / pow(r[n - 1], (double)(l + 1)) / (2 * l + 1));
-    bc[c] = smin * (pow(r[0], (double)l) / (2 * l + 1));
-  }
-  __syncthreads();
-  // -- 1b. FEM right-hand side from the transformed source f = -4 pi rho, one
-  // row per thread
-  for (int row = tid; row < n2; row += nt) {
-    long lo = 2 * (row / 2 - 1), hi = 2 * (row / 2 + 2);
-    if (lo < 0) lo = 0;
-    if (hi > n2) hi = n2;
-    double ov[6];  // the row's Hermite overlaps, shared by all columns
-#pragma unroll
-    for (int t = 0; t < 6; ++t) ov[t] = lo + t < hi ? ov2_d(xmax, row, 0, lo + t, 0) : 0.0;
-    for (int c = 0; c < nm; ++c) {
-      double acc = 0.0;
-      if (row == 0) {
-        acc = bc[c];
-      } else if (row == n2 - 2) {
-        acc = bc[ncol + c];
-      } else {
-#pragma unroll
-        for (int t = 0; t < 6; ++t) {
-          const long k = lo + t;
-          if (k >= hi) break;
-          const int i = (int)(k / 2);
-          const double fy = op.fscale * Y[i * ncol + c];
-          const double jsq = j1[i] * j1[i];
-          double fk;
-          if ((k & 1) == 0) {
-            fk = fy * jsq;
-          } else {
-            const double fdx = op.fscale * (buf[i * ncol + c] / j1[i]);
-            fk = (fdx * jsq + 2 * fy * j2[i]) * j1[i];
-          }
-          if (fk != 0) acc += fk * ov[t];
-        }
+      const int j = i + R1 - 1;  // y index the refill brings, for step i + R1 - 2
+      ring_copy(q + back2(slot, R1) * nt, Y + (j < n ? j : 0) * ls, j < n);
+      ring_commit();
+      ring_wait<R1 - 2>();
+      const double yn = q[slot * nt];
+      slot = slot + 1 == R1 ? 0 : slot + 1;
+      const double rhs = (i < n - 1) ? 3.0 * (yn - ym) : 3.0 * (yc - ym);
+      prev = fma(-prev, rden[i], rhs * rden[i]);
+      S[i * ls] = prev;
+      if (moments) {
+        smax = fma(yc, rlw[i], smax);
+        smin = fma(yc, rmw[i], smin);
       }
-      R[row * ncol + c] = acc;
+      ym = yc;
+      yc = yn;
     }
+    ring_wait<0>();
   }
-  __syncthreads();
-  // -- 1c. the system's LU factors into shared memory, over buf and Y (no
-  // longer needed): the substitutions below are chains of dependent steps
-  double *sband = buf;                 // [n2][kW]
-  double *smult = sband + n2 * kW;     // [n2][kKL]
-  int *spiv = reinterpret_cast<int *>(smult + n2 * kKL);
-  for (int e = tid; e < n2 * kW; e += nt) sband[e] = band[e];
-  for (int e = tid; e < n2 * kKL; e += nt) smult[e] = mult[e];
-  for (int e = tid; e < n2; e += nt) spiv[e] = piv[e];
-  __syncthreads();
-  // -- 2. forward elimination with the stored factors, one column (m) per
-  // thread (the same operations, in the same order, as during the factoring)
-  for (int c = tid; c < nm; c += nt) {
-    for (int k = 0; k < n2; ++k) {
-      const int p = spiv[k];
-      if (p != k) {
-        const double t = R[k * ncol + c];
-        R[k * ncol + c] = R[p * ncol + c];
-        R[p * ncol + c] = t;
-      }
-      const int im = min(k + kKL, n2 - 1);
-      const double rk = R[k * ncol + c];
-      for (int i = k + 1; i <= im; ++i) R[i * ncol + c] -= smult[k * kKL + (i - k - 1)] * rk;
+  __threadfence_block();  // the stores above before the ring's reads below
+  {
+    // step t reads prev_i, i = n - 2 - t, from slot t % R1
+    for (int t = 0; t < R1 - 2; ++t) {
+      const int i = n - 2 - t;
+      ring_copy(q + t * nt, S + (i >= 0 ? i : 0) * ls, i >= 0);
+      ring_commit();
     }
-  }
-  // -- 3. back substitution, one column (m) per thread
-  for (int c = tid; c < nm; c += nt) {
-    for (int i = n2 - 1; i >= 0; --i) {
-      double x = R[i * ncol + c];
-      const int je = min(i + kKL + kKU, n2 - 1);
-      for (int j = i + 1; j <= je; ++j) x -= AB(sband, i, j) * R[j * ncol + c];
-      R[i * ncol + c] = x / AB(sband, i, i);
+    double dn = prev;  // dt[n - 1]
+    int slot = 0;
+    for (int t = 0; t < n - 1; ++t) {
+      const int i = n - 2 - t, j = i - (R1 - 2);  // the refill is for step t + R1 - 2
+      ring_copy(q + back2(slot, R1) * nt, S + (j >= 0 ? j : 0) * ls, j >= 0);
+      ring_commit();
+      ring_wait<R1 - 2>();
+      const double pn = q[slot * nt];
+      slot = slot + 1 == R1 ? 0 : slot + 1;
+      dn = fma(-upm[i], dn, pn);
+      S[i * ls] = dn;
     }
+    ring_wait<0>();
   }
-  __syncthreads();
-  // -- 4. output: raw splines, scaled cubic coefficients, extrapolation
+  double bcmin = 0.0, bcmax = 0.0;
+  if (moments) {
+    const double *rad = P.rad + at.rad_off;
+    bcmax = smax / (pow(rad[kRadR * n + n - 1], (double)(l + 1)) * (2 * l + 1));
+    bcmin = smin * (pow(rad[kRadR * n], (double)l) / (2 * l + 1));
+  }
+  __threadfence_block();
+
+  // -- 2. FEM right-hand side (source f = fscale f_lm) row by row, eliminated
+  // with the factors as it is assembled.  Node i contributes fe = fy j1^2 to
+  // the sums of even rows and fo = (fdx j1^2 + 2 fy j2) j1 to odd ones
+  // (fy = fscale f_lm(r_i), fdx = fscale dt_i / j1_i).
+  const double fs = op.fscale;
+  auto node_f = [&](int i, double y, double dt, double &fe, double &fo) {
+    if (i >= n) {
+      fe = fo = 0.0;
+      return;
+    }
+    const double fy = fs * y;
+    const double jsq = j1[i] * j1[i];
+    fe = fy * jsq;
+    fo = fma(fs * (dt * rj1[i]), jsq, 2 * fy * j2[i]) * j1[i];
+  };
+  // nodes q - 1, q, q + 1 of the rows 2q, 2q + 1 being assembled
+  double ae = 0.0, ao = 0.0, be, bo, ce, co;
+  auto rhs_row = [&](int row) -> double {
+    if (row == 0) return bcmin;
+    if (row == n2 - 2) return bcmax;
+    if (row >= n2) return 0.0;
+    const double *o = ovr + 6 * row;
+    double acc = ae * o[0];
+    acc = fma(ao, o[1], acc);
+    acc = fma(be, o[2], acc);
+    acc = fma(bo, o[3], acc);
+    acc = fma(ce, o[4], acc);
+    return fma(co, o[5], acc);
+  };
+  node_f(0, Y[0], S[0], be, bo);
+  node_f(1, Y[ls], S[ls], ce, co);
+  double w0 = rhs_row(0), w1 = rhs_row(1), w2, w3;  // rows k .. k + 3
+  ae = be;
+  ao = bo;
+  be = ce;
+  bo = co;
+  node_f(2, n > 2 ? Y[2 * ls] : 0.0, n > 2 ? S[2 * ls] : 0.0, ce, co);
+  w2 = rhs_row(2);
+  w3 = rhs_row(3);
+  auto step = [&](int k) {
+    const int d = piv[k] - k;
+    const double m0 = mult[k * kKL], m1 = mult[k * kKL + 1], m2 = mult[k * kKL + 2];
+    const double t0 = w0;
+    w0 = d == 1 ? w1 : (d == 2 ? w2 : (d == 3 ? w3 : w0));
+    w1 = d == 1 ? t0 : w1;
+    w2 = d == 2 ? t0 : w2;
+    w3 = d == 3 ? t0 : w3;
+    const double rk = w0;
+    w1 = fma(-m0, rk, w1);
+    w2 = fma(-m1, rk, w2);
+    w3 = fma(-m2, rk, w3);
+    E[k * ls] = rk;
+    w0 = w1;
+    w1 = w2;
+    w2 = w3;
+  };
+  {
+    // iteration it brings in node it + 3: (f_lm, dt) from slot it % R2 of
+    // the two rings
+    for (int s = 0; s < R2 - 2; ++s) {
+      const int i = s + 3;
+      ring_copy(qa + s * nt, Y + (i < n ? i : 0) * ls, i < n);
+      ring_copy(qb + s * nt, S + (i < n ? i : 0) * ls, i < n);
+      ring_commit();
+    }
+    int slot = 0;
+    for (int it = 0; it < n; ++it) {
+      const int k = 2 * it, i = it + 3 + (R2 - 2);  // node of the refill
+      const int rs = back2(slot, R2);
+      ring_copy(qa + rs * nt, Y + (i < n ? i : 0) * ls, i < n);
+      ring_copy(qb + rs * nt, S + (i < n ? i : 0) * ls, i < n);
+      ring_commit();
+      step(k);
+      ring_wait<R2 - 2>();
+      const double yv = qa[slot * nt], dv = qb[slot * nt];
+      slot = slot + 1 == R2 ? 0 : slot + 1;
+      ae = be;
+      ao = bo;
+      be = ce;
+      bo = co;
+      node_f(it + 3, yv, dv, ce, co);
+      w3 = rhs_row(k + 4);
+      step(k + 1);
+      w3 = rhs_row(k + 5);
+    }
+    ring_wait<0>();
+  }
+  __threadfence_block();
+
+  // -- 3. back substitution, x_i = E_i / U_ii - sum_j (U_ij / U_ii) x_j;
+  // node j's values (rows 2j, 2j + 1) leave as the cubic of interval j (scaled
+  // by sqrt(2l+1)/sqrt(4 pi)), raw (y, dy/dt) and the extrapolation amplitudes.
+  // Step t handles row i = n2 - 1 - t, E_i from slot t % R1.
   const double fl = sqrt((double)(2 * l + 1)) * kInvSqrt4Pi;
-  if (P.raw_y) {
-    for (int e = tid; e < n * nm; e += nt) {
-      const int c = e / n, i = e - c * n;
-      const long o = at.raw_off + (long)(l * l + c0 + c) * n + i;
-      P.raw_y[o] = R[(2 * i) * ncol + c];
-      P.raw_dt[o] = (R[(2 * i + 1) * ncol + c] / j1[i]) * j1[i];
+  double *spl = P.spl + bat * P.spl_stride + at.spl_off + (long)lm * 4;
+  double *amp = P.amp + bat * P.amp_stride + at.amp_off + lm * 2;
+  double x1 = 0.0, x2 = 0.0, x3 = 0.0, x4 = 0.0, x5 = 0.0, x6 = 0.0;  // rows i + 1 .. i + 6
+  double dnext = 0.0;  // dy/dt of node j + 1
+  for (int t = 0; t < R1 - 2; ++t) {
+    const int i = n2 - 1 - t;
+    ring_copy(q + t * nt, E + (i >= 0 ? i : 0) * ls, i >= 0);
+    ring_commit();
+  }
+  int slot = 0;
+  for (int i = n2 - 1; i >= 0; --i) {
+    const int j = i - (R1 - 2);
+    ring_copy(q + back2(slot, R1) * nt, E + (j >= 0 ? j : 0) * ls, j >= 0);
+    ring_commit();
+    ring_wait<R1 - 2>();
+    const double ei = q[slot * nt];
+    slot = slot + 1 == R1 ? 0 : slot + 1;
+    const double *ui = ub + 6 * i;  // zero beyond the last row
+    double x = ei * rU[i];
+    x = fma(-ui[5], x6, x);
+    x = fma(-ui[4], x5, x);
+    x = fma(-ui[3], x4, x);
+    x = fma(-ui[2], x3, x);
+    x = fma(-ui[1], x2, x);
+    x = fma(-ui[0], x1, x);
+    if ((i & 1) == 0) {
+      const int jn = i / 2;
+      const double d0 = (x1 * rj1[jn]) * j1[jn];
+      if (P.raw_y) {
+        const long o = at.raw_off + (long)lm * n + jn;
+        P.raw_y[o] = x;
+        P.raw_dt[o] = d0;
+      }
+      if (jn < n - 1) {
+        const double z = x2 - x;
+        double *cf = spl + (long)jn * lsize * 4;
+        cf[0] = x * fl;
+        cf[1] = d0 * fl;
+        cf[2] = (3 * z - 2 * d0 - dnext) * fl;
+        cf[3] = (-2 * z + d0 + dnext) * fl;
+      } else {
+        amp[1] = x * pow(at.last_x, (double)(l + 1)) * fl;
+      }
+      if (i == 0) amp[0] = x / pow(at.first_x, (double)l) * fl;
+      dnext = d0;
     }
+    x6 = x5;
+    x5 = x4;
+    x4 = x3;
+    x3 = x2;
+    x2 = x1;
+    x1 = x;
   }
-  for (int e = tid; e < (n - 1) * nm; e += nt) {
-    const int j = e / nm, c = e - j * nm;
-    const double y0 = R[(2 * j) * ncol + c], y1 = R[(2 * j + 2) * ncol + c];
-    const double d0 = (R[(2 * j + 1) * ncol + c] / j1[j]) * j1[j];
-    const double d1 = (R[(2 * j + 3) * ncol + c] / j1[j + 1]) * j1[j + 1];
-    const double z = y1 - y0;
-    double *cf = spl + at.spl_off + ((long)j * lsize + l * l + c0 + c) * 4;
-    cf[0] = y0 * fl;
-    cf[1] = d0 * fl;
-    cf[2] = (3 * z - 2 * d0 - d1) * fl;
-    cf[3] = (-2 * z + d0 + d1) * fl;
-  }
-  for (int c = tid; c < nm; c += nt) {
-    const int lm = l * l + c0 + c;
-    amp[at.amp_off + lm * 2 + 0] = R[c] / pow(at.first_x, (double)l) * fl;
-    amp[at.amp_off + lm * 2 + 1] = R[(2 * (n - 1)) * ncol + c] * pow(at.last_x, (double)(l + 1)) * fl;
-  }
+  ring_wait<0>();
 }
 
 // ------------------------------------------------------------------ kinetic
@@ -1171,21 +1317,6 @@ cudaError_t launch_poisson_project(const PoissonDev &P, const double *rho,
 
 constexpr size_t kMaxSmem = 227 * 1024;
 
-size_t poisson_radial_smem(int max_nrad, int ncol) {
-  const size_t n = (size_t)max_nrad;
-  return (2 * n * ncol + (size_t)radial_region_doubles(max_nrad, ncol) + 8 * n + 2 * (size_t)ncol) *
-         sizeof(double);
-}
-
-// Columns (m) per radial CTA: 32, halved while the CTA's shared memory would
-// exceed the limit (long radial grids); systems with 2l + 1 > ncol use several
-// CTAs.  0 when even one column does not fit.
-int poisson_radial_ncol(int max_nrad) {
-  for (int ncol = 32; ncol >= 1; ncol /= 2)
-    if (poisson_radial_smem(max_nrad, ncol) <= kMaxSmem) return ncol;
-  return 0;
-}
-
 size_t poisson_factor_doubles(int nsys, int max_nrad) {
   return (size_t)nsys * 2 * max_nrad * (kW + kKL);
 }
@@ -1211,17 +1342,21 @@ cudaError_t launch_poisson_factor(const PoissonDev &P, cudaStream_t s) {
 
 cudaError_t launch_radial_solve(const PoissonDev &P, const RadialOp &op, cudaStream_t s) {
   if (P.nsys == 0) return cudaSuccess;
-  const int ncol = poisson_radial_ncol(P.max_nrad);
-  if (ncol == 0) return cudaErrorInvalidValue;
-  const size_t smem = poisson_radial_smem(P.max_nrad, ncol);
+  // one warp per CTA for single solves (idle lanes' shared memory would limit
+  // the CTAs per SM), up to kRadialThreads for batches; the CTAs of a system
+  // take radial_solves_per_cta(l, threads) solves each, and the grid's y
+  // covers the batch for the largest l (CTAs past it return)
+  const long cols = (long)(2 * P.max_lmax + 1) * P.nbatch;
+  const int threads = (int)std::min<long>(kRadialThreads, (cols + 31) / 32 * 32);
+  const size_t smem = radial_smem_bytes(P.max_nrad, threads);
+  if (smem > kMaxSmem || 2 * P.max_lmax + 1 > kRadialThreads || !P.rscr)
+    return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(radial_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  const int nchunk = (2 * P.max_lmax + 1 + ncol - 1) / ncol;
-  // 4 warps: the per-column chains (spline, substitutions) use the first, the
-  // row-parallel stages (right-hand side, outputs, staging) all four
-  radial_kernel<<<dim3(P.nsys, nchunk * P.nbatch), 128, smem, s>>>(P, ncol, op);
+  const int spc = radial_solves_per_cta(P.max_lmax, threads);
+  const int groups = (P.nbatch + spc - 1) / spc;
+  radial_kernel<<<dim3(P.nsys, groups), threads, smem, s>>>(P, op);
   return cudaGetLastError();
 }
 

@@ -25,7 +25,9 @@ struct PoissonAtom {
   int raw_off;    // [lsize][nrad] solution values y and t-derivatives dt
   int mol_point_start, mol_npoint;  // points of this atom's molecule
   int bucket_off;  // [nrad + 1] buckets: 0 left tail, 1 + j interval j, nrad right tail
+  int sys_off;     // radial system of (this atom, l) = sys_off + l
   long pair_off;   // this atom's slice of the (atom, point) pair arrays
+  long scr_off;    // radial-solve scratch: [3 nrad][lsize]
 };
 
 // One CTA of the bucketed evaluation: `count` (<= kEvalChunk) pairs of one
@@ -75,6 +77,10 @@ struct PoissonDev {
   double *lmul = nullptr;
   int *lpiv = nullptr;
   int lu_stride = 0;
+  // radial-solve scratch per column (spline t-derivatives, eliminated
+  // right-hand side); one solve's scratch is rscr_stride doubles long
+  double *rscr = nullptr;
+  long rscr_stride = 0;
   // bucketed evaluation (built once per grid): for every atom the points of
   // its molecule sorted by spline interval, and a partial potential per pair
   long npair = 0;
@@ -123,7 +129,8 @@ cudaError_t launch_poisson_project(const PoissonDev &P, const double *rho,
                                    cudaStream_t s);
 // Assembles and LU-factors the radial FEM matrices (once per grid).
 cudaError_t launch_poisson_factor(const PoissonDev &P, cudaStream_t s);
-// projected density -> spline tables of the potential (one CTA per (atom, l)).
+// projected density -> spline tables of the potential (one thread per (solve,
+// l, m) column, one CTA per (atom, l) and group of solves); needs P.rscr.
 cudaError_t launch_poisson_radial(const PoissonDev &P, cudaStream_t s);
 // The same two stages for another radial operator (factors into P.lu, P.lmul,
 // P.lpiv; raw spline output skipped when P.raw_y is null).

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "common.h"
+#include "dmma.cuh"
 #include "host.h"
 #include "poisson.cuh"
 #include "solid_harmonics.h"
@@ -110,17 +111,21 @@ __device__ __forceinline__ double rt_inv(const RTParams &rt, double r) {
 // ------------------------------------------------------------------ project
 // proj[s][lm] = sum_j g[s][j] Y[j][lm] / sigma[s] * sqrt(4 pi (2l + 1)) per atom,
 // g[s][j] = rho wb w at the atom's point (shell s, direction j): a small GEMM
-// (nrad x nang) x (nang x lsize).  CTA = (64 lm, 64 shells, atom), 256
-// threads each holding a 4 x 4 tile of the result; j runs in chunks of 32
-// staged in shared memory (g transposed, Y as is).  Every output is one FMA
-// chain over j in increasing order, as in a plain loop.
-constexpr int kProjTile = 64, kProjK = 32, kProjThreads = 256;
+// (nrad x nang) x (nang x lsize) on the FP64 tensor pipe (DMMA m16n8k8).
+// CTA = (64 lm, 64 shells, atom x solve), 4 warps of 32 shells x 32 lm; the
+// directions run in chunks of 16, staged in shared memory (g as [shell][j],
+// Y as [j][lm], row strides = 4 mod 16 doubles so that each half-warp's
+// fragment loads hit 16 distinct banks) and double-buffered: the next chunk
+// is read into registers while the current one is multiplied.
+constexpr int kProjTile = 64, kProjK = 16, kProjThreads = 128;
+constexpr int kProjLda = kProjK + 4, kProjLdb = kProjTile + 4;
+constexpr int kProjPer = kProjTile * kProjK / kProjThreads;  // elements per thread per chunk
 
 __global__ void __launch_bounds__(kProjThreads)
 project_kernel(PoissonDev P, const double *__restrict__ rho,
                const double *__restrict__ wb, const double *__restrict__ w) {
-  __shared__ double gs[kProjK][kProjTile + 1];  // [j][shell]
-  __shared__ __align__(16) double ys[kProjK][kProjTile];  // [j][lm]
+  __shared__ __align__(16) double as[2][kProjTile][kProjLda];  // [shell][j]
+  __shared__ __align__(16) double bs[2][kProjK][kProjLdb];     // [j][lm]
   const int bat = blockIdx.z / P.natom;  // solve of a batch
   const PoissonAtom at = P.atoms[blockIdx.z - bat * P.natom];
   rho += bat * P.batch_ld;
@@ -128,62 +133,102 @@ project_kernel(PoissonDev P, const double *__restrict__ rho,
   const int lsize = (at.lmax + 1) * (at.lmax + 1);
   const int lm0 = blockIdx.x * kProjTile, s0 = blockIdx.y * kProjTile;
   if (lm0 >= lsize || s0 >= at.nrad) return;
-  const int nang = at.nang;
-  const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+  const int nang = at.nang, nrad = at.nrad;
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int wr = (wid >> 1) * 32, wc = (wid & 1) * 32;  // warp tile origin
   const double *Y = P.ytab + at.ytab_off;
-  double acc[4][4];
+  double ra[kProjPer], rb[kProjPer];
+  // chunk j0 into registers: g products and Y values (zero outside)
+  auto fetch = [&](int j0) {
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int k = 0; k < 4; ++k) acc[i][k] = 0.0;
-  for (int j0 = 0; j0 < nang; j0 += kProjK) {
-    // g tile: 64 shells x 32 directions (contiguous in j for each shell)
-    for (int e = t; e < kProjTile * kProjK; e += kProjThreads) {
-      const int sl = e / kProjK, jj = e % kProjK;
-      const int sh = s0 + sl, j = j0 + jj;
-      double v = 0.0;
-      if (sh < at.nrad && j < nang) {
-        const long p = at.point_off + (long)sh * nang + j;
-        v = rho[p] * wb[p] * w[p];
+    for (int r = 0; r < kProjPer; ++r) {
+      const int e = t + r * kProjThreads;
+      {
+        const int sl = e / kProjK, jj = e % kProjK;
+        const int sh = s0 + sl, j = j0 + jj;
+        double v = 0.0;
+        if (sh < nrad && j < nang) {
+          const long p = at.point_off + (long)sh * nang + j;
+          v = rho[p] * wb[p] * w[p];
+        }
+        ra[r] = v;
       }
-      gs[jj][sl] = v;
+      {
+        const int jj = e / kProjTile, ll = e % kProjTile;
+        const int j = j0 + jj, lm = lm0 + ll;
+        rb[r] = (j < nang && lm < lsize) ? __ldg(Y + (long)j * lsize + lm) : 0.0;
+      }
     }
-    // Y tile: 32 directions x 64 lm (contiguous in lm)
-    for (int e = t; e < kProjK * kProjTile; e += kProjThreads) {
-      const int jj = e / kProjTile, ll = e % kProjTile;
-      const int j = j0 + jj, lm = lm0 + ll;
-      ys[jj][ll] = (j < nang && lm < lsize) ? __ldg(Y + (long)j * lsize + lm) : 0.0;
+  };
+  auto stash = [&](int buf) {
+#pragma unroll
+    for (int r = 0; r < kProjPer; ++r) {
+      const int e = t + r * kProjThreads;
+      as[buf][e / kProjK][e % kProjK] = ra[r];
+      bs[buf][e / kProjTile][e % kProjTile] = rb[r];
     }
-    __syncthreads();
-    const int jn = min(kProjK, nang - j0);
-    for (int jj = 0; jj < jn; ++jj) {
-      double a[4], y[4];
+  };
+  double acc[2][4][4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = gs[jj][ty * 4 + i];
-      const double2 y01 = *reinterpret_cast<const double2 *>(&ys[jj][tx * 4]);
-      const double2 y23 = *reinterpret_cast<const double2 *>(&ys[jj][tx * 4 + 2]);
-      y[0] = y01.x;
-      y[1] = y01.y;
-      y[2] = y23.x;
-      y[3] = y23.y;
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+    for (int k = 0; k < 4; ++k)
 #pragma unroll
-        for (int k = 0; k < 4; ++k) acc[i][k] = fma(y[k], a[i], acc[i][k]);
+      for (int c = 0; c < 4; ++c) acc[i][k][c] = 0.0;
+  fetch(0);
+  stash(0);
+  __syncthreads();
+  int buf = 0;
+  for (int j0 = 0; j0 < nang; j0 += kProjK) {
+    const bool more = j0 + kProjK < nang;
+    if (more) fetch(j0 + kProjK);
+#pragma unroll
+    for (int kk = 0; kk < kProjK; kk += 8) {
+      double a[2][4], b[4][2];
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt) {
+        const int r0 = wr + mt * 16 + g;
+        a[mt][0] = as[buf][r0][kk + q];
+        a[mt][1] = as[buf][r0 + 8][kk + q];
+        a[mt][2] = as[buf][r0][kk + q + 4];
+        a[mt][3] = as[buf][r0 + 8][kk + q + 4];
+      }
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const int c0 = wc + nt * 8 + g;
+        b[nt][0] = bs[buf][kk + q][c0];
+        b[nt][1] = bs[buf][kk + q + 4][c0];
+      }
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) dmma(acc[mt][nt], a[mt], b[nt]);
     }
-    __syncthreads();
+    if (more) {
+      stash(buf ^ 1);  // the other buffer: last read before the previous barrier
+      __syncthreads();
+      buf ^= 1;
+    }
   }
-  const double *sigma = P.rad + at.rad_off + kRadSigma * at.nrad;
+  const double *sigma = P.rad + at.rad_off + kRadSigma * nrad;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const int lm = lm0 + tx * 4 + k;
-    if (lm >= lsize) continue;
-    const int l = (int)sqrt((double)lm + 0.5);
-    const double fac = sqrt(4.0 * M_PI * (2.0 * l + 1));
+  for (int nt = 0; nt < 4; ++nt) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int sh = s0 + ty * 4 + i;
-      if (sh < at.nrad) proj[at.proj_off + (long)sh * lsize + lm] = acc[i][k] / sigma[sh] * fac;
+    for (int c = 0; c < 2; ++c) {
+      const int lm = lm0 + wc + nt * 8 + 2 * q + c;
+      if (lm >= lsize) continue;
+      const int l = (int)sqrt((double)lm + 0.5);
+      const double fac = sqrt(4.0 * M_PI * (2.0 * l + 1));
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int sh = s0 + wr + mt * 16 + g + 8 * h;
+          if (sh < nrad)
+            proj[at.proj_off + (long)sh * lsize + lm] = acc[mt][nt][2 * h + c] / sigma[sh] * fac;
+        }
+      }
     }
   }
 }

@@ -43,6 +43,9 @@ __constant__ double c_shnorm[(kMaxLmax + 1) * (kMaxLmax + 1)];  // [l][m]
 __constant__ double c_rec_a[(kMaxLmax + 1) * (kMaxLmax + 1)];      // A_lm at [l][m]
 __constant__ double c_rec_gamma[(kMaxLmax + 1) * (kMaxLmax + 1)];  // gamma at [lm]
 __constant__ double c_rec_start[kMaxLmax + 1];
+// global copy of c_rec_gamma for staging loops whose lanes read different
+// entries (constant memory serves one address at a time)
+__device__ double g_rec_gamma[(kMaxLmax + 1) * (kMaxLmax + 1)];
 // Finite-difference weights of the radial second derivative (integers over
 // common denominators, host deriv2_stencils()): [0, 28) first derivative at
 // the four edge nodes (7 weights each), [28, 56) second derivative, [56, 65)
@@ -1096,14 +1099,36 @@ __device__ __forceinline__ void pair_values(const double *cf, int lmaxA, const d
 }
 
 
+// max over 0 <= u <= 1 of |c0 + c1 u + c2 u^2 + c3 u^3|: the ends and the
+// interior zeros of the derivative (stable quadratic roots), plus 1e-12 of
+// sum_k |c_k| for the rounding of the evaluation and of the roots.
+__device__ double cubic_max_abs(const double *c) {
+  auto val = [&](double u) { return c[0] + u * (c[1] + u * (c[2] + u * c[3])); };
+  double m = fmax(fabs(c[0]), fabs(val(1.0)));
+  const double a = 3.0 * c[3], b = 2.0 * c[2], cc = c[1];
+  if (a != 0.0) {
+    const double disc = b * b - 4.0 * a * cc;
+    if (disc >= 0.0) {
+      const double h = -0.5 * (b + copysign(sqrt(disc), b));
+      const double r1 = h / a, r2 = h != 0.0 ? cc / h : r1;
+      if (r1 > 0.0 && r1 < 1.0) m = fmax(m, fabs(val(r1)));
+      if (r2 > 0.0 && r2 < 1.0) m = fmax(m, fabs(val(r2)));
+    }
+  } else if (b != 0.0) {
+    const double r = -cc / b;
+    if (r > 0.0 && r < 1.0) m = fmax(m, fabs(val(r)));
+  }
+  return m + 1e-12 * (fabs(c[0]) + fabs(c[1]) + fabs(c[2]) + fabs(c[3]));
+}
+
 // Truncation of the expansion per (atom, bucket) when P.eval_tol > 0.  With
 // Racah-normalised harmonics sum_m S_lm(r_hat)^2 = 1, so by Cauchy-Schwarz the
 // l-block adds at most bound_l = sqrt(sum_m c_lm^2) to the potential of any
-// pair of the bucket, with c_lm = sum_k |c_k,lm| inside the grid (0 <= u <= 1),
-// |a_lm| first_x^l below the first radial point (d^l <= first_x^l) and
-// |a_lm| last_x^-(l+1) beyond the last.  The bucket keeps l <= L, the smallest
-// L whose dropped blocks sum to at most eval_tol.  Grid (max nrad + 1, natom),
-// one warp: lane l bounds block l.
+// pair of the bucket, with c_lm = max |U_lm(u)| over the interval's cubic
+// (0 <= u <= 1) inside the grid, |a_lm| first_x^l below the first radial point
+// (d^l <= first_x^l) and |a_lm| last_x^-(l+1) beyond the last.  The bucket
+// keeps l <= L, the smallest L whose dropped blocks sum to at most eval_tol.
+// Grid (max nrad + 1, natom), one warp: lane l bounds block l.
 __global__ void __launch_bounds__(32) bucket_lcut_kernel(PoissonDev P) {
   __shared__ double bound[32];
   const int bat = blockIdx.y / P.natom;  // solve of a batch
@@ -1120,8 +1145,7 @@ __global__ void __launch_bounds__(32) bucket_lcut_kernel(PoissonDev P) {
     for (int lm = l * l; lm < (l + 1) * (l + 1); ++lm) {
       double c;
       if (region == 0) {
-        const double *cf = spl + at.spl_off + ((long)(b - 1) * lsize + lm) * 4;
-        c = fabs(cf[0]) + fabs(cf[1]) + fabs(cf[2]) + fabs(cf[3]);
+        c = cubic_max_abs(spl + at.spl_off + ((long)(b - 1) * lsize + lm) * 4);
       } else {
         c = fabs(amp[at.amp_off + lm * 2 + (region == 1 ? 0 : 1)]);
       }
@@ -1164,11 +1188,11 @@ eval_pairs_kernel(PoissonDev P, const double *__restrict__ gx,
   if (region == 0) {
     const double *src =
         P.spl + bat * P.spl_stride + at.spl_off + (long)(it.bucket - 1) * lsize * 4;
-    for (int e = threadIdx.x; e < lkeep * 4; e += blockDim.x) cf[e] = src[e] * c_rec_gamma[e >> 2];
+    for (int e = threadIdx.x; e < lkeep * 4; e += blockDim.x) cf[e] = src[e] * g_rec_gamma[e >> 2];
   } else {
     const double *src = P.amp + bat * P.amp_stride + at.amp_off;
     for (int e = threadIdx.x; e < lkeep; e += blockDim.x)
-      cf[e] = src[2 * e + (region == 1 ? 0 : 1)] * c_rec_gamma[e];
+      cf[e] = src[2 * e + (region == 1 ? 0 : 1)] * g_rec_gamma[e];
   }
   __syncthreads();
   // thread t evaluates the pairs t and t + blockDim.x of the item (the
@@ -1327,6 +1351,9 @@ cudaError_t poisson_init_constants() {
     if ((e = cudaMemcpyToSymbol(c_rec_a, A.data(), A.size() * sizeof(double))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(c_rec_gamma, gam_lm.data(), gam_lm.size() * sizeof(double))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(c_rec_start, st.data(), st.size() * sizeof(double))) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(g_rec_gamma, gam_lm.data(), gam_lm.size() * sizeof(double))) !=
+        cudaSuccess)
+      return e;
   }
   {
     const Deriv2Stencils &st = deriv2_stencils();

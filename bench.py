@@ -42,7 +42,8 @@ TRAFFIC_SOURCE = ('ncu dram__bytes_read.sum + dram__bytes_write.sum of eval_pair
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument('--gpus', type=int, default=1)
-    p.add_argument('--steps', type=int, default=10)
+    p.add_argument('--steps', type=int, default=None,
+                   help='timed steps (default 100 for c4, whose builds take 15 ms, else 10)')
     p.add_argument('--warmup', type=int, default=3)
     p.add_argument('--impl', default='napmo_b200')
     p.add_argument('--nrad', type=int, default=100)
@@ -59,12 +60,19 @@ def parse():
     p.add_argument('--precision', default='auto', choices=['auto', 'fp64'],
                    help='auto: headline is the int8-slice tensor-core build when its energy '
                         'is within 1e-6 Eh of FP64 (checked in the same run), else FP64')
-    return p.parse_args()
+    args = p.parse_args()
+    if args.steps is None:
+        # c4 builds take 15 ms: 100 of them span the clock sampler's 100 ms
+        # period many times; the reference arm's steps are 2 s CPU samples
+        args.steps = 100 if args.workload == 'c4' and args.impl != 'reference' else 10
+    return args
 
 
 # ------------------------------------------------------------------ helpers
 class ClockSampler(object):
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms.  start()
+    returns once the first sample has arrived (nvidia-smi takes a moment to
+    come up), so the timed region that follows is covered from its start."""
     QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
@@ -78,10 +86,13 @@ class ClockSampler(object):
         try:
             self.proc = subprocess.Popen(
                 ['nvidia-smi', '-i', str(self.index), '--query-gpu=' + self.QUERY,
-                 '--format=csv,noheader,nounits', '-lms', '200'],
+                 '--format=csv,noheader,nounits', '-lms', '100'],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
 

@@ -45,6 +45,7 @@ struct PoissonPlan {
   DevBuf<double> rad, ytab, proj, spl, amp, raw_y, raw_dt, lu, lmul;
   DevBuf<int> lpiv;
   DevBuf<double> rscr;  // radial-solve scratch of one solve
+  DevBuf<double> pg;    // projection scratch of one solve (rho wb w per point)
   DevBuf<int> pairs;
   DevBuf<EvalItem> items;
   int nitems = 0, nitems_in = 0;  // items, of which the first nitems_in are interior
@@ -101,7 +102,7 @@ int build_poisson_plan(const std::vector<const AtomLayout *> &atoms,
   std::vector<double> rad, ytab;
   std::map<std::pair<int, int>, int> ykey;  // (atom-rule id via nang,lmax) -> offset
   std::vector<int> sys_atom, sys_l;
-  long proj = 0, spl = 0, amp = 0, raw = 0, pairs = 0, scr = 0;
+  long proj = 0, spl = 0, amp = 0, raw = 0, pairs = 0, scr = 0, npts = 0;
   int buckets = 0;
   std::vector<int> atom_mol(natom, 0);
   for (int m = 0; m + 1 < (int)mol_atom_off.size(); ++m)
@@ -164,6 +165,7 @@ int build_poisson_plan(const std::vector<const AtomLayout *> &atoms,
     raw += (long)lsize * n;
     A.scr_off = scr;
     scr += 3L * n * lsize;
+    npts = std::max(npts, (long)L.point_off + (long)n * L.nang);
     A.sys_off = (int)sys_atom.size();
     const int mol = atom_mol[a];
     A.mol_point_start = mol_point_off[mol];
@@ -195,6 +197,7 @@ int build_poisson_plan(const std::vector<const AtomLayout *> &atoms,
   NAPMO_TRY_CUDA(plan->raw_y.alloc(raw), "alloc");
   NAPMO_TRY_CUDA(plan->raw_dt.alloc(raw), "alloc");
   NAPMO_TRY_CUDA(plan->rscr.alloc(scr), "alloc");
+  NAPMO_TRY_CUDA(plan->pg.alloc(npts), "alloc");
   d.atoms = plan->atoms.p;
   d.mol_atom_off = plan->mol_atom_off.p;
   d.mol_point_off = plan->mol_point_off.p;
@@ -208,6 +211,7 @@ int build_poisson_plan(const std::vector<const AtomLayout *> &atoms,
   d.raw_y = plan->raw_y.p;
   d.raw_dt = plan->raw_dt.p;
   d.rscr = plan->rscr.p;
+  d.pg = plan->pg.p;
   d.npair = pairs;
   // LU factors of the radial systems (they depend on the grid only)
   d.lu_stride = 2 * d.max_nrad;
@@ -501,7 +505,7 @@ int run_poisson_many(BeckeGrid *g, PoissonPlan *p, int k, const double *rho_dev,
   int st = select_pair_lists(p, g, keep, key, s);
   if (st) return st;
   const PoissonDev &d = p->d;
-  const size_t nd = p->proj.n + p->spl.n + p->amp.n + p->pair_v.n + p->rscr.n;
+  const size_t nd = p->proj.n + p->spl.n + p->amp.n + p->pair_v.n + p->rscr.n + p->pg.n;
   const size_t per = nd * sizeof(double) + p->lcut.n * sizeof(int);
   // grid limits: the projection and truncation launches use natom x B blocks
   // in y/z, the radial one B in y
@@ -533,7 +537,9 @@ int run_poisson_many(BeckeGrid *g, PoissonPlan *p, int k, const double *rho_dev,
   P.amp = P.spl + P.spl_stride * B;
   P.pair_v = P.amp + P.amp_stride * B;
   P.rscr = P.pair_v + P.pairv_stride * B;
-  P.lcut = tol > 0.0 ? (int *)(P.rscr + P.rscr_stride * B) : nullptr;
+  P.pg_stride = (long)p->pg.n;
+  P.pg = P.rscr + P.rscr_stride * B;
+  P.lcut = tol > 0.0 ? (int *)(P.pg + P.pg_stride * B) : nullptr;
   P.eval_tol = tol;
   P.raw_y = nullptr;
   P.raw_dt = nullptr;

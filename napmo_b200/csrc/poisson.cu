@@ -115,61 +115,73 @@ __device__ __forceinline__ double rt_inv(const RTParams &rt, double r) {
 // proj[s][lm] = sum_j g[s][j] Y[j][lm] / sigma[s] * sqrt(4 pi (2l + 1)) per atom,
 // g[s][j] = rho wb w at the atom's point (shell s, direction j): a small GEMM
 // (nrad x nang) x (nang x lsize) on the FP64 tensor pipe (DMMA m16n8k8).
-// CTA = (64 lm, 64 shells, atom x solve), 4 warps of 32 shells x 32 lm; the
-// directions run in chunks of 16, staged in shared memory (g as [shell][j],
-// Y as [j][lm], row strides = 4 mod 16 doubles so that each half-warp's
-// fragment loads hit 16 distinct banks) and double-buffered: the next chunk
-// is read into registers while the current one is multiplied.
-constexpr int kProjTile = 64, kProjK = 16, kProjThreads = 128;
+// g is first formed once per point into the plan's scratch P.pg (project_g_kernel),
+// so that both operands stream straight from memory: CTA = (64 lm, 64 shells,
+// atom x solve), 4 warps of 32 shells x 32 lm; the directions run in chunks of
+// 16 through a kProjStages-deep cp.async ring in shared memory (g as
+// [shell][j], Y as [j][lm], row strides = 4 mod 16 doubles so that each
+// half-warp's fragment loads hit 16 distinct banks), each chunk's loads issued
+// kProjStages - 1 chunks ahead of its products.
+constexpr int kProjTile = 64, kProjK = 16, kProjThreads = 128, kProjStages = 3;
 constexpr int kProjLda = kProjK + 4, kProjLdb = kProjTile + 4;
-constexpr int kProjPer = kProjTile * kProjK / kProjThreads;  // elements per thread per chunk
+constexpr int kProjPer = kProjTile * kProjK / kProjThreads;  // copies per thread per chunk
+constexpr size_t kProjStageDoubles = kProjTile * kProjLda + kProjK * kProjLdb;
 
-__global__ void __launch_bounds__(kProjThreads)
-project_kernel(PoissonDev P, const double *__restrict__ rho,
-               const double *__restrict__ wb, const double *__restrict__ w) {
-  __shared__ __align__(16) double as[2][kProjTile][kProjLda];  // [shell][j]
-  __shared__ __align__(16) double bs[2][kProjK][kProjLdb];     // [j][lm]
+// pg[solve][p] = rho wb w at every point of every atom (the same product, in
+// the same order, the projection used to form per element).
+__global__ void project_g_kernel(PoissonDev P, const double *__restrict__ rho,
+                                 const double *__restrict__ wb,
+                                 const double *__restrict__ w) {
+  const int bat = blockIdx.y / P.natom;
+  const PoissonAtom &at = P.atoms[blockIdx.y - bat * P.natom];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= at.nrad * at.nang) return;
+  const long p = at.point_off + i;
+  P.pg[bat * P.pg_stride + p] = rho[bat * P.batch_ld + p] * wb[p] * w[p];
+}
+
+__device__ __forceinline__ void proj_copy8(double *dst, const double *src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src),
+               "r"(valid ? 8 : 0)
+               : "memory");
+}
+
+__global__ void __launch_bounds__(kProjThreads, 3) project_kernel(PoissonDev P) {
+  extern __shared__ __align__(16) double psm[];
   const int bat = blockIdx.z / P.natom;  // solve of a batch
   const PoissonAtom at = P.atoms[blockIdx.z - bat * P.natom];
-  rho += bat * P.batch_ld;
+  const double *g = P.pg + bat * P.pg_stride;
   double *proj = P.proj + bat * P.proj_stride;
   const int lsize = (at.lmax + 1) * (at.lmax + 1);
   const int lm0 = blockIdx.x * kProjTile, s0 = blockIdx.y * kProjTile;
   if (lm0 >= lsize || s0 >= at.nrad) return;
   const int nang = at.nang, nrad = at.nrad;
   const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-  const int g = lane >> 2, q = lane & 3;
+  const int gq = lane >> 2, q = lane & 3;
   const int wr = (wid >> 1) * 32, wc = (wid & 1) * 32;  // warp tile origin
   const double *Y = P.ytab + at.ytab_off;
-  double ra[kProjPer], rb[kProjPer];
-  // chunk j0 into registers: g products and Y values (zero outside)
-  auto fetch = [&](int j0) {
+  const int nchunk = (nang + kProjK - 1) / kProjK;
+  // chunk c into ring stage c % kProjStages (zero outside the atom's table)
+  auto issue = [&](int c) {
+    double *as = psm + (c % kProjStages) * kProjStageDoubles;
+    double *bs = as + kProjTile * kProjLda;
+    const int j0 = c * kProjK;
 #pragma unroll
     for (int r = 0; r < kProjPer; ++r) {
       const int e = t + r * kProjThreads;
       {
         const int sl = e / kProjK, jj = e % kProjK;
         const int sh = s0 + sl, j = j0 + jj;
-        double v = 0.0;
-        if (sh < nrad && j < nang) {
-          const long p = at.point_off + (long)sh * nang + j;
-          v = rho[p] * wb[p] * w[p];
-        }
-        ra[r] = v;
+        const bool ok = sh < nrad && j < nang;
+        proj_copy8(as + sl * kProjLda + jj, ok ? g + at.point_off + (long)sh * nang + j : g, ok);
       }
       {
         const int jj = e / kProjTile, ll = e % kProjTile;
         const int j = j0 + jj, lm = lm0 + ll;
-        rb[r] = (j < nang && lm < lsize) ? __ldg(Y + (long)j * lsize + lm) : 0.0;
+        const bool ok = j < nang && lm < lsize;
+        proj_copy8(bs + jj * kProjLdb + ll, ok ? Y + (long)j * lsize + lm : Y, ok);
       }
-    }
-  };
-  auto stash = [&](int buf) {
-#pragma unroll
-    for (int r = 0; r < kProjPer; ++r) {
-      const int e = t + r * kProjThreads;
-      as[buf][e / kProjK][e % kProjK] = ra[r];
-      bs[buf][e / kProjTile][e % kProjTile] = rb[r];
     }
   };
   double acc[2][4][4];
@@ -179,41 +191,42 @@ project_kernel(PoissonDev P, const double *__restrict__ rho,
     for (int k = 0; k < 4; ++k)
 #pragma unroll
       for (int c = 0; c < 4; ++c) acc[i][k][c] = 0.0;
-  fetch(0);
-  stash(0);
-  __syncthreads();
-  int buf = 0;
-  for (int j0 = 0; j0 < nang; j0 += kProjK) {
-    const bool more = j0 + kProjK < nang;
-    if (more) fetch(j0 + kProjK);
+#pragma unroll
+  for (int c = 0; c < kProjStages - 1; ++c) {
+    if (c < nchunk) issue(c);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  }
+  for (int c = 0; c < nchunk; ++c) {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(kProjStages - 2) : "memory");
+    __syncthreads();  // chunk c is in for every thread; stage (c - 1) is free
+    if (c + kProjStages - 1 < nchunk) issue(c + kProjStages - 1);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    const double *as = psm + (c % kProjStages) * kProjStageDoubles;
+    const double *bs = as + kProjTile * kProjLda;
 #pragma unroll
     for (int kk = 0; kk < kProjK; kk += 8) {
       double a[2][4], b[4][2];
 #pragma unroll
       for (int mt = 0; mt < 2; ++mt) {
-        const int r0 = wr + mt * 16 + g;
-        a[mt][0] = as[buf][r0][kk + q];
-        a[mt][1] = as[buf][r0 + 8][kk + q];
-        a[mt][2] = as[buf][r0][kk + q + 4];
-        a[mt][3] = as[buf][r0 + 8][kk + q + 4];
+        const double *ar = as + (wr + mt * 16 + gq) * kProjLda + kk + q;
+        a[mt][0] = ar[0];
+        a[mt][1] = ar[8 * kProjLda];
+        a[mt][2] = ar[4];
+        a[mt][3] = ar[8 * kProjLda + 4];
       }
 #pragma unroll
       for (int nt = 0; nt < 4; ++nt) {
-        const int c0 = wc + nt * 8 + g;
-        b[nt][0] = bs[buf][kk + q][c0];
-        b[nt][1] = bs[buf][kk + q + 4][c0];
+        const double *br = bs + (kk + q) * kProjLdb + wc + nt * 8 + gq;
+        b[nt][0] = br[0];
+        b[nt][1] = br[4 * kProjLdb];
       }
 #pragma unroll
       for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) dmma(acc[mt][nt], a[mt], b[nt]);
     }
-    if (more) {
-      stash(buf ^ 1);  // the other buffer: last read before the previous barrier
-      __syncthreads();
-      buf ^= 1;
-    }
   }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   const double *sigma = P.rad + at.rad_off + kRadSigma * nrad;
 #pragma unroll
   for (int nt = 0; nt < 4; ++nt) {
@@ -227,7 +240,7 @@ project_kernel(PoissonDev P, const double *__restrict__ rho,
       for (int mt = 0; mt < 2; ++mt) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          const int sh = s0 + wr + mt * 16 + g + 8 * h;
+          const int sh = s0 + wr + mt * 16 + gq + 8 * h;
           if (sh < nrad)
             proj[at.proj_off + (long)sh * lsize + lm] = acc[mt][nt][2 * h + c] / sigma[sh] * fac;
         }
@@ -1380,10 +1393,20 @@ cudaError_t launch_poisson_project(const PoissonDev &P, const double *rho,
                                    const double *wb, const double *w,
                                    cudaStream_t s) {
   if (P.natom == 0) return cudaSuccess;
+  if (!P.pg) return cudaErrorInvalidValue;
+  const int maxpts = P.max_nrad * P.max_nang;
+  project_g_kernel<<<dim3((maxpts + 255) / 256, P.natom * P.nbatch), 256, 0, s>>>(P, rho, wb,
+                                                                                 w);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
   const int lsize = (P.max_lmax + 1) * (P.max_lmax + 1);
   dim3 grid((lsize + kProjTile - 1) / kProjTile, (P.max_nrad + kProjTile - 1) / kProjTile,
             P.natom * P.nbatch);
-  project_kernel<<<grid, kProjThreads, 0, s>>>(P, rho, wb, w);
+  constexpr size_t smem = kProjStages * kProjStageDoubles * sizeof(double);
+  e = cudaFuncSetAttribute(project_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+  if (e != cudaSuccess) return e;
+  project_kernel<<<grid, kProjThreads, smem, s>>>(P);
   return cudaGetLastError();
 }
 

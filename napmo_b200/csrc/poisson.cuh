@@ -81,6 +81,10 @@ struct PoissonDev {
   // right-hand side); one solve's scratch is rscr_stride doubles long
   double *rscr = nullptr;
   long rscr_stride = 0;
+  // projection scratch: rho wb w at every grid point (one solve's is
+  // pg_stride doubles long)
+  double *pg = nullptr;
+  long pg_stride = 0;
   // bucketed evaluation (built once per grid): for every atom the points of
   // its molecule sorted by spline interval, and a partial potential per pair
   long npair = 0;

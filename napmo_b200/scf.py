@@ -57,6 +57,25 @@ def epc17_2_device(torch, rho_e, rho_n):
     return tuple(out)
 
 
+def grid_exchange(torch, fb, phi, psi, W, max_bytes=1 << 31):
+    """K_mu,nu = sum_i sum_p W phi_mu psi_i V[psi_i phi_nu], symmetrised (grid
+    exchange of the orbitals psi, nocc x N, in the basis phi, n x N).  The
+    pair densities psi_i phi_nu of as many orbitals as fit in max_bytes (with
+    their potentials and weighted products) are solved in one library call,
+    and their part of K is one batched product.  Returns (K, solves)."""
+    n, N = phi.shape
+    nocc = psi.shape[0]
+    step = max(1, min(nocc, max_bytes // (3 * n * N * 8)))
+    K = torch.zeros((n, n), dtype=torch.float64, device='cuda')
+    for i0 in range(0, nocc, step):
+        ps = psi[i0:i0 + step]
+        k = ps.shape[0]
+        V = fb.coulomb_potentials((ps[:, None, :] * phi[None, :, :]).reshape(k * n, N))
+        A = phi[None, :, :] * (W * ps)[:, None, :]
+        K += torch.matmul(A, V.reshape(k, n, N).transpose(1, 2)).sum(0)
+    return 0.5 * (K + K.T), nocc * n
+
+
 def nuclear_repulsion(point_charges):
     E = 0.0
     for i, a in enumerate(point_charges):
@@ -135,16 +154,10 @@ class GridRHF(object):
 
     def exchange_matrix(self, Cocc):
         """K_mu,nu = sum_i sum_p W phi_mu psi_i V[psi_i phi_nu] (symmetrised)."""
-        t = self.torch
         phi = self._phi()
-        psi = Cocc.T @ phi                                  # nocc x N
-        K = t.zeros((self.n, self.n), dtype=t.float64, device='cuda')
-        for i in range(psi.shape[0]):
-            # the n pair densities psi_i phi_nu solved in one call
-            V = self.fb.coulomb_potentials(psi[i] * phi)
-            self.poisson_solves += self.n
-            K += (phi * (self.W * psi[i])) @ V.T
-        return 0.5 * (K + K.T)
+        K, solves = grid_exchange(self.torch, self.fb, phi, Cocc.T @ phi, self.W)
+        self.poisson_solves += solves
+        return K
 
     def fock(self, D, Cocc):
         """(F, E_electronic) for density D."""
@@ -342,15 +355,11 @@ class GridAPMO(object):
         self.poisson_solves = 0
 
     def _exchange(self, Cocc):
-        sp, t = self.e, self.torch
+        sp = self.e
         phi = sp.fb.phi()[:, :sp.N]
-        psi = Cocc.T @ phi
-        K = t.zeros((sp.n, sp.n), dtype=t.float64, device='cuda')
-        for i in range(psi.shape[0]):
-            V = sp.fb.coulomb_potentials(psi[i] * phi)
-            self.poisson_solves += sp.n
-            K += (phi * (self.W * psi[i])) @ V.T
-        return 0.5 * (K + K.T)
+        K, solves = grid_exchange(self.torch, sp.fb, phi, Cocc.T @ phi, self.W)
+        self.poisson_solves += solves
+        return K
 
     def fock(self, De, Dn, Ce=None):
         """(F_e, F_n, E) for densities De, Dn (Ce: electron orbitals, for HF
@@ -530,15 +539,10 @@ class GridMultiSCF(object):
         self.poisson_solves = 0
 
     def _exchange(self, sp, Cocc):
-        t = self.torch
         phi = sp.fb.phi()[:, :sp.N]
-        psi = Cocc.T @ phi
-        K = t.zeros((sp.n, sp.n), dtype=t.float64, device='cuda')
-        for i in range(psi.shape[0]):
-            V = sp.fb.coulomb_potentials(psi[i] * phi)
-            self.poisson_solves += sp.n
-            K += (phi * (self.W * psi[i])) @ V.T
-        return 0.5 * (K + K.T)
+        K, solves = grid_exchange(self.torch, sp.fb, phi, Cocc.T @ phi, self.W)
+        self.poisson_solves += solves
+        return K
 
     def fock(self, Ds, Cs):
         """(list of F_s, E) for densities Ds and orbitals Cs."""

@@ -290,6 +290,15 @@ int napmo_grid_set_poisson_tolerance(void *grid, double tol);
  * (napmo/functional/xc_interface.py:62-90, LibXC lda_x / lda_c_vwn). */
 int napmo_gpu_lda_xc(long n, const double *rho, double *x_zk, double *x_vrho, double *c_zk,
                      double *c_vrho, void *stream);
+/* Spin-polarised LDA exchange and VWN5 correlation of (rho_a, rho_b) (device,
+ * n values each): energies per particle of the total density and both spins'
+ * potentials, any output may be null; replaces Functional('lda') with spin
+ * 'polarized' (xc_interface.py:62-90, LibXC lda_x / lda_c_vwn), which nAPMO's
+ * DFT uses for open shells (dft_solver.py:35).  nAPMO interleaves the spins in
+ * one array; here they are two. */
+int napmo_gpu_lda_xc_polarized(long n, const double *rho_a, const double *rho_b, double *x_zk,
+                               double *x_va, double *x_vb, double *c_zk, double *c_va,
+                               double *c_vb, void *stream);
 /* epc17-2 electron-proton correlation at n common points (device): energy per
  * electron and both species' potentials; replaces epc17_2
  * (napmo/functional/interspecies_correlation.py:36-68). */

@@ -200,6 +200,9 @@ _SIGS = [
     ('napmo_grid_set_poisson_tolerance', c_int, [c_void_p, c_double]),
     ('napmo_gpu_lda_xc', c_int,
      [c_long, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ('napmo_gpu_lda_xc_polarized', c_int,
+     [c_long, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+      c_void_p]),
     ('napmo_gpu_epc17_2', c_int,
      [c_long, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ('napmo_gpu_kinetic', c_int,

@@ -68,6 +68,80 @@ __global__ void lda_xc_kernel(long n, const double *__restrict__ rho, double *__
   }
 }
 
+// Spin-polarised LDA (nAPMO's DFT with spin 'polarized' for open shells,
+// dft_solver.py:35, LibXC lda_x and lda_c_vwn with two spin densities):
+//   exchange  e_x = -3/4 (6/pi)^(1/3) (rho_a^(4/3) + rho_b^(4/3)),
+//             v_s = -(6 rho_s / pi)^(1/3);
+//   VWN5      e_c(r_s, z) = e_P + a_c f(z) / f''(0) (1 - z^4)
+//                         + (e_F - e_P) f(z) z^4,  z = (rho_a - rho_b) / rho,
+//             f(z) = ((1+z)^(4/3) + (1-z)^(4/3) - 2) / (2^(4/3) - 2),
+//             v_s = e_c - (r_s / 3) de_c/dr_s + (s - z) de_c/dz (s = +1, -1),
+//   with the paramagnetic (P), ferromagnetic (F) and spin-stiffness (a_c)
+//   fits of Vosko, Wilk and Nusair.  zk are energies per particle of the
+//   total density; zero where rho_a + rho_b < 1e-24, negative spin
+//   densities counting as zero.
+constexpr double kVwnFA = 0.01554535, kVwnFB = 7.06042, kVwnFC = 18.0578, kVwnFX0 = -0.32500;
+constexpr double kVwnAB = 1.13107, kVwnAC = 13.0045, kVwnAX0 = -0.0047584;
+
+__device__ __forceinline__ void vwn_fit(double x, double A, double b, double c, double x0,
+                                        double &g, double &dg) {
+  const double X = x * x + b * x + c;
+  const double X0 = x0 * x0 + b * x0 + c;
+  const double Q = sqrt(4.0 * c - b * b);
+  const double at = atan(Q / (2.0 * x + b));
+  g = A * (log(x * x / X) + 2.0 * b / Q * at -
+           b * x0 / X0 * (log((x - x0) * (x - x0) / X) + 2.0 * (b + 2.0 * x0) / Q * at));
+  const double dX = 2.0 * x + b;
+  const double den = dX * dX + Q * Q;
+  dg = A * (2.0 / x - dX / X - 4.0 * b / den -
+            b * x0 / X0 * (2.0 / (x - x0) - dX / X - 4.0 * (b + 2.0 * x0) / den));
+}
+
+__global__ void lda_xc_pol_kernel(long n, const double *__restrict__ rho_a,
+                                  const double *__restrict__ rho_b, double *__restrict__ xzk,
+                                  double *__restrict__ xva, double *__restrict__ xvb,
+                                  double *__restrict__ czk, double *__restrict__ cva,
+                                  double *__restrict__ cvb) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double ra = fmax(rho_a[i], 0.0), rb = fmax(rho_b[i], 0.0);
+  const double rho = ra + rb;
+  const bool on = rho >= kDensCut;
+  if (xzk || xva || xvb) {
+    const double c = -cbrt(6.0 / M_PI);
+    const double a13 = cbrt(ra), b13 = cbrt(rb);
+    if (xzk) xzk[i] = on ? 0.75 * c * (ra * a13 + rb * b13) / rho : 0.0;
+    if (xva) xva[i] = on ? c * a13 : 0.0;
+    if (xvb) xvb[i] = on ? c * b13 : 0.0;
+  }
+  if (czk || cva || cvb) {
+    double ec = 0.0, va = 0.0, vb = 0.0;
+    if (on) {
+      const double z = fmin(fmax((ra - rb) / rho, -1.0), 1.0);
+      const double x = sqrt(cbrt(3.0 / (4.0 * M_PI * rho)));
+      double eP, dP, eF, dF, ac, dac;
+      vwn_fit(x, kVwnA, kVwnB, kVwnC, kVwnX0, eP, dP);
+      vwn_fit(x, kVwnFA, kVwnFB, kVwnFC, kVwnFX0, eF, dF);
+      vwn_fit(x, -1.0 / (6.0 * M_PI * M_PI), kVwnAB, kVwnAC, kVwnAX0, ac, dac);
+      const double fden = exp2(4.0 / 3.0) - 2.0;
+      const double fpp = 4.0 / (9.0 * (cbrt(2.0) - 1.0));
+      const double zp = cbrt(1.0 + z), zm = cbrt(1.0 - z);
+      const double f = ((1.0 + z) * zp + (1.0 - z) * zm - 2.0) / fden;
+      const double df = (4.0 / 3.0) * (zp - zm) / fden;
+      const double z3 = z * z * z, z4 = z3 * z;
+      ec = eP + ac * f / fpp * (1.0 - z4) + (eF - eP) * f * z4;
+      const double dx = dP + dac * f / fpp * (1.0 - z4) + (dF - dP) * f * z4;
+      const double dz = ac / fpp * (df * (1.0 - z4) - 4.0 * z3 * f) + (eF - eP) * (df * z4 + 4.0 * z3 * f);
+      const double base = ec - x / 6.0 * dx;
+      va = base + (1.0 - z) * dz;
+      vb = base - (1.0 + z) * dz;
+    }
+    if (czk) czk[i] = ec;
+    if (cva) cva[i] = va;
+    if (cvb) cvb[i] = vb;
+  }
+}
+
 // 1 when any density of the current epc17-2 call is below 1e-200 (reset by
 // the first kernel of each call; calls that overlap on the device race on it)
 __device__ int g_epc_tiny = 0;
@@ -124,6 +198,26 @@ int napmo_gpu_lda_xc(long n, const double *rho, double *x_zk, double *x_vrho, do
     lda_xc_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
         n, rho, x_zk, x_vrho, c_zk, c_vrho);
     NAPMO_TRY_CUDA(cudaGetLastError(), "lda xc");
+    return kOk;
+  });
+}
+
+// Spin-polarised LDA exchange and VWN5 correlation of (rho_a, rho_b) (device,
+// n values each): energies per particle of the total density and the
+// potentials of both spins (device outputs; any may be null).  Replaces
+// Functional.compute_exchange / compute_correlation with spin 'polarized'
+// (xc_interface.py:62-90, LibXC lda_x and lda_c_vwn), which nAPMO's DFT uses
+// for open shells (dft_solver.py:35); nAPMO interleaves the two spins in one
+// array, this takes them as two.
+int napmo_gpu_lda_xc_polarized(long n, const double *rho_a, const double *rho_b, double *x_zk,
+                               double *x_va, double *x_vb, double *c_zk, double *c_va,
+                               double *c_vb, void *stream) {
+  return guarded([&] {
+    NAPMO_REQUIRE(n >= 0, "negative size");
+    if (n == 0) return kOk;
+    lda_xc_pol_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        n, rho_a, rho_b, x_zk, x_va, x_vb, c_zk, c_va, c_vb);
+    NAPMO_TRY_CUDA(cudaGetLastError(), "polarised lda xc");
     return kOk;
   });
 }

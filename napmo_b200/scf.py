@@ -47,6 +47,19 @@ def lda_xc(torch, rho):
     return xv + cv, xzk + czk
 
 
+def lda_xc_polarized(torch, rho_a, rho_b):
+    """(v_xc of alpha, v_xc of beta, e_xc per particle of the total density)
+    of spin-polarised LDA exchange + VWN5 correlation (device tensors), by
+    napmo_gpu_lda_xc_polarized."""
+    n = rho_a.numel()
+    out = [torch.empty(n, dtype=torch.float64, device='cuda') for _ in range(6)]
+    checked(cext.lib.napmo_gpu_lda_xc_polarized(n, rho_a.data_ptr(), rho_b.data_ptr(),
+                                                *[o.data_ptr() for o in out],
+                                                torch.cuda.current_stream().cuda_stream))
+    xzk, xva, xvb, czk, cva, cvb = out
+    return xva + cva, xvb + cvb, xzk + czk
+
+
 def epc17_2_device(torch, rho_e, rho_n):
     """(energy per electron, v_e, v_n) of epc17-2 (device tensors)."""
     n = rho_e.numel()
@@ -502,15 +515,17 @@ class GridMultiSCF(object):
         nuclear: symbol of the quantum-nucleus species or None.
         charge: molecular charge (electrons = sum Z - charge).
         multiplicity: spin multiplicity (default 1 or 2 by parity).
-        exchange: 'hf' or 'none' for the electrons.
+        exchange: 'hf', 'lda' (spin-polarised LDA exchange + VWN5 correlation
+            of the two spin densities, nAPMO's DFT for open shells) or 'none'
+            for the electrons.
     """
 
     def __init__(self, ms, nuclear=None, nrad=50, nang=110, lmax=None, charge=0,
                  multiplicity=None, precision='fp64', diis=6, mass=PROTON_MASS, exchange='hf'):
         torch = _torch()
         self.torch = torch
-        if exchange not in ('hf', 'none'):
-            raise ValueError("exchange must be 'hf' or 'none' in the unrestricted drivers")
+        if exchange not in ('hf', 'lda', 'none'):
+            raise ValueError("exchange must be 'hf', 'lda' or 'none' in the unrestricted drivers")
         self.exchange = exchange
         self.ms = ms
         e = ms['e-']
@@ -551,6 +566,11 @@ class GridMultiSCF(object):
         vs = [sps[0].fb.coulomb_potential(r) for r in rhos]
         self.poisson_solves += len(rhos)
         Fs, E = [], self.Enn
+        vxc = [None] * len(sps)
+        if self.exchange == 'lda':
+            va, vb, exc = lda_xc_polarized(self.torch, rhos[0], rhos[1])
+            vxc[0], vxc[1] = va, vb
+            E += float((self.W * (rhos[0] + rhos[1]) * exc).sum())
         for s, sp in enumerate(sps):
             pot = None
             for u, (tp, v) in enumerate(zip(sps, vs)):
@@ -558,7 +578,7 @@ class GridMultiSCF(object):
                     continue
                 term = (sp.q * tp.q) * v
                 pot = term if pot is None else pot + term
-            F = sp.H + sp.fb.quadrature(1.0, pot)
+            F = sp.H + sp.fb.quadrature(1.0, pot, vext=vxc[s])
             E += float((Ds[s] * sp.H).sum()) + 0.5 * float((self.W * rhos[s] * pot).sum())
             if self.exchange == 'hf' and self.is_electron[s] and sp.nocc > 0:
                 K = self._exchange(sp, Cs[s][:, :sp.nocc])

@@ -152,9 +152,19 @@ class DFT(_Solver):
         xc = func.get('e-', 'lda')
         if xc != 'lda':
             raise NotImplementedError(str(xc) + ' Functional NOT available!')
-        if self._open_shell():
-            raise NotImplementedError('spin-polarised functionals are not built')
         kw = dict(precision=self.get('precision'), diis=int(self.get('diis')))
+        if self._open_shell():
+            # nAPMO's DFT takes spin 'polarized' for open shells (dft_solver.py:35)
+            if nuc is None:
+                drv = _scf.GridUHF(self.system, nrad, nang, charge=self._charge(),
+                                   multiplicity=self._multiplicity(), exchange='lda', **kw)
+            else:
+                if func.get('e-:' + nuc, func.get(nuc + ':e-')):
+                    raise NotImplementedError('electron-nucleus correlation with spin-polarised '
+                                              'electrons is not built')
+                drv = _scf.GridMultiSCF(self.system, nuc, nrad, nang, charge=self._charge(),
+                                        multiplicity=self._multiplicity(), exchange='lda', **kw)
+            return self._run(drv)
         if nuc is None:
             drv = _scf.GridRHF(self.system, nrad, nang, exchange='lda', **kw)
         else:

@@ -37,6 +37,7 @@ from threadpoolctl import threadpool_limits
 
 import oracle as O
 import ints as OI
+import xc as OX
 
 PROTON_MASS = 1836.15267247      # electron masses (napmo/data/constants.py)
 BOHR = 0.52917724924             # napmo/data/constants.py
@@ -461,13 +462,20 @@ class GridMultiSCF(object):
         rhos = [O.density(sp.phi, D) for sp, D in zip(sps, Ds)]
         vs = poisson_many(self.plan, np.stack(rhos))
         Fs, E = [], self.Enn
+        vxc = [None] * len(sps)
+        if self.exchange == 'lda':   # spin-polarised LDA of the two spin densities
+            zx, xa, xb = OX.lda_x_polarized(rhos[0], rhos[1])
+            zc, ca, cb = OX.lda_c_vwn_polarized(rhos[0], rhos[1])
+            vxc[0], vxc[1] = xa + ca, xb + cb
+            E += float((self.W * (rhos[0] + rhos[1]) * (zx + zc)).sum())
         for s, sp in enumerate(sps):
             pot = np.zeros(g.size)
             for u, (tp, v) in enumerate(zip(sps, vs)):
                 if u == s and not self.is_electron[s]:
                     continue
                 pot = pot + (sp.q * tp.q) * v
-            F = sp.H + O.quadrature(sp.phi, pot, g.becke, g.weights)
+            F = sp.H + O.quadrature(sp.phi, pot if vxc[s] is None else pot + vxc[s], g.becke,
+                                    g.weights)
             E += float((Ds[s] * sp.H).sum()) + 0.5 * float((self.W * rhos[s] * pot).sum())
             if self.exchange == 'hf' and self.is_electron[s] and sp.nocc > 0:
                 K = self._exchange(sp, Cs[s][:, :sp.nocc])

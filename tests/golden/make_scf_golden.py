@@ -9,14 +9,17 @@ configurations, written to tests/golden/scf_oracle.json (+ .npz densities):
   uhf_oh         UHF of the OH radical (O at 0, H at 0.97 A along z; doublet),
                  cc-pVDZ, 50 x 110;
   apmo_uhf_oh    APMO-UHF of the OH radical (doublet) with the H nucleus
-                 quantum (5s5p), 50 x 110.
+                 quantum (5s5p), 50 x 110;
+  uks_oh         unrestricted Kohn-Sham of the OH radical (doublet) with the
+                 spin-polarised LDA (Slater + VWN5 of the two spin densities),
+                 cc-pVDZ, 50 x 110.
 
 Both stop at |dE| < 1e-9 Eh with max |X^T (FDS - SDF) X| < 1e-4 (the rule of
 napmo_b200.scf), DIIS with 6 vectors.  The GPU tests compare the device
 drivers' converged energies and iteration counts with these.  The C2 SCF
 takes about ten minutes on 8 host cores.
 
-Usage: python tests/golden/make_scf_golden.py [c1] [c2] [uhf_oh] [apmo_uhf_oh]
+Usage: python tests/golden/make_scf_golden.py [c1] [c2] [uhf_oh] [apmo_uhf_oh] [uks_oh]
 """
 import json
 import os
@@ -55,6 +58,9 @@ def run(case):
     elif case == 'uhf_oh':
         res = OS.GridMultiSCF(OH, lib, el, (), 50, 110).run(tol=TOL)
         arrays = {'uhf_oh_Da': res['D'][0], 'uhf_oh_Db': res['D'][1]}
+    elif case == 'uks_oh':
+        res = OS.GridMultiSCF(OH, lib, el, (), 50, 110, exchange='lda').run(tol=TOL)
+        arrays = {}
     elif case == 'apmo_uhf_oh':
         res = OS.GridMultiSCF(OH, lib, el, (1,), 50, 110).run(tol=TOL)
         arrays = {}

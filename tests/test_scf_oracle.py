@@ -61,3 +61,16 @@ def test_reference_arm_geometry_equals_the_product_one():
     a, b = workloads.alkane_geometry(20), alkane_geometry(20)
     assert [s for s, _ in a] == [s for s, _ in b]
     assert np.array_equal(np.array([x for _, x in a]), np.array([x for _, x in b]))
+
+
+def test_uks_scf_reproduces_the_fixture(basis_library, elements):
+    """Spin-polarised LDA (unrestricted Kohn-Sham) of the OH radical: the
+    oracle reproduces the committed fixture the GPU test compares with."""
+    import scf as OS
+    with open(os.path.join(GOLDEN, 'scf_oracle.json')) as f:
+        ref = json.load(f)['uks_oh']
+    oh = [('O', (0.0, 0.0, 0.0)), ('H', (0.0, 0.0, 0.97))]
+    res = OS.GridMultiSCF(oh, basis_library, elements, (), 50, 110,
+                          exchange='lda').run(tol=ref['tol'])
+    assert res['converged'] and res['iterations'] == ref['iterations']
+    assert abs(res['energy'] - ref['energy']) <= 1e-10

@@ -671,15 +671,19 @@ def run_scf_c1(args, world, rank):
     from napmo_b200.scf import GridRHF
     from napmo_b200.system import build_system
     atoms = [('O', (0.0, 0.0, 0.0)), ('H', (0.0, 0.757, 0.587)), ('H', (0.0, -0.757, 0.587))]
-    out = {}
+    out, clocks = {}, {}
     for prec in ('fp64', 'int8x4'):
         times, res = [], None
+        sampler = ClockSampler(torch.cuda.current_device())
         for k in range(args.warmup + args.steps):
             scf = GridRHF(build_system(atoms, 'CC-PVDZ'), 50, 110, exchange='hf',
                           precision=prec)
+            if k == args.warmup:
+                sampler.start()
             res = scf.run(tol=1e-8)
             if k >= args.warmup:
                 times.append(res['seconds'])
+        clocks[prec] = sampler.stop()
         out[prec] = {'seconds': statistics.median(times), 'energy': res['energy'],
                      'iterations': res['iterations'], 'converged': res['converged'],
                      'fock_builds': res['fock_builds'], 'poisson_solves': res['poisson_solves']}
@@ -694,7 +698,7 @@ def run_scf_c1(args, world, rank):
             'config': {'workload': 'C1: H2O cc-pVDZ (25 Cartesian functions), 50x110 per atom '
                                    '(16,500 points), lmax 8, grid J and exchange, DIIS(6), 1e-8 Eh',
                        'parallelism': 'single GPU'},
-            'scf': out, 'energy_difference_eh': dE,
+            'scf': out, 'energy_difference_eh': dE, 'clocks': clocks[head],
             'e2e': {'value': t, 'unit': 's per SCF', 'h2d_bytes_per_step': 0,
                     'd2h_bytes_per_step': 8},
             'cpu_baseline': None}
@@ -710,17 +714,23 @@ def run_scf_c2(args, world, rank):
     species; electron-nucleus coupling by grid quadrature of the device
     Poisson potentials, electron exchange from orbital-pair Poisson solves,
     one DIIS (6) over both species, converged to 1e-8 Eh."""
+    import torch
     from napmo_b200.scf import GridAPMO
     from napmo_b200.system import build_system
     atoms = [('H', (0.0, 0.0, 0.0)), ('C', (0.0, 0.0, 1.066)), ('N', (0.0, 0.0, 2.222))]
-    out = {}
+    out, clocks = {}, {}
     for prec in ('fp64', 'int8x4'):
         times, res = [], None
+        sampler = ClockSampler(torch.cuda.current_device())
         for k in range(args.warmup + args.steps):
             ms = build_system(atoms, 'CC-PVDZ', quantum=(0,))
-            res = GridAPMO(ms, 'H_1', 100, 302, precision=prec).run(tol=1e-8)
+            drv = GridAPMO(ms, 'H_1', 100, 302, precision=prec)
+            if k == args.warmup:
+                sampler.start()
+            res = drv.run(tol=1e-8)
             if k >= args.warmup:
                 times.append(res['seconds'])
+        clocks[prec] = sampler.stop()
         out[prec] = {'seconds': statistics.median(times), 'energy': res['energy'],
                      'iterations': res['iterations'], 'converged': res['converged'],
                      'poisson_solves': res['poisson_solves']}
@@ -735,7 +745,7 @@ def run_scf_c2(args, world, rank):
             'config': {'workload': 'C2: HCN, e- cc-pVDZ (35) + H nucleus 5s5p (20), 100x302 per '
                                    'atom (90,600 points), lmax 14, DIIS(6), 1e-8 Eh',
                        'parallelism': 'single GPU'},
-            'scf': out, 'energy_difference_eh': dE,
+            'scf': out, 'energy_difference_eh': dE, 'clocks': clocks[head],
             'e2e': {'value': t, 'unit': 's per SCF', 'h2d_bytes_per_step': 0,
                     'd2h_bytes_per_step': 8},
             'cpu_baseline': None}

@@ -173,11 +173,14 @@ def test_spherical_expansion(oracle, elements):
     assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
-def test_poisson_solver_splines(oracle, basis_library, elements):
+@pytest.mark.parametrize('nrad', [2, 3, 5, 17, 40])
+def test_poisson_solver_splines(oracle, basis_library, elements, nrad):
+    """Radial solutions against the oracle, down to radial grids shorter than
+    the radial kernel's prefetch rings (the sweeps' prologues and tails)."""
     import napmo_b200 as nb
     atoms = [('O', (0.0, 0.0, 0.0)), ('H', (0.0, 0.757, 0.587))]
-    ms, grid = product_system(atoms, nrad=40, nang=86)
-    og, fb = oracle_system(oracle, basis_library, elements, atoms, nrad=40, nang=86)
+    ms, grid = product_system(atoms, nrad=nrad, nang=86)
+    og, fb = oracle_system(oracle, basis_library, elements, atoms, nrad=nrad, nang=86)
     phi = oracle.basis_compute(fb, og.points)
     rho = oracle.density(phi.T.copy(), random_density(phi.shape[1], 4))
     U = nb.poisson_solver(grid, rho, 7)

@@ -1,14 +1,15 @@
 // Becke-Dickson Poisson pipeline on the device (see poisson.cuh).
 //
 // 1. project:  f_lm(r_i) = sqrt(4 pi (2l+1)) sum_j rho wb w S_lm(u_j) / sum_j w
-//    per atom and radial shell, as a small FP64 product of the per-rule table
-//    S_lm(u_j) with the shell's weighted density (reference:
+//    per atom and radial shell, as a small FP64 product (DMMA tiles) of the
+//    shell's weighted density with the per-rule table S_lm(u_j) (reference:
 //    AtomicGrid::spherical_expansion, src/grid/atomic_grid.cpp:82-136).
-// 2. radial:   one CTA per (atom, l) builds the cubic spline of every f_lm,
-//    the transformed FEM right-hand sides and Dirichlet values, the Hermite
-//    FEM matrix of u'' + b u' + a u = f on the uniform t-axis (shared by the
-//    2l+1 values of m), factors it once by banded LU with partial pivoting and
-//    solves all m together (reference: poisson_solver.py:42-118, ode2.py,
+// 2. radial:   the Hermite FEM matrix of u'' + b u' + a u = f on the uniform
+//    t-axis depends on (atom, l) only: it is assembled and factored by banded
+//    LU with partial pivoting once per grid (radial_factor_kernel).  Per solve,
+//    one thread per (l, m) column builds the cubic spline of f_lm, the
+//    transformed FEM right-hand side and Dirichlet values, and substitutes
+//    (radial_kernel; reference: poisson_solver.py:42-118, ode2.py,
 //    src/horton/ode2.cpp:232-321; the reference solves each (l, m) with
 //    scipy's sparse LU).  The solution splines are written as scaled cubic
 //    coefficients for step 3 and as raw (y, dy/dt) for the Python API.

@@ -323,14 +323,17 @@ __global__ void radial_factor_kernel(PoissonDev P, RadialOp op) {
     long lo = 2 * (row / 2 - 1), hi = 2 * (row / 2 + 2);
     if (lo < 0) lo = 0;
     if (hi > n2) hi = n2;
-    for (long col = lo; col < hi; ++col) {
-      double cf = 0.0;
-      cf -= ov2_d(xmax, row, 1, col, 1, s_ov2);
-      for (long k = lo; k < hi; ++k) {
+    // the coefficient functions b, a at the row's (at most 6) FEM functions
+    // k, shared by all of its columns
+    double bks[6], aks[6];
+#pragma unroll
+    for (int t = 0; t < 6; ++t) {
+      const long k = lo + t;
+      double bk = 0.0, ak = 0.0;
+      if (k < hi) {
         const int i = (int)(k / 2);
         const double ri = r[i], r2 = ri * ri;
         const double jsq = j1[i] * j1[i];
-        double bk, ak;
         if (bd) {
           // b = (2 r^-1, -2 r^-2) as ndpsi.py:55 forms it
           const double rinv = 1.0 / ri, r2inv = 1.0 / r2;
@@ -351,6 +354,18 @@ __global__ void radial_factor_kernel(PoissonDev P, RadialOp op) {
           const double ay = -l2l / r2, adx = 2 * l2l / (r2 * ri);
           ak = (adx * jsq + 2 * ay * j2[i]) * j1[i];
         }
+      }
+      bks[t] = bk;
+      aks[t] = ak;
+    }
+    for (long col = lo; col < hi; ++col) {
+      double cf = 0.0;
+      cf -= ov2_d(xmax, row, 1, col, 1, s_ov2);
+#pragma unroll
+      for (int t = 0; t < 6; ++t) {
+        const long k = lo + t;
+        if (k >= hi) break;
+        const double bk = bks[t], ak = aks[t];
         if (bk != 0) cf += bk * ov3_d(xmax, row, 0, col, 1, k, 0, s_ov3);
         if (ak != 0) cf += ak * ov3_d(xmax, row, 0, col, 0, k, 0, s_ov3);
       }

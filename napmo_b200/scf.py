@@ -233,18 +233,7 @@ class GridRHF(object):
                 break
             E_prev = E
             if len(Fs) > 1:
-                m = len(Fs)
-                B = torch.empty((m + 1, m + 1), dtype=torch.float64, device='cuda')
-                for a in range(m):
-                    for b in range(a + 1):
-                        B[a, b] = B[b, a] = (errs[a] * errs[b]).sum()
-                B[m, :m] = -1.0
-                B[:m, m] = -1.0
-                B[m, m] = 0.0
-                rhs = torch.zeros(m + 1, dtype=torch.float64, device='cuda')
-                rhs[m] = -1.0
-                c = torch.linalg.solve(B, rhs)
-                F = sum(c[a] * Fs[a] for a in range(m))
+                F = _diis_extrapolate(torch, Fs, errs)
             e, C = self._diag(F)
             Cocc = C[:, :self.nocc]
             D = 2.0 * Cocc @ Cocc.T
@@ -257,19 +246,26 @@ class GridRHF(object):
                     electrons=nel, history=history)
 
 
-def _diis_extrapolate(torch, Fs, errs):
-    m = len(Fs)
-    B = torch.empty((m + 1, m + 1), dtype=torch.float64, device='cuda')
-    for a in range(m):
-        for b in range(a + 1):
-            B[a, b] = B[b, a] = (errs[a] * errs[b]).sum()
+def _diis_coefficients(torch, errs):
+    """DIIS coefficients (summing to 1) of the stored iterations whose error
+    combination has the least norm; errs[a] is iteration a's error matrix or a
+    tuple of them (one per species, one DIIS over all).  The errors' overlap
+    matrix is one product of their stacked, concatenated vectors."""
+    ev = torch.stack([torch.cat([x.reshape(-1) for x in (e if isinstance(e, (tuple, list))
+                                                          else (e,))]) for e in errs])
+    m = ev.shape[0]
+    B = torch.zeros((m + 1, m + 1), dtype=torch.float64, device='cuda')
+    B[:m, :m] = ev @ ev.T
     B[m, :m] = -1.0
     B[:m, m] = -1.0
-    B[m, m] = 0.0
     rhs = torch.zeros(m + 1, dtype=torch.float64, device='cuda')
     rhs[m] = -1.0
-    c = torch.linalg.solve(B, rhs)
-    return sum(c[a] * Fs[a] for a in range(m))
+    return torch.linalg.solve(B, rhs)[:m]
+
+
+def _diis_extrapolate(torch, Fs, errs):
+    """The DIIS combination of the stored Fock matrices."""
+    return torch.tensordot(_diis_coefficients(torch, errs), torch.stack(Fs), dims=1)
 
 
 class _Species(object):
@@ -460,19 +456,9 @@ class GridAPMO(object):
             E_prev = E
             m = len(Fs)
             if m > 1:
-                B = torch.empty((m + 1, m + 1), dtype=torch.float64, device='cuda')
-                for a in range(m):
-                    for b in range(a + 1):
-                        B[a, b] = B[b, a] = ((errs[a][0] * errs[b][0]).sum() +
-                                             (errs[a][1] * errs[b][1]).sum())
-                B[m, :m] = -1.0
-                B[:m, m] = -1.0
-                B[m, m] = 0.0
-                rhs = torch.zeros(m + 1, dtype=torch.float64, device='cuda')
-                rhs[m] = -1.0
-                c = torch.linalg.solve(B, rhs)
-                Fe = sum(c[a] * Fs[a][0] for a in range(m))
-                Fn = sum(c[a] * Fs[a][1] for a in range(m))
+                c = _diis_coefficients(torch, errs)
+                Fe = torch.tensordot(c, torch.stack([f[0] for f in Fs]), dims=1)
+                Fn = torch.tensordot(c, torch.stack([f[1] for f in Fs]), dims=1)
             Ce, _, De = e.diag(Fe)
             Cn, _, Dn = n.diag(Fn)
         torch.cuda.synchronize()
@@ -648,17 +634,9 @@ class GridMultiSCF(object):
             E_prev = E
             m = len(Fh)
             if m > 1:
-                B = torch.empty((m + 1, m + 1), dtype=torch.float64, device='cuda')
-                for a in range(m):
-                    for b in range(a + 1):
-                        B[a, b] = B[b, a] = sum((ea * eb).sum() for ea, eb in zip(errs[a], errs[b]))
-                B[m, :m] = -1.0
-                B[:m, m] = -1.0
-                B[m, m] = 0.0
-                rhs = torch.zeros(m + 1, dtype=torch.float64, device='cuda')
-                rhs[m] = -1.0
-                c = torch.linalg.solve(B, rhs)
-                Fs = [sum(c[a] * Fh[a][s] for a in range(m)) for s in range(len(sps))]
+                c = _diis_coefficients(torch, errs)
+                Fs = [torch.tensordot(c, torch.stack([f[s] for f in Fh]), dims=1)
+                      for s in range(len(sps))]
             Cs, Ds = [], []
             for sp, F in zip(sps, Fs):
                 C, _, D = sp.diag(F)

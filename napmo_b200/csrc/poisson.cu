@@ -1157,9 +1157,12 @@ __device__ double cubic_max_abs(const double *c) {
 // (0 <= u <= 1) inside the grid, |a_lm| first_x^l below the first radial point
 // (d^l <= first_x^l) and |a_lm| last_x^-(l+1) beyond the last.  The bucket
 // keeps l <= L, the smallest L whose dropped blocks sum to at most eval_tol.
-// Grid (max nrad + 1, natom), one warp: lane l bounds block l.
+// Grid (max nrad + 1, natom), one warp: the lanes bound the (l, m) terms
+// lane, lane + 32, ... (every lane busy, whatever l), then lane l sums block l
+// in m order.
 __global__ void __launch_bounds__(32) bucket_lcut_kernel(PoissonDev P) {
   __shared__ double bound[32];
+  extern __shared__ double cterm[];  // (max_lmax + 1)^2
   const int bat = blockIdx.y / P.natom;  // solve of a batch
   const PoissonAtom &at = P.atoms[blockIdx.y - bat * P.natom];
   const double *const spl = P.spl + bat * P.spl_stride;
@@ -1169,17 +1172,13 @@ __global__ void __launch_bounds__(32) bucket_lcut_kernel(PoissonDev P) {
   const int lmaxA = at.lmax;
   const int lsize = (lmaxA + 1) * (lmaxA + 1);
   const int region = (b == 0) ? 1 : (b == at.nrad ? 2 : 0);
+  for (int lm = l; lm < lsize; lm += 32)
+    cterm[lm] = region == 0 ? cubic_max_abs(spl + at.spl_off + ((long)(b - 1) * lsize + lm) * 4)
+                            : fabs(amp[at.amp_off + lm * 2 + (region == 1 ? 0 : 1)]);
+  __syncwarp();
   if (l <= lmaxA) {
     double s2 = 0.0;
-    for (int lm = l * l; lm < (l + 1) * (l + 1); ++lm) {
-      double c;
-      if (region == 0) {
-        c = cubic_max_abs(spl + at.spl_off + ((long)(b - 1) * lsize + lm) * 4);
-      } else {
-        c = fabs(amp[at.amp_off + lm * 2 + (region == 1 ? 0 : 1)]);
-      }
-      s2 = fma(c, c, s2);
-    }
+    for (int lm = l * l; lm < (l + 1) * (l + 1); ++lm) s2 = fma(cterm[lm], cterm[lm], s2);
     const double g = region == 0 ? 1.0
                                  : (region == 1 ? pow(at.first_x, (double)l)
                                                 : pow(at.last_x, -(double)(l + 1)));
@@ -1294,7 +1293,8 @@ cudaError_t launch_eval_l(const PoissonDev &P, int npoint, const double *x,
                           cudaStream_t s) {
   if (P.items && P.nitems > 0) {
     if (P.lcut) {
-      bucket_lcut_kernel<<<dim3(P.max_nrad + 1, P.natom * P.nbatch), 32, 0, s>>>(P);
+      bucket_lcut_kernel<<<dim3(P.max_nrad + 1, P.natom * P.nbatch), 32,
+                           (size_t)(P.max_lmax + 1) * (P.max_lmax + 1) * sizeof(double), s>>>(P);
       cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) return e;
     }

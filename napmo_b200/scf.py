@@ -74,18 +74,21 @@ def grid_exchange(torch, fb, phi, psi, W, max_bytes=1 << 31):
     """K_mu,nu = sum_i sum_p W phi_mu psi_i V[psi_i phi_nu], symmetrised (grid
     exchange of the orbitals psi, nocc x N, in the basis phi, n x N).  The
     pair densities psi_i phi_nu of as many orbitals as fit in max_bytes (with
-    their potentials and weighted products) are solved in one library call,
-    and their part of K is one batched product.  Returns (K, solves)."""
+    their potentials and weighted products) are solved in one library call.
+    Their part of K is phi B^T with B_nu(p) = sum_i W psi_i(p) V[psi_i phi_nu](p):
+    one pass over the potentials and one product over the grid (k products of
+    n x n over N points each would run as skinny GEMMs far below the memory
+    rate).  Returns (K, solves)."""
     n, N = phi.shape
     nocc = psi.shape[0]
     step = max(1, min(nocc, max_bytes // (3 * n * N * 8)))
-    K = torch.zeros((n, n), dtype=torch.float64, device='cuda')
+    B = torch.zeros((n, N), dtype=torch.float64, device='cuda')
     for i0 in range(0, nocc, step):
         ps = psi[i0:i0 + step]
         k = ps.shape[0]
         V = fb.coulomb_potentials((ps[:, None, :] * phi[None, :, :]).reshape(k * n, N))
-        A = phi[None, :, :] * (W * ps)[:, None, :]
-        K += torch.matmul(A, V.reshape(k, n, N).transpose(1, 2)).sum(0)
+        B += (V.reshape(k, n, N) * (W * ps)[:, None, :]).sum(0)
+    K = phi @ B.T
     return 0.5 * (K + K.T), nocc * n
 
 

@@ -41,7 +41,8 @@
 //
 // Kernels: warp 8 (one thread) streams stages into a 3-slot ring
 // (cp.async.bulk + mbarrier transaction counts), warp 9 (one thread) issues
-// the MMAs and owns TMEM, warps 0-7 drain TMEM.  Every mbarrier wait is
+// the MMAs and owns TMEM, warps 0-7 drain TMEM (the density: warps 12 and 13,
+// and twelve drain warps).  Every mbarrier wait is
 // bounded (2 s of globaltimer, or another role's abort): on timeout the kernel
 // records an error in g_tc_error, the roles stop, copies and MMAs in flight
 // are waited for (bounded) and TMEM is freed before the CTA exits.
@@ -71,8 +72,14 @@ constexpr int DN = 96;            // density N tile: 5 diagonals x 96 columns
 constexpr int QKB = 1024;         // quadrature exponent block (points)
 constexpr int QBLK_STAGES = QKB / KS;
 constexpr int NSTAGE = 3;
-constexpr int NEPI = 256;         // drain threads (warps 0-7)
+constexpr int NEPI = 256;         // quadrature drain threads (warps 0-7)
 constexpr int NTHR = NEPI + 64;   // + producer warp 8 + MMA warp 9
+// The density drain has three warps per TMEM lane quadrant (32 of the 96
+// columns each): its per-column work waits on global loads and conversions,
+// and the MMAs of the next pass wait for it.
+constexpr int DEPI = 384;         // density drain threads (warps 0-11)
+constexpr int DTHR = DEPI + 64;   // + producer warp 12 + MMA warp 13
+constexpr int DCW = 96 / (DEPI / 128);  // columns per density drain warp
 constexpr int kTmemCols = 512;
 constexpr int kEmin = -960;
 constexpr unsigned long long kTimeoutNs = 2000000000ull;
@@ -173,13 +180,13 @@ __device__ bool wait_phase(uint64_t *bar, uint32_t parity, volatile int *abort) 
 }
 
 // The drain warps' wait: thread 0 polls, the outcome is shared through smem so
-// that all 256 drain threads take the same branch.
+// that all nepi drain threads take the same branch.
 __device__ bool group_wait(uint64_t *bar, uint32_t parity, volatile int *abort,
-                           volatile int *flag) {
+                           volatile int *flag, int nepi) {
   if (threadIdx.x == 0) *flag = wait_phase(bar, parity, abort) ? 1 : 0;
-  named_sync(1, NEPI);
+  named_sync(1, nepi);
   const bool ok = *flag != 0;
-  named_sync(1, NEPI);
+  named_sync(1, nepi);
   return ok;
 }
 
@@ -754,7 +761,7 @@ __device__ __forceinline__ void quad_i8_body(const QuadArgs &g, uint8_t *smem, i
     for (int i = 0; i < 48; ++i) part[i] = 0.0;
     bool ok = true;
     for (int bi = 0; bi < nb; ++bi) {
-      if (!group_wait(&accfull, bi & 1, abort, &flag_sh)) {
+      if (!group_wait(&accfull, bi & 1, abort, &flag_sh, NEPI)) {
         ok = false;
         break;
       }
@@ -876,13 +883,13 @@ struct DensArgs {
 // m): T[p][mu] = sum_nu phi[nu][p] D'[mu][nu] for the 128 points and the 96
 // functions of block m, accumulated in TMEM over nu >= 64 dens_first_stage(m)
 // (D' is zero below, see dsym_kernel); the drain adds phi[mu][p] T[p][mu]
-// into rho[p] (thread = point, 48 functions each).
+// into rho[p] (thread = point, DCW functions each).
 __device__ __forceinline__ void density_i8_body(const DensArgs &g, uint8_t *smem, int bx,
                                                 int gx) {
   __shared__ __align__(8) uint64_t full[NSTAGE], empty[NSTAGE], accfull, accempty, done;
   __shared__ uint32_t tmem_sh;
   __shared__ int abort_sh, flag_sh;
-  __shared__ double red[2][TM];
+  __shared__ double red[DEPI / 128][TM];
   constexpr uint32_t A_BYTES = stage_bytes(TM), B_BYTES = NSL_D * DN * KS;
   constexpr uint32_t STAGE = A_BYTES + B_BYTES;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
@@ -894,12 +901,12 @@ __device__ __forceinline__ void density_i8_body(const DensArgs &g, uint8_t *smem
       mbar_init(&empty[s], 1);
     }
     mbar_init(&accfull, 1);
-    mbar_init(&accempty, NEPI);
+    mbar_init(&accempty, DEPI);
     mbar_init(&done, 1);
     abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 9) {
+  if (warp == DEPI / 32 + 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(&tmem_sh)),
                  "r"(kTmemCols));
@@ -910,7 +917,7 @@ __device__ __forceinline__ void density_i8_body(const DensArgs &g, uint8_t *smem
   fence_after_sync();
   const uint32_t tmem = tmem_sh;
 
-  if (warp == 8) {
+  if (warp == DEPI / 32) {
     if (lane == 0) {
       int it = 0;
       bool ok = true;
@@ -931,7 +938,7 @@ __device__ __forceinline__ void density_i8_body(const DensArgs &g, uint8_t *smem
       for (int k = max(0, it - NSTAGE); k < it; ++k)
         wait_phase(&full[k % NSTAGE], (k / NSTAGE) & 1, nullptr);
     }
-  } else if (warp == 9) {
+  } else if (warp == DEPI / 32 + 1) {
     if (lane == 0) {
       int it = 0, pass = 0;
       bool ok = true;
@@ -968,18 +975,18 @@ __device__ __forceinline__ void density_i8_body(const DensArgs &g, uint8_t *smem
       const long p = (long)pt * TM + row;
       double acc = 0.0;
       for (int m = 0; m < g.nmt; ++m, ++pass) {
-        if (!group_wait(&accfull, pass & 1, abort, &flag_sh)) {
+        if (!group_wait(&accfull, pass & 1, abort, &flag_sh, DEPI)) {
           ok = false;
           break;
         }
         fence_after_sync();
 #pragma unroll 1
-        for (int c = 0; c < 48; c += 16) {
+        for (int c = 0; c < DCW; c += 16) {
           int32_t v[5][16];
 #pragma unroll
           for (int dg = 0; dg < 5; ++dg) {
-            tmem_ld8(tmem + lane_off + dg * DN + 48 * h + c, v[dg]);
-            tmem_ld8(tmem + lane_off + dg * DN + 48 * h + c + 8, v[dg] + 8);
+            tmem_ld8(tmem + lane_off + dg * DN + DCW * h + c, v[dg]);
+            tmem_ld8(tmem + lane_off + dg * DN + DCW * h + c + 8, v[dg] + 8);
           }
           tmem_wait_ld();
 #pragma unroll
@@ -988,7 +995,7 @@ __device__ __forceinline__ void density_i8_body(const DensArgs &g, uint8_t *smem
             tie8(v[dg] + 8);
           }
           // functions mu0 .. mu0 + 15 lie in one 64-wide stage of phi^T
-          const int mu0 = m * DN + 48 * h + c;
+          const int mu0 = m * DN + DCW * h + c;
           if (mu0 < g.nks * KS) {
             const int8_t *pa = g.a + ((long)pt * g.nks + mu0 / KS) * A_BYTES +
                                core_off(row, mu0 % KS);
@@ -1023,18 +1030,20 @@ __device__ __forceinline__ void density_i8_body(const DensArgs &g, uint8_t *smem
       }
       if (!ok) break;
       red[h][row] = acc;
-      named_sync(1, NEPI);
+      named_sync(1, DEPI);
       if (h == 0 && p < g.npoint) {
         const int ep = __ldg(g.ea + p);
-        g.rho[g.pidx ? __ldg(g.pidx + p) : p] =
-            (red[0][row] + red[1][row]) * pow2(ep - 37) * pow2(ep - 37);
+        double sum = red[0][row];
+#pragma unroll
+        for (int k = 1; k < DEPI / 128; ++k) sum += red[k][row];
+        g.rho[g.pidx ? __ldg(g.pidx + p) : p] = sum * pow2(ep - 37) * pow2(ep - 37);
       }
-      named_sync(1, NEPI);
+      named_sync(1, DEPI);
     }
   }
   fence_before_sync();
   __syncthreads();
-  if (warp == 9) {
+  if (warp == DEPI / 32 + 1) {
     if (lane == 0) wait_phase(&done, 0, nullptr);
     __syncwarp();
     fence_after_sync();
@@ -1043,7 +1052,7 @@ __device__ __forceinline__ void density_i8_body(const DensArgs &g, uint8_t *smem
   }
 }
 
-__global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
+__global__ void __launch_bounds__(DTHR, 1) density_i8_kernel(DensArgs g) {
   extern __shared__ __align__(1024) uint8_t smem[];
   density_i8_body(g, smem, blockIdx.x, gridDim.x);
 }
@@ -1256,7 +1265,7 @@ int int8_density(Int8Plan *p, const double *D, double *rho, cudaStream_t s) {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                  "density_i8 smem");
   const int grid = p->npt < p->budget ? p->npt : p->budget;
-  density_i8_kernel<<<grid, NTHR, smem, s>>>(g);
+  density_i8_kernel<<<grid, DTHR, smem, s>>>(g);
   NAPMO_TRY_CUDA(cudaGetLastError(), "density_i8");
   return kOk;
 }
@@ -1340,7 +1349,7 @@ __global__ void __launch_bounds__(256) slice_d_batch_kernel(const SliceArg *__re
                          g.nks, g.img, g.e, nullptr, bx, by);
 }
 
-__global__ void __launch_bounds__(NTHR, 1) density_i8_batch_kernel(const DensArgs *__restrict__ a,
+__global__ void __launch_bounds__(DTHR, 1) density_i8_batch_kernel(const DensArgs *__restrict__ a,
                                                                    BatchMap m) {
   extern __shared__ __align__(1024) uint8_t smem[];
   int bx, by;
@@ -1488,7 +1497,7 @@ int int8_batch_density(Int8Batch *b, cudaStream_t s) {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                  "density_i8 smem");
   if (b->m_dens.total)
-    density_i8_batch_kernel<<<b->m_dens.total, NTHR, smem, s>>>(b->dens.p, b->m_dens.map());
+    density_i8_batch_kernel<<<b->m_dens.total, DTHR, smem, s>>>(b->dens.p, b->m_dens.map());
   NAPMO_TRY_CUDA(cudaGetLastError(), "density_i8");
   return kOk;
 }

@@ -39,10 +39,9 @@
 // only (idx[k] = grid index of compacted point k); rho is scattered back and
 // is 0 at dropped points.
 //
-// Kernels: warp 8 (one thread) streams stages into a 3-slot ring
-// (cp.async.bulk + mbarrier transaction counts), warp 9 (one thread) issues
-// the MMAs and owns TMEM, warps 0-7 drain TMEM (the density: warps 12 and 13,
-// and twelve drain warps).  Every mbarrier wait is
+// Kernels: warp 12 (one thread) streams stages into a 3-slot ring
+// (cp.async.bulk + mbarrier transaction counts), warp 13 (one thread) issues
+// the MMAs and owns TMEM, warps 0-11 drain TMEM.  Every mbarrier wait is
 // bounded (2 s of globaltimer, or another role's abort): on timeout the kernel
 // records an error in g_tc_error, the roles stop, copies and MMAs in flight
 // are waited for (bounded) and TMEM is freed before the CTA exits.
@@ -72,14 +71,13 @@ constexpr int DN = 96;            // density N tile: 5 diagonals x 96 columns
 constexpr int QKB = 1024;         // quadrature exponent block (points)
 constexpr int QBLK_STAGES = QKB / KS;
 constexpr int NSTAGE = 3;
-constexpr int NEPI = 256;         // quadrature drain threads (warps 0-7)
-constexpr int NTHR = NEPI + 64;   // + producer warp 8 + MMA warp 9
-// The density drain has three warps per TMEM lane quadrant (32 of the 96
-// columns each): its per-column work waits on global loads and conversions,
-// and the MMAs of the next pass wait for it.
-constexpr int DEPI = 384;         // density drain threads (warps 0-11)
-constexpr int DTHR = DEPI + 64;   // + producer warp 12 + MMA warp 13
-constexpr int DCW = 96 / (DEPI / 128);  // columns per density drain warp
+// Three drain warps per TMEM lane quadrant, 32 of the 96 columns each: the
+// drain's per-column work waits on TMEM and global loads, and the MMAs of the
+// next pass (or exponent block) wait for it.
+constexpr int NEPI = 384;         // drain threads (warps 0-11)
+constexpr int NTHR = NEPI + 64;   // + producer warp 12 + MMA warp 13
+constexpr int kWarpP = NEPI / 32, kWarpM = NEPI / 32 + 1;  // producer, MMA warps
+constexpr int DCW = 96 / (NEPI / 128);  // columns per drain warp
 constexpr int kTmemCols = 512;
 constexpr int kEmin = -960;
 constexpr unsigned long long kTimeoutNs = 2000000000ull;
@@ -694,7 +692,7 @@ __device__ __forceinline__ void quad_i8_body(const QuadArgs &g, uint8_t *smem, i
     abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 9) {
+  if (warp == kWarpM) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(&tmem_sh)),
                  "r"(kTmemCols));
@@ -705,7 +703,7 @@ __device__ __forceinline__ void quad_i8_body(const QuadArgs &g, uint8_t *smem, i
   fence_after_sync();
   const uint32_t tmem = tmem_sh;
 
-  if (warp == 8) {
+  if (warp == kWarpP) {
     if (lane == 0) {
       int it = 0;
       for (int bi = 0; bi < nb; ++bi) {
@@ -729,7 +727,7 @@ __device__ __forceinline__ void quad_i8_body(const QuadArgs &g, uint8_t *smem, i
       for (int k = max(0, it - NSTAGE); k < it; ++k)
         wait_phase(&full[k % NSTAGE], (k / NSTAGE) & 1, nullptr);
     }
-  } else if (warp == 9) {
+  } else if (warp == kWarpM) {
     if (lane == 0) {
       int it = 0;
       bool ok = true;
@@ -754,11 +752,11 @@ __device__ __forceinline__ void quad_i8_body(const QuadArgs &g, uint8_t *smem, i
   } else {
     const uint32_t lane_off = (uint32_t)(32 * (warp & 3)) << 16;
     const int row = 32 * (warp & 3) + lane;
-    const int col0 = 48 * (warp >> 2);
+    const int col0 = DCW * (warp >> 2);
     const long mu = (long)I * TM + row;
-    double part[48];
+    double part[DCW];
 #pragma unroll
-    for (int i = 0; i < 48; ++i) part[i] = 0.0;
+    for (int i = 0; i < DCW; ++i) part[i] = 0.0;
     bool ok = true;
     for (int bi = 0; bi < nb; ++bi) {
       if (!group_wait(&accfull, bi & 1, abort, &flag_sh, NEPI)) {
@@ -768,9 +766,9 @@ __device__ __forceinline__ void quad_i8_body(const QuadArgs &g, uint8_t *smem, i
       fence_after_sync();
       const int blk = b0 + bi;
       const int ea = __ldg(g.ea + mu * g.nblk + blk);
-      const int *eb = g.eb + (long)blk * g.ebld + J * QN + col0;  // 48 contiguous
+      const int *eb = g.eb + (long)blk * g.ebld + J * QN + col0;  // DCW contiguous
 #pragma unroll
-      for (int c = 0; c < 48; c += 8) {
+      for (int c = 0; c < DCW; c += 8) {
         int32_t v[5][8];
 #pragma unroll
         for (int d = 0; d < 5; ++d) tmem_ld8(tmem + lane_off + d * QN + col0 + c, v[d]);
@@ -794,12 +792,12 @@ __device__ __forceinline__ void quad_i8_body(const QuadArgs &g, uint8_t *smem, i
     if (ok) {
       double *out = g.work + (((long)by * g.npair + bx) * TM + row) * QN + col0;
 #pragma unroll
-      for (int i = 0; i < 48; ++i) out[i] = part[i];
+      for (int i = 0; i < DCW; ++i) out[i] = part[i];
     }
   }
   fence_before_sync();
   __syncthreads();
-  if (warp == 9) {
+  if (warp == kWarpM) {
     if (lane == 0) wait_phase(&done, 0, nullptr);
     __syncwarp();
     fence_after_sync();
@@ -889,7 +887,7 @@ __device__ __forceinline__ void density_i8_body(const DensArgs &g, uint8_t *smem
   __shared__ __align__(8) uint64_t full[NSTAGE], empty[NSTAGE], accfull, accempty, done;
   __shared__ uint32_t tmem_sh;
   __shared__ int abort_sh, flag_sh;
-  __shared__ double red[DEPI / 128][TM];
+  __shared__ double red[NEPI / 128][TM];
   constexpr uint32_t A_BYTES = stage_bytes(TM), B_BYTES = NSL_D * DN * KS;
   constexpr uint32_t STAGE = A_BYTES + B_BYTES;
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
@@ -901,12 +899,12 @@ __device__ __forceinline__ void density_i8_body(const DensArgs &g, uint8_t *smem
       mbar_init(&empty[s], 1);
     }
     mbar_init(&accfull, 1);
-    mbar_init(&accempty, DEPI);
+    mbar_init(&accempty, NEPI);
     mbar_init(&done, 1);
     abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == DEPI / 32 + 1) {
+  if (warp == kWarpM) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(&tmem_sh)),
                  "r"(kTmemCols));
@@ -917,7 +915,7 @@ __device__ __forceinline__ void density_i8_body(const DensArgs &g, uint8_t *smem
   fence_after_sync();
   const uint32_t tmem = tmem_sh;
 
-  if (warp == DEPI / 32) {
+  if (warp == kWarpP) {
     if (lane == 0) {
       int it = 0;
       bool ok = true;
@@ -938,7 +936,7 @@ __device__ __forceinline__ void density_i8_body(const DensArgs &g, uint8_t *smem
       for (int k = max(0, it - NSTAGE); k < it; ++k)
         wait_phase(&full[k % NSTAGE], (k / NSTAGE) & 1, nullptr);
     }
-  } else if (warp == DEPI / 32 + 1) {
+  } else if (warp == kWarpM) {
     if (lane == 0) {
       int it = 0, pass = 0;
       bool ok = true;
@@ -975,7 +973,7 @@ __device__ __forceinline__ void density_i8_body(const DensArgs &g, uint8_t *smem
       const long p = (long)pt * TM + row;
       double acc = 0.0;
       for (int m = 0; m < g.nmt; ++m, ++pass) {
-        if (!group_wait(&accfull, pass & 1, abort, &flag_sh, DEPI)) {
+        if (!group_wait(&accfull, pass & 1, abort, &flag_sh, NEPI)) {
           ok = false;
           break;
         }
@@ -1030,20 +1028,20 @@ __device__ __forceinline__ void density_i8_body(const DensArgs &g, uint8_t *smem
       }
       if (!ok) break;
       red[h][row] = acc;
-      named_sync(1, DEPI);
+      named_sync(1, NEPI);
       if (h == 0 && p < g.npoint) {
         const int ep = __ldg(g.ea + p);
         double sum = red[0][row];
 #pragma unroll
-        for (int k = 1; k < DEPI / 128; ++k) sum += red[k][row];
+        for (int k = 1; k < NEPI / 128; ++k) sum += red[k][row];
         g.rho[g.pidx ? __ldg(g.pidx + p) : p] = sum * pow2(ep - 37) * pow2(ep - 37);
       }
-      named_sync(1, DEPI);
+      named_sync(1, NEPI);
     }
   }
   fence_before_sync();
   __syncthreads();
-  if (warp == DEPI / 32 + 1) {
+  if (warp == kWarpM) {
     if (lane == 0) wait_phase(&done, 0, nullptr);
     __syncwarp();
     fence_after_sync();
@@ -1052,7 +1050,7 @@ __device__ __forceinline__ void density_i8_body(const DensArgs &g, uint8_t *smem
   }
 }
 
-__global__ void __launch_bounds__(DTHR, 1) density_i8_kernel(DensArgs g) {
+__global__ void __launch_bounds__(NTHR, 1) density_i8_kernel(DensArgs g) {
   extern __shared__ __align__(1024) uint8_t smem[];
   density_i8_body(g, smem, blockIdx.x, gridDim.x);
 }
@@ -1265,7 +1263,7 @@ int int8_density(Int8Plan *p, const double *D, double *rho, cudaStream_t s) {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                  "density_i8 smem");
   const int grid = p->npt < p->budget ? p->npt : p->budget;
-  density_i8_kernel<<<grid, DTHR, smem, s>>>(g);
+  density_i8_kernel<<<grid, NTHR, smem, s>>>(g);
   NAPMO_TRY_CUDA(cudaGetLastError(), "density_i8");
   return kOk;
 }
@@ -1349,7 +1347,7 @@ __global__ void __launch_bounds__(256) slice_d_batch_kernel(const SliceArg *__re
                          g.nks, g.img, g.e, nullptr, bx, by);
 }
 
-__global__ void __launch_bounds__(DTHR, 1) density_i8_batch_kernel(const DensArgs *__restrict__ a,
+__global__ void __launch_bounds__(NTHR, 1) density_i8_batch_kernel(const DensArgs *__restrict__ a,
                                                                    BatchMap m) {
   extern __shared__ __align__(1024) uint8_t smem[];
   int bx, by;
@@ -1497,7 +1495,7 @@ int int8_batch_density(Int8Batch *b, cudaStream_t s) {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                  "density_i8 smem");
   if (b->m_dens.total)
-    density_i8_batch_kernel<<<b->m_dens.total, DTHR, smem, s>>>(b->dens.p, b->m_dens.map());
+    density_i8_batch_kernel<<<b->m_dens.total, NTHR, smem, s>>>(b->dens.p, b->m_dens.map());
   NAPMO_TRY_CUDA(cudaGetLastError(), "density_i8");
   return kOk;
 }

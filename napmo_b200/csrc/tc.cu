@@ -71,6 +71,7 @@ constexpr int DN = 96;            // density N tile: 5 diagonals x 96 columns
 constexpr int QKB = 1024;         // quadrature exponent block (points)
 constexpr int QBLK_STAGES = QKB / KS;
 constexpr int NSTAGE = 3;
+constexpr int kScaleWarps = 8;    // warps of a B-image CTA (2 stages each)
 // Three drain warps per TMEM lane quadrant, 32 of the 96 columns each: the
 // drain's per-column work waits on TMEM and global loads, and the MMAs of the
 // next pass (or exponent block) wait for it.
@@ -537,20 +538,20 @@ gscale_kernel(int npoint, const double *__restrict__ wv, const double *__restric
 // e = group exponent of max |x| over the block, so B keeps 31 bits of its own
 // block maximum; eb[b][row] = ea[row][b] + eg[b] - s (block-major, ebld rows
 // per block, so a drain thread's columns are contiguous).  CTA = (8-row group,
-// block), 4 warps; in every stage the row group's 8 rows x 64 points of one
-// slice are 512 contiguous bytes, so lane c holds the 16-byte chunk of row
-// c & 7, points 16 (c >> 3) .. +15.  Warp w takes stages 4w .. 4w + 3 and keeps
-// their Y_A, decoded once from the digits, in registers across both passes
-// (row maxima: lanes c, c ^ 8, c ^ 16, c ^ 24, then the four warps through
-// shared memory; digits of B), so A is read from memory once.
+// block), kScaleWarps warps; in every stage the row group's 8 rows x 64
+// points of one slice are 512 contiguous bytes, so lane c holds the 16-byte
+// chunk of row c & 7, points 16 (c >> 3) .. +15.  Warp w takes SPW stages from
+// SPW w and keeps their Y_A, decoded once from the digits, in registers across
+// both passes (row maxima: lanes c, c ^ 8, c ^ 16, c ^ 24, then the warps
+// through shared memory; digits of B), so A is read from memory once.
 __device__ __forceinline__ void scale_image_body(const int8_t *__restrict__ qa,
                                                  int8_t *__restrict__ qb,
                                                  const double *__restrict__ gs,
                                                  const int *__restrict__ ea,
                                                  const int *__restrict__ eg, int *__restrict__ eb,
                                                  int nks, int nblk, int ebld, int bx, int by) {
-  constexpr int SPW = QBLK_STAGES / 4;  // stages per warp
-  __shared__ double smax[4][8];
+  constexpr int SPW = QBLK_STAGES / kScaleWarps;  // stages per warp
+  __shared__ double smax[kScaleWarps][8];
   const int c = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int rg = bx, b = by;
   const int t = rg >> 4, r = c & 7, kc = c >> 3;
@@ -586,7 +587,9 @@ __device__ __forceinline__ void scale_image_body(const int8_t *__restrict__ qa,
   mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 16));
   if (c < 8) smax[w][c] = mx;
   __syncthreads();
-  mx = fmax(fmax(smax[0][r], smax[1][r]), fmax(smax[2][r], smax[3][r]));
+  mx = smax[0][r];
+#pragma unroll
+  for (int k = 1; k < kScaleWarps; ++k) mx = fmax(mx, smax[k][r]);
   const int sh = 30 - group_exponent(mx);
   if (w == 0 && c < 8) eb[(long)b * ebld + row] = ea[(long)row * nblk + b] + eg[b] - sh;
   const double scale = ldexp(1.0, sh);
@@ -602,7 +605,7 @@ __device__ __forceinline__ void scale_image_body(const int8_t *__restrict__ qa,
   }
 }
 
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(32 * kScaleWarps)
 scale_image_kernel(const int8_t *__restrict__ qa, int8_t *__restrict__ qb,
                    const double *__restrict__ gs, const int *__restrict__ ea,
                    const int *__restrict__ eg, int *__restrict__ eb, int nks, int nblk,
@@ -1274,7 +1277,7 @@ int int8_quadrature(Int8Plan *p, const double *phi, const double *wv, double *F,
   gscale_kernel<<<p->nblk, 256, 0, s>>>(p->npoint, wv, p->isc.p,
                                         p->screened ? p->idx.p : nullptr, p->gs.p, p->eg.p);
   NAPMO_TRY_CUDA(cudaGetLastError(), "block scales");
-  scale_image_kernel<<<dim3((p->n + 7) / 8, p->nblk), 128, 0, s>>>(
+  scale_image_kernel<<<dim3((p->n + 7) / 8, p->nblk), 32 * kScaleWarps, 0, s>>>(
       p->qa.p, p->qb.p, p->gs.p, p->qa_e.p, p->eg.p, p->qb_e.p, p->nks_q, p->nblk,
       p->nimg * TM);
   NAPMO_TRY_CUDA(cudaGetLastError(), "wv phi image");
@@ -1362,7 +1365,7 @@ __global__ void __launch_bounds__(256) gscale_batch_kernel(const GscaleArg *__re
   gscale_body(g.npoint, g.wv, g.isc, g.pidx, g.gs, g.eg, bx);
 }
 
-__global__ void __launch_bounds__(128) scale_image_batch_kernel(const ScaleArg *__restrict__ a,
+__global__ void __launch_bounds__(32 * kScaleWarps) scale_image_batch_kernel(const ScaleArg *__restrict__ a,
                                                                 BatchMap m) {
   int bx, by;
   const ScaleArg g = a[map_cta(m, &bx, &by)];
@@ -1506,7 +1509,8 @@ int int8_batch_quadrature(Int8Batch *b, cudaStream_t s) {
     gscale_batch_kernel<<<b->m_gscale.total, 256, 0, s>>>(b->gscale.p, b->m_gscale.map());
   NAPMO_TRY_CUDA(cudaGetLastError(), "block scales");
   if (b->m_scale.total)
-    scale_image_batch_kernel<<<b->m_scale.total, 128, 0, s>>>(b->scale.p, b->m_scale.map());
+    scale_image_batch_kernel<<<b->m_scale.total, 32 * kScaleWarps, 0, s>>>(b->scale.p,
+                                                                          b->m_scale.map());
   NAPMO_TRY_CUDA(cudaGetLastError(), "wv phi image");
   const int smem = NSTAGE * (stage_bytes(TM) + stage_bytes(QN));
   NAPMO_TRY_CUDA(cudaFuncSetAttribute(quad_i8_batch_kernel,

@@ -35,7 +35,7 @@ struct PoissonAtom {
 struct EvalItem {
   int atom, bucket, start, count;
 };
-constexpr int kEvalChunk = 128;
+constexpr int kEvalChunk = 256;
 constexpr int kEvalPerThread = 2;  // pairs evaluated by one thread
 
 // Radial table slots (each nrad long, at rad_off + slot * nrad).

@@ -49,13 +49,14 @@ struct PoissonPlan {
   DevBuf<int> pairs;
   DevBuf<EvalItem> items;
   int nitems = 0, nitems_in = 0;  // items, of which the first nitems_in are interior
+  int chunk = kEvalChunk;         // pairs per item
   DevBuf<double> pair_v;
   DevBuf<int> lcut;  // per bucket, for truncated evaluations
   // pair lists of the points kept by a screening mask (built for the last
   // mask used; the mask is owned by the caller's int8 plan)
   DevBuf<int> pairs_s;
   DevBuf<EvalItem> items_s;
-  int nitems_s = 0, nitems_in_s = 0;
+  int nitems_s = 0, nitems_in_s = 0, chunk_s = kEvalChunk;
   unsigned long long screen_key = 0;  // serial of the mask's int8 plan (0: none)
   // Becke-Dickson workspace (source, shell averages, LU factors), kept
   // between calls: an allocation per call would return to the driver at
@@ -229,9 +230,28 @@ int build_poisson_plan(const std::vector<const AtomLayout *> &atoms,
 // at the points (x, y, z) (device, all molecules concatenated), into pairs /
 // items; with `keep` only the points whose flag is set.  Built once per grid
 // (and once per screening mask); about 12 bytes per pair.  Synchronises `s`.
+// Pairs per evaluation item (CTA of chunk / 2 threads): a larger item shares
+// one staging of its interval's coefficients among more pairs, but leaves
+// fewer CTAs and fewer resident warps (72 registers, 256 threads).  On B200,
+// 512-pair items made the C20H42 100x302 evaluation 5 % faster (about 15,000
+// pairs per interior bucket) and the H2O 50x110 and HCN 100x302 SCFs (300
+// and 900 pairs) slower than 128-pair items.
+static int eval_chunk_for(const std::vector<int> &count, const std::vector<PoissonAtom> &ha) {
+  long pairs = 0, buckets = 0;
+  for (const PoissonAtom &a : ha)
+    for (int b = 1; b < a.nrad; ++b) {
+      const int c = count[a.bucket_off + b];
+      if (c > 0) {
+        pairs += c;
+        ++buckets;
+      }
+    }
+  return buckets > 0 && pairs >= 4096L * buckets ? kEvalChunkMax : kEvalChunk;
+}
+
 int build_pair_lists(PoissonPlan *plan, const double *x, const double *y, const double *z,
                      const int *keep, DevBuf<int> &pairs, DevBuf<EvalItem> &items, int &nitems,
-                     int &nitems_in, cudaStream_t s) {
+                     int &nitems_in, int &chunk, cudaStream_t s) {
   PoissonDev &d = plan->d;
   const std::vector<PoissonAtom> &ha = plan->h_atoms;
   int nb = 0;
@@ -250,13 +270,14 @@ int build_pair_lists(PoissonPlan *plan, const double *x, const double *y, const 
   // exclusive scan per atom -> bucket starts (relative to the atom's slice)
   std::vector<int> start(nb);
   std::vector<EvalItem> hitems;
+  chunk = eval_chunk_for(hc, ha);
   for (int a = 0; a < (int)ha.size(); ++a) {
     int acc = 0;
     for (int b = 0; b <= ha[a].nrad; ++b) {
       const int k = ha[a].bucket_off + b;
       start[k] = acc;
-      for (int c = 0; c < hc[k]; c += kEvalChunk)
-        hitems.push_back(EvalItem{a, b, acc + c, std::min(kEvalChunk, hc[k] - c)});
+      for (int c = 0; c < hc[k]; c += chunk)
+        hitems.push_back(EvalItem{a, b, acc + c, std::min(chunk, hc[k] - c)});
       acc += hc[k];
     }
   }
@@ -288,7 +309,7 @@ static int select_pair_lists(PoissonPlan *p, BeckeGrid *g, const int *keep,
   if (keep && key != p->screen_key) {
     p->screen_key = 0;
     const int st = build_pair_lists(p, g->dev.x, g->dev.y, g->dev.z, keep, p->pairs_s,
-                                    p->items_s, p->nitems_s, p->nitems_in_s, s);
+                                    p->items_s, p->nitems_s, p->nitems_in_s, p->chunk_s, s);
     if (st) return st;
     p->screen_key = key;
   }
@@ -297,6 +318,7 @@ static int select_pair_lists(PoissonPlan *p, BeckeGrid *g, const int *keep,
   d.items = keep ? p->items_s.p : p->items.p;
   d.nitems = keep ? p->nitems_s : p->nitems;
   d.nitems_inner = keep ? p->nitems_in_s : p->nitems_in;
+  d.eval_chunk = keep ? p->chunk_s : p->chunk;
   return kOk;
 }
 
@@ -335,7 +357,7 @@ int grid_poisson_plan(BeckeGrid *g, int lmax, cudaStream_t s, PoissonPlan **out)
     return st;
   }
   st = build_pair_lists(p, g->dev.x, g->dev.y, g->dev.z, nullptr, p->pairs, p->items,
-                        p->nitems, p->nitems_in, s);
+                        p->nitems, p->nitems_in, p->chunk, s);
   if (st != kOk) {
     delete p;
     return st;
@@ -343,6 +365,7 @@ int grid_poisson_plan(BeckeGrid *g, int lmax, cudaStream_t s, PoissonPlan **out)
   p->d.items = p->items.p;
   p->d.nitems = p->nitems;
   p->d.nitems_inner = p->nitems_in;
+  p->d.eval_chunk = p->chunk;
   p->lmax = lmax;
   g->poisson = p;
   *out = p;
@@ -405,11 +428,13 @@ int grid_concat(const std::vector<BeckeGrid *> &grids, const std::vector<int> &l
   for (auto &L : g->layout) atoms.push_back(&L);
   int st = build_poisson_plan(atoms, lm, mol_atom_off, o, s, p);
   if (st != kOk) return st;
-  st = build_pair_lists(p, d.x, d.y, d.z, nullptr, p->pairs, p->items, p->nitems, p->nitems_in, s);
+  st = build_pair_lists(p, d.x, d.y, d.z, nullptr, p->pairs, p->items, p->nitems, p->nitems_in,
+                        p->chunk, s);
   if (st != kOk) return st;
   p->d.items = p->items.p;
   p->d.nitems = p->nitems;
   p->d.nitems_inner = p->nitems_in;
+  p->d.eval_chunk = p->chunk;
   p->lmax = -3;  // not a single-grid cutoff: grid_poisson_plan never reuses it
   NAPMO_TRY_CUDA(cudaStreamSynchronize(s), "batch grid");
   *off = o;

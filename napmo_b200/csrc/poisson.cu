@@ -1199,7 +1199,7 @@ __global__ void __launch_bounds__(32) bucket_lcut_kernel(PoissonDev P) {
 // instance carries no batch offsets (its registers, and occupancy, stay those
 // the recursion was tuned at)
 template <int LMAX, bool TAILS, bool BATCH>
-__global__ void __launch_bounds__(kEvalChunk / kEvalPerThread)
+__global__ void __launch_bounds__(kEvalChunkMax / kEvalPerThread)
 eval_pairs_kernel(PoissonDev P, const double *__restrict__ gx,
                   const double *__restrict__ gy, const double *__restrict__ gz) {
   extern __shared__ double cf[];
@@ -1300,7 +1300,7 @@ cudaError_t launch_eval_l(const PoissonDev &P, int npoint, const double *x,
     }
     const size_t smem = (size_t)(L + 1) * (L + 1) * 4 * sizeof(double);
     const dim3 gin(P.nitems_inner, P.nbatch), gtail(P.nitems - P.nitems_inner, P.nbatch);
-    constexpr int kT = kEvalChunk / kEvalPerThread;
+    const int kT = P.eval_chunk / kEvalPerThread;
     if (P.nitems_inner > 0) {
       if (P.nbatch > 1)
         eval_pairs_kernel<L, false, true><<<gin, kT, smem, s>>>(P, x, y, z);

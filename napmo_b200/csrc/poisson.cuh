@@ -30,13 +30,14 @@ struct PoissonAtom {
   long scr_off;    // radial-solve scratch: [3 nrad][lsize]
 };
 
-// One CTA of the bucketed evaluation: `count` (<= kEvalChunk) pairs of one
+// One CTA of the bucketed evaluation: `count` (<= the plan's chunk) pairs of one
 // atom that share one spline interval (or tail) of that atom.
 struct EvalItem {
   int atom, bucket, start, count;
 };
-constexpr int kEvalChunk = 256;
-constexpr int kEvalPerThread = 2;  // pairs evaluated by one thread
+constexpr int kEvalChunk = 128;     // default pairs per item
+constexpr int kEvalChunkMax = 512;  // largest item (PoissonDev::eval_chunk)
+constexpr int kEvalPerThread = 2;   // pairs evaluated by one thread
 
 // Radial table slots (each nrad long, at rad_off + slot * nrad).
 enum : int {
@@ -90,6 +91,7 @@ struct PoissonDev {
   long npair = 0;
   int nitems = 0;
   int nitems_inner = 0;        // items [0, nitems_inner) lie inside their atom's grid
+  int eval_chunk = kEvalChunk;  // pairs per item (<= kEvalChunkMax); CTA = chunk / 2 threads
   int *pairs = nullptr;        // point index, bucket-sorted per atom
   EvalItem *items = nullptr;
   double *pair_v = nullptr;    // [atom][molecule point] contribution

@@ -226,13 +226,9 @@ int build_poisson_plan(const std::vector<const AtomLayout *> &atoms,
   return kOk;
 }
 
-// Bucket-sorted (atom, point) pair lists for the evaluation of the potential
-// at the points (x, y, z) (device, all molecules concatenated), into pairs /
-// items; with `keep` only the points whose flag is set.  Built once per grid
-// (and once per screening mask); about 12 bytes per pair.  Synchronises `s`.
 // Pairs per evaluation item (CTA of chunk / 2 threads): a larger item shares
 // one staging of its interval's coefficients among more pairs, but leaves
-// fewer CTAs and fewer resident warps (72 registers, 256 threads).  On B200,
+// fewer CTAs and, at 256 threads and 76 registers, fewer resident warps.  On B200,
 // 512-pair items made the C20H42 100x302 evaluation 5 % faster (about 15,000
 // pairs per interior bucket) and the H2O 50x110 and HCN 100x302 SCFs (300
 // and 900 pairs) slower than 128-pair items.
@@ -249,6 +245,10 @@ static int eval_chunk_for(const std::vector<int> &count, const std::vector<Poiss
   return buckets > 0 && pairs >= 4096L * buckets ? kEvalChunkMax : kEvalChunk;
 }
 
+// Bucket-sorted (atom, point) pair lists for the evaluation of the potential
+// at the points (x, y, z) (device, all molecules concatenated), into pairs /
+// items; with `keep` only the points whose flag is set.  Built once per grid
+// (and once per screening mask); about 12 bytes per pair.  Synchronises `s`.
 int build_pair_lists(PoissonPlan *plan, const double *x, const double *y, const double *z,
                      const int *keep, DevBuf<int> &pairs, DevBuf<EvalItem> &items, int &nitems,
                      int &nitems_in, int &chunk, cudaStream_t s) {

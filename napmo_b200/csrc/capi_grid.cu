@@ -47,6 +47,7 @@ struct PoissonPlan {
   DevBuf<double> rscr;  // radial-solve scratch of one solve
   DevBuf<double> pg;    // projection scratch of one solve (rho wb w per point)
   DevBuf<int> pairs;
+  DevBuf<double> pair_u;  // interval coordinate of each interior pair
   DevBuf<EvalItem> items;
   int nitems = 0, nitems_in = 0;  // items, of which the first nitems_in are interior
   int chunk = kEvalChunk;         // pairs per item
@@ -55,6 +56,7 @@ struct PoissonPlan {
   // pair lists of the points kept by a screening mask (built for the last
   // mask used; the mask is owned by the caller's int8 plan)
   DevBuf<int> pairs_s;
+  DevBuf<double> pair_u_s;
   DevBuf<EvalItem> items_s;
   int nitems_s = 0, nitems_in_s = 0, chunk_s = kEvalChunk;
   unsigned long long screen_key = 0;  // serial of the mask's int8 plan (0: none)
@@ -250,8 +252,9 @@ static int eval_chunk_for(const std::vector<int> &count, const std::vector<Poiss
 // items; with `keep` only the points whose flag is set.  Built once per grid
 // (and once per screening mask); about 12 bytes per pair.  Synchronises `s`.
 int build_pair_lists(PoissonPlan *plan, const double *x, const double *y, const double *z,
-                     const int *keep, DevBuf<int> &pairs, DevBuf<EvalItem> &items, int &nitems,
-                     int &nitems_in, int &chunk, cudaStream_t s) {
+                     const int *keep, DevBuf<int> &pairs, DevBuf<double> &pair_u,
+                     DevBuf<EvalItem> &items, int &nitems, int &nitems_in, int &chunk,
+                     cudaStream_t s) {
   PoissonDev &d = plan->d;
   const std::vector<PoissonAtom> &ha = plan->h_atoms;
   int nb = 0;
@@ -283,8 +286,10 @@ int build_pair_lists(PoissonPlan *plan, const double *x, const double *y, const 
   }
   NAPMO_TRY_CUDA(count.upload(start, s), "pair lists");  // reused as the cursor
   NAPMO_TRY_CUDA(pairs.alloc(d.npair), "pair lists");
+  NAPMO_TRY_CUDA(pair_u.alloc(d.npair), "pair lists");
   d.pairs = pairs.p;
-  NAPMO_TRY_CUDA(launch_pair_scatter(d, plan->max_mol_npoint, bucket_of.p, count.p, s),
+  d.pair_u = pair_u.p;
+  NAPMO_TRY_CUDA(launch_pair_scatter(d, plan->max_mol_npoint, x, y, z, bucket_of.p, count.p, s),
                  "pair scatter");
   // interior buckets first, the tails after them: the evaluation runs them as
   // two kernels, each with the code of its own region only
@@ -309,12 +314,14 @@ static int select_pair_lists(PoissonPlan *p, BeckeGrid *g, const int *keep,
   if (keep && key != p->screen_key) {
     p->screen_key = 0;
     const int st = build_pair_lists(p, g->dev.x, g->dev.y, g->dev.z, keep, p->pairs_s,
-                                    p->items_s, p->nitems_s, p->nitems_in_s, p->chunk_s, s);
+                                    p->pair_u_s, p->items_s, p->nitems_s, p->nitems_in_s,
+                                    p->chunk_s, s);
     if (st) return st;
     p->screen_key = key;
   }
   d.keep = keep;
   d.pairs = keep ? p->pairs_s.p : p->pairs.p;
+  d.pair_u = keep ? p->pair_u_s.p : p->pair_u.p;
   d.items = keep ? p->items_s.p : p->items.p;
   d.nitems = keep ? p->nitems_s : p->nitems;
   d.nitems_inner = keep ? p->nitems_in_s : p->nitems_in;
@@ -356,8 +363,8 @@ int grid_poisson_plan(BeckeGrid *g, int lmax, cudaStream_t s, PoissonPlan **out)
     delete p;
     return st;
   }
-  st = build_pair_lists(p, g->dev.x, g->dev.y, g->dev.z, nullptr, p->pairs, p->items,
-                        p->nitems, p->nitems_in, p->chunk, s);
+  st = build_pair_lists(p, g->dev.x, g->dev.y, g->dev.z, nullptr, p->pairs, p->pair_u,
+                        p->items, p->nitems, p->nitems_in, p->chunk, s);
   if (st != kOk) {
     delete p;
     return st;
@@ -428,8 +435,8 @@ int grid_concat(const std::vector<BeckeGrid *> &grids, const std::vector<int> &l
   for (auto &L : g->layout) atoms.push_back(&L);
   int st = build_poisson_plan(atoms, lm, mol_atom_off, o, s, p);
   if (st != kOk) return st;
-  st = build_pair_lists(p, d.x, d.y, d.z, nullptr, p->pairs, p->items, p->nitems, p->nitems_in,
-                        p->chunk, s);
+  st = build_pair_lists(p, d.x, d.y, d.z, nullptr, p->pairs, p->pair_u, p->items, p->nitems,
+                        p->nitems_in, p->chunk, s);
   if (st != kOk) return st;
   p->d.items = p->items.p;
   p->d.nitems = p->nitems;

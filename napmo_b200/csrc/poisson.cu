@@ -1010,7 +1010,20 @@ __global__ void pair_bucket_kernel(PoissonDev P, const double *__restrict__ gx,
   if (b >= 0 && lanes_below(group) == 0) atomicAdd(&count[at.bucket_off + b], __popc(group));
 }
 
-__global__ void pair_scatter_kernel(PoissonDev P, const int *__restrict__ bucket_of,
+// Distance of point p from the atom, as the evaluation computes it.
+__device__ __forceinline__ double pair_distance(const PoissonAtom &at, const double *gx,
+                                                const double *gy, const double *gz, int p,
+                                                double *dx, double *dy, double *dz) {
+  *dx = gx[p] - at.cx;
+  *dy = gy[p] - at.cy;
+  *dz = gz[p] - at.cz;
+  return sqrt(*dx * *dx + *dy * *dy + *dz * *dz);
+}
+
+__global__ void pair_scatter_kernel(PoissonDev P, const double *__restrict__ gx,
+                                    const double *__restrict__ gy,
+                                    const double *__restrict__ gz,
+                                    const int *__restrict__ bucket_of,
                                     int *__restrict__ cursor) {
   const PoissonAtom &at = P.atoms[blockIdx.y];
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1021,7 +1034,16 @@ __global__ void pair_scatter_kernel(PoissonDev P, const int *__restrict__ bucket
   if (b >= 0 && (int)(threadIdx.x & 31) == leader)
     base = atomicAdd(&cursor[at.bucket_off + b], __popc(group));
   base = __shfl_sync(0xffffffffu, base, leader);
-  if (b >= 0) P.pairs[at.pair_off + base + lanes_below(group)] = at.mol_point_start + q;
+  if (b >= 0) {
+    const long slot = at.pair_off + base + lanes_below(group);
+    const int p = at.mol_point_start + q;
+    P.pairs[slot] = p;
+    if (b > 0 && b < at.nrad) {  // interior: the interval coordinate of the evaluation
+      double dx, dy, dz;
+      const double d = pair_distance(at, gx, gy, gz, p, &dx, &dy, &dz);
+      P.pair_u[slot] = rt_inv(at.rt, d) - (b - 1);
+    }
+  }
 }
 
 // One CTA per EvalItem: the coefficient block of the item's spline interval
@@ -1233,15 +1255,16 @@ eval_pairs_kernel(PoissonDev P, const double *__restrict__ gx,
 #pragma unroll
   for (int j = 0; j < kEvalPerThread; ++j) {
     const int e = t + j * (int)blockDim.x;
-    pidx[j] = P.pairs[at.pair_off + it.start + (e < it.count ? e : t)];
-    const int p = pidx[j];
-    const double dx = gx[p] - at.cx, dy = gy[p] - at.cy, dz = gz[p] - at.cz;
-    d[j] = sqrt(dx * dx + dy * dy + dz * dz);
+    const long slot = at.pair_off + it.start + (e < it.count ? e : t);
+    pidx[j] = P.pairs[slot];
+    double dx, dy, dz;
+    d[j] = pair_distance(at, gx, gy, gz, pidx[j], &dx, &dy, &dz);
     inv[j] = 1.0 / d[j];
     x[j] = dx * inv[j];
     y[j] = dy * inv[j];
     z[j] = dz * inv[j];
-    u[j] = region == 0 ? rt_inv(at.rt, d[j]) - (it.bucket - 1) : 0.0;
+    // interval coordinate stored with the pair lists (interior buckets)
+    u[j] = region == 0 ? P.pair_u[slot] : 0.0;
   }
   if (!TAILS)
     pair_values<LMAX, 0, kEvalPerThread>(cf, lcut, x, y, z, d, inv, u, v);
@@ -1505,10 +1528,11 @@ cudaError_t launch_pair_buckets(const PoissonDev &P, int max_mol_npoint, const d
   return cudaGetLastError();
 }
 
-cudaError_t launch_pair_scatter(const PoissonDev &P, int max_mol_npoint, const int *bucket_of,
+cudaError_t launch_pair_scatter(const PoissonDev &P, int max_mol_npoint, const double *x,
+                                const double *y, const double *z, const int *bucket_of,
                                 int *cursor, cudaStream_t s) {
   dim3 grid((max_mol_npoint + 255) / 256, P.natom);
-  pair_scatter_kernel<<<grid, 256, 0, s>>>(P, bucket_of, cursor);
+  pair_scatter_kernel<<<grid, 256, 0, s>>>(P, x, y, z, bucket_of, cursor);
   return cudaGetLastError();
 }
 

@@ -47,7 +47,7 @@ struct PoissonPlan {
   DevBuf<double> rscr;  // radial-solve scratch of one solve
   DevBuf<double> pg;    // projection scratch of one solve (rho wb w per point)
   DevBuf<int> pairs;
-  DevBuf<double> pair_u;  // interval coordinate of each interior pair
+  DevBuf<double2> pair_u;  // (u, 1/d) of each interior pair
   DevBuf<EvalItem> items;
   int nitems = 0, nitems_in = 0;  // items, of which the first nitems_in are interior
   int chunk = kEvalChunk;         // pairs per item
@@ -56,7 +56,7 @@ struct PoissonPlan {
   // pair lists of the points kept by a screening mask (built for the last
   // mask used; the mask is owned by the caller's int8 plan)
   DevBuf<int> pairs_s;
-  DevBuf<double> pair_u_s;
+  DevBuf<double2> pair_u_s;
   DevBuf<EvalItem> items_s;
   int nitems_s = 0, nitems_in_s = 0, chunk_s = kEvalChunk;
   unsigned long long screen_key = 0;  // serial of the mask's int8 plan (0: none)
@@ -252,7 +252,7 @@ static int eval_chunk_for(const std::vector<int> &count, const std::vector<Poiss
 // items; with `keep` only the points whose flag is set.  Built once per grid
 // (and once per screening mask); about 12 bytes per pair.  Synchronises `s`.
 int build_pair_lists(PoissonPlan *plan, const double *x, const double *y, const double *z,
-                     const int *keep, DevBuf<int> &pairs, DevBuf<double> &pair_u,
+                     const int *keep, DevBuf<int> &pairs, DevBuf<double2> &pair_u,
                      DevBuf<EvalItem> &items, int &nitems, int &nitems_in, int &chunk,
                      cudaStream_t s) {
   PoissonDev &d = plan->d;

@@ -1012,12 +1012,9 @@ __global__ void pair_bucket_kernel(PoissonDev P, const double *__restrict__ gx,
 
 // Distance of point p from the atom, as the evaluation computes it.
 __device__ __forceinline__ double pair_distance(const PoissonAtom &at, const double *gx,
-                                                const double *gy, const double *gz, int p,
-                                                double *dx, double *dy, double *dz) {
-  *dx = gx[p] - at.cx;
-  *dy = gy[p] - at.cy;
-  *dz = gz[p] - at.cz;
-  return sqrt(*dx * *dx + *dy * *dy + *dz * *dz);
+                                                const double *gy, const double *gz, int p) {
+  const double dx = gx[p] - at.cx, dy = gy[p] - at.cy, dz = gz[p] - at.cz;
+  return sqrt(dx * dx + dy * dy + dz * dz);
 }
 
 __global__ void pair_scatter_kernel(PoissonDev P, const double *__restrict__ gx,
@@ -1038,10 +1035,9 @@ __global__ void pair_scatter_kernel(PoissonDev P, const double *__restrict__ gx,
     const long slot = at.pair_off + base + lanes_below(group);
     const int p = at.mol_point_start + q;
     P.pairs[slot] = p;
-    if (b > 0 && b < at.nrad) {  // interior: the interval coordinate of the evaluation
-      double dx, dy, dz;
-      const double d = pair_distance(at, gx, gy, gz, p, &dx, &dy, &dz);
-      P.pair_u[slot] = rt_inv(at.rt, d) - (b - 1);
+    if (b > 0 && b < at.nrad) {  // interior: the evaluation's u and 1/d
+      const double d = pair_distance(at, gx, gy, gz, p);
+      P.pair_u[slot] = make_double2(rt_inv(at.rt, d) - (b - 1), 1.0 / d);
     }
   }
 }
@@ -1257,14 +1253,21 @@ eval_pairs_kernel(PoissonDev P, const double *__restrict__ gx,
     const int e = t + j * (int)blockDim.x;
     const long slot = at.pair_off + it.start + (e < it.count ? e : t);
     pidx[j] = P.pairs[slot];
-    double dx, dy, dz;
-    d[j] = pair_distance(at, gx, gy, gz, pidx[j], &dx, &dy, &dz);
-    inv[j] = 1.0 / d[j];
+    const int p = pidx[j];
+    const double dx = gx[p] - at.cx, dy = gy[p] - at.cy, dz = gz[p] - at.cz;
+    if (region == 0) {  // u and 1/d stored with the pair lists
+      const double2 ui = P.pair_u[slot];
+      u[j] = ui.x;
+      inv[j] = ui.y;
+      d[j] = 0.0;  // unused inside the grid
+    } else {
+      d[j] = pair_distance(at, gx, gy, gz, p);
+      inv[j] = 1.0 / d[j];
+      u[j] = 0.0;
+    }
     x[j] = dx * inv[j];
     y[j] = dy * inv[j];
     z[j] = dz * inv[j];
-    // interval coordinate stored with the pair lists (interior buckets)
-    u[j] = region == 0 ? P.pair_u[slot] : 0.0;
   }
   if (!TAILS)
     pair_values<LMAX, 0, kEvalPerThread>(cf, lcut, x, y, z, d, inv, u, v);

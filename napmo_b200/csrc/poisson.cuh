@@ -93,7 +93,7 @@ struct PoissonDev {
   int nitems_inner = 0;        // items [0, nitems_inner) lie inside their atom's grid
   int eval_chunk = kEvalChunk;  // pairs per item (<= kEvalChunkMax); CTA = chunk / 2 threads
   int *pairs = nullptr;        // point index, bucket-sorted per atom
-  double *pair_u = nullptr;    // interval coordinate of each interior pair (slot order)
+  double2 *pair_u = nullptr;   // (u, 1/d) of each interior pair (slot order)
   EvalItem *items = nullptr;
   double *pair_v = nullptr;    // [atom][molecule point] contribution
   // Truncation of the bucketed evaluation: with lcut null every (l, m) <=
@@ -162,7 +162,8 @@ cudaError_t launch_pair_buckets(const PoissonDev &P, int max_mol_npoint, const d
                                 const double *y, const double *z, const int *keep,
                                 int *bucket_of, int *count, cudaStream_t s);
 // The scatter also stores, for the pairs of interior buckets, the spline
-// interval coordinate u = rt_inv(|p - A|) - j in P.pair_u (slot order).
+// interval coordinate u = rt_inv(|p - A|) - j and 1 / |p - A| in P.pair_u
+// (slot order).
 cudaError_t launch_pair_scatter(const PoissonDev &P, int max_mol_npoint, const double *x,
                                 const double *y, const double *z, const int *bucket_of,
                                 int *cursor, cudaStream_t s);

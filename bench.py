@@ -33,10 +33,11 @@ SEED = 20261203
 # DRAM bytes per (atom, point) pair of the potential evaluation kernel
 # (profiles/poisson_kernels_C8H18_ncu.md: 122 MB read + 125 MB written for
 # 26 atoms x 785,200 points); scaled by the pairs of the measured workload
-EVAL_DRAM_BYTES_PER_PAIR = (122e6 + 125e6) / (26 * 785200)
-TRAFFIC_SOURCE = ('ncu dram__bytes_read.sum + dram__bytes_write.sum of eval_pairs_kernel at '
-                  'C8H18 100x302 (profiles/poisson_kernels_C8H18_ncu.md), 12.1 B per (atom, '
-                  'point) pair, scaled to this workload\'s pairs')
+EVAL_DRAM_BYTES_PER_PAIR = 297.079e9 * 2.051616e-3 / (26 * 785200)
+TRAFFIC_SOURCE = ('ncu dram__bytes.sum.per_second x gpu__time_duration.sum of eval_pairs_kernel '
+                  '(FP64 mode, first launch) at C8H18 100x302 (profiles/eval_pairs_C8H18_ncu.md): '
+                  '0.61 GB for 20.4 M pairs, 29.9 B per (atom, point) pair (pair list, stored '
+                  'u and 1/d, partial potential), scaled to this workload\'s pairs')
 
 
 def parse():
@@ -1196,9 +1197,9 @@ def main():
             issued = {'executed_fp64_tflops': flops_exec / td / 1e12,
                       'frac_executed': flops_exec / td / 1e12 / fp64}
             kernel_name = 'poisson(eval_pairs dominant)'
-            # DRAM bytes of the evaluation per launch: 12.1 B per (atom, point)
-            # pair (ncu at C8H18: 122 MB read + 125 MB written for 20.4 M
-            # pairs; pair lists and partial potentials grow with the pairs)
+            # DRAM bytes of the evaluation per launch: 29.9 B per (atom, point)
+            # pair (ncu at C8H18: 0.61 GB for 20.4 M pairs; pair lists, stored
+            # u and 1/d and partial potentials grow with the pairs)
             traffic = EVAL_DRAM_BYTES_PER_PAIR * natom * N
         else:
             traffic = None
